@@ -1,0 +1,164 @@
+/*
+ * pe_nsga3.h -- C ABI of the B200 NSGA-III codon-design engine.
+ *
+ * The reference (CAU-HPCL/Protein_encoding_v2_NSGA-III) has no library API: its
+ * hot path sits behind the device-function signatures of include/utils.cuh,
+ * include/mutation.cuh and include/sorting.cuh, the kernel argument lists of
+ * src/main.cu:26,121,409 and the command line `Protein_NSGA3 <fasta> <N> <G> <m>
+ * <Pm>` (src/main.cu:456-489).  Each entry point below names the reference
+ * interface it replaces.  Problem data that the reference keeps in __constant__
+ * and __device__ globals (include/common.cuh:45-76) lives in a per-instance
+ * handle here, so many problems can share one GPU.
+ *
+ * Conventions: every function returns PE_OK (0) or a pe_status code and never
+ * throws; pe_last_error() describes the last failure of the calling thread.
+ * Host pointers are owned by the caller; device memory is owned by the
+ * instance.  One host thread drives an instance at a time.
+ *
+ * Layouts (all row-major, host memory):
+ *   codon ids   uint8  [n_solutions][m][L]   global codon id 0..63 (table order)
+ *   objectives  float  [n_solutions][M]      minimisation form (see PE_OBJ_*)
+ *   objidx      int8   [n_solutions][2M]     [2k] CDS index for objective k,
+ *                                            [2k+1] second CDS (HD) or GC direction
+ *   pql         int32  [n_solutions][3]      hairpin stem p, q, length
+ */
+#ifndef PE_NSGA3_H
+#define PE_NSGA3_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PE_NUM_AMINO 21
+#define PE_NUM_CODON 64
+#define PE_NUM_SENSE 61
+#define PE_MAX_OBJ 6
+
+typedef enum {
+    PE_OK = 0,
+    PE_ERR_ARG = 1,         /* invalid argument or unsupported size */
+    PE_ERR_OOM = 2,         /* device or host allocation failed */
+    PE_ERR_CUDA = 3,        /* CUDA runtime error */
+    PE_ERR_TIMEOUT = 4,     /* a bounded device wait gave up */
+    PE_ERR_STATE = 5,       /* call out of order (e.g. step before init) */
+    PE_ERR_IO = 6,          /* file could not be read or parsed */
+    PE_ERR_NO_DEVICE = 7    /* no CUDA device available */
+} pe_status;
+
+/* Objective sets.  REF6 is the reference's six (include/common.cuh:23-29):
+ *   0 -minCAI, 1 -minCBP, 2 -minHSC, 3 -minHD, 4 max GC3 deviation, 5 max hairpin stem.
+ * BASE4 keeps 0 -minCAI, 1 -minHD, 2 max GC(3) deviation, 3 max hairpin stem. */
+typedef enum { PE_OBJ_REF6 = 0, PE_OBJ_BASE4 = 1 } pe_objective_set;
+typedef enum { PE_GC3 = 0, PE_GC_ALL = 1 } pe_gc_mode;
+
+/* Genetic code and scores (reference: include/info.cuh:6-54). */
+typedef struct pe_codon_table {
+    uint8_t nt[PE_NUM_CODON][3];             /* A=0 C=1 G=2 U=3 */
+    float weight[PE_NUM_CODON];              /* relative adaptiveness, > 0 */
+    float cps[PE_NUM_SENSE * PE_NUM_SENSE];  /* codon-pair score (REF6 only) */
+    int8_t start[PE_NUM_AMINO];              /* first codon id per amino acid */
+    int8_t count[PE_NUM_AMINO];              /* synonymous codons per amino acid */
+    float ref_gc3;                           /* reference GC3 fraction */
+    float ref_gc;                            /* reference GC fraction */
+} pe_codon_table;
+
+/* Run configuration (reference argv, src/main.cu:481-489, plus explicit knobs). */
+typedef struct pe_config {
+    int32_t n_cds;          /* m >= 2 */
+    int32_t pop_size;       /* N >= 1 */
+    float mutation_prob;    /* Pm in [0,1] */
+    int32_t objectives;     /* pe_objective_set */
+    int32_t gc_mode;        /* pe_gc_mode */
+    int32_t ref_p;          /* Das-Dennis partitions; 0 = reference rule (src/main.cu:564-576) */
+    uint64_t seed;          /* replaces rand() seeding (src/main.cu:469,525) */
+} pe_config;
+
+typedef struct pe_info {
+    int32_t L;              /* amino-acid positions incl. stop */
+    int32_t m, N, M, R, p;
+    uint32_t generation;    /* generations completed */
+    int32_t initialized;
+} pe_info;
+
+typedef struct pe_select_info {
+    int32_t rank_count;     /* solutions in fronts 0..last */
+    int32_t last_front_size;
+    int32_t n_fronts;
+    int32_t cut;            /* fronts filled N exactly (no niching) */
+    int32_t hyp_exception;  /* 1: nadir from the MNDF fallback */
+    float ideal[PE_MAX_OBJ], worst[PE_MAX_OBJ], nadir[PE_MAX_OBJ];
+} pe_select_info;
+
+typedef struct pe_instance pe_instance;
+
+/* --- lifecycle: replaces main()'s allocation + cudaMemcpyToSymbol uploads
+ *     (src/main.cu:630-678).  cuda_stream may be NULL (the instance makes one). */
+int pe_create(const pe_config *cfg, const int8_t *aa_idx, int32_t aa_len, const pe_codon_table *table,
+              void *cuda_stream, pe_instance **out);
+int pe_destroy(pe_instance *inst);
+int pe_get_info(const pe_instance *inst, pe_info *info);
+
+/* --- initializationKernel (src/main.cu:26-119): N random solutions (solution 0
+ *     = highest-weight codons), evaluated; extreme points seeded. */
+int pe_init_population(pe_instance *inst);
+
+/* --- the generation loop (src/main.cu:708-728): mutationKernel + sortingKernel,
+ *     `generations` times, on the device (CUDA-graph replay). */
+int pe_step(pe_instance *inst, int32_t generations);
+int pe_synchronize(pe_instance *inst);
+
+/* Current 2N set (parents then offspring of the last generation) and survivors
+ * (src/main.cu:772-787).  Any pointer may be NULL. */
+int pe_get_population(pe_instance *inst, uint8_t *codon_idx, float *obj, int8_t *objidx, int32_t *pql,
+                      int32_t *survivors);
+/* Objectives only (2N*M floats): the per-generation progress read. */
+int pe_get_objectives(pe_instance *inst, float *obj);
+
+/* --- operator-level entry points (one device function family each) --- */
+
+/* calMinimumCAI/CBP/HSC/HD, calMaximumGC3/GC, calMaximumSL
+ * (include/utils.cuh:271-888) on caller-supplied solutions. */
+int pe_eval_objectives(pe_instance *inst, const uint8_t *codon_idx, int32_t n_solutions, float *obj,
+                       int8_t *objidx, int32_t *pql);
+
+/* mutationKernel's variation step (src/main.cu:172-211, include/mutation.cuh):
+ * child i = mutate(parent i) as offspring index idx[i] of `generation`;
+ * ops[i] receives the operator (0 random, 1 CAI, 2 CBP, 3 HSC, 4 HD, 5 GC, 6 SL). */
+int pe_mutate(pe_instance *inst, uint32_t generation, const int32_t *idx, int32_t n, const uint8_t *parents,
+              const float *pobj, const int8_t *pobjidx, const int32_t *ppql, uint8_t *children, int32_t *ops);
+
+/* sortingKernel (src/main.cu:409-454; include/sorting.cuh:94-1282): fronts,
+ * ideal/worst/nadir, extreme points (in/out, M*M), niching -> N survivors. */
+int pe_select(pe_instance *inst, uint32_t generation, const float *obj, float *extremes, int32_t *survivors,
+              int32_t *front, pe_select_info *info);
+
+/* combinationRepetition (include/sorting.cuh:1338): R*M points; out may be NULL
+ * to query R. */
+int pe_reference_points(int32_t M, int32_t p, float *out, int32_t *R);
+
+/* --- host-side inputs (no device needed) --- */
+
+/* FASTA loader of src/main.cu:491-523 (header line skipped, newlines dropped,
+ * trailing stop 'Z' appended).  aa_out receives amino indices 0..20. */
+int pe_parse_fasta(const char *path, int8_t *aa_out, int32_t capacity, int32_t *aa_len);
+/* L amino acids i.i.d. uniform over the 20 standard letters, then the stop. */
+int pe_synthetic_protein(int32_t L, uint64_t seed, int8_t *aa_out);
+/* Standard genetic code; per-amino-acid weights Dirichlet(1) scaled to max 1,
+ * codons ordered by ascending weight; seeded codon-pair scores. */
+int pe_dirichlet_table(uint64_t seed, pe_codon_table *out);
+/* Text table: 64 lines "<CODON> <amino letter> <weight>" in id order, optional
+ * "gc3 <v>", "gc <v>", then optional 61*61 CPS values. */
+int pe_load_codon_table(const char *path, pe_codon_table *out);
+
+/* Exact hypervolume of n points (d <= 6) in minimisation form w.r.t. ref. */
+int pe_hypervolume(const double *pts, int32_t n, int32_t d, const double *ref, double *out);
+
+const char *pe_last_error(void);
+const char *pe_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

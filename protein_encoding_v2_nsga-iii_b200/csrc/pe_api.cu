@@ -1,0 +1,806 @@
+// pe_api.cu -- C ABI (include/pe_nsga3.h): instances, the CUDA-graph
+// generation loop, operator-level entry points and host-side input helpers.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "pe_internal.h"
+
+using namespace pe;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CK(call)                                                                                           \
+    do {                                                                                                   \
+        cudaError_t e_ = (call);                                                                           \
+        if (e_ != cudaSuccess)                                                                             \
+            return fail(e_ == cudaErrorMemoryAllocation ? PE_ERR_OOM : PE_ERR_CUDA, "%s: %s (%s:%d)", #call, \
+                        cudaGetErrorString(e_), __FILE__, __LINE__);                                       \
+    } while (0)
+
+const char kAmino[22] = "ACDEFGHIKLMNPQRSTVWYZ";
+
+int amino_index(char c)
+{
+    // binary search over the sorted amino letters (findAminoIndex, include/utils.cuh:60-86)
+    int lo = 0, hi = 20;
+    while (lo <= hi) {
+        int mid = (lo + hi) / 2;
+        if (kAmino[mid] == c) return mid;
+        if (kAmino[mid] > c) hi = mid - 1;
+        else lo = mid + 1;
+    }
+    return -1;
+}
+
+uint64_t bincoef(int n, int r)
+{
+    if (r < 0 || n < r) return 0;
+    if (2 * r > n) r = n - r;
+    uint64_t res = 1;
+    for (int i = 0; i < r; i++) res = (res * (uint64_t)(n - i)) / (uint64_t)(i + 1);
+    return res;
+}
+
+// Das-Dennis points: rank -> multiset unranking (include/sorting.cuh:1285-1354)
+void das_dennis(int M, int p, float *out)
+{
+    int R = (int)bincoef(M + p - 1, p);
+    std::fill(out, out + (size_t)R * M, 0.0f);
+    const int mm = M + p - 1;
+    const float inc = 1.0f / (float)p;
+    for (int r0 = 0; r0 < R; r0++) {
+        int r = r0, x = 1;
+        float *pt = out + (size_t)r0 * M;
+        for (int i = 1; i <= p; i++) {
+            uint64_t y = bincoef(mm - x - i + 1, p - i);
+            bool stop = false;
+            while (y <= (uint64_t)r) {
+                r -= (int)y;
+                x++;
+                if (x > mm) {
+                    stop = true;
+                    break;
+                }
+                y = bincoef(mm - x - i + 1, p - i);
+            }
+            if (stop) break;
+            pt[x - 1] += inc;
+        }
+    }
+}
+
+uint64_t splitmix64(uint64_t &x)
+{
+    uint64_t z = (x += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+}  // namespace
+
+struct pe_instance {
+    Shape s{};
+    pe_config cfg{};
+    int p = 0;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    DevTables *d_tab = nullptr;
+    int8_t *d_aa = nullptr;
+    float *d_ref = nullptr;
+    PopBuf buf[2]{};
+    int32_t *d_surv = nullptr;
+    SelectScratch sc{};
+    int2 *d_part = nullptr;
+    int32_t *d_counter = nullptr;
+    int32_t *d_status = nullptr;
+    float *d_ext = nullptr;
+    uint32_t *d_gen = nullptr;
+    int cur = 0;
+    bool initialized = false;
+    uint32_t generation = 0;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    std::vector<void *> allocs;
+
+    template <class T> int alloc(T **p, size_t count)
+    {
+        void *v = nullptr;
+        cudaError_t e = cudaMalloc(&v, std::max<size_t>(count, 1) * sizeof(T));
+        if (e != cudaSuccess) return fail(PE_ERR_OOM, "cudaMalloc(%zu bytes): %s", count * sizeof(T), cudaGetErrorString(e));
+        allocs.push_back(v);
+        *p = (T *)v;
+        return PE_OK;
+    }
+};
+
+namespace {
+
+int alloc_pop(pe_instance *in, PopBuf &b, int nsol)
+{
+    const Shape &s = in->s;
+    int rc;
+    if ((rc = in->alloc(&b.ids, (size_t)nsol * s.m * s.Lp))) return rc;
+    if ((rc = in->alloc(&b.planes, (size_t)nsol * s.m * s.Wp))) return rc;
+    if ((rc = in->alloc(&b.obj, (size_t)nsol * s.M))) return rc;
+    if ((rc = in->alloc(&b.objidx, (size_t)nsol * 2 * s.M))) return rc;
+    if ((rc = in->alloc(&b.pql, (size_t)nsol * 3))) return rc;
+    CK(cudaMemsetAsync(b.ids, 0, (size_t)nsol * s.m * s.Lp, in->stream));
+    CK(cudaMemsetAsync(b.planes, 0, (size_t)nsol * s.m * s.Wp * sizeof(uint2), in->stream));
+    CK(cudaMemsetAsync(b.obj, 0, (size_t)nsol * s.M * sizeof(float), in->stream));
+    CK(cudaMemsetAsync(b.objidx, 0, (size_t)nsol * 2 * s.M, in->stream));
+    CK(cudaMemsetAsync(b.pql, 0, (size_t)nsol * 3 * sizeof(int32_t), in->stream));
+    return PE_OK;
+}
+
+// temporary device buffers for the operator-level entry points
+struct TempBufs {
+    std::vector<void *> v;
+    ~TempBufs()
+    {
+        for (void *p : v) cudaFree(p);
+    }
+    template <class T> int get(T **p, size_t count)
+    {
+        void *q = nullptr;
+        cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
+        if (e != cudaSuccess) return fail(PE_ERR_OOM, "cudaMalloc: %s", cudaGetErrorString(e));
+        v.push_back(q);
+        *p = (T *)q;
+        return PE_OK;
+    }
+    int pop(const Shape &s, PopBuf &b, int nsol)
+    {
+        int rc;
+        if ((rc = get(&b.ids, (size_t)nsol * s.m * s.Lp))) return rc;
+        if ((rc = get(&b.planes, (size_t)nsol * s.m * s.Wp))) return rc;
+        if ((rc = get(&b.obj, (size_t)nsol * s.M))) return rc;
+        if ((rc = get(&b.objidx, (size_t)nsol * 2 * s.M))) return rc;
+        if ((rc = get(&b.pql, (size_t)nsol * 3))) return rc;
+        return PE_OK;
+    }
+};
+
+int check_status(pe_instance *in)
+{
+    int32_t st = 0;
+    CK(cudaMemcpyAsync(&st, in->d_status, sizeof st, cudaMemcpyDeviceToHost, in->stream));
+    CK(cudaStreamSynchronize(in->stream));
+    if (st) return fail(PE_ERR_TIMEOUT, "a bounded device wait gave up (status %d)", st);
+    return PE_OK;
+}
+
+cudaError_t enqueue_generation(pe_instance *in, int src)
+{
+    const Shape &s = in->s;
+    int dst = 1 - src;
+    cudaError_t e = launch_mutate(s, in->d_tab, in->d_aa, in->buf[src], in->buf[dst], in->d_surv, nullptr, s.N, 0,
+                                  s.N, in->d_gen, nullptr, in->stream);
+    if (e != cudaSuccess) return e;
+    e = launch_sl(s, in->buf[dst], s.N, s.N, in->d_part, in->d_counter, in->d_status, in->stream);
+    if (e != cudaSuccess) return e;
+    return launch_select(s, in->buf[dst].obj, in->d_ext, in->d_ref, in->sc, in->d_surv, in->d_gen, 1, in->stream);
+}
+
+int build_graphs(pe_instance *in)
+{
+    for (int src = 0; src < 2; src++) {
+        if (in->graph[src]) continue;
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(in->stream, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e = enqueue_generation(in, src);
+        cudaError_t e2 = cudaStreamEndCapture(in->stream, &g);
+        if (e != cudaSuccess || e2 != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return fail(PE_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
+        }
+        cudaError_t e3 = cudaGraphInstantiate(&in->graph[src], g, 0);
+        cudaGraphDestroy(g);
+        if (e3 != cudaSuccess) return fail(PE_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e3));
+    }
+    return PE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *pe_last_error(void) { return g_err.c_str(); }
+const char *pe_version(void) { return "pe_nsga3 1.0 (sm_100a)"; }
+
+int pe_reference_points(int32_t M, int32_t p, float *out, int32_t *R)
+{
+    if (M < 1 || M > PE_MAX_OBJ || p < 1 || !R) return fail(PE_ERR_ARG, "bad reference point request M=%d p=%d", M, p);
+    uint64_t r = bincoef(M + p - 1, p);
+    if (r > 1000000) return fail(PE_ERR_ARG, "too many reference points (%llu)", (unsigned long long)r);
+    *R = (int32_t)r;
+    if (out) das_dennis(M, p, out);
+    return PE_OK;
+}
+
+int pe_create(const pe_config *cfg, const int8_t *aa_idx, int32_t aa_len, const pe_codon_table *table,
+              void *cuda_stream, pe_instance **out)
+{
+    if (!cfg || !aa_idx || !table || !out) return fail(PE_ERR_ARG, "null argument");
+    *out = nullptr;
+    const int L = aa_len, m = cfg->n_cds, N = cfg->pop_size;
+    if (L < 3) return fail(PE_ERR_ARG, "protein too short: %d positions (need >= 3 incl. stop)", L);
+    if (m < 2 || m > kMaxCds) return fail(PE_ERR_ARG, "n_cds must be in [2, %d], got %d", kMaxCds, m);
+    if (N < 1 || N > (1 << 20)) return fail(PE_ERR_ARG, "pop_size out of range: %d", N);
+    if (!(cfg->mutation_prob >= 0.0f && cfg->mutation_prob <= 1.0f))
+        return fail(PE_ERR_ARG, "mutation_prob must be in [0,1]");
+    if (cfg->objectives != PE_OBJ_REF6 && cfg->objectives != PE_OBJ_BASE4) return fail(PE_ERR_ARG, "bad objective set");
+    if (cfg->gc_mode != PE_GC3 && cfg->gc_mode != PE_GC_ALL) return fail(PE_ERR_ARG, "bad gc mode");
+    // table validation
+    {
+        int expect = 0;
+        for (int a = 0; a < PE_NUM_AMINO; a++) {
+            if (table->start[a] != expect || table->count[a] < 1 || table->count[a] > 6)
+                return fail(PE_ERR_ARG, "codon table: amino %d has start %d count %d", a, table->start[a], table->count[a]);
+            expect += table->count[a];
+        }
+        if (expect != PE_NUM_CODON) return fail(PE_ERR_ARG, "codon table covers %d codons", expect);
+        if (table->count[20] != 3) return fail(PE_ERR_ARG, "stop group must hold the last 3 codons");
+        for (int c = 0; c < PE_NUM_CODON; c++) {
+            for (int b = 0; b < 3; b++)
+                if (table->nt[c][b] > 3) return fail(PE_ERR_ARG, "codon %d: bad nucleotide code", c);
+            if (!(table->weight[c] >= 0.0f) || !std::isfinite(table->weight[c]))
+                return fail(PE_ERR_ARG, "codon %d: weight must be finite and >= 0", c);
+        }
+    }
+    for (int a = 0; a < L; a++)
+        if (aa_idx[a] < 0 || aa_idx[a] >= PE_NUM_AMINO) return fail(PE_ERR_ARG, "amino index %d at %d", aa_idx[a], a);
+
+    Shape s{};
+    s.L = L;
+    s.Lp = (L + 15) & ~15;
+    s.m = m;
+    s.N = N;
+    s.objset = cfg->objectives;
+    s.gcmode = cfg->gc_mode;
+    s.M = cfg->objectives == PE_OBJ_BASE4 ? 4 : 6;
+    s.n = 3 * L;
+    s.W = (s.n + 31) / 32;
+    s.Wp = (s.W + 2) & ~1;  // >= 1 zero guard word, even
+    s.K = (s.n - 4) / 2;
+    s.pm = cfg->mutation_prob;
+    s.seed = cfg->seed;
+    {
+        static const int ref6[6] = {K_CAI, K_CBP, K_HSC, K_HD, K_GC, K_SL};
+        static const int base4[4] = {K_CAI, K_HD, K_GC, K_SL};
+        for (int k = 0; k < 6; k++) s.slot[k] = -1;
+        const int *kinds = s.M == 4 ? base4 : ref6;
+        for (int i = 0; i < s.M; i++) s.slot[kinds[i]] = i;
+    }
+    int p = cfg->ref_p;
+    if (p <= 0) {
+        // src/main.cu:564-576: largest p with C(M+p-1, p) <= N
+        p = 1;
+        while ((int64_t)bincoef(s.M + p - 1, p) <= N) p++;
+        p -= 1;
+        if (p < 1) return fail(PE_ERR_ARG, "pop_size %d too small for the reference-point rule (M=%d)", N, s.M);
+    }
+    uint64_t R = bincoef(s.M + p - 1, p);
+    if (R < 1 || R > 65536) return fail(PE_ERR_ARG, "reference points out of range (%llu)", (unsigned long long)R);
+    s.R = (int)R;
+    if ((size_t)m * L > 120000) return fail(PE_ERR_ARG, "m*L = %d exceeds the per-CTA solution limit (120000)", m * L);
+
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(PE_ERR_NO_DEVICE, "no CUDA device");
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    int smem_optin = 0;
+    CK(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    if (sl_smem_bytes(s) > (size_t)smem_optin || var_smem_bytes(s) > (size_t)smem_optin ||
+        select_smem_bytes(s) > (size_t)smem_optin)
+        return fail(PE_ERR_ARG, "problem too large for one CTA (L=%d m=%d N=%d)", L, m, N);
+
+    pe_instance *in = new pe_instance();
+    in->s = s;
+    in->cfg = *cfg;
+    in->p = p;
+    in->device = dev;
+    if (cuda_stream) {
+        in->stream = (cudaStream_t)cuda_stream;
+    } else {
+        if (cudaStreamCreateWithFlags(&in->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            delete in;
+            return fail(PE_ERR_CUDA, "stream creation failed");
+        }
+        in->own_stream = true;
+    }
+    int rc = PE_OK;
+    auto cleanup = [&](int code) {
+        pe_destroy(in);
+        return code;
+    };
+    // tables
+    DevTables ht;
+    memset(&ht, 0, sizeof ht);
+    for (int c = 0; c < 64; c++) {
+        for (int b = 0; b < 3; b++) ht.nt[c][b] = table->nt[c][b];
+        double w = (double)table->weight[c];
+        ht.wzero[c] = !(w > 0.0);
+        ht.lw[c] = w > 0.0 ? (int64_t)llrint(log(w) * 4294967296.0) : 0;
+        ht.gc3[c] = table->nt[c][2] == 1 || table->nt[c][2] == 2;
+        ht.gcn[c] = 0;
+        for (int b = 0; b < 3; b++) ht.gcn[c] += table->nt[c][b] == 1 || table->nt[c][b] == 2;
+    }
+    for (int a = 0; a < 21; a++) {
+        ht.start[a] = table->start[a];
+        ht.count[a] = table->count[a];
+        for (int j = 0; j < table->count[a]; j++) ht.aa_of[table->start[a] + j] = (int8_t)a;
+    }
+    auto is_stop = [&](int x, int y, int z) {
+        for (int c = 61; c < 64; c++)
+            if (table->nt[c][0] == x && table->nt[c][1] == y && table->nt[c][2] == z) return 1;
+        return 0;
+    };
+    for (int x = 0; x < 64; x++)
+        for (int y = 0; y < 64; y++)
+            ht.hsc[x * 64 + y] = (uint8_t)(is_stop(table->nt[x][1], table->nt[x][2], table->nt[y][0]) +
+                                           is_stop(table->nt[x][2], table->nt[y][0], table->nt[y][1]));
+    for (int i = 0; i < 61 * 61; i++) {
+        ht.cps[i] = table->cps[i];
+        ht.cpsf[i] = (int64_t)llrint((double)table->cps[i] * 4294967296.0);
+    }
+    ht.ref_gc3 = table->ref_gc3;
+    ht.ref_gc = table->ref_gc;
+
+    if ((rc = in->alloc(&in->d_tab, 1))) return cleanup(rc);
+    if ((rc = in->alloc(&in->d_aa, (size_t)L))) return cleanup(rc);
+    if ((rc = in->alloc(&in->d_ref, (size_t)s.R * s.M))) return cleanup(rc);
+    for (int b = 0; b < 2; b++)
+        if ((rc = alloc_pop(in, in->buf[b], 2 * N))) return cleanup(rc);
+    const int N2 = 2 * N, words = (N2 + 31) / 32;
+    if ((rc = in->alloc(&in->d_surv, (size_t)N))) return cleanup(rc);
+    if ((rc = in->alloc(&in->sc.dom, (size_t)N2 * words))) return cleanup(rc);
+    if ((rc = in->alloc(&in->sc.np, (size_t)N2))) return cleanup(rc);
+    if ((rc = in->alloc(&in->sc.front, (size_t)N2))) return cleanup(rc);
+    if ((rc = in->alloc(&in->sc.sorted, (size_t)N2))) return cleanup(rc);
+    if ((rc = in->alloc(&in->sc.assoc, (size_t)N2))) return cleanup(rc);
+    if ((rc = in->alloc(&in->sc.dist, (size_t)N2))) return cleanup(rc);
+    if ((rc = in->alloc(&in->sc.rho, (size_t)s.R))) return cleanup(rc);
+    if ((rc = in->alloc(&in->sc.fill, (size_t)s.R))) return cleanup(rc);
+    if ((rc = in->alloc(&in->sc.ncand, (size_t)s.R))) return cleanup(rc);
+    if ((rc = in->alloc(&in->sc.coff, (size_t)s.R + 1))) return cleanup(rc);
+    if ((rc = in->alloc(&in->sc.cand, (size_t)N2))) return cleanup(rc);
+    if ((rc = in->alloc(&in->sc.info, 8))) return cleanup(rc);
+    if ((rc = in->alloc(&in->sc.finfo, 3 * PE_MAX_OBJ))) return cleanup(rc);
+    if ((rc = in->alloc(&in->d_part, (size_t)N2 * m))) return cleanup(rc);
+    if ((rc = in->alloc(&in->d_counter, (size_t)N2))) return cleanup(rc);
+    if ((rc = in->alloc(&in->d_status, 1))) return cleanup(rc);
+    if ((rc = in->alloc(&in->d_ext, (size_t)s.M * s.M))) return cleanup(rc);
+    if ((rc = in->alloc(&in->d_gen, 1))) return cleanup(rc);
+    std::vector<float> ref((size_t)s.R * s.M);
+    das_dennis(s.M, p, ref.data());
+    cudaStream_t st = in->stream;
+#define CKC(call)                                                                                   \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess) return cleanup(fail(PE_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_))); \
+    } while (0)
+    CKC(cudaMemcpyAsync(in->d_tab, &ht, sizeof ht, cudaMemcpyHostToDevice, st));
+    CKC(cudaMemcpyAsync(in->d_aa, aa_idx, (size_t)L, cudaMemcpyHostToDevice, st));
+    CKC(cudaMemcpyAsync(in->d_ref, ref.data(), ref.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+    CKC(cudaMemsetAsync(in->d_counter, 0, (size_t)N2 * sizeof(int32_t), st));
+    CKC(cudaMemsetAsync(in->d_status, 0, sizeof(int32_t), st));
+    CKC(cudaMemsetAsync(in->d_ext, 0, (size_t)s.M * s.M * sizeof(float), st));
+    CKC(cudaMemsetAsync(in->d_gen, 0, sizeof(uint32_t), st));
+    CKC(cudaStreamSynchronize(st));
+#undef CKC
+    *out = in;
+    return PE_OK;
+}
+
+int pe_destroy(pe_instance *in)
+{
+    if (!in) return PE_OK;
+    if (in->stream) cudaStreamSynchronize(in->stream);
+    for (int i = 0; i < 2; i++)
+        if (in->graph[i]) cudaGraphExecDestroy(in->graph[i]);
+    for (void *p : in->allocs) cudaFree(p);
+    if (in->own_stream && in->stream) cudaStreamDestroy(in->stream);
+    delete in;
+    return PE_OK;
+}
+
+int pe_get_info(const pe_instance *in, pe_info *info)
+{
+    if (!in || !info) return fail(PE_ERR_ARG, "null argument");
+    info->L = in->s.L;
+    info->m = in->s.m;
+    info->N = in->s.N;
+    info->M = in->s.M;
+    info->R = in->s.R;
+    info->p = in->p;
+    info->generation = in->generation;
+    info->initialized = in->initialized;
+    return PE_OK;
+}
+
+int pe_init_population(pe_instance *in)
+{
+    if (!in) return fail(PE_ERR_ARG, "null instance");
+    const Shape &s = in->s;
+    CK(launch_init(s, in->d_tab, in->d_aa, in->buf[0], in->d_surv, in->stream));
+    CK(launch_sl(s, in->buf[0], 0, s.N, in->d_part, in->d_counter, in->d_status, in->stream));
+    // extreme points start as the objective vectors of solutions 0..M-1
+    // (initializationKernel, src/main.cu:106-109)
+    CK(cudaMemsetAsync(in->d_ext, 0, (size_t)s.M * s.M * sizeof(float), in->stream));
+    int rows = std::min(s.M, s.N);
+    CK(cudaMemcpyAsync(in->d_ext, in->buf[0].obj, (size_t)rows * s.M * sizeof(float), cudaMemcpyDeviceToDevice,
+                       in->stream));
+    CK(cudaMemsetAsync(in->d_gen, 0, sizeof(uint32_t), in->stream));
+    in->cur = 0;
+    in->generation = 0;
+    in->initialized = true;
+    return check_status(in);
+}
+
+int pe_step(pe_instance *in, int32_t generations)
+{
+    if (!in) return fail(PE_ERR_ARG, "null instance");
+    if (!in->initialized) return fail(PE_ERR_STATE, "pe_step before pe_init_population");
+    if (generations < 0) return fail(PE_ERR_ARG, "negative generation count");
+    int rc = build_graphs(in);
+    if (rc) return rc;
+    for (int g = 0; g < generations; g++) {
+        CK(cudaGraphLaunch(in->graph[in->cur], in->stream));
+        in->cur = 1 - in->cur;
+        in->generation++;
+    }
+    return PE_OK;
+}
+
+int pe_synchronize(pe_instance *in)
+{
+    if (!in) return fail(PE_ERR_ARG, "null instance");
+    CK(cudaStreamSynchronize(in->stream));
+    return check_status(in);
+}
+
+int pe_get_population(pe_instance *in, uint8_t *codon_idx, float *obj, int8_t *objidx, int32_t *pql,
+                      int32_t *survivors)
+{
+    if (!in) return fail(PE_ERR_ARG, "null instance");
+    if (!in->initialized) return fail(PE_ERR_STATE, "population not initialised");
+    const Shape &s = in->s;
+    const PopBuf &b = in->buf[in->cur];
+    // after init only the first N slots hold solutions
+    const int nsol = in->generation == 0 ? s.N : 2 * s.N;
+    if (codon_idx) {
+        if (in->generation == 0) memset(codon_idx, 0, (size_t)2 * s.N * s.m * s.L);
+        CK(cudaMemcpy2DAsync(codon_idx, (size_t)s.L, b.ids, (size_t)s.Lp, (size_t)s.L, (size_t)nsol * s.m,
+                             cudaMemcpyDeviceToHost, in->stream));
+    }
+    if (obj) CK(cudaMemcpyAsync(obj, b.obj, (size_t)2 * s.N * s.M * sizeof(float), cudaMemcpyDeviceToHost, in->stream));
+    if (objidx) CK(cudaMemcpyAsync(objidx, b.objidx, (size_t)2 * s.N * 2 * s.M, cudaMemcpyDeviceToHost, in->stream));
+    if (pql) CK(cudaMemcpyAsync(pql, b.pql, (size_t)2 * s.N * 3 * sizeof(int32_t), cudaMemcpyDeviceToHost, in->stream));
+    if (survivors)
+        CK(cudaMemcpyAsync(survivors, in->d_surv, (size_t)s.N * sizeof(int32_t), cudaMemcpyDeviceToHost, in->stream));
+    CK(cudaStreamSynchronize(in->stream));
+    return check_status(in);
+}
+
+int pe_get_objectives(pe_instance *in, float *obj)
+{
+    return pe_get_population(in, nullptr, obj, nullptr, nullptr, nullptr);
+}
+
+int pe_eval_objectives(pe_instance *in, const uint8_t *codon_idx, int32_t n, float *obj, int8_t *objidx, int32_t *pql)
+{
+    if (!in || !codon_idx || n < 0) return fail(PE_ERR_ARG, "bad arguments");
+    if (n == 0) return PE_OK;
+    const Shape &s = in->s;
+    for (size_t i = 0; i < (size_t)n * s.m * s.L; i++)
+        if (codon_idx[i] >= PE_NUM_CODON) return fail(PE_ERR_ARG, "codon id out of range at %zu", i);
+    TempBufs t;
+    PopBuf b{};
+    int2 *part;
+    int32_t *counter;
+    int rc;
+    if ((rc = t.pop(s, b, n))) return rc;
+    if ((rc = t.get(&part, (size_t)n * s.m))) return rc;
+    if ((rc = t.get(&counter, (size_t)n))) return rc;
+    CK(cudaMemsetAsync(b.ids, 0, (size_t)n * s.m * s.Lp, in->stream));
+    CK(cudaMemsetAsync(b.obj, 0, (size_t)n * s.M * sizeof(float), in->stream));
+    CK(cudaMemsetAsync(b.objidx, 0, (size_t)n * 2 * s.M, in->stream));
+    CK(cudaMemsetAsync(counter, 0, (size_t)n * sizeof(int32_t), in->stream));
+    CK(cudaMemcpy2DAsync(b.ids, (size_t)s.Lp, codon_idx, (size_t)s.L, (size_t)s.L, (size_t)n * s.m,
+                         cudaMemcpyHostToDevice, in->stream));
+    CK(launch_light_eval(s, in->d_tab, in->d_aa, b, 0, n, in->stream));
+    CK(launch_sl(s, b, 0, n, part, counter, in->d_status, in->stream));
+    if (obj) CK(cudaMemcpyAsync(obj, b.obj, (size_t)n * s.M * sizeof(float), cudaMemcpyDeviceToHost, in->stream));
+    if (objidx) CK(cudaMemcpyAsync(objidx, b.objidx, (size_t)n * 2 * s.M, cudaMemcpyDeviceToHost, in->stream));
+    if (pql) CK(cudaMemcpyAsync(pql, b.pql, (size_t)n * 3 * sizeof(int32_t), cudaMemcpyDeviceToHost, in->stream));
+    CK(cudaStreamSynchronize(in->stream));
+    return check_status(in);
+}
+
+int pe_mutate(pe_instance *in, uint32_t generation, const int32_t *idx, int32_t n, const uint8_t *parents,
+              const float *pobj, const int8_t *pobjidx, const int32_t *ppql, uint8_t *children, int32_t *ops)
+{
+    if (!in || !idx || !parents || !pobj || !pobjidx || !ppql || n < 0) return fail(PE_ERR_ARG, "bad arguments");
+    if (n == 0) return PE_OK;
+    const Shape &s = in->s;
+    for (size_t i = 0; i < (size_t)n * s.m * s.L; i++)
+        if (parents[i] >= PE_NUM_CODON) return fail(PE_ERR_ARG, "codon id out of range at %zu", i);
+    TempBufs t;
+    PopBuf src{}, dst{};
+    int32_t *d_par, *d_idx, *d_ops;
+    uint32_t *d_g;
+    int rc;
+    if ((rc = t.pop(s, src, n))) return rc;
+    if ((rc = t.pop(s, dst, n))) return rc;
+    if ((rc = t.get(&d_par, (size_t)n))) return rc;
+    if ((rc = t.get(&d_idx, (size_t)n))) return rc;
+    if ((rc = t.get(&d_ops, (size_t)n))) return rc;
+    if ((rc = t.get(&d_g, 1))) return rc;
+    std::vector<int32_t> ident(n);
+    for (int i = 0; i < n; i++) ident[i] = i;
+    CK(cudaMemsetAsync(src.ids, 0, (size_t)n * s.m * s.Lp, in->stream));
+    CK(cudaMemcpy2DAsync(src.ids, (size_t)s.Lp, parents, (size_t)s.L, (size_t)s.L, (size_t)n * s.m,
+                         cudaMemcpyHostToDevice, in->stream));
+    CK(cudaMemcpyAsync(src.obj, pobj, (size_t)n * s.M * sizeof(float), cudaMemcpyHostToDevice, in->stream));
+    CK(cudaMemcpyAsync(src.objidx, pobjidx, (size_t)n * 2 * s.M, cudaMemcpyHostToDevice, in->stream));
+    CK(cudaMemcpyAsync(src.pql, ppql, (size_t)n * 3 * sizeof(int32_t), cudaMemcpyHostToDevice, in->stream));
+    CK(cudaMemcpyAsync(d_par, ident.data(), (size_t)n * sizeof(int32_t), cudaMemcpyHostToDevice, in->stream));
+    CK(cudaMemcpyAsync(d_idx, idx, (size_t)n * sizeof(int32_t), cudaMemcpyHostToDevice, in->stream));
+    CK(cudaMemcpyAsync(d_g, &generation, sizeof(uint32_t), cudaMemcpyHostToDevice, in->stream));
+    CK(launch_mutate(s, in->d_tab, in->d_aa, src, dst, d_par, d_idx, n, -1, 0, d_g, d_ops, in->stream));
+    if (children)
+        CK(cudaMemcpy2DAsync(children, (size_t)s.L, dst.ids, (size_t)s.Lp, (size_t)s.L, (size_t)n * s.m,
+                             cudaMemcpyDeviceToHost, in->stream));
+    if (ops) CK(cudaMemcpyAsync(ops, d_ops, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost, in->stream));
+    CK(cudaStreamSynchronize(in->stream));
+    return PE_OK;
+}
+
+int pe_select(pe_instance *in, uint32_t generation, const float *obj, float *extremes, int32_t *survivors,
+              int32_t *front, pe_select_info *info)
+{
+    if (!in || !obj || !extremes) return fail(PE_ERR_ARG, "bad arguments");
+    const Shape &s = in->s;
+    const int N2 = 2 * s.N;
+    TempBufs t;
+    float *d_obj, *d_ext;
+    int32_t *d_sv;
+    uint32_t *d_g;
+    int rc;
+    if ((rc = t.get(&d_obj, (size_t)N2 * s.M))) return rc;
+    if ((rc = t.get(&d_ext, (size_t)s.M * s.M))) return rc;
+    if ((rc = t.get(&d_sv, (size_t)s.N))) return rc;
+    if ((rc = t.get(&d_g, 1))) return rc;
+    CK(cudaMemcpyAsync(d_obj, obj, (size_t)N2 * s.M * sizeof(float), cudaMemcpyHostToDevice, in->stream));
+    CK(cudaMemcpyAsync(d_ext, extremes, (size_t)s.M * s.M * sizeof(float), cudaMemcpyHostToDevice, in->stream));
+    CK(cudaMemsetAsync(d_sv, 0xff, (size_t)s.N * sizeof(int32_t), in->stream));
+    CK(cudaMemcpyAsync(d_g, &generation, sizeof(uint32_t), cudaMemcpyHostToDevice, in->stream));
+    CK(launch_select(s, d_obj, d_ext, in->d_ref, in->sc, d_sv, d_g, 0, in->stream));
+    CK(cudaMemcpyAsync(extremes, d_ext, (size_t)s.M * s.M * sizeof(float), cudaMemcpyDeviceToHost, in->stream));
+    if (survivors) CK(cudaMemcpyAsync(survivors, d_sv, (size_t)s.N * sizeof(int32_t), cudaMemcpyDeviceToHost, in->stream));
+    if (front) CK(cudaMemcpyAsync(front, in->sc.front, (size_t)N2 * sizeof(int32_t), cudaMemcpyDeviceToHost, in->stream));
+    int32_t hi[8];
+    float hf[3 * PE_MAX_OBJ];
+    CK(cudaMemcpyAsync(hi, in->sc.info, sizeof hi, cudaMemcpyDeviceToHost, in->stream));
+    CK(cudaMemcpyAsync(hf, in->sc.finfo, sizeof hf, cudaMemcpyDeviceToHost, in->stream));
+    CK(cudaStreamSynchronize(in->stream));
+    if (info) {
+        memset(info, 0, sizeof *info);
+        info->rank_count = hi[0];
+        info->last_front_size = hi[1];
+        info->n_fronts = hi[2];
+        info->cut = hi[3];
+        info->hyp_exception = hi[4];
+        for (int k = 0; k < s.M; k++) {
+            info->ideal[k] = hf[k];
+            info->worst[k] = hf[s.M + k];
+            info->nadir[k] = hf[2 * s.M + k];
+        }
+    }
+    return PE_OK;
+}
+
+// ---------------------------------------------------------------- host inputs
+
+int pe_parse_fasta(const char *path, int8_t *aa_out, int32_t capacity, int32_t *aa_len)
+{
+    // src/main.cu:491-523: first line (<= 255 chars) skipped, '\n' dropped,
+    // the final read (EOF) replaced by the stop letter 'Z'
+    if (!path || !aa_len) return fail(PE_ERR_ARG, "null argument");
+    FILE *fp = fopen(path, "r");
+    if (!fp) return fail(PE_ERR_IO, "cannot open %s", path);
+    char buffer[256];
+    if (!fgets(buffer, 256, fp)) {
+        fclose(fp);
+        return fail(PE_ERR_IO, "%s: empty file", path);
+    }
+    std::string seq;
+    int ch;
+    while ((ch = fgetc(fp)) != EOF)
+        if (ch != '\n') seq.push_back((char)ch);
+    fclose(fp);
+    seq.push_back('Z');
+    if (seq.size() < 3) return fail(PE_ERR_IO, "%s: sequence too short", path);
+    *aa_len = (int32_t)seq.size();
+    if (!aa_out) return PE_OK;
+    if ((int32_t)seq.size() > capacity) return fail(PE_ERR_ARG, "capacity %d < %zu", capacity, seq.size());
+    for (size_t i = 0; i < seq.size(); i++) {
+        int a = amino_index(seq[i]);
+        if (a < 0) return fail(PE_ERR_IO, "%s: unknown amino letter '%c' at %zu", path, seq[i], i);
+        aa_out[i] = (int8_t)a;
+    }
+    return PE_OK;
+}
+
+int pe_synthetic_protein(int32_t L, uint64_t seed, int8_t *aa_out)
+{
+    if (L < 2 || !aa_out) return fail(PE_ERR_ARG, "bad arguments");
+    uint64_t x = seed;
+    for (int i = 0; i < L; i++) aa_out[i] = (int8_t)(((splitmix64(x) >> 32) * 20ull) >> 32);
+    aa_out[L] = 20;
+    return PE_OK;
+}
+
+static void standard_code(pe_codon_table *t)
+{
+    // the standard genetic code, grouped by amino acid in index order
+    static const char *groups[21] = {"GCU GCC GCA GCG", "UGU UGC", "GAU GAC", "GAA GAG", "UUU UUC",
+                                     "GGU GGC GGA GGG", "CAU CAC", "AUU AUC AUA", "AAA AAG",
+                                     "UUA UUG CUU CUC CUA CUG", "AUG", "AAU AAC", "CCU CCC CCA CCG", "CAA CAG",
+                                     "CGU CGC CGA CGG AGA AGG", "UCU UCC UCA UCG AGU AGC", "ACU ACC ACA ACG",
+                                     "GUU GUC GUA GUG", "UGG", "UAU UAC", "UAA UAG UGA"};
+    int id = 0;
+    for (int a = 0; a < 21; a++) {
+        t->start[a] = (int8_t)id;
+        int k = 0;
+        for (const char *p = groups[a]; *p; p += (p[3] ? 4 : 3)) {
+            for (int b = 0; b < 3; b++) {
+                char c = p[b];
+                t->nt[id][b] = c == 'A' ? 0 : c == 'C' ? 1 : c == 'G' ? 2 : 3;
+            }
+            id++;
+            k++;
+            if (!p[3]) break;
+        }
+        t->count[a] = (int8_t)k;
+    }
+}
+
+int pe_dirichlet_table(uint64_t seed, pe_codon_table *out)
+{
+    if (!out) return fail(PE_ERR_ARG, "null table");
+    memset(out, 0, sizeof *out);
+    pe_codon_table base;
+    memset(&base, 0, sizeof base);
+    standard_code(&base);
+    uint64_t x = seed;
+    for (int a = 0; a < 21; a++) {
+        int k = base.count[a], st = base.start[a];
+        double g[6], gmax = 0.0;
+        for (int j = 0; j < k; j++) {
+            double u = (double)((splitmix64(x) >> 11) + 1) * (1.0 / 9007199254740992.0);
+            g[j] = -log(u);  // Gamma(1) draw; Dirichlet(1) after normalisation
+            gmax = std::max(gmax, g[j]);
+        }
+        float w[6];
+        int order[6];
+        for (int j = 0; j < k; j++) {
+            w[j] = (float)(g[j] / gmax);
+            order[j] = j;
+        }
+        // ascending weight inside the group (the reference assumes the last codon is the best)
+        std::stable_sort(order, order + k, [&](int p, int q) { return w[p] < w[q]; });
+        out->start[a] = base.start[a];
+        out->count[a] = base.count[a];
+        for (int j = 0; j < k; j++) {
+            for (int b = 0; b < 3; b++) out->nt[st + j][b] = base.nt[st + order[j]][b];
+            out->weight[st + j] = w[order[j]];
+        }
+    }
+    for (int i = 0; i < 61 * 61; i++) {
+        double u = (double)(splitmix64(x) >> 11) * (1.0 / 9007199254740992.0);
+        out->cps[i] = (float)(0.8 * u - 0.4);
+    }
+    out->ref_gc3 = 0.3810f;
+    out->ref_gc = 0.3977f;
+    return PE_OK;
+}
+
+int pe_load_codon_table(const char *path, pe_codon_table *out)
+{
+    if (!path || !out) return fail(PE_ERR_ARG, "null argument");
+    FILE *fp = fopen(path, "r");
+    if (!fp) return fail(PE_ERR_IO, "cannot open %s", path);
+    memset(out, 0, sizeof *out);
+    out->ref_gc3 = 0.3810f;
+    out->ref_gc = 0.3977f;
+    char line[256];
+    int id = 0, last_aa = -1;
+    int counts[21] = {0};
+    int ncps = 0;
+    bool in_cps = false;
+    while (fgets(line, sizeof line, fp)) {
+        char *p = line;
+        while (*p == ' ' || *p == '\t') p++;
+        if (*p == '#' || *p == '\n' || *p == 0) continue;
+        if (in_cps) {
+            char *e = p;
+            while (*e) {
+                char *q;
+                double v = strtod(e, &q);
+                if (q == e) break;
+                if (ncps < 61 * 61) out->cps[ncps++] = (float)v;
+                e = q;
+            }
+            continue;
+        }
+        if (!strncmp(p, "cps", 3)) {
+            in_cps = true;
+            continue;
+        }
+        if (!strncmp(p, "gc3 ", 4)) {
+            out->ref_gc3 = strtof(p + 4, nullptr);
+            continue;
+        }
+        if (!strncmp(p, "gc ", 3)) {
+            out->ref_gc = strtof(p + 3, nullptr);
+            continue;
+        }
+        char cod[8], aa;
+        float w;
+        if (sscanf(p, "%7s %c %f", cod, &aa, &w) != 3 || strlen(cod) != 3) {
+            fclose(fp);
+            return fail(PE_ERR_IO, "%s: cannot parse line '%s'", path, p);
+        }
+        int a = amino_index(aa);
+        if (a < 0 || id >= 64 || a < last_aa) {
+            fclose(fp);
+            return fail(PE_ERR_IO, "%s: codon %d (%s %c) out of order", path, id, cod, aa);
+        }
+        for (int b = 0; b < 3; b++) {
+            char c = cod[b];
+            if (c != 'A' && c != 'C' && c != 'G' && c != 'U') {
+                fclose(fp);
+                return fail(PE_ERR_IO, "%s: bad codon %s", path, cod);
+            }
+            out->nt[id][b] = c == 'A' ? 0 : c == 'C' ? 1 : c == 'G' ? 2 : 3;
+        }
+        out->weight[id] = w;
+        counts[a]++;
+        last_aa = a;
+        id++;
+    }
+    fclose(fp);
+    if (id != 64) return fail(PE_ERR_IO, "%s: %d codons (need 64)", path, id);
+    int st = 0;
+    for (int a = 0; a < 21; a++) {
+        out->start[a] = (int8_t)st;
+        out->count[a] = (int8_t)counts[a];
+        st += counts[a];
+    }
+    return PE_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,1065 @@
+// pe_eval.cu -- variation and objective-evaluation kernels for sm_100a.
+//
+//  k_variation<MODE>  one CTA per solution: initialise (initializationKernel,
+//                     src/main.cu:26-119), mutate (mutationKernel,
+//                     src/main.cu:121-240) or just re-evaluate a supplied
+//                     solution; then packs the nucleotide bit planes and
+//                     evaluates every objective except the hairpin stem.
+//  k_sl               one CTA per (solution, CDS): the hairpin-stem scan
+//                     (calMaximumSL, include/utils.cuh:712-888) on bit planes;
+//                     the last CTA of a solution combines its CDSs.
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "pe_device.cuh"
+#include "pe_internal.h"
+
+namespace pe {
+
+enum { MODE_INIT = 0, MODE_EVAL = 1, MODE_MUTATE = 2 };
+
+// small per-CTA copies of the codon tables
+struct SmemTab {
+    uint8_t nt[64][4];
+    int64_t lw[64];
+    uint8_t wzero[64];
+    uint8_t gc3[64];
+    uint8_t gcn[64];
+    int8_t start[21];
+    int8_t count[21];
+    int8_t pad[2];
+};
+
+__device__ __forceinline__ void load_tab(SmemTab &st, const DevTables *gt, int tid, int nth)
+{
+    for (int i = tid; i < 64; i += nth) {
+        *(uint32_t *)st.nt[i] = *(const uint32_t *)gt->nt[i];
+        st.lw[i] = gt->lw[i];
+        st.wzero[i] = gt->wzero[i];
+        st.gc3[i] = gt->gc3[i];
+        st.gcn[i] = gt->gcn[i];
+    }
+    for (int i = tid; i < 21; i += nth) {
+        st.start[i] = gt->start[i];
+        st.count[i] = gt->count[i];
+    }
+}
+
+__device__ __forceinline__ int nt_at(const SmemTab &st, const uint8_t *row, int x)
+{
+    int a = x / 3;
+    return st.nt[row[a]][x - 3 * a];
+}
+
+// Pack codon ids of every CDS into (lo, hi) nucleotide bit planes:
+// bit b of word w holds nucleotide 32w+b (A=00, C=01, G=10, U=11).
+__device__ void pack_planes(const Shape &s, const SmemTab &st, const uint8_t *ids, uint2 *planes, int tid, int nth)
+{
+    const int total = s.m * s.Wp;
+    for (int e = tid; e < total; e += nth) {
+        int c = e / s.Wp, w = e - c * s.Wp;
+        uint32_t lo = 0, hi = 0;
+        if (w < s.W) {
+            const uint8_t *row = ids + c * s.Lp;
+            int base = 32 * w;
+            int a = base / 3, b = base - 3 * a;
+            int lim = min(32, s.n - base);
+            for (int i = 0; i < lim; i++) {
+                uint32_t code = st.nt[row[a]][b];
+                lo |= (code & 1u) << i;
+                hi |= (code >> 1) << i;
+                if (++b == 3) {
+                    b = 0;
+                    a++;
+                }
+            }
+        }
+        planes[e] = make_uint2(lo, hi);
+    }
+}
+
+// True when the CDS holds a stem of length K = (n-4)/2 with a loop of >= 4
+// nucleotides: the only case in which mutationSL's undo branch runs
+// (include/mutation.cuh:843).  Uniform result for the CTA.
+__device__ bool cta_full_hairpin(const Shape &s, const SmemTab &st, const uint8_t *row, int tid, int nth)
+{
+    const int n = s.n, K = s.K;
+    if (K <= 0) return false;
+    bool found = false;
+    for (int ri = K - 1; ri < n && !found; ri++) {
+        for (int ci = ri + 5; ci + K - 1 <= n - 1 && !found; ci++) {
+            int ok = 1;
+            for (int u = tid; u < K; u += nth) ok &= (nt_at(st, row, ri - u) ^ nt_at(st, row, ci + u)) == 3;
+            found = __syncthreads_and(ok) != 0;
+        }
+    }
+    return found;
+}
+
+struct VarSmem {
+    SmemTab tab;
+    int64_t cds_val[kMaxCds];   // per-CDS sums
+    int32_t cds_cnt[kMaxCds];
+    int32_t pair_cnt[kMaxCds * (kMaxCds - 1) / 2 > 2016 ? 2016 : kMaxCds * (kMaxCds - 1) / 2];
+    float pobj[kMaxObj];
+    int8_t pobjidx[2 * kMaxObj];
+    int32_t ppql[3];
+    int32_t sl_old;
+    int32_t sl_mut;
+    int32_t op;
+};
+
+// Every objective except the hairpin stem, for the solution in smem.
+// Reference evaluators: include/utils.cuh:271-710.  Per-CDS sums are exact
+// integers (fixed-point log weights for CAI, fixed-point CPS), so the result
+// does not depend on the reduction order.
+__device__ void light_eval(const Shape &s, const DevTables *gt, VarSmem &sm, const uint8_t *ids, const uint2 *planes,
+                           float *obj, int8_t *objidx, int tid, int nth)
+{
+    const int warp = tid >> 5, lane = tid & 31, nwarps = nth >> 5;
+    const int L = s.L, m = s.m;
+    const SmemTab &st = sm.tab;
+    int slot;
+    // ---- CAI: exp(mean log w) per CDS
+    if ((slot = s.slot[K_CAI]) >= 0) {
+        for (int c = warp; c < m; c += nwarps) {
+            const uint8_t *row = ids + c * s.Lp;
+            long long S = 0;
+            int z = 0;
+            for (int a = lane; a < L; a += 32) {
+                int id = row[a];
+                S += st.lw[id];
+                z |= st.wzero[id];
+            }
+            S = warp_sum(S);
+            z = __any_sync(0xffffffffu, z);
+            if (lane == 0) {
+                double x = __ddiv_rn(__dmul_rn((double)S, 1.0 / 4294967296.0), (double)L);
+                float cai = z ? 0.0f : (float)det_exp(x);
+                sm.cds_val[c] = (int64_t)__float_as_int(cai);
+            }
+        }
+        __syncthreads();
+        if (tid == 0) {
+            float best = 0.0f;
+            int bi = 0;
+            for (int c = 0; c < m; c++) {
+                float v = -__int_as_float((int)sm.cds_val[c]);
+                if (c == 0 || v >= best) {
+                    best = v;
+                    bi = c;
+                }
+            }
+            obj[slot] = best;
+            objidx[2 * slot] = (int8_t)bi;
+            objidx[2 * slot + 1] = 0;
+        }
+        __syncthreads();
+    }
+    // ---- CBP: mean codon-pair score over pairs a in [0, L-3]
+    if ((slot = s.slot[K_CBP]) >= 0) {
+        for (int c = warp; c < m; c += nwarps) {
+            const uint8_t *row = ids + c * s.Lp;
+            long long S = 0;
+            for (int a = lane; a < L - 2; a += 32) {
+                int c1 = row[a], c2 = row[a + 1];
+                if (c1 < 61 && c2 < 61) S += __ldg(&gt->cpsf[c1 * 61 + c2]);
+            }
+            S = warp_sum(S);
+            if (lane == 0) sm.cds_val[c] = S;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            float best = 0.0f;
+            int bi = 0;
+            for (int c = 0; c < m; c++) {
+                double x = __ddiv_rn(__dmul_rn((double)sm.cds_val[c], 1.0 / 4294967296.0), (double)(L - 2));
+                float v = -(float)x;
+                if (c == 0 || v >= best) {
+                    best = v;
+                    bi = c;
+                }
+            }
+            obj[slot] = best;
+            objidx[2 * slot] = (int8_t)bi;
+            objidx[2 * slot + 1] = 0;
+        }
+        __syncthreads();
+    }
+    // ---- HSC: hidden stop codons in the +1/+2 frames per boundary
+    if ((slot = s.slot[K_HSC]) >= 0) {
+        for (int c = warp; c < m; c += nwarps) {
+            const uint8_t *row = ids + c * s.Lp;
+            int cnt = 0;
+            for (int a = lane; a < L - 1; a += 32) cnt += __ldg(&gt->hsc[row[a] * 64 + row[a + 1]]);
+            cnt = warp_sum(cnt);
+            if (lane == 0) sm.cds_cnt[c] = cnt;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            float best = 0.0f;
+            int bi = 0;
+            for (int c = 0; c < m; c++) {
+                float v = -__fdiv_rn((float)sm.cds_cnt[c], (float)(L - 1));
+                if (c == 0 || v >= best) {
+                    best = v;
+                    bi = c;
+                }
+            }
+            obj[slot] = best;
+            objidx[2 * slot] = (int8_t)bi;
+            objidx[2 * slot + 1] = 0;
+        }
+        __syncthreads();
+    }
+    // ---- HD: nucleotide mismatches over CDS pairs (i<j), XOR/popcount of planes
+    if ((slot = s.slot[K_HD]) >= 0) {
+        const int npairs = m * (m - 1) / 2;
+        for (int pi = warp; pi < npairs; pi += nwarps) {
+            int i = 0, rem = pi;
+            while (rem >= m - 1 - i) {
+                rem -= m - 1 - i;
+                i++;
+            }
+            int j = i + 1 + rem;
+            const uint2 *A = planes + i * s.Wp, *B = planes + j * s.Wp;
+            int cnt = 0;
+            for (int w = lane; w < s.W; w += 32) {
+                uint2 x = A[w], y = B[w];
+                cnt += __popc((x.x ^ y.x) | (x.y ^ y.y));
+            }
+            cnt = warp_sum(cnt);
+            if (lane == 0) sm.pair_cnt[pi] = cnt;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            float best = 0.0f;
+            int bi = 0, bj = 1, pi = 0;
+            for (int i = 0; i < m - 1; i++)
+                for (int j = i + 1; j < m; j++, pi++) {
+                    float v = -__fdiv_rn((float)sm.pair_cnt[pi], (float)s.n);
+                    if (pi == 0 || v >= best) {
+                        best = v;
+                        bi = i;
+                        bj = j;
+                    }
+                }
+            obj[slot] = best;
+            objidx[2 * slot] = (int8_t)bi;
+            objidx[2 * slot + 1] = (int8_t)bj;
+        }
+        __syncthreads();
+    }
+    // ---- GC3 (or whole-CDS GC) deviation from the reference fraction
+    if ((slot = s.slot[K_GC]) >= 0) {
+        for (int c = warp; c < m; c += nwarps) {
+            int cnt = 0;
+            if (s.gcmode == PE_GC3) {
+                const uint8_t *row = ids + c * s.Lp;
+                for (int a = lane; a < L; a += 32) cnt += st.gc3[row[a]];
+            } else {
+                const uint2 *A = planes + c * s.Wp;
+                for (int w = lane; w < s.W; w += 32) cnt += __popc(A[w].x ^ A[w].y);
+            }
+            cnt = warp_sum(cnt);
+            if (lane == 0) sm.cds_cnt[c] = cnt;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            float best = 0.0f;
+            int bi = 0, dir = 1;
+            for (int c = 0; c < m; c++) {
+                float dev, diff;
+                if (s.gcmode == PE_GC3) {
+                    diff = __fsub_rn(__fdiv_rn((float)sm.cds_cnt[c], (float)L), gt->ref_gc3);
+                    dev = fabsf(diff);
+                } else {
+                    float refGC = __fmul_rn((float)s.n, gt->ref_gc);
+                    diff = __fsub_rn((float)sm.cds_cnt[c], refGC);
+                    dev = __fdiv_rn(fabsf(diff), refGC);
+                }
+                if (c == 0 || dev >= best) {
+                    best = dev;
+                    bi = c;
+                    dir = diff < 0.0f ? 1 : -1;
+                }
+            }
+            obj[slot] = best;
+            objidx[2 * slot] = (int8_t)bi;
+            objidx[2 * slot + 1] = (int8_t)dir;
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// mutation operators (include/mutation.cuh), each thread owns one codon
+// ---------------------------------------------------------------------------
+
+#define MDRAW(pos, j) draw(s.seed, TAG_MUT, gen, ridx, (uint32_t)(pos), (uint32_t)(j))
+
+__device__ __forceinline__ void shuffle_k(const Shape &s, uint32_t gen, uint32_t ridx, int pos, int k, int *arr)
+{
+    // indexArrayShuffling (include/utils.cuh:203-218): draws 1..k-1
+    for (int i = 0; i < 6; i++) arr[i] = i;
+    int d = 1;
+    for (int i = k - 1; i > 0; i--) {
+        int j = (int)rng_uint(MDRAW(pos, d), (uint32_t)(i + 1));
+        d++;
+        int t = arr[i];
+        arr[i] = arr[j];
+        arr[j] = t;
+    }
+}
+
+__device__ void mutate_solution(const Shape &s, const DevTables *gt, VarSmem &sm, const int8_t *aa, uint8_t *ids,
+                                uint32_t gen, uint32_t ridx, int tid, int nth)
+{
+    const SmemTab &st = sm.tab;
+    const int L = s.L, m = s.m;
+    const float pm = s.pm;
+    const int op = sm.op;
+    switch (op) {
+    case 0: {  // mutationRandom (:16-63)
+        for (int pos = tid; pos < m * L; pos += nth) {
+            int c = pos / L, a = pos - c * L;
+            int am = aa[a];
+            int k = st.count[am];
+            if (rng_u01(MDRAW(pos, 0)) > pm || k == 1) continue;
+            uint8_t *cell = ids + c * s.Lp + a;
+            int cur = *cell - st.start[am];
+            int nw = (int)rng_uint(MDRAW(pos, 1), (uint32_t)(k - 1));
+            if (nw >= cur) nw++;
+            *cell = (uint8_t)(st.start[am] + nw);
+        }
+        break;
+    }
+    case 1: {  // mutationCAI, SELECT_UPPER_RANDOM (:65-142)
+        int c = sm.pobjidx[2 * s.slot[K_CAI]];
+        for (int a = tid; a < L; a += nth) {
+            int am = aa[a];
+            int k = st.count[am];
+            if (rng_u01(MDRAW(a, 0)) > pm || k == 1) continue;
+            uint8_t *cell = ids + c * s.Lp + a;
+            int cur = *cell - st.start[am];
+            if (cur == k - 1) continue;
+            int nw = cur + 1 + (int)rng_uint(MDRAW(a, 1), (uint32_t)(k - 1 - cur));
+            *cell = (uint8_t)(st.start[am] + nw);
+        }
+        break;
+    }
+    case 2: {  // mutationCBP, SELECT_UPPER_RANDOM, prob 2Pm, positions of parity gen%2 (:144-262)
+        int c = sm.pobjidx[2 * s.slot[K_CBP]];
+        float pm2 = __fmul_rn(pm, 2.0f);
+        int parity = (int)(gen & 1u);
+        uint8_t *row = ids + c * s.Lp;
+        for (int a = tid; a < L - 1; a += nth) {
+            if ((a & 1) != parity) continue;
+            int am = aa[a];
+            int k = st.count[am];
+            if (rng_u01(MDRAW(a, 0)) > pm2 || k == 1) continue;
+            int curg = row[a];
+            int cur = curg - st.start[am];
+            int left = a > 0 ? row[a - 1] : -1;
+            int right = row[a + 1];
+            float curs = 0.0f;
+            if (left >= 0 && left < 61 && curg < 61) curs = __ldg(&gt->cps[left * 61 + curg]);
+            if (right < 61 && curg < 61) curs = __fadd_rn(curs, __ldg(&gt->cps[curg * 61 + right]));
+            int up[6], nup = 0;
+            for (int j = 0; j < k; j++) {
+                if (j == cur) continue;
+                int g = st.start[am] + j;
+                float ns = 0.0f;
+                if (left >= 0 && left < 61 && g < 61) ns = __fadd_rn(ns, __ldg(&gt->cps[left * 61 + g]));
+                if (right < 61 && g < 61) ns = __fadd_rn(ns, __ldg(&gt->cps[g * 61 + right]));
+                if (ns > curs) up[nup++] = j;
+            }
+            if (nup > 0) row[a] = (uint8_t)(st.start[am] + up[rng_uint(MDRAW(a, 1), (uint32_t)nup)]);
+        }
+        break;
+    }
+    case 3: {  // mutationHSC, SELECT_UPPER_RANDOM, prob 2Pm, parity gen%2 (:264-388)
+        int c = sm.pobjidx[2 * s.slot[K_HSC]];
+        float pm2 = __fmul_rn(pm, 2.0f);
+        int parity = (int)(gen & 1u);
+        uint8_t *row = ids + c * s.Lp;
+        for (int a = tid; a < L; a += nth) {
+            if ((a & 1) != parity) continue;
+            int am = aa[a];
+            int k = st.count[am];
+            if (rng_u01(MDRAW(a, 0)) > pm2 || k == 1) continue;
+            int cur = row[a] - st.start[am];
+            bool hl = a > 0, hr = a < L - 1;
+            int lft = hl ? row[a - 1] : 0, rgt = hr ? row[a + 1] : 0;
+            int curs = (hl ? __ldg(&gt->hsc[lft * 64 + row[a]]) : 0) + (hr ? __ldg(&gt->hsc[row[a] * 64 + rgt]) : 0);
+            int up[6], nup = 0;
+            for (int j = 0; j < k; j++) {
+                if (j == cur) continue;
+                int g = st.start[am] + j;
+                int ns = (hl ? __ldg(&gt->hsc[lft * 64 + g]) : 0) + (hr ? __ldg(&gt->hsc[g * 64 + rgt]) : 0);
+                if (ns > curs) up[nup++] = j;
+            }
+            if (nup > 0) row[a] = (uint8_t)(st.start[am] + up[rng_uint(MDRAW(a, 1), (uint32_t)nup)]);
+        }
+        break;
+    }
+    case 4: {  // mutationHD (:390-534)
+        int hs = s.slot[K_HD];
+        int c1 = sm.pobjidx[2 * hs], c2 = sm.pobjidx[2 * hs + 1];
+        for (int a = tid; a < L; a += nth) {
+            int am = aa[a];
+            int k = st.count[am];
+            if (rng_u01(MDRAW(a, 0)) > pm || k == 1) continue;
+            int arr[6];
+            shuffle_k(s, gen, ridx, a, k, arr);
+            int x = ids[c1 * s.Lp + a];
+            int cur = x - st.start[am];
+            int y2 = ids[c2 * s.Lp + a];
+            int cur_pair = 0;
+            for (int b = 0; b < 3; b++) cur_pair += st.nt[x][b] != st.nt[y2][b];
+            int cur_m = 127;
+            for (int j = 0; j < m; j++) {
+                if (j == c1) continue;
+                int yj = ids[j * s.Lp + a], d = 0;
+                for (int b = 0; b < 3; b++) d += st.nt[x][b] != st.nt[yj][b];
+                cur_m = min(cur_m, d);
+            }
+            int best_pair = -1, best_m = -1, best = -1;
+            for (int u = 0; u < k; u++) {
+                int sh = arr[u];
+                if (sh == cur) continue;
+                int g = st.start[am] + sh;
+                int np = 0;
+                for (int b = 0; b < 3; b++) np += st.nt[g][b] != st.nt[y2][b];
+                int nm = 127;
+                for (int j = 0; j < m; j++) {
+                    if (j == c1) continue;
+                    int yj = ids[j * s.Lp + a], d = 0;
+                    for (int b = 0; b < 3; b++) d += st.nt[g][b] != st.nt[yj][b];
+                    nm = min(nm, d);
+                }
+                if (nm > cur_m && nm > best_m) {
+                    best_m = nm;
+                    best = sh;
+                } else if (best_m == -1 && nm == cur_m && np > cur_pair && np > best_pair) {
+                    best_pair = np;
+                    best = sh;
+                }
+            }
+            if (best_m != -1 || best_pair != -1) ids[c1 * s.Lp + a] = (uint8_t)(st.start[am] + best);
+        }
+        break;
+    }
+    case 5: {  // mutationGC3 (:536-653) / mutationGC (:655-773), direction from objidx
+        int gs = s.slot[K_GC];
+        int c = sm.pobjidx[2 * gs];
+        int dir = sm.pobjidx[2 * gs + 1];
+        if (dir != 1 && dir != -1) break;
+        float prob;
+        if (s.gcmode == PE_GC3) {
+            prob = sm.pobj[gs];
+        } else {
+            float refGC = __fmul_rn((float)(3 * L), gt->ref_gc);
+            prob = __fdiv_rn(__fmul_rn(sm.pobj[gs], refGC), (float)L);
+        }
+        uint8_t *row = ids + c * s.Lp;
+        for (int a = tid; a < L; a += nth) {
+            int am = aa[a];
+            int k = st.count[am];
+            if (rng_u01(MDRAW(a, 0)) > prob || k == 1) continue;
+            int arr[6];
+            shuffle_k(s, gen, ridx, a, k, arr);
+            int curg = row[a];
+            int cur = curg - st.start[am];
+            int cgc = s.gcmode == PE_GC3 ? st.gc3[curg] : st.gcn[curg];
+            for (int u = 0; u < k; u++) {
+                int sh = arr[u];
+                if (sh == cur) continue;
+                int g = st.start[am] + sh;
+                int ngc = s.gcmode == PE_GC3 ? st.gc3[g] : st.gcn[g];
+                if ((dir == 1 && ngc > cgc) || (dir == -1 && ngc < cgc)) {
+                    row[a] = (uint8_t)g;
+                    break;
+                }
+            }
+        }
+        break;
+    }
+    case 6: {  // mutationSL (:775-969): attempts at the stem's centre codons
+        int ss = s.slot[K_SL];
+        int c = sm.pobjidx[2 * ss];
+        float v = sm.pobj[ss];
+        int P = sm.ppql[0], Ls = sm.ppql[2];
+        int l_idx = P / 3;
+        int r_idx = (P + Ls - 1) / 3;
+        int mid = (r_idx + l_idx) / 2;
+        int stem = r_idx - l_idx + 1;
+        int half = stem / 2;
+        int odd = (stem % 2) == 1;
+        int npos = odd + 2 * min(half, 4096);
+        uint8_t *row = ids + c * s.Lp;
+        for (int u = 0; u < npos; u++) {
+            int a;
+            if (odd && u == 0) {
+                a = mid;
+            } else {
+                int v2 = u - odd;
+                a = (v2 & 1) ? (mid + 1 + (v2 >> 1)) : ((odd ? mid - 1 : mid) - (v2 >> 1));
+            }
+            if (a < 0 || a >= L) break;
+            if (tid == 0) {
+                int am = aa[a];
+                int k = st.count[am];
+                uint32_t r0 = draw(s.seed, TAG_SLMUT, gen, ridx, (uint32_t)u, 0);
+                uint32_t r1 = draw(s.seed, TAG_SLMUT, gen, ridx, (uint32_t)u, 1);
+                sm.sl_mut = 0;
+                if (rng_u01(r0) <= pm && k > 1) {
+                    int old = row[a];
+                    int cur = old - st.start[am];
+                    int nw = (int)rng_uint(r1, (uint32_t)(k - 1));
+                    if (nw == cur) nw++;
+                    row[a] = (uint8_t)(st.start[am] + nw);
+                    sm.sl_old = old;
+                    sm.sl_mut = 1;
+                }
+            }
+            __syncthreads();
+            bool full = cta_full_hairpin(s, st, row, tid, nth);
+            float thr = full ? 1.0f : 0.0f;
+            if (s.K > 0 && v > thr) break;  // keep the change
+            if (tid == 0 && sm.sl_mut) row[a] = (uint8_t)sm.sl_old;
+            __syncthreads();
+        }
+        break;
+    }
+    default:
+        break;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// k_variation: one CTA (kVarThreads) per solution
+// ---------------------------------------------------------------------------
+template <int MODE>
+__global__ void __launch_bounds__(kVarThreads) k_variation(Shape s, const DevTables *__restrict__ gt,
+                                                           const int8_t *__restrict__ aa_g, PopBuf src, PopBuf dst,
+                                                           const int32_t *__restrict__ parent_of,
+                                                           const int32_t *__restrict__ rng_idx, int copy_base,
+                                                           int child_base, const uint32_t *__restrict__ d_gen,
+                                                           int32_t *ops, int32_t *surv)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    VarSmem &sm = *reinterpret_cast<VarSmem *>(smem_raw);
+    uint8_t *ids = smem_raw + ((sizeof(VarSmem) + 15) & ~size_t(15));
+    uint2 *planes = reinterpret_cast<uint2 *>(ids + (size_t)s.m * s.Lp);
+    int8_t *aa = reinterpret_cast<int8_t *>(planes + (size_t)s.m * s.Wp);
+
+    const int tid = threadIdx.x, nth = blockDim.x;
+    const int i = blockIdx.x;
+    const size_t sol_bytes = (size_t)s.m * s.Lp;
+    const size_t sol_words = (size_t)s.m * s.Wp;
+
+    load_tab(sm.tab, gt, tid, nth);
+    for (int a = tid; a < s.L; a += nth) aa[a] = aa_g[a];
+
+    uint32_t gen = 0, ridx = (uint32_t)i;
+    int out_slot = i;
+    if (MODE == MODE_INIT) {
+        __syncthreads();
+        for (int pos = tid; pos < s.m * s.L; pos += nth) {
+            int c = pos / s.L, a = pos - c * s.L;
+            int am = aa[a];
+            int k = sm.tab.count[am];
+            int choice = (i == 0) ? k - 1 : (int)rng_uint(draw(s.seed, TAG_INIT, 0, (uint32_t)i, (uint32_t)pos, 0), k);
+            ids[c * s.Lp + a] = (uint8_t)(sm.tab.start[am] + choice);
+        }
+        for (int c = 0; c < s.m; c++)
+            for (int a = s.L + tid; a < s.Lp; a += nth) ids[c * s.Lp + a] = 0;
+        if (tid == 0 && surv) surv[i] = i;
+    } else if (MODE == MODE_EVAL) {
+        const uint4 *g = reinterpret_cast<const uint4 *>(dst.ids + (size_t)i * sol_bytes);
+        uint4 *d = reinterpret_cast<uint4 *>(ids);
+        for (size_t e = tid; e < sol_bytes / 16; e += nth) d[e] = g[e];
+    } else {  // MODE_MUTATE
+        gen = *d_gen;
+        ridx = rng_idx ? (uint32_t)rng_idx[i] : (uint32_t)i;
+        int par = parent_of[i];
+        const uint4 *g = reinterpret_cast<const uint4 *>(src.ids + (size_t)par * sol_bytes);
+        uint4 *d = reinterpret_cast<uint4 *>(ids);
+        for (size_t e = tid; e < sol_bytes / 16; e += nth) d[e] = g[e];
+        if (tid < s.M) sm.pobj[tid] = src.obj[(size_t)par * s.M + tid];
+        if (tid < 2 * s.M) sm.pobjidx[tid] = src.objidx[(size_t)par * 2 * s.M + tid];
+        if (tid < 3) sm.ppql[tid] = src.pql[(size_t)par * 3 + tid];
+        if (copy_base >= 0) {
+            // the surviving parent keeps its slot: copy ids, planes and objectives
+            size_t dslot = (size_t)(copy_base + i);
+            uint4 *gd = reinterpret_cast<uint4 *>(dst.ids + dslot * sol_bytes);
+            for (size_t e = tid; e < sol_bytes / 16; e += nth) gd[e] = g[e];
+            const uint4 *ps = reinterpret_cast<const uint4 *>(src.planes + (size_t)par * sol_words);
+            uint4 *pd = reinterpret_cast<uint4 *>(dst.planes + dslot * sol_words);
+            for (size_t e = tid; e < sol_words / 2; e += nth) pd[e] = ps[e];
+            if (tid < s.M) dst.obj[dslot * s.M + tid] = src.obj[(size_t)par * s.M + tid];
+            if (tid < 2 * s.M) dst.objidx[dslot * 2 * s.M + tid] = src.objidx[(size_t)par * 2 * s.M + tid];
+            if (tid < 3) dst.pql[dslot * 3 + tid] = src.pql[(size_t)par * 3 + tid];
+        }
+        out_slot = child_base + i;
+        if (tid == 0) {
+            uint32_t r = draw(s.seed, TAG_OP, gen, ridx, 0, 0);
+            int op;
+            if (s.objset == PE_OBJ_REF6) {
+                op = (int)rng_uint(r, 7);
+            } else {
+                const int map5[5] = {0, 1, 4, 5, 6};
+                op = map5[rng_uint(r, 5)];
+            }
+            sm.op = op;
+            if (ops) ops[i] = op;
+        }
+        __syncthreads();
+        mutate_solution(s, gt, sm, aa, ids, gen, ridx, tid, nth);
+    }
+    __syncthreads();
+    pack_planes(s, sm.tab, ids, planes, tid, nth);
+    __syncthreads();
+    // write the (new) solution
+    if (MODE != MODE_EVAL) {
+        uint4 *gd = reinterpret_cast<uint4 *>(dst.ids + (size_t)out_slot * sol_bytes);
+        const uint4 *d = reinterpret_cast<const uint4 *>(ids);
+        for (size_t e = tid; e < sol_bytes / 16; e += nth) gd[e] = d[e];
+    }
+    {
+        uint4 *pd = reinterpret_cast<uint4 *>(dst.planes + (size_t)out_slot * sol_words);
+        const uint4 *ps = reinterpret_cast<const uint4 *>(planes);
+        for (size_t e = tid; e < sol_words / 2; e += nth) pd[e] = ps[e];
+    }
+    light_eval(s, gt, sm, ids, planes, dst.obj + (size_t)out_slot * s.M, dst.objidx + (size_t)out_slot * 2 * s.M, tid,
+               nth);
+}
+
+size_t var_smem_bytes(const Shape &s)
+{
+    return ((sizeof(VarSmem) + 15) & ~size_t(15)) + (size_t)s.m * s.Lp + (size_t)s.m * s.Wp * sizeof(uint2) +
+           (size_t)((s.L + 15) & ~15);
+}
+
+template <int MODE> static cudaError_t set_var_attr(size_t smem)
+{
+    return cudaFuncSetAttribute(k_variation<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+cudaError_t launch_init(const Shape &s, const DevTables *tab, const int8_t *aa, PopBuf dst, int32_t *surv,
+                        cudaStream_t st)
+{
+    size_t smem = var_smem_bytes(s);
+    cudaError_t e = set_var_attr<MODE_INIT>(smem);
+    if (e != cudaSuccess) return e;
+    k_variation<MODE_INIT><<<s.N, kVarThreads, smem, st>>>(s, tab, aa, dst, dst, nullptr, nullptr, -1, 0, nullptr,
+                                                            nullptr, surv);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_light_eval(const Shape &s, const DevTables *tab, const int8_t *aa, PopBuf buf, int base, int count,
+                              cudaStream_t st)
+{
+    if (count <= 0) return cudaSuccess;
+    size_t smem = var_smem_bytes(s);
+    cudaError_t e = set_var_attr<MODE_EVAL>(smem);
+    if (e != cudaSuccess) return e;
+    PopBuf b = buf;
+    size_t sol_bytes = (size_t)s.m * s.Lp, sol_words = (size_t)s.m * s.Wp;
+    b.ids += (size_t)base * sol_bytes;
+    b.planes += (size_t)base * sol_words;
+    b.obj += (size_t)base * s.M;
+    b.objidx += (size_t)base * 2 * s.M;
+    b.pql += (size_t)base * 3;
+    k_variation<MODE_EVAL><<<count, kVarThreads, smem, st>>>(s, tab, aa, b, b, nullptr, nullptr, -1, 0, nullptr,
+                                                              nullptr, nullptr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mutate(const Shape &s, const DevTables *tab, const int8_t *aa, PopBuf src, PopBuf dst,
+                          const int32_t *parent_of, const int32_t *rng_idx, int count, int copy_base, int child_base,
+                          const uint32_t *d_gen, int32_t *ops, cudaStream_t st)
+{
+    if (count <= 0) return cudaSuccess;
+    size_t smem = var_smem_bytes(s);
+    cudaError_t e = set_var_attr<MODE_MUTATE>(smem);
+    if (e != cudaSuccess) return e;
+    k_variation<MODE_MUTATE><<<count, kVarThreads, smem, st>>>(s, tab, aa, src, dst, parent_of, rng_idx, copy_base,
+                                                                child_base, d_gen, ops, nullptr);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// k_sl: hairpin-stem scan on bit planes
+// ---------------------------------------------------------------------------
+//
+// For one CDS s (n nucleotides) with reverse complement t (t[i] = comp(s[n-1-i]))
+// the cell (r, c) of the reference's anti-diagonal sweep pairs iff
+// s[r] == t[r + delta] with delta = n-1-(r+c).  The counted cells of
+// anti-diagonal d = r+c are r in [max(0, d-n+1), floor((d-5)/2)] (upper
+// triangle, loop of >= 4 nucleotides); their longest run of pairing cells is
+// that anti-diagonal's stem length, and the lower triangle never exceeds it
+// (include/utils.cuh:743-774).  Each lane owns one shift delta and walks its
+// cells 32 at a time:
+//     match word = ~((S.lo ^ T.lo) | (S.hi ^ T.hi))
+// with runs carried across words by ffs/clz and long interior runs caught by
+// an AND-shift tower.  T is kept as 32 pre-shifted copies, transposed so that
+// the 32 lanes of a warp read 32 consecutive 8-byte words.
+
+__device__ __forceinline__ uint32_t fshr(uint32_t lo, uint32_t hi, int sh) { return __funnelshift_r(lo, hi, sh); }
+
+template <bool MASKED, bool EXACT>
+__device__ __forceinline__ void sl_word(uint2 sv, uint2 tv, int k, int r_lo, int r_hi, int &cur, int &dbest)
+{
+    uint32_t m = ~((sv.x ^ tv.x) | (sv.y ^ tv.y));
+    if (MASKED) {
+        int lo_b = r_lo - 32 * k, hi_b = r_hi - 32 * k;
+        uint32_t mk = (lo_b > 31 || hi_b < 0 || lo_b > hi_b)
+                          ? 0u
+                          : ((0xffffffffu << max(lo_b, 0)) & (0xffffffffu >> (31 - min(hi_b, 31))));
+        m &= mk;
+    }
+    if (m == 0xffffffffu) {
+        cur += 32;
+    } else {
+        uint32_t z = ~m;
+        int lo = __ffs(z) - 1;
+        dbest = max(dbest, cur + lo);
+        cur = __clz(z);
+        uint32_t x = m & (m >> 1);
+        x &= x >> 2;
+        x &= x >> 4;
+        if (EXACT || x) {
+            uint32_t y = m;
+            int len = 0;
+            while (y) {
+                y &= y >> 1;
+                len++;
+            }
+            dbest = max(dbest, len);
+        }
+    }
+}
+
+template <bool EXACT>
+__device__ void sl_scan(const uint2 *__restrict__ S, const uint2 *__restrict__ Tc, int n, int warp, int nwarps,
+                        int lane, int &best, int &bestd)
+{
+    const int dmax = n - 6;
+    if (dmax < 0) return;
+    const int ndiag = 2 * dmax + 1;
+    const int nchunks = (ndiag + 31) >> 5;
+    for (int ch = warp; ch < nchunks; ch += nwarps) {
+        const int delta = -dmax + 32 * ch + lane;
+        const bool valid = delta <= dmax;
+        int r_lo = valid ? max(0, -delta) : 1;
+        int r_hi = valid ? ((n - 6 - delta) >> 1) : 0;
+        const int klo = r_lo >> 5, khi = r_hi >> 5;
+        const int kmin = warp_min_i(valid ? klo : 0x7fffffff);
+        const int kmax = warp_max_i(valid ? khi : -1);
+        // words fully inside every valid lane's range need no mask
+        const int full_lo = (r_lo + 31) >> 5, full_hi = ((r_hi + 1) >> 5) - 1;
+        const bool allvalid = __all_sync(0xffffffffu, valid);
+        int kf_lo = warp_max_i(full_lo), kf_hi = warp_min_i(full_hi);
+        if (!allvalid) {
+            kf_lo = kmax + 1;
+            kf_hi = kmax;
+        }
+        kf_lo = max(kf_lo, kmin);
+        kf_hi = min(kf_hi, kmax);
+        const uint2 *trow = Tc + (ptrdiff_t)((delta >> 5) + kSlGuardRows) * 32 + (delta & 31);
+        int cur = 0, dbest = 0;
+        int k = kmin;
+        for (; k < kf_lo; k++) sl_word<true, EXACT>(S[k], trow[k * 32], k, r_lo, r_hi, cur, dbest);
+#pragma unroll 4
+        for (; k <= kf_hi; k++) sl_word<false, EXACT>(S[k], trow[k * 32], k, r_lo, r_hi, cur, dbest);
+        for (; k <= kmax; k++) sl_word<true, EXACT>(S[k], trow[k * 32], k, r_lo, r_hi, cur, dbest);
+        dbest = max(dbest, cur);
+        if (valid) {
+            int d = n - 1 - delta;
+            if (dbest > best) {
+                best = dbest;
+                bestd = d;
+            } else if (dbest == best && d < bestd) {
+                bestd = d;
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void pair_reduce(int &best, int &bestd, int ob, int od)
+{
+    if (ob > best || (ob == best && od < bestd)) {
+        best = ob;
+        bestd = od;
+    }
+}
+
+struct SlSmem {
+    int wbest[kSlThreads / 32];
+    int wbestd[kSlThreads / 32];
+    int last;
+    int res[3];
+};
+
+__device__ __forceinline__ int plane_nt(const uint2 *P, int x)
+{
+    uint2 w = P[x >> 5];
+    int b = x & 31;
+    return (int)(((w.x >> b) & 1u) | (((w.y >> b) & 1u) << 1));
+}
+
+__global__ void __launch_bounds__(kSlThreads) k_sl(Shape s, PopBuf buf, int base, int2 *part, int32_t *counter,
+                                                 int32_t *status)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SlSmem &sm = *reinterpret_cast<SlSmem *>(smem_raw);
+    const int G = kSlGuardRows;
+    const int W = s.W, n = s.n;
+    uint2 *S = reinterpret_cast<uint2 *>(smem_raw + ((sizeof(SlSmem) + 15) & ~size_t(15)));  // W + 2
+    uint32_t *Tlo = reinterpret_cast<uint32_t *>(S + (W + 2));                               // W + 2G + 1
+    uint32_t *Thi = Tlo + (W + 2 * G + 1);
+    uint2 *Tc = reinterpret_cast<uint2 *>(Thi + (W + 2 * G + 1));
+    Tc = reinterpret_cast<uint2 *>((reinterpret_cast<uintptr_t>(Tc) + 15) & ~uintptr_t(15));
+
+    const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarps = nth >> 5;
+    const int sol = blockIdx.x / s.m, c = blockIdx.x - sol * s.m;
+    const size_t gsol = (size_t)(base + sol);
+    const uint2 *P = buf.planes + (gsol * s.m + c) * s.Wp;
+
+    // stage S (the CDS planes) with one bulk async copy (TMA engine)
+    {
+        __shared__ __align__(8) uint64_t bar;
+        const uint32_t bytes = (uint32_t)(s.Wp * sizeof(uint2));
+        uint32_t bar_a = (uint32_t)__cvta_generic_to_shared(&bar);
+        if (tid == 0) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a));
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncthreads();
+        if (tid == 0) {
+            uint32_t dst_a = (uint32_t)__cvta_generic_to_shared(S);
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a), "r"(bytes) : "memory");
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst_a),
+                "l"(P), "r"(bytes), "r"(bar_a)
+                : "memory");
+        }
+        // bounded wait on phase 0
+        int done = 0;
+        for (int it = 0; it < (1 << 22) && !done; it++) {
+            uint32_t ok;
+            asm volatile(
+                "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+                : "=r"(ok)
+                : "r"(bar_a), "r"(0u)
+                : "memory");
+            done = (int)ok;
+        }
+        // the copy engine never completed: flag it, give the copy a second
+        // bounded window to land, and leave this CTA (the host reports PE_ERR_TIMEOUT)
+        if (__syncthreads_or(!done)) {
+            if (tid == 0) atomicOr(status, 1);
+            for (int it = 0; it < (1 << 20) && !done; it++) {
+                uint32_t ok;
+                asm volatile(
+                    "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+                    : "=r"(ok)
+                    : "r"(bar_a), "r"(0u)
+                    : "memory");
+                done = (int)ok;
+            }
+            return;
+        }
+        if (tid == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(bar_a));
+        for (int w = s.Wp + tid; w < W + 2; w += nth) S[w] = make_uint2(0u, 0u);
+    }
+    __syncthreads();
+    // reverse complement planes, zero outside [0, W)
+    for (int e = tid; e < W + 2 * G + 1; e += nth) {
+        int w = e - G;
+        uint32_t lo = 0, hi = 0;
+        if (w >= 0 && w < W) {
+            int start = n - 32 - 32 * w;  // source bit of T bit 31 ... bit 0 is source n-1-32w
+            int q = start >> 5, sh = start & 31;
+            uint32_t a0 = (q >= 0 && q < W) ? S[q].x : 0u, a1 = (q + 1 >= 0 && q + 1 < W) ? S[q + 1].x : 0u;
+            uint32_t b0 = (q >= 0 && q < W) ? S[q].y : 0u, b1 = (q + 1 >= 0 && q + 1 < W) ? S[q + 1].y : 0u;
+            lo = ~__brev(fshr(a0, a1, sh));
+            hi = ~__brev(fshr(b0, b1, sh));
+        }
+        Tlo[e] = lo;
+        Thi[e] = hi;
+    }
+    __syncthreads();
+    // 32 shifted copies, transposed: Tc[row][sh] = T bits [32(row-G)+sh, +31]
+    const int rows = W + 2 * G;
+    for (int e = tid; e < rows * 32; e += nth) {
+        int row = e >> 5, sh = e & 31;
+        Tc[e] = make_uint2(fshr(Tlo[row], Tlo[row + 1], sh), fshr(Thi[row], Thi[row + 1], sh));
+    }
+    __syncthreads();
+
+    int best = 0, bestd = 0x7fffffff;
+    sl_scan<false>(S, Tc, n, warp, nwarps, lane, best, bestd);
+    // CTA reduction of (best, smallest anti-diagonal)
+    for (int o = 16; o > 0; o >>= 1) {
+        int ob = __shfl_xor_sync(0xffffffffu, best, o), od = __shfl_xor_sync(0xffffffffu, bestd, o);
+        pair_reduce(best, bestd, ob, od);
+    }
+    if (lane == 0) {
+        sm.wbest[warp] = best;
+        sm.wbestd[warp] = bestd;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        int b = sm.wbest[0], d = sm.wbestd[0];
+        for (int w = 1; w < nwarps; w++) pair_reduce(b, d, sm.wbest[w], sm.wbestd[w]);
+        sm.res[0] = b;
+        sm.res[1] = d;
+    }
+    __syncthreads();
+    if (sm.res[0] < 8) {
+        // short maxima may hide inside a word: rescan with exact per-word runs
+        best = 0;
+        bestd = 0x7fffffff;
+        sl_scan<true>(S, Tc, n, warp, nwarps, lane, best, bestd);
+        for (int o = 16; o > 0; o >>= 1) {
+            int ob = __shfl_xor_sync(0xffffffffu, best, o), od = __shfl_xor_sync(0xffffffffu, bestd, o);
+            pair_reduce(best, bestd, ob, od);
+        }
+        __syncthreads();
+        if (lane == 0) {
+            sm.wbest[warp] = best;
+            sm.wbestd[warp] = bestd;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            int b = sm.wbest[0], d = sm.wbestd[0];
+            for (int w = 1; w < nwarps; w++) pair_reduce(b, d, sm.wbest[w], sm.wbestd[w]);
+            sm.res[0] = b;
+            sm.res[1] = d;
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        part[(size_t)sol * s.m + c] = make_int2(sm.res[0], sm.res[1]);
+        __threadfence();
+        int old = atomicAdd(&counter[sol], 1);
+        sm.last = (old == s.m - 1);
+    }
+    __syncthreads();
+    if (!sm.last) return;
+    __threadfence();
+    // ---- last CTA of this solution: combine CDSs (largest CDS index on ties)
+    if (tid == 0) {
+        int Lb = -1, cb = 0, db = 0;
+        for (int cc = 0; cc < s.m; cc++) {
+            int2 v = __ldcg(&part[(size_t)sol * s.m + cc]);
+            if (v.x >= Lb) {
+                Lb = v.x;
+                cb = cc;
+                db = v.y;
+            }
+        }
+        sm.res[0] = Lb;
+        sm.res[1] = cb;
+        sm.res[2] = db;
+        counter[sol] = 0;
+    }
+    __syncthreads();
+    const int Lb = sm.res[0], cb = sm.res[1], d = sm.res[2];
+    const int slot = s.slot[K_SL];
+    float *obj = buf.obj + gsol * s.M;
+    int8_t *objidx = buf.objidx + gsol * 2 * s.M;
+    int32_t *pql = buf.pql + gsol * 3;
+    if (Lb <= 0) {
+        if (tid == 0) {
+            obj[slot] = 0.0f;
+            objidx[2 * slot] = 0;
+            objidx[2 * slot + 1] = 0;
+            pql[0] = pql[1] = pql[2] = 0;
+        }
+        return;
+    }
+    // Position of the stem the reference's serial sweep records last on
+    // anti-diagonal d: the outermost stem of exactly Lb pairs closed on both
+    // sides inside the counted cells (recorded again, later, from the lower
+    // triangle), else the run cut at the loop limit.
+    if (warp == 0) {
+        const uint2 *Q = buf.planes + (gsol * s.m + cb) * s.Wp;
+        const int r_lo = max(0, d - (n - 1)), r_hi = (d - 5) >> 1;
+        int run = 0, first = -1, typeII = 0;
+        for (int r0 = r_lo; r0 <= r_hi + 1; r0 += 32) {
+            int r = r0 + lane;
+            int bit = 0;
+            if (r <= r_hi + 1) bit = ((plane_nt(Q, r) ^ plane_nt(Q, d - r)) == 3);
+            uint32_t word = __ballot_sync(0xffffffffu, bit);
+            if (lane == 0) {
+                int lim = min(32, r_hi + 2 - r0);
+                for (int b = 0; b < lim; b++) {
+                    int rr = r0 + b, on = (word >> b) & 1u;
+                    if (rr <= r_hi) {
+                        if (on) {
+                            run++;
+                        } else {
+                            if (run == Lb && first < 0) first = rr - run;
+                            run = 0;
+                        }
+                    } else {
+                        if (run == Lb) {
+                            if (!on) {
+                                if (first < 0) first = rr - run;
+                            } else {
+                                typeII = 1;
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        if (lane == 0) {
+            int p, q;
+            if (first >= 0) {
+                p = first;
+                q = d - (first + Lb - 1);
+            } else if (typeII) {
+                p = r_hi - Lb + 1;
+                q = d - r_hi;
+            } else {
+                p = -1;
+                q = -1;
+            }
+            obj[slot] = __fdiv_rn((float)Lb, (float)s.K);
+            objidx[2 * slot] = (int8_t)cb;
+            objidx[2 * slot + 1] = 0;
+            pql[0] = p;
+            pql[1] = q;
+            pql[2] = Lb;
+        }
+    }
+}
+
+size_t sl_smem_bytes(const Shape &s)
+{
+    const int G = kSlGuardRows, W = s.W;
+    size_t b = (sizeof(SlSmem) + 15) & ~size_t(15);
+    b += (size_t)(W + 2) * sizeof(uint2);
+    b += 2 * (size_t)(W + 2 * G + 1) * sizeof(uint32_t);
+    b += 16;  // alignment of Tc
+    b += (size_t)(W + 2 * G) * 32 * sizeof(uint2);
+    return b;
+}
+
+cudaError_t launch_sl(const Shape &s, PopBuf buf, int base, int count, int2 *part, int32_t *counter, int32_t *status,
+                      cudaStream_t st)
+{
+    if (count <= 0) return cudaSuccess;
+    size_t smem = sl_smem_bytes(s);
+    cudaError_t e = cudaFuncSetAttribute(k_sl, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_sl<<<count * s.m, kSlThreads, smem, st>>>(s, buf, base, part, counter, status);
+    return cudaGetLastError();
+}
+
+}  // namespace pe

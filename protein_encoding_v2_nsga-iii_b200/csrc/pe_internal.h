@@ -1,0 +1,101 @@
+// pe_internal.h -- internal types shared by the engine's translation units.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/pe_nsga3.h"
+
+namespace pe {
+
+// objective kinds in the reference's REF6 slot order (include/common.cuh:23-29)
+enum Kind { K_CAI = 0, K_CBP = 1, K_HSC = 2, K_HD = 3, K_GC = 4, K_SL = 5 };
+
+constexpr int kMaxObj = 6;
+constexpr int kMaxCds = 64;          // objidx stores CDS indices as int8
+constexpr int kSlThreads = 256;      // SL scan CTA
+constexpr int kVarThreads = 256;     // variation / light-eval CTA
+constexpr int kSelThreads = 1024;    // selection CTA
+constexpr int kSlGuardRows = 8;      // zero guard rows around the shifted T copies
+
+// RNG stream tags (Philox counter word 0)
+constexpr uint32_t TAG_INIT = 1u, TAG_OP = 2u, TAG_MUT = 3u, TAG_SLMUT = 4u, TAG_NICHE = 5u;
+
+// Problem shape, passed by value to every kernel.
+struct Shape {
+    int L;        // amino-acid positions incl. stop
+    int Lp;       // codon-id row stride (L rounded up to 16)
+    int m;        // CDSs per solution
+    int N;        // population
+    int M;        // objectives
+    int n;        // nucleotides per CDS (3L)
+    int W;        // 32-bit words per nucleotide plane
+    int Wp;       // plane row stride in uint2 (W + 1 zero guard, rounded to even)
+    int K;        // (n-4)/2, the stem normaliser
+    int R;        // reference points
+    int objset, gcmode;
+    float pm;
+    uint64_t seed;
+    int slot[6];  // slot of each Kind or -1
+};
+
+// Device-resident tables derived from pe_codon_table.
+struct DevTables {
+    uint8_t nt[64][4];       // nucleotide codes
+    int64_t lw[64];          // log w in 2^-32 fixed point
+    uint8_t wzero[64];       // w == 0
+    uint8_t gc3[64];         // third nucleotide is C or G
+    uint8_t gcn[64];         // number of C/G nucleotides
+    int8_t start[21];
+    int8_t count[21];
+    int8_t aa_of[64];        // amino acid of each codon id
+    uint8_t hsc[64 * 64];    // hidden stops across a codon boundary
+    int64_t cpsf[61 * 61];   // CPS in 2^-32 fixed point
+    float cps[61 * 61];
+    float ref_gc3, ref_gc;
+};
+
+// One population buffer (2N solutions).
+struct PopBuf {
+    uint8_t *ids;      // [2N][m][Lp]
+    uint2 *planes;     // [2N][m][Wp]  (lo, hi) nucleotide bit planes
+    float *obj;        // [2N][M]
+    int8_t *objidx;    // [2N][2M]
+    int32_t *pql;      // [2N][3]
+};
+
+struct SelectScratch {
+    uint32_t *dom;       // [2N][2N/32] bit j of row i: j dominates i
+    int32_t *np;         // [2N]
+    int32_t *front;      // [2N]
+    int32_t *sorted;     // [2N] fronts 0..last
+    int32_t *assoc;      // [2N]
+    float *dist;         // [2N]
+    int32_t *rho;        // [R]
+    int32_t *fill;       // [R]
+    int32_t *ncand;      // [R]
+    int32_t *coff;       // [R+1]
+    int32_t *cand;       // [2N]
+    int32_t *info;       // [8] rank_count, last_size, n_fronts, cut, hyp_exc, status
+    float *finfo;        // [3*M] ideal, worst, nadir
+};
+
+// launchers (pe_eval.cu)
+cudaError_t launch_init(const Shape &s, const DevTables *tab, const int8_t *aa, PopBuf dst, int32_t *surv,
+                        cudaStream_t st);
+cudaError_t launch_light_eval(const Shape &s, const DevTables *tab, const int8_t *aa, PopBuf buf, int base, int count,
+                              cudaStream_t st);
+cudaError_t launch_mutate(const Shape &s, const DevTables *tab, const int8_t *aa, PopBuf src, PopBuf dst,
+                          const int32_t *parent_of, const int32_t *rng_idx, int count, int copy_base, int child_base,
+                          const uint32_t *d_gen, int32_t *ops, cudaStream_t st);
+cudaError_t launch_sl(const Shape &s, PopBuf buf, int base, int count, int2 *part, int32_t *counter,
+                      int32_t *status, cudaStream_t st);
+size_t sl_smem_bytes(const Shape &s);
+size_t var_smem_bytes(const Shape &s);
+
+// launchers (pe_select.cu)
+cudaError_t launch_select(const Shape &s, const float *obj, float *ext, const float *refpts, SelectScratch sc,
+                          int32_t *surv, uint32_t *d_gen, int bump_gen, cudaStream_t st);
+size_t select_smem_bytes(const Shape &s);
+
+}  // namespace pe

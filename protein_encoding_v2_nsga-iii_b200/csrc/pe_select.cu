@@ -1,0 +1,512 @@
+// pe_select.cu -- environmental selection (sortingKernel, src/main.cu:409-454).
+//
+//  k_dominance  one CTA per solution i: row i of the 2N x 2N dominance bit
+//               matrix (bit j set when j dominates i) built with __ballot_sync,
+//               and np[i] = popc(row) -- replaces the reference's two (2N)^2
+//               bool matrices (include/sorting.cuh:974-1089).
+//  k_select     one CTA: front peeling on the bit matrix, ideal / worst,
+//               extreme points, hyperplane (Gaussian elimination) or MNDF nadir,
+//               reference-point association and niche selection, stopping at
+//               exactly N survivors (include/sorting.cuh:94-1282).
+//
+// Deterministic rules (the reference decides these by atomic order):
+// fronts are listed in ascending solution index; each niche level visits
+// reference points in ascending index; random niche picks come from Philox
+// keyed by (generation, reference point, level).
+#include <cfloat>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "pe_device.cuh"
+#include "pe_internal.h"
+
+namespace pe {
+
+__device__ __forceinline__ bool dominates(const float *a, const float *b, int M)
+{
+    // dominate (include/sorting.cuh:94-130): |a-b| <= 1e-6 counts as equal
+    int eq = 0;
+    bool worse = false;
+    for (int k = 0; k < M; k++) {
+        float d = fabsf(__fsub_rn(a[k], b[k]));
+        if (d > 1e-6f) {
+            if (a[k] > b[k]) worse = true;
+        } else {
+            eq++;
+        }
+    }
+    return eq != M && !worse;
+}
+
+__global__ void __launch_bounds__(256) k_dominance(Shape s, const float *__restrict__ obj, uint32_t *__restrict__ dom,
+                                                   int32_t *__restrict__ np)
+{
+    __shared__ int wsum[8];
+    const int N2 = 2 * s.N, words = (N2 + 31) >> 5;
+    const int i = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    float oi[kMaxObj];
+    for (int k = 0; k < s.M; k++) oi[k] = obj[(size_t)i * s.M + k];
+    int cnt = 0;
+    for (int w = warp; w < words; w += 8) {
+        int j = 32 * w + lane;
+        bool bit = false;
+        if (j < N2 && j != i) {
+            float oj[kMaxObj];
+            for (int k = 0; k < s.M; k++) oj[k] = __ldg(&obj[(size_t)j * s.M + k]);
+            bit = dominates(oj, oi, s.M);
+        }
+        uint32_t word = __ballot_sync(0xffffffffu, bit);
+        if (lane == 0) dom[(size_t)i * words + w] = word;
+        cnt += __popc(word);
+    }
+    if (lane == 0) wsum[warp] = cnt;
+    __syncthreads();
+    if (tid == 0) {
+        int t = 0;
+        for (int w = 0; w < 8; w++) t += wsum[w];
+        np[i] = t;
+    }
+}
+
+struct SelSmem {
+    int warp_tot[33];
+    int i0, i1, i2, i3, i4;
+    int rc, fstart, fsize, cut, nfront, count, level, hyp;
+    float ideal[kMaxObj], worst[kMaxObj], nadir[kMaxObj];
+    float red[64 * kMaxObj];
+};
+
+// exclusive block scan of a 0/1 flag over kSelThreads threads; returns the
+// prefix and leaves the total in *total (all threads)
+__device__ __forceinline__ int block_scan_flag(int flag, SelSmem &sm, int *total)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+    uint32_t b = __ballot_sync(0xffffffffu, flag);
+    int wp = __popc(b & ((1u << lane) - 1u));
+    if (lane == 0) sm.warp_tot[warp] = __popc(b);
+    __syncthreads();
+    if (warp == 0) {
+        int v = lane < nwarps ? sm.warp_tot[lane] : 0;
+        int inc = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            int u = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += u;
+        }
+        sm.warp_tot[lane] = inc - v;
+        if (lane == 31) sm.warp_tot[32] = inc;
+    }
+    __syncthreads();
+    int res = sm.warp_tot[warp] + wp;
+    *total = sm.warp_tot[32];
+    __syncthreads();
+    return res;
+}
+
+__device__ __forceinline__ float asf_val(const float *x, const float *ideal, int i, int M)
+{
+    // ASF (include/sorting.cuh:428-449) with weights 1 (objective i) / 1e-6
+    float mx = -FLT_MAX;
+    for (int k = 0; k < M; k++) {
+        float tmp = __fsub_rn(x[k], ideal[k]);
+        if ((double)tmp < 0.001) tmp = 0.0f;
+        float q = __fdiv_rn(tmp, k == i ? 1.0f : 1e-6f);
+        if (q > mx) mx = q;
+    }
+    return mx;
+}
+
+__global__ void __launch_bounds__(kSelThreads) k_select(Shape s, const float *__restrict__ obj, float *ext,
+                                                        const float *__restrict__ refpts, SelectScratch sc,
+                                                        int32_t *surv, uint32_t *d_gen, int bump_gen)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SelSmem &sm = *reinterpret_cast<SelSmem *>(smem_raw);
+    const int N = s.N, N2 = 2 * N, M = s.M, R = s.R;
+    const int words = (N2 + 31) >> 5;
+    uint32_t *fmask = reinterpret_cast<uint32_t *>(smem_raw + ((sizeof(SelSmem) + 15) & ~size_t(15)));
+    float *tbuf = reinterpret_cast<float *>(fmask + ((words + 3) & ~3));
+    int32_t *tix = reinterpret_cast<int32_t *>(tbuf + ((N2 + M + 3) & ~3));
+    const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t gen = *d_gen;
+
+    // ---------------- front 0 (np == 0), ascending index
+    for (int i = tid; i < N2; i += nth) sc.front[i] = -1;
+    if (tid == 0) sm.rc = 0;
+    __syncthreads();
+    for (int base = 0; base < N2; base += nth) {
+        int i = base + tid;
+        int flag = (i < N2) && sc.np[i] == 0;
+        int tot;
+        int pos = block_scan_flag(flag, sm, &tot);
+        if (flag) {
+            sc.front[i] = 0;
+            sc.sorted[sm.rc + pos] = i;
+        }
+        __syncthreads();
+        if (tid == 0) sm.rc += tot;
+        __syncthreads();
+    }
+    const int f0 = sm.rc;
+    if (tid == 0) {
+        sm.fstart = 0;
+        sm.fsize = f0;
+        sm.cut = (f0 == N);
+        sm.nfront = 1;
+    }
+    __syncthreads();
+    // ---------------- later fronts (only while fewer than N are assigned)
+    if (f0 < N) {
+        for (int it = 0; it < N2 - 1; it++) {
+            for (int w = tid; w < words; w += nth) fmask[w] = 0u;
+            __syncthreads();
+            for (int u = sm.fstart + tid; u < sm.fstart + sm.fsize; u += nth) {
+                int j = sc.sorted[u];
+                atomicOr(&fmask[j >> 5], 1u << (j & 31));
+            }
+            __syncthreads();
+            const int rc0 = sm.rc;
+            const int cf = sm.nfront;
+            for (int base = 0; base < N2; base += nth) {
+                int i = base + tid;
+                int flag = 0;
+                if (i < N2 && sc.front[i] < 0) {
+                    const uint32_t *row = sc.dom + (size_t)i * words;
+                    int dec = 0;
+                    for (int w = 0; w < words; w++) {
+                        uint32_t f = fmask[w];
+                        if (f) dec += __popc(row[w] & f);
+                    }
+                    int v = sc.np[i] - dec;
+                    sc.np[i] = v;
+                    flag = (v == 0);
+                }
+                int tot;
+                int pos = block_scan_flag(flag, sm, &tot);
+                if (flag) {
+                    sc.front[i] = cf;
+                    sc.sorted[sm.rc + pos] = i;
+                }
+                __syncthreads();
+                if (tid == 0) sm.rc += tot;
+                __syncthreads();
+            }
+            if (tid == 0) {
+                sm.fstart = rc0;
+                sm.fsize = sm.rc - rc0;
+                sm.nfront = cf + 1;
+                if (sm.rc >= N) sm.cut = (sm.rc == N);
+            }
+            __syncthreads();
+            if (sm.rc >= N) break;
+        }
+    }
+    const int rc = sm.rc;
+    const int last_size = sm.fsize;
+
+    // ---------------- ideal / worst (exact min / max)
+    {
+        float mn[kMaxObj], mx[kMaxObj];
+        for (int k = 0; k < M; k++) {
+            mn[k] = FLT_MAX;
+            mx[k] = -FLT_MAX;
+        }
+        for (int i = tid; i < N2; i += nth)
+            for (int k = 0; k < M; k++) {
+                float v = obj[(size_t)i * M + k];
+                if (v < mn[k]) mn[k] = v;
+                if (v > mx[k]) mx[k] = v;
+            }
+        for (int k = 0; k < M; k++) {
+            for (int o = 16; o > 0; o >>= 1) {
+                float a = __shfl_xor_sync(0xffffffffu, mn[k], o), b = __shfl_xor_sync(0xffffffffu, mx[k], o);
+                if (a < mn[k]) mn[k] = a;
+                if (b > mx[k]) mx[k] = b;
+            }
+        }
+        if (lane == 0)
+            for (int k = 0; k < M; k++) {
+                sm.red[warp * kMaxObj + k] = mn[k];
+                sm.red[32 * kMaxObj + warp * kMaxObj + k] = mx[k];
+            }
+        __syncthreads();
+        if (tid < M) {
+            float a = FLT_MAX, b = -FLT_MAX;
+            for (int w = 0; w < (nth >> 5); w++) {
+                float u = sm.red[w * kMaxObj + tid], v = sm.red[32 * kMaxObj + w * kMaxObj + tid];
+                if (u < a) a = u;
+                if (v > b) b = v;
+            }
+            sm.ideal[tid] = a;
+            sm.worst[tid] = b;
+        }
+        __syncthreads();
+    }
+
+    // ---------------- extreme points (findExtremePoints, :601-683), tree order of findMinValue
+    {
+        const int B = N2 + M;
+        for (int i = 0; i < M; i++) {
+            for (int t = tid; t < B; t += nth) {
+                float v = FLT_MAX;
+                int ix = -1;
+                if (t < f0) {
+                    int sol = sc.sorted[t];
+                    v = asf_val(obj + (size_t)sol * M, sm.ideal, i, M);
+                    ix = sol;
+                } else if (t < f0 + M) {
+                    v = asf_val(ext + (size_t)(t - f0) * M, sm.ideal, i, M);
+                    ix = N2 + (t - f0);
+                }
+                tbuf[t] = v;
+                tix[t] = ix;
+            }
+            __syncthreads();
+            for (int half = B / 2;; half /= 2) {
+                for (int t = tid; t < half; t += nth)
+                    if (tbuf[t + half] < tbuf[t]) {
+                        tbuf[t] = tbuf[t + half];
+                        tix[t] = tix[t + half];
+                    }
+                __syncthreads();
+                if (half == 1) break;
+                if ((half & 1) && tid == 0 && tbuf[half - 1] < tbuf[0]) {
+                    tbuf[0] = tbuf[half - 1];
+                    tix[0] = tix[half - 1];
+                }
+                __syncthreads();
+            }
+            if (tid == 0) {
+                int sel = tix[0];
+                float tmp[kMaxObj];
+                if (sel >= N2) {
+                    for (int k = 0; k < M; k++) tmp[k] = ext[(sel - N2) * M + k];
+                    for (int k = 0; k < M; k++) ext[i * M + k] = tmp[k];
+                } else if (sel >= 0) {
+                    for (int k = 0; k < M; k++) ext[i * M + k] = obj[(size_t)sel * M + k];
+                }
+            }
+            __syncthreads();
+        }
+    }
+
+    // ---------------- hyperplane intercepts (GaussianElimination :555-599, check :929-956)
+    if (tid == 0) {
+        float AB[kMaxObj][kMaxObj + 1], x[kMaxObj];
+        for (int i = 0; i < M; i++) {
+            for (int j = 0; j < M; j++) AB[i][j] = ext[i * M + j];
+            AB[i][M] = 1.0f;
+        }
+        for (int c = 0; c < M; c++) {
+            if ((double)fabsf(AB[c][c]) <= 1e-6) {
+                int r = c;
+                while (r < M && !((double)fabsf(AB[r][c]) > 1e-6)) r++;
+                if (r < M)
+                    for (int j = c; j <= M; j++) AB[c][j] = __fadd_rn(AB[c][j], AB[r][j]);
+            }
+            for (int r = c + 1; r < M; r++) {
+                float f = __fdiv_rn(AB[r][c], AB[c][c]);
+                for (int j = c; j <= M; j++) AB[r][j] = __fsub_rn(AB[r][j], __fmul_rn(f, AB[c][j]));
+            }
+        }
+        for (int r = M - 1; r >= 0; r--) {
+            float sacc = 0.0f;
+            for (int j = r + 1; j < M; j++) sacc = __fadd_rn(sacc, __fmul_rn(AB[r][j], x[j]));
+            x[r] = __fdiv_rn(__fsub_rn(AB[r][M], sacc), AB[r][r]);
+        }
+        int exc = 0;
+        for (int k = 0; k < M; k++) {
+            float res = 0.0f;
+            for (int i = 0; i < M; i++) res = __fadd_rn(res, __fmul_rn(x[i], __fsub_rn(ext[k * M + i], sm.ideal[i])));
+            if (fabsf(__fsub_rn(res, 1.0f)) > 1e-6f || isnan(res) || isinf(res)) exc = 1;
+            float icp = __fdiv_rn(1.0f, x[k]);
+            if (icp <= 1e-6f || isnan(icp) || isinf(icp)) exc = 1;
+            sm.nadir[k] = __fadd_rn(sm.ideal[k], icp);
+        }
+        sm.hyp = exc;
+    }
+    __syncthreads();
+    if (sm.hyp) {
+        // updateNadirValue_MNDF (:685-884): max over front 0, worst when too close to ideal
+        float mx[kMaxObj];
+        for (int k = 0; k < M; k++) mx[k] = -FLT_MAX;
+        for (int t = tid; t < f0; t += nth) {
+            int sol = sc.sorted[t];
+            for (int k = 0; k < M; k++) {
+                float v = obj[(size_t)sol * M + k];
+                if (v > mx[k]) mx[k] = v;
+            }
+        }
+        for (int k = 0; k < M; k++)
+            for (int o = 16; o > 0; o >>= 1) {
+                float b = __shfl_xor_sync(0xffffffffu, mx[k], o);
+                if (b > mx[k]) mx[k] = b;
+            }
+        __syncthreads();
+        if (lane == 0)
+            for (int k = 0; k < M; k++) sm.red[warp * kMaxObj + k] = mx[k];
+        __syncthreads();
+        if (tid < M) {
+            float b = -FLT_MAX;
+            for (int w = 0; w < (nth >> 5); w++) {
+                float v = sm.red[w * kMaxObj + tid];
+                if (v > b) b = v;
+            }
+            sm.nadir[tid] = __fsub_rn(b, sm.ideal[tid]) > 1e-6f ? b : sm.worst[tid];
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        sc.info[0] = rc;
+        sc.info[1] = last_size;
+        sc.info[2] = sm.nfront;
+        sc.info[3] = sm.cut;
+        sc.info[4] = sm.hyp;
+        for (int k = 0; k < M; k++) {
+            sc.finfo[k] = sm.ideal[k];
+            sc.finfo[M + k] = sm.worst[k];
+            sc.finfo[2 * M + k] = sm.nadir[k];
+        }
+    }
+    if (sm.cut) {
+        for (int t = tid; t < N; t += nth) surv[t] = sc.sorted[t];
+        __syncthreads();
+        if (tid == 0 && bump_gen) *d_gen = gen + 1;
+        return;
+    }
+
+    // ---------------- association (referenceBasedSorting phase 1, :1105-1180)
+    const int count0 = rc - last_size;
+    for (int j = tid; j < R; j += nth) {
+        sc.rho[j] = 0;
+        sc.ncand[j] = 0;
+    }
+    __syncthreads();
+    for (int t = tid; t < rc; t += nth) {
+        int sol = sc.sorted[t];
+        float f[kMaxObj];
+        for (int k = 0; k < M; k++)
+            f[k] = __fdiv_rn(__fsub_rn(obj[(size_t)sol * M + k], sm.ideal[k]), __fsub_rn(sm.nadir[k], sm.ideal[k]));
+        float best = FLT_MAX;
+        int bj = 0;
+        for (int j = 0; j < R; j++) {
+            // perpendicularDistance (include/utils.cuh:1149-1171)
+            const float *w = refpts + (size_t)j * M;
+            float num = 0.0f, den = 0.0f;
+            for (int k = 0; k < M; k++) {
+                num = __fadd_rn(num, __fmul_rn(w[k], f[k]));
+                den = __fadd_rn(den, __fmul_rn(w[k], w[k]));
+            }
+            float kk = __fdiv_rn(num, den);
+            float d2 = 0.0f;
+            for (int k = 0; k < M; k++) {
+                float e = __fsub_rn(__fmul_rn(kk, w[k]), f[k]);
+                d2 = __fadd_rn(d2, __fmul_rn(e, e));
+            }
+            float d = __fsqrt_rn(d2);
+            if (d < best) {
+                best = d;
+                bj = j;
+            }
+        }
+        sc.dist[sol] = best;
+        sc.assoc[t] = bj;
+        if (t < count0) atomicAdd(&sc.rho[bj], 1);
+        else atomicAdd(&sc.ncand[bj], 1);
+    }
+    __syncthreads();
+    // candidate lists per reference point, ascending position
+    if (tid == 0) {
+        int acc = 0;
+        for (int j = 0; j < R; j++) {
+            sc.coff[j] = acc;
+            acc += sc.ncand[j];
+        }
+        sc.coff[R] = acc;
+    }
+    __syncthreads();
+    int32_t *fill = sc.fill;
+    for (int j = tid; j < R; j += nth) fill[j] = 0;
+    __syncthreads();
+    if (warp == 0) {
+        for (int base = count0; base < rc; base += 32) {
+            int t = base + lane;
+            bool act = t < rc;
+            int j = act ? sc.assoc[t] : -1 - lane;
+            uint32_t peers = __match_any_sync(0xffffffffu, j);
+            int rank = __popc(peers & ((1u << lane) - 1u));
+            int f0v = act ? fill[j] : 0;
+            __syncwarp();
+            if (act) sc.cand[sc.coff[j] + f0v + rank] = sc.sorted[t];
+            __syncwarp();
+            if (act && rank == 0) fill[j] = f0v + __popc(peers);
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    // ---------------- niching (phase 2, :1182-1279), exactly N survivors
+    for (int t = tid; t < count0; t += nth) surv[t] = sc.sorted[t];
+    if (tid == 0) {
+        sm.count = count0;
+        sm.level = 0;
+    }
+    __syncthreads();
+    while (sm.count < N && sm.level <= N2 + 2) {
+        const int level = sm.level;
+        for (int jb = 0; jb < R; jb += nth) {
+            int j = jb + tid;
+            int flag = (j < R) && sc.rho[j] == level && sc.ncand[j] > 0;
+            int tot;
+            int pos = block_scan_flag(flag, sm, &tot);
+            int out = sm.count + pos;
+            if (flag && out < N) {
+                int *cl = sc.cand + sc.coff[j];
+                int nc = sc.ncand[j];
+                int slot = 0;
+                if (level == 0) {
+                    float bd = sc.dist[cl[0]];
+                    for (int u = 1; u < nc; u++) {
+                        float dv = sc.dist[cl[u]];
+                        if (dv < bd) {
+                            bd = dv;
+                            slot = u;
+                        }
+                    }
+                } else {
+                    slot = (int)rng_uint(draw(s.seed, TAG_NICHE, gen, (uint32_t)j, (uint32_t)level, 0), (uint32_t)nc);
+                }
+                surv[out] = cl[slot];
+                sc.rho[j] = level + 1;
+                sc.ncand[j] = nc - 1;
+                cl[slot] = cl[nc - 1];
+            }
+            __syncthreads();
+            if (tid == 0) sm.count = min(N, sm.count + tot);
+            __syncthreads();
+        }
+        if (tid == 0) sm.level = level + 1;
+        __syncthreads();
+    }
+    if (tid == 0 && bump_gen) *d_gen = gen + 1;
+}
+
+size_t select_smem_bytes(const Shape &s)
+{
+    const int N2 = 2 * s.N, words = (N2 + 31) >> 5;
+    return ((sizeof(SelSmem) + 15) & ~size_t(15)) + (size_t)((words + 3) & ~3) * 4 +
+           (size_t)((N2 + s.M + 3) & ~3) * 4 + (size_t)(N2 + s.M) * 4;
+}
+
+cudaError_t launch_select(const Shape &s, const float *obj, float *ext, const float *refpts, SelectScratch sc,
+                          int32_t *surv, uint32_t *d_gen, int bump_gen, cudaStream_t st)
+{
+    k_dominance<<<2 * s.N, 256, 0, st>>>(s, obj, sc.dom, sc.np);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    size_t smem = select_smem_bytes(s);
+    e = cudaFuncSetAttribute(k_select, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_select<<<1, kSelThreads, smem, st>>>(s, obj, ext, refpts, sc, surv, d_gen, bump_gen);
+    return cudaGetLastError();
+}
+
+}  // namespace pe
