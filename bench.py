@@ -1,0 +1,294 @@
+#!/usr/bin/env python
+"""Benchmark: generations/s of the plain NSGA-III codon-design loop on B200.
+
+Workload (one step = one generation): one synthetic protein of L=1000 amino
+acids (+ stop), m=8 CDSs per solution, population N=1024, mutation probability
+0.02, four objectives (min CAI, min pairwise Hamming distance, GC3 deviation,
+longest hairpin stem), Das-Dennis M=4 p=8 (165 reference points); a full design
+job is 500 generations (designs/s = generations/s / 500).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU: one independent replica per rank (its own seed, no data-path
+collective); `value` = generations of all ranks / the slowest rank's time.
+The reference arm times the CPU restatement of the reference algorithm on the
+host cores (the reference itself has no CPU implementation).
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import importlib.util
+import io
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+L_AA, M_CDS, POP, PM, P_REF, G_JOB, SEED = 1000, 8, 1024, 0.02, 8, 500, 2024
+WORKLOAD = (f"plain NSGA-III, one synthetic protein L={L_AA} aa (+stop), m={M_CDS} CDSs, N={POP}, Pm={PM}, "
+            f"4 objectives, Das-Dennis M=4 p={P_REF} (165 points), design job = {G_JOB} generations")
+METRIC = "generations/s"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def load_pkg():
+    spec = importlib.util.spec_from_file_location("pe_b200", ROOT / "protein_encoding_v2_nsga-iii_b200" / "__init__.py")
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["pe_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def hairpin_cells_per_cds(n: int) -> int:
+    """Counted cells of the stem scan for one CDS of n nucleotides: the upper-triangle
+    pairs (r, c) with c - r >= 5 over all anti-diagonals."""
+    k = n - 5
+    return k * (k + 1) // 2 if k > 0 else 0
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while timing."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.rows = []
+        if self.proc is None:
+            return
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        for r in csv.reader(io.StringIO(out)):
+            if len(r) >= 9:
+                self.rows.append([x.strip() for x in r])
+
+    def summary(self):
+        rows = getattr(self, "rows", [])
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i, v in enumerate(r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_reference(pe, orc, eng_pop, aa, table, steps: int, threads: int):
+    """Time the CPU restatement of one generation on a bounded sample: variation +
+    evaluation of S offspring (all host threads) and selection on the full 2N set;
+    seconds per generation = t_offspring * N / S + t_select."""
+    ids, obj, objidx, pql, surv = eng_pop
+    prob = orc.Problem(aa, table.arrays(), M_CDS, POP, PM, objset=1, p=P_REF, seed=SEED)
+    S = max(8, 2 * threads)
+    par = surv[:S]
+    rates = []
+    for k in range(steps):
+        t0 = time.perf_counter()
+        prob.mutate(k, np.arange(S, dtype=np.int32), ids[par], obj[par], objidx[par], pql[par], threads=threads)
+        t1 = time.perf_counter()
+        ext = obj[:4].copy()
+        prob.select(k, obj, ext)
+        t2 = time.perf_counter()
+        sec_per_gen = (t1 - t0) * POP / S + (t2 - t1)
+        rates.append(1.0 / sec_per_gen)
+    sample = (f"{S} offspring mutated + evaluated (of {POP}) with {threads} threads, scaled to {POP}, "
+              f"plus selection on the full 2N={2 * POP} set, per step")
+    return rates, sample
+
+
+def run_reference(args, world, rank):
+    """The reference arm: the CPU restatement of the reference algorithm on host cores."""
+    if rank != 0:
+        return
+    pe = load_pkg()
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pe_oracle as orc
+    threads = os.cpu_count() or 1
+    aa = pe.synthetic_protein(L_AA, SEED)
+    table = pe.dirichlet_table(SEED)
+    prob = orc.Problem(aa, table.arrays(), M_CDS, POP, PM, objset=1, p=P_REF, seed=SEED)
+    # parents: a population generated and evaluated by the oracle itself (bounded: 2*threads solutions)
+    S = max(8, 2 * threads)
+    ids = np.stack([prob.gen_solution(i) for i in range(S)])
+    obj, objidx, pql = prob.evaluate(ids, threads=threads)
+    fake_obj = np.concatenate([obj] * ((2 * POP + S - 1) // S))[:2 * POP]
+    fake_obj = fake_obj + np.random.default_rng(0).random(fake_obj.shape).astype(np.float32) * 1e-3
+    pop = (ids, fake_obj, np.concatenate([objidx] * ((2 * POP + S - 1) // S))[:2 * POP],
+           np.concatenate([pql] * ((2 * POP + S - 1) // S))[:2 * POP], np.arange(S, dtype=np.int32))
+    for _ in range(max(0, args.warmup > 0)):
+        cpu_reference(pe, orc, pop, aa, table, 1, threads)
+    t0 = time.perf_counter()
+    rates, sample = cpu_reference(pe, orc, pop, aa, table, args.steps, threads)
+    wall = time.perf_counter() - t0
+    value = statistics.median(rates)
+    line = {"metric": METRIC, "value": value, "unit": "generations/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "designs_per_s": value / G_JOB},
+            "cpu_baseline": {"value": value, "unit": "generations/s", "cores": threads, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "generations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "wall_s": wall}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    pe = load_pkg()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    stream = torch.cuda.Stream(device=dev)
+    aa = pe.synthetic_protein(L_AA, SEED)
+    table = pe.dirichlet_table(SEED)
+    eng = pe.Engine(aa, table, M_CDS, POP, PM, objectives=pe.OBJ_BASE4, ref_p=P_REF, seed=SEED + rank,
+                    stream=stream.cuda_stream)
+    eng.init()
+    eng.set_profiling(True)
+    for _ in range(args.warmup):
+        eng.step(1)
+    eng.synchronize()
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    stage = np.zeros(3)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize(dev)
+    with ClockSampler(local) as clk:
+        t_wall = time.perf_counter()
+        for k in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()                       # L2 flush between timed steps (not timed)
+                ev[k][0].record(stream)
+                eng.step(1)
+                ev[k][1].record(stream)
+            eng.synchronize()
+            stage += eng.stage_times()
+        torch.cuda.synchronize(dev)
+        t_wall = time.perf_counter() - t_wall
+    if world > 1:
+        torch.distributed.barrier()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_s = sum(step_ms) / 1000.0
+    t = torch.tensor([total_s], dtype=torch.float64, device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    max_s = float(t.item())
+    value = world * args.steps / max_s
+    stage_ms = stage / args.steps
+    n_nt = 3 * (L_AA + 1)
+    cells = POP * M_CDS * hairpin_cells_per_cds(n_nt)
+    sl_s = stage_ms[1] / 1000.0
+
+    line = None
+    if rank == 0:
+        # end-to-end through the public API with host buffers: a design job of G_E2E generations
+        G_E2E = 20
+        obj_host = np.zeros((2 * POP, 4), np.float32)
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        e2 = pe.Engine(aa, table, M_CDS, POP, PM, objectives=pe.OBJ_BASE4, ref_p=P_REF, seed=SEED + 7)
+        e2.init()
+        for _ in range(G_E2E):
+            e2.step(1)
+            e2.objectives(obj_host)                 # per-generation device->host read of the objective block
+        final = e2.population()
+        e2.close()
+        e2e_s = time.perf_counter() - t0
+        h2d = aa.nbytes + 4 * (64 * 4 + 61 * 61 + 12)
+        d2h = obj_host.nbytes + sum(a.nbytes for a in final) / G_E2E
+
+        # CPU baseline: the oracle on this host, bounded sample (N=1 only)
+        cpu = None
+        if world == 1:
+            sys.path.insert(0, str(ROOT / "oracle"))
+            import pe_oracle as orc
+            threads = os.cpu_count() or 1
+            rates, sample = cpu_reference(pe, orc, eng.population(), aa, table, 1, threads)
+            cpu = {"value": rates[0], "unit": "generations/s", "cores": threads, "kind": "port", "sample": sample}
+
+        peaks = {}
+        try:
+            peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+        except Exception:
+            pass
+        clocks = clk.summary()
+        line = {
+            "metric": METRIC, "value": value, "unit": "generations/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * max_s / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "global_batch": POP * world, "parallelism": f"replicas{world}",
+                       "l2": "flushed between timed steps (256 MiB write, untimed)",
+                       "designs_per_s": value / G_JOB,
+                       "stage_ms": {"variation_eval": stage_ms[0], "hairpin_scan": stage_ms[1],
+                                    "selection": stage_ms[2]}},
+            "roofline": {"bound": "alu", "kernel": "k_sl (hairpin-stem scan)", "achieved": cells / sl_s / 1e9,
+                         "unit": "Gcells/s", "peak": None, "frac": None, "traffic": None,
+                         "cells_per_launch": cells},
+            "clocks": clocks,
+            "e2e": {"value": G_E2E / e2e_s, "unit": "generations/s", "h2d_bytes_per_step": h2d / G_E2E,
+                    "d2h_bytes_per_step": d2h, "job": f"create + init + {G_E2E} generations + reads"},
+            "gpu_launches": 4 * args.steps,
+            "wall_s": t_wall,
+            "peaks_file": {k: peaks.get(k) for k in ("hbm_gbs", "bf16_tflops", "sm_max_mhz")},
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+    else:
+        run_ours(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -152,6 +152,16 @@ int pe_dirichlet_table(uint64_t seed, pe_codon_table *out);
  * "gc3 <v>", "gc <v>", then optional 61*61 CPS values. */
 int pe_load_codon_table(const char *path, pe_codon_table *out);
 
+/* --- instrumentation (no counterpart in the reference, which only times the
+ *     whole loop with cudaEvents, src/main.cu:702-731) --- */
+
+/* Record CUDA events around the three stages of each generation (variation +
+ * light evaluation, hairpin-stem scan, selection); rebuilds the graphs. */
+int pe_set_profiling(pe_instance *inst, int32_t enable);
+/* Device milliseconds of those stages in the last completed generation
+ * (call after pe_synchronize). */
+int pe_stage_times(pe_instance *inst, float *ms3);
+
 /* Exact hypervolume of n points (d <= 6) in minimisation form w.r.t. ref. */
 int pe_hypervolume(const double *pts, int32_t n, int32_t d, const double *ref, double *out);
 

@@ -114,6 +114,7 @@ def lib() -> C.CDLL:
             "pe_dirichlet_table": [C.c_uint64, C.POINTER(CodonTable)],
             "pe_load_codon_table": [C.c_char_p, C.POINTER(CodonTable)],
             "pe_hypervolume": [P, C.c_int32, C.c_int32, P, C.POINTER(C.c_double)],
+            "pe_set_profiling": [P, C.c_int32], "pe_stage_times": [P, P],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -235,6 +236,15 @@ class Engine:
 
     def synchronize(self):
         _ck(lib().pe_synchronize(self._h))
+
+    def set_profiling(self, enable: bool = True):
+        _ck(lib().pe_set_profiling(self._h, int(enable)))
+
+    def stage_times(self):
+        """Device ms of (variation + light evaluation, hairpin scan, selection) in the last generation."""
+        out = np.zeros(3, np.float32)
+        _ck(lib().pe_stage_times(self._h, _ptr(out)))
+        return out
 
     def population(self):
         N2 = 2 * self.N

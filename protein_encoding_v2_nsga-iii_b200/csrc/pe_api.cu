@@ -122,6 +122,8 @@ struct pe_instance {
     bool initialized = false;
     uint32_t generation = 0;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    bool profiling = false;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     std::vector<void *> allocs;
 
     template <class T> int alloc(T **p, size_t count)
@@ -191,16 +193,28 @@ int check_status(pe_instance *in)
     return PE_OK;
 }
 
+cudaError_t mark(pe_instance *in, int k)
+{
+    if (!in->profiling) return cudaSuccess;
+    return cudaEventRecordWithFlags(in->ev[k], in->stream, cudaEventRecordExternal);
+}
+
 cudaError_t enqueue_generation(pe_instance *in, int src)
 {
     const Shape &s = in->s;
     int dst = 1 - src;
-    cudaError_t e = launch_mutate(s, in->d_tab, in->d_aa, in->buf[src], in->buf[dst], in->d_surv, nullptr, s.N, 0,
-                                  s.N, in->d_gen, nullptr, in->stream);
+    cudaError_t e = mark(in, 0);
     if (e != cudaSuccess) return e;
+    e = launch_mutate(s, in->d_tab, in->d_aa, in->buf[src], in->buf[dst], in->d_surv, nullptr, s.N, 0, s.N, in->d_gen,
+                      nullptr, in->stream);
+    if (e != cudaSuccess) return e;
+    if ((e = mark(in, 1)) != cudaSuccess) return e;
     e = launch_sl(s, in->buf[dst], s.N, s.N, in->d_part, in->d_counter, in->d_status, in->stream);
     if (e != cudaSuccess) return e;
-    return launch_select(s, in->buf[dst].obj, in->d_ext, in->d_ref, in->sc, in->d_surv, in->d_gen, 1, in->stream);
+    if ((e = mark(in, 2)) != cudaSuccess) return e;
+    e = launch_select(s, in->buf[dst].obj, in->d_ext, in->d_ref, in->sc, in->d_surv, in->d_gen, 1, in->stream);
+    if (e != cudaSuccess) return e;
+    return mark(in, 3);
 }
 
 int build_graphs(pe_instance *in)
@@ -414,12 +428,39 @@ int pe_create(const pe_config *cfg, const int8_t *aa_idx, int32_t aa_len, const 
     return PE_OK;
 }
 
+int pe_set_profiling(pe_instance *in, int32_t enable)
+{
+    if (!in) return fail(PE_ERR_ARG, "null instance");
+    CK(cudaStreamSynchronize(in->stream));
+    for (int k = 0; k < 4; k++)
+        if (!in->ev[k]) CK(cudaEventCreate(&in->ev[k]));
+    if ((bool)enable != in->profiling) {
+        for (int i = 0; i < 2; i++)
+            if (in->graph[i]) {
+                cudaGraphExecDestroy(in->graph[i]);
+                in->graph[i] = nullptr;
+            }
+        in->profiling = enable != 0;
+    }
+    return PE_OK;
+}
+
+int pe_stage_times(pe_instance *in, float *ms3)
+{
+    if (!in || !ms3) return fail(PE_ERR_ARG, "null argument");
+    if (!in->profiling) return fail(PE_ERR_STATE, "profiling is off");
+    for (int k = 0; k < 3; k++) CK(cudaEventElapsedTime(&ms3[k], in->ev[k], in->ev[k + 1]));
+    return PE_OK;
+}
+
 int pe_destroy(pe_instance *in)
 {
     if (!in) return PE_OK;
     if (in->stream) cudaStreamSynchronize(in->stream);
     for (int i = 0; i < 2; i++)
         if (in->graph[i]) cudaGraphExecDestroy(in->graph[i]);
+    for (int k = 0; k < 4; k++)
+        if (in->ev[k]) cudaEventDestroy(in->ev[k]);
     for (void *p : in->allocs) cudaFree(p);
     if (in->own_stream && in->stream) cudaStreamDestroy(in->stream);
     delete in;
@@ -736,12 +777,18 @@ int pe_load_codon_table(const char *path, pe_codon_table *out)
     memset(out, 0, sizeof *out);
     out->ref_gc3 = 0.3810f;
     out->ref_gc = 0.3977f;
-    char line[256];
+    std::vector<char> linebuf(1 << 16);
+    char *line = linebuf.data();
     int id = 0, last_aa = -1;
     int counts[21] = {0};
     int ncps = 0;
     bool in_cps = false;
-    while (fgets(line, sizeof line, fp)) {
+    while (fgets(line, (int)linebuf.size(), fp)) {
+        size_t len = strlen(line);
+        if (len == linebuf.size() - 1 && line[len - 1] != '\n' && !feof(fp)) {
+            fclose(fp);
+            return fail(PE_ERR_IO, "%s: line longer than %zu characters", path, linebuf.size() - 2);
+        }
         char *p = line;
         while (*p == ' ' || *p == '\t') p++;
         if (*p == '#' || *p == '\n' || *p == 0) continue;
@@ -794,6 +841,7 @@ int pe_load_codon_table(const char *path, pe_codon_table *out)
     }
     fclose(fp);
     if (id != 64) return fail(PE_ERR_IO, "%s: %d codons (need 64)", path, id);
+    if (in_cps && ncps != 61 * 61) return fail(PE_ERR_IO, "%s: %d CPS values (need %d)", path, ncps, 61 * 61);
     int st = 0;
     for (int a = 0; a < 21; a++) {
         out->start[a] = (int8_t)st;

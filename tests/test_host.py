@@ -12,7 +12,7 @@ B7KHU9 = "MIEPLVLGLVMGLVPITLAGLFVAAYLQYKRGNQLNLD"
 
 def test_library_exports_every_declared_symbol(pe):
     names = pe.declared_symbols()
-    assert len(names) == 19 and "pe_step" in names and "pe_hypervolume" in names
+    assert len(names) == 21 and "pe_step" in names and "pe_hypervolume" in names
     lib = pe.lib()
     for n in names:
         assert hasattr(lib, n), n
@@ -82,6 +82,10 @@ def test_reference_table_file(pe):
     assert t["count"].tolist() == [4, 2, 2, 2, 2, 4, 2, 3, 2, 6, 1, 2, 4, 2, 6, 6, 4, 4, 1, 2, 3]
     assert t["weight"][2] == np.float32(7223) / np.float32(135063.0)
     assert abs(t["ref_gc3"] - 0.381) < 1e-7 and abs(t["ref_gc"] - 0.3977) < 1e-7
+    # include/info.cuh:54 (61x61 codon-pair scores; long lines must parse whole)
+    cps = t["cps"]
+    assert cps[:3].tolist() == [np.float32(0.007921), np.float32(0.060698), np.float32(-0.159742)]
+    assert np.abs(cps).max() < 1.0 and np.count_nonzero(cps) > 3600
 
 
 def test_reference_points_match_oracle(pe, orc):
