@@ -162,6 +162,25 @@ int pe_set_profiling(pe_instance *inst, int32_t enable);
  * (call after pe_synchronize). */
 int pe_stage_times(pe_instance *inst, float *ms3);
 
+/* --- allocation-free hairpin-stem evaluation (no counterpart in the reference).
+ *
+ * For callers that may not allocate device memory (their host application's
+ * memory manager already owns the GPU, or their loop cannot afford
+ * cudaMalloc/cudaFree): the longest-stem objective of n solutions already on the
+ * device, computed with no allocation.  All pointers are device pointers:
+ *   d_nt     uint8 [n][m][3L]  nucleotide codes (A=0 C=1 G=2 U=3)
+ *   d_value  float [n]         stem length / ((3L-4)/2)  (NaN if a scan did not finish)
+ *   d_pql    int32 [n][3]      stem p, q, length
+ *   d_cds    int8  [n]         CDS holding the stem
+ * Scratch is one fixed 8 MiB device array held by every GPU that loads the
+ * library until exit; calls needing more (roughly n*m*3L/4 bytes) return
+ * PE_ERR_ARG.  The first call on a device looks the array up (no allocation);
+ * make that call before capturing work on the stream.  Asynchronous on
+ * cuda_stream (NULL = default stream).  Every call shares the array, so calls
+ * that overlap on the GPU race and give wrong results. */
+int pe_hairpin_noalloc(const uint8_t *d_nt, int32_t n_solutions, int32_t m, int32_t L, float *d_value,
+                       int32_t *d_pql, int8_t *d_cds, void *cuda_stream);
+
 /* Exact hypervolume of n points (d <= 6) in minimisation form w.r.t. ref. */
 int pe_hypervolume(const double *pts, int32_t n, int32_t d, const double *ref, double *out);
 

@@ -115,6 +115,7 @@ def lib() -> C.CDLL:
             "pe_load_codon_table": [C.c_char_p, C.POINTER(CodonTable)],
             "pe_hypervolume": [P, C.c_int32, C.c_int32, P, C.POINTER(C.c_double)],
             "pe_set_profiling": [P, C.c_int32], "pe_stage_times": [P, P],
+            "pe_hairpin_noalloc": [P, C.c_int32, C.c_int32, C.c_int32, P, P, P, P],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -177,6 +178,13 @@ def reference_points(M: int, p: int) -> np.ndarray:
     out = np.zeros((R.value, M), np.float32)
     _ck(lib().pe_reference_points(M, p, _ptr(out), C.byref(R)))
     return out
+
+
+def hairpin_noalloc(d_nt: int, n_solutions: int, m: int, L: int, d_value: int, d_pql: int, d_cds: int,
+                    stream: int = 0):
+    """Allocation-free stem evaluation on device pointers (see pe_hairpin_noalloc)."""
+    _ck(lib().pe_hairpin_noalloc(C.c_void_p(d_nt), n_solutions, m, L, C.c_void_p(d_value), C.c_void_p(d_pql),
+                                 C.c_void_p(d_cds), C.c_void_p(stream) if stream else None))
 
 
 def hypervolume(points, ref) -> float:

@@ -100,6 +100,8 @@ uint64_t splitmix64(uint64_t &x)
 
 }  // namespace
 
+void pe::set_error_text(const char *msg) { g_err = msg ? msg : ""; }
+
 struct pe_instance {
     Shape s{};
     pe_config cfg{};

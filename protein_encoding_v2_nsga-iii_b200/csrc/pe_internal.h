@@ -93,6 +93,9 @@ cudaError_t launch_sl(const Shape &s, PopBuf buf, int base, int count, int2 *par
 size_t sl_smem_bytes(const Shape &s);
 size_t var_smem_bytes(const Shape &s);
 
+// records a message for pe_last_error() (pe_api.cu)
+void set_error_text(const char *msg);
+
 // launchers (pe_select.cu)
 cudaError_t launch_select(const Shape &s, const float *obj, float *ext, const float *refpts, SelectScratch sc,
                           int32_t *surv, uint32_t *d_gen, int bump_gen, cudaStream_t st);
