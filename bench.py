@@ -54,7 +54,7 @@ def hairpin_cells_per_cds(n: int) -> int:
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms while timing."""
+    """nvidia-smi clocks / throttle reasons sampled every 100 ms while timing."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -67,7 +67,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
@@ -106,26 +106,37 @@ def dist_setup():
     return world, rank, local
 
 
-def cpu_reference(pe, orc, eng_pop, aa, table, steps: int, threads: int):
-    """Time the CPU restatement of one generation on a bounded sample: variation +
-    evaluation of S offspring (all host threads) and selection on the full 2N set;
-    seconds per generation = t_offspring * N / S + t_select."""
-    ids, obj, objidx, pql, surv = eng_pop
+SL_STRIDE = 16
+
+
+def cpu_reference(pe, orc, pop, aa, table, steps: int, threads: int):
+    """Time the CPU restatement of one generation on bounded samples, scaled to the
+    full workload.  Per step: (1) mutation + every objective but the stem for S
+    offspring, (2) the reference's serial anti-diagonal stem sweep of `threads` CDSs
+    restricted to every 16th anti-diagonal (rotating), (3) selection on the full 2N set.
+    seconds/generation = t1*N/S + t2*16*(N*m)/threads + t3."""
+    ids, obj, objidx, pql, surv = pop
     prob = orc.Problem(aa, table.arrays(), M_CDS, POP, PM, objset=1, p=P_REF, seed=SEED)
-    S = max(8, 2 * threads)
+    S = min(len(surv), max(8, threads))
     par = surv[:S]
+    nt = np.asarray(table.arrays()["nt"])
+    cds = np.stack([nt[ids[par[i % S], i % M_CDS]].reshape(-1) for i in range(threads)]).astype(np.uint8)
     rates = []
     for k in range(steps):
         t0 = time.perf_counter()
-        prob.mutate(k, np.arange(S, dtype=np.int32), ids[par], obj[par], objidx[par], pql[par], threads=threads)
+        prob.mutate_light(k, np.arange(S, dtype=np.int32), ids[par], obj[par], objidx[par], pql[par],
+                          threads=threads)
         t1 = time.perf_counter()
+        orc.sl_sample(cds, k % SL_STRIDE, SL_STRIDE, threads=threads)
+        t2 = time.perf_counter()
         ext = obj[:4].copy()
         prob.select(k, obj, ext)
-        t2 = time.perf_counter()
-        sec_per_gen = (t1 - t0) * POP / S + (t2 - t1)
+        t3 = time.perf_counter()
+        sec_per_gen = (t1 - t0) * POP / S + (t2 - t1) * SL_STRIDE * (POP * M_CDS) / threads + (t3 - t2)
         rates.append(1.0 / sec_per_gen)
-    sample = (f"{S} offspring mutated + evaluated (of {POP}) with {threads} threads, scaled to {POP}, "
-              f"plus selection on the full 2N={2 * POP} set, per step")
+    sample = (f"per step: mutation + non-stem objectives of {S} offspring, the serial stem sweep of {threads} CDSs "
+              f"on every {SL_STRIDE}th anti-diagonal, selection on the full 2N={2 * POP} set; "
+              f"{threads} threads; scaled to N={POP}, m={M_CDS}")
     return rates, sample
 
 
@@ -140,8 +151,8 @@ def run_reference(args, world, rank):
     aa = pe.synthetic_protein(L_AA, SEED)
     table = pe.dirichlet_table(SEED)
     prob = orc.Problem(aa, table.arrays(), M_CDS, POP, PM, objset=1, p=P_REF, seed=SEED)
-    # parents: a population generated and evaluated by the oracle itself (bounded: 2*threads solutions)
-    S = max(8, 2 * threads)
+    # parents: a population generated and evaluated by the oracle itself (bounded: `threads` solutions)
+    S = max(8, threads)
     ids = np.stack([prob.gen_solution(i) for i in range(S)])
     obj, objidx, pql = prob.evaluate(ids, threads=threads)
     fake_obj = np.concatenate([obj] * ((2 * POP + S - 1) // S))[:2 * POP]
@@ -279,11 +290,22 @@ def run_ours(args, world, rank, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="only build the bench instance, init and run 2 generations (for ncu captures)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
+    if args.profile_case:
+        pe = load_pkg()
+        eng = pe.Engine(pe.synthetic_protein(L_AA, SEED), pe.dirichlet_table(SEED), M_CDS, POP, PM,
+                        objectives=pe.OBJ_BASE4, ref_p=P_REF, seed=SEED)
+        eng.init()
+        eng.step(2)
+        eng.synchronize()
+        eng.close()
+        return
     if args.impl == "reference":
         run_reference(args, world, rank)
     else:

@@ -278,6 +278,52 @@ int or_sl_serial_one(const uint8_t *nt, int n)
     return l;
 }
 
+/* The same sweep restricted to anti-diagonals t = offset, offset+stride, ...
+ * (a bounded sample of the work, for timing). Returns that sample's max run. */
+int or_sl_serial_strided(const uint8_t *s, int n, int offset, int stride)
+{
+    int l = 0;
+    for (int t = offset; t < 2 * n + 1; t += stride) {
+        int diag_len, st_r, st_c;
+        if (t < n + 1) {
+            diag_len = t + 1;
+            st_r = n - diag_len;
+            st_c = n;
+        } else {
+            diag_len = 2 * n + 1 - t;
+            st_r = -1;
+            st_c = diag_len - 1;
+        }
+        int tmp = 0;
+        for (int j = 1; j < diag_len; j++) {
+            int r = st_r + j, c = st_c - j;
+            if (compat(s[r], s[c])) {
+                tmp++;
+                if (c > r) {
+                    if (c - r > 4 && tmp >= l) l = tmp;
+                } else if ((r - tmp + 1) > (c + tmp - 1)) {
+                    if (((r - tmp + 1) - (c + tmp - 1)) > 4 && tmp >= l) l = tmp;
+                } else {
+                    tmp = 0;
+                }
+            } else {
+                tmp = 0;
+            }
+        }
+    }
+    return l;
+}
+
+/* count CDSs (n nucleotides each) swept in parallel on the sampled anti-diagonals */
+void or_sl_sample_batch(const uint8_t *nt, int count, int n, int offset, int stride, int threads, int32_t *out)
+{
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel for schedule(dynamic, 1)
+#endif
+    for (int i = 0; i < count; i++) out[i] = or_sl_serial_strided(nt + (size_t)i * n, n, offset, stride);
+}
+
 static void expand_nt(const or_problem *pr, const uint8_t *sol, uint8_t *nt)
 {
     int n = 3 * pr->L;
@@ -290,7 +336,7 @@ static void expand_nt(const or_problem *pr, const uint8_t *sol, uint8_t *nt)
         }
 }
 
-void or_eval(const or_problem *pr, const uint8_t *sol, float *obj, int8_t *objidx, int32_t *pql)
+static void eval_impl(const or_problem *pr, const uint8_t *sol, float *obj, int8_t *objidx, int32_t *pql, int with_sl)
 {
     const or_codon_table *t = pr->tab;
     const int L = pr->L, m = pr->m, n = 3 * L;
@@ -394,7 +440,7 @@ void or_eval(const or_problem *pr, const uint8_t *sol, float *obj, int8_t *objid
         }
     }
     /* calMaximumSL (include/utils.cuh:712-888) */
-    if ((s = or_slot_of(pr->objset, OR_K_SL)) >= 0) {
+    if ((s = or_slot_of(pr->objset, OR_K_SL)) >= 0 && with_sl) {
         int l, p, q, c;
         sl_serial(nt, m, n, &l, &p, &q, &c);
         int K = (n - 4) / 2;
@@ -407,6 +453,17 @@ void or_eval(const or_problem *pr, const uint8_t *sol, float *obj, int8_t *objid
         pql[0] = pql[1] = pql[2] = 0;
     }
     free(nt);
+}
+
+void or_eval(const or_problem *pr, const uint8_t *sol, float *obj, int8_t *objidx, int32_t *pql)
+{
+    eval_impl(pr, sol, obj, objidx, pql, 1);
+}
+
+/* every objective except the hairpin stem (timing sample helper) */
+void or_eval_light(const or_problem *pr, const uint8_t *sol, float *obj, int8_t *objidx, int32_t *pql)
+{
+    eval_impl(pr, sol, obj, objidx, pql, 0);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -1161,6 +1218,21 @@ void or_mutate_eval_batch(const or_problem *pr, uint32_t gen, const int32_t *idx
                            ppql + (size_t)i * 3, child + (size_t)i * sl);
         if (ops) ops[i] = op;
         or_eval(pr, child + (size_t)i * sl, cobj + (size_t)i * M, cobjidx + (size_t)i * 2 * M, cpql + (size_t)i * 3);
+    }
+}
+
+void or_mutate_eval_light_batch(const or_problem *pr, uint32_t gen, const int32_t *idx, int n, const uint8_t *parents,
+                                 const float *pobj, const int8_t *pobjidx, const int32_t *ppql, uint8_t *child,
+                                 float *cobj, int8_t *cobjidx, int32_t *cpql, int threads)
+{
+    int M = or_num_obj(pr->objset);
+    size_t sl = (size_t)pr->m * pr->L;
+    set_threads(threads);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int i = 0; i < n; i++) {
+        or_mutate(pr, gen, idx[i], parents + (size_t)i * sl, pobj + (size_t)i * M, pobjidx + (size_t)i * 2 * M,
+                  ppql + (size_t)i * 3, child + (size_t)i * sl);
+        or_eval_light(pr, child + (size_t)i * sl, cobj + (size_t)i * M, cobjidx + (size_t)i * 2 * M, cpql + (size_t)i * 3);
     }
 }
 

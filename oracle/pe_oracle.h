@@ -75,6 +75,13 @@ void or_eval(const or_problem *pr, const uint8_t *sol, float *obj, int8_t *objid
 int  or_mutate(const or_problem *pr, uint32_t gen, int idx, const uint8_t *parent,
                const float *pobj, const int8_t *pobjidx, const int32_t *ppql, uint8_t *child);
 int  or_sl_serial_one(const uint8_t *nt, int n);   /* calOneCDS_SL max l */
+/* timing-sample helpers (bounded slices of the same work) */
+void or_eval_light(const or_problem *pr, const uint8_t *sol, float *obj, int8_t *objidx, int32_t *pql);
+int  or_sl_serial_strided(const uint8_t *nt, int n, int offset, int stride);
+void or_sl_sample_batch(const uint8_t *nt, int count, int n, int offset, int stride, int threads, int32_t *out);
+void or_mutate_eval_light_batch(const or_problem *pr, uint32_t gen, const int32_t *idx, int n, const uint8_t *parents,
+                                 const float *pobj, const int8_t *pobjidx, const int32_t *ppql, uint8_t *child,
+                                 float *cobj, int8_t *cobjidx, int32_t *cpql, int threads);
 
 typedef struct {
     int32_t rank_count;      /* solutions in fronts 0..last */

@@ -70,6 +70,9 @@ def lib():
         L.or_eval_batch.argtypes = [C.POINTER(OrProblem), P, C.c_int, P, P, P, C.c_int]
         L.or_mutate_eval_batch.argtypes = [C.POINTER(OrProblem), C.c_uint32, P, C.c_int, P, P, P, P, P, P, P, P, P,
                                            C.c_int]
+        L.or_sl_sample_batch.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P]
+        L.or_mutate_eval_light_batch.argtypes = [C.POINTER(OrProblem), C.c_uint32, P, C.c_int, P, P, P, P, P, P, P,
+                                                 P, C.c_int]
         L.or_hypervolume.argtypes = [P, C.c_int, C.c_int, P]
         L.or_hypervolume.restype = C.c_double
         _lib = L
@@ -144,6 +147,22 @@ class Problem:
                                    _p(cpql), _p(ops), threads)
         return child, ops, cobj, cobjidx, cpql
 
+    def mutate_light(self, generation: int, idx, parents, pobj, pobjidx, ppql, threads: int = 0):
+        """mutation + every objective except the hairpin stem (timing sample)"""
+        parents = np.ascontiguousarray(parents, np.uint8).reshape(-1, self.m, self.L)
+        n = parents.shape[0]
+        idx = np.ascontiguousarray(idx, np.int32)
+        child = np.zeros_like(parents)
+        cobj = np.zeros((n, self.M), np.float32)
+        cobjidx = np.zeros((n, 2 * self.M), np.int8)
+        cpql = np.zeros((n, 3), np.int32)
+        lib().or_mutate_eval_light_batch(C.byref(self.c), generation, _p(idx), n, _p(parents),
+                                         _p(np.ascontiguousarray(pobj, np.float32)),
+                                         _p(np.ascontiguousarray(pobjidx, np.int8)),
+                                         _p(np.ascontiguousarray(ppql, np.int32)), _p(child), _p(cobj),
+                                         _p(cobjidx), _p(cpql), threads)
+        return child
+
     def select(self, generation: int, obj, extremes):
         obj = np.ascontiguousarray(obj, np.float32)
         ext = np.array(extremes, np.float32, copy=True).reshape(self.M, self.M)
@@ -212,6 +231,14 @@ def det_exp(x: float) -> float:
 def sl_serial_one(nt) -> int:
     nt = np.ascontiguousarray(nt, np.uint8)
     return lib().or_sl_serial_one(_p(nt), len(nt))
+
+
+def sl_sample(nt_cds, offset: int, stride: int, threads: int = 0) -> np.ndarray:
+    """serial stem sweep of each CDS (rows of nt_cds) on anti-diagonals offset, offset+stride, ..."""
+    nt_cds = np.ascontiguousarray(nt_cds, np.uint8)
+    out = np.zeros(nt_cds.shape[0], np.int32)
+    lib().or_sl_sample_batch(_p(nt_cds), nt_cds.shape[0], nt_cds.shape[1], offset, stride, threads, _p(out))
+    return out
 
 
 def hypervolume(points, ref) -> float:
