@@ -721,12 +721,12 @@ __device__ __forceinline__ void sl_word(uint2 sv, uint2 tv, int k, int r_lo, int
         m &= mk;
     }
     if (m == 0xffffffffu) {
-        cur += 32;
+        cur += 32;  // the run goes on through the whole word
     } else {
-        uint32_t z = ~m;
-        int lo = __ffs(z) - 1;
-        dbest = max(dbest, cur + lo);
-        cur = __clz(z);
+        const uint32_t z = ~m;
+        dbest = max(dbest, cur + __ffs(z) - 1);  // run carried in + ones at the low end
+        cur = __clz(z);                          // ones at the high end carry out
+        // starts of 8 consecutive ones inside the word (rare: exact length below)
         uint32_t x = m & (m >> 1);
         x &= x >> 2;
         x &= x >> 4;
@@ -743,14 +743,22 @@ __device__ __forceinline__ void sl_word(uint2 sv, uint2 tv, int k, int r_lo, int
 }
 
 template <bool EXACT>
-__device__ void sl_scan(const uint2 *__restrict__ S, const uint2 *__restrict__ Tc, int n, int warp, int nwarps,
-                        int lane, int &best, int &bestd)
+__device__ void sl_scan(const uint2 *__restrict__ S, const uint2 *__restrict__ Tc, int n, int *next_chunk, int lane,
+                        int &best, int &bestd)
 {
     const int dmax = n - 6;
     if (dmax < 0) return;
     const int ndiag = 2 * dmax + 1;
     const int nchunks = (ndiag + 31) >> 5;
-    for (int ch = warp; ch < nchunks; ch += nwarps) {
+    const int c0 = nchunks >> 1;
+    for (;;) {
+        // warps take chunks of 32 anti-diagonals from the centre outwards (longest
+        // first), so the CTA's warps finish together
+        int t = 0;
+        if (lane == 0) t = atomicAdd(next_chunk, 1);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= nchunks) break;
+        const int ch = (t & 1) ? c0 - 1 - (t >> 1) : c0 + (t >> 1);
         const int delta = -dmax + 32 * ch + lane;
         const bool valid = delta <= dmax;
         int r_lo = valid ? max(0, -delta) : 1;
@@ -801,6 +809,7 @@ struct SlSmem {
     int wbestd[kSlThreads / 32];
     int last;
     int res[3];
+    int next_chunk;
 };
 
 __device__ __forceinline__ int plane_nt(const uint2 *P, int x)
@@ -898,10 +907,11 @@ __global__ void __launch_bounds__(kSlThreads) k_sl(Shape s, PopBuf buf, int base
         int row = e >> 5, sh = e & 31;
         Tc[e] = make_uint2(fshr(Tlo[row], Tlo[row + 1], sh), fshr(Thi[row], Thi[row + 1], sh));
     }
+    if (tid == 0) sm.next_chunk = 0;
     __syncthreads();
 
     int best = 0, bestd = 0x7fffffff;
-    sl_scan<false>(S, Tc, n, warp, nwarps, lane, best, bestd);
+    sl_scan<false>(S, Tc, n, &sm.next_chunk, lane, best, bestd);
     // CTA reduction of (best, smallest anti-diagonal)
     for (int o = 16; o > 0; o >>= 1) {
         int ob = __shfl_xor_sync(0xffffffffu, best, o), od = __shfl_xor_sync(0xffffffffu, bestd, o);
@@ -917,13 +927,14 @@ __global__ void __launch_bounds__(kSlThreads) k_sl(Shape s, PopBuf buf, int base
         for (int w = 1; w < nwarps; w++) pair_reduce(b, d, sm.wbest[w], sm.wbestd[w]);
         sm.res[0] = b;
         sm.res[1] = d;
+        sm.next_chunk = 0;
     }
     __syncthreads();
     if (sm.res[0] < 8) {
         // short maxima may hide inside a word: rescan with exact per-word runs
         best = 0;
         bestd = 0x7fffffff;
-        sl_scan<true>(S, Tc, n, warp, nwarps, lane, best, bestd);
+        sl_scan<true>(S, Tc, n, &sm.next_chunk, lane, best, bestd);
         for (int o = 16; o > 0; o >>= 1) {
             int ob = __shfl_xor_sync(0xffffffffu, best, o), od = __shfl_xor_sync(0xffffffffu, bestd, o);
             pair_reduce(best, bestd, ob, od);

@@ -13,6 +13,7 @@
 // fronts are listed in ascending solution index; each niche level visits
 // reference points in ascending index; random niche picks come from Philox
 // keyed by (generation, reference point, level).
+#include <algorithm>
 #include <cfloat>
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -127,7 +128,8 @@ __global__ void __launch_bounds__(kSelThreads) k_select(Shape s, const float *__
     float *tbuf = reinterpret_cast<float *>(fmask + ((words + 3) & ~3));
     int32_t *tix = reinterpret_cast<int32_t *>(tbuf + ((N2 + M + 3) & ~3));
     const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5;
-    const uint32_t gen = *d_gen;
+    (void)d_gen;
+    (void)bump_gen;
 
     // ---------------- front 0 (np == 0), ascending index
     for (int i = tid; i < N2; i += nth) sc.front[i] = -1;
@@ -369,27 +371,40 @@ __global__ void __launch_bounds__(kSelThreads) k_select(Shape s, const float *__
     }
     if (sm.cut) {
         for (int t = tid; t < N; t += nth) surv[t] = sc.sorted[t];
-        __syncthreads();
-        if (tid == 0 && bump_gen) *d_gen = gen + 1;
-        return;
+        return;  // k_niche advances the generation counter
     }
 
-    // ---------------- association (referenceBasedSorting phase 1, :1105-1180)
-    const int count0 = rc - last_size;
+    // niche counts are filled by k_assoc
     for (int j = tid; j < R; j += nth) {
         sc.rho[j] = 0;
         sc.ncand[j] = 0;
     }
-    __syncthreads();
-    for (int t = tid; t < rc; t += nth) {
-        int sol = sc.sorted[t];
+    if (tid == 0) sc.info[5] = rc - last_size;
+}
+
+// referenceBasedSorting phase 1 (:1105-1180) on the whole grid: one warp per
+// solution of fronts 0..last, lanes over reference points; perpendicular
+// distance (include/utils.cuh:1149-1171), argmin with the lowest index on ties.
+__global__ void __launch_bounds__(256) k_assoc(Shape s, const float *__restrict__ obj,
+                                               const float *__restrict__ refpts, SelectScratch sc)
+{
+    if (sc.info[3]) return;  // fronts filled N exactly: no niching
+    const int M = s.M, R = s.R;
+    const int rc = sc.info[0], count0 = sc.info[5];
+    const int lane = threadIdx.x & 31;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+    float ideal[kMaxObj], span[kMaxObj];
+    for (int k = 0; k < M; k++) {
+        ideal[k] = sc.finfo[k];
+        span[k] = __fsub_rn(sc.finfo[2 * M + k], ideal[k]);
+    }
+    for (int t = gw; t < rc; t += nw) {
+        const int sol = sc.sorted[t];
         float f[kMaxObj];
-        for (int k = 0; k < M; k++)
-            f[k] = __fdiv_rn(__fsub_rn(obj[(size_t)sol * M + k], sm.ideal[k]), __fsub_rn(sm.nadir[k], sm.ideal[k]));
+        for (int k = 0; k < M; k++) f[k] = __fdiv_rn(__fsub_rn(obj[(size_t)sol * M + k], ideal[k]), span[k]);
         float best = FLT_MAX;
         int bj = 0;
-        for (int j = 0; j < R; j++) {
-            // perpendicularDistance (include/utils.cuh:1149-1171)
+        for (int j = lane; j < R; j += 32) {
             const float *w = refpts + (size_t)j * M;
             float num = 0.0f, den = 0.0f;
             for (int k = 0; k < M; k++) {
@@ -408,12 +423,35 @@ __global__ void __launch_bounds__(kSelThreads) k_select(Shape s, const float *__
                 bj = j;
             }
         }
-        sc.dist[sol] = best;
-        sc.assoc[t] = bj;
-        if (t < count0) atomicAdd(&sc.rho[bj], 1);
-        else atomicAdd(&sc.ncand[bj], 1);
+        for (int o = 16; o > 0; o >>= 1) {
+            float ob = __shfl_xor_sync(0xffffffffu, best, o);
+            int oj = __shfl_xor_sync(0xffffffffu, bj, o);
+            if (ob < best || (ob == best && oj < bj)) {
+                best = ob;
+                bj = oj;
+            }
+        }
+        if (lane == 0) {
+            sc.dist[sol] = best;
+            sc.assoc[t] = bj;
+            atomicAdd(t < count0 ? &sc.rho[bj] : &sc.ncand[bj], 1);
+        }
     }
-    __syncthreads();
+}
+
+// referenceBasedSorting phase 2 (:1182-1279): candidate lists and niche levels
+__global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc, int32_t *surv, uint32_t *d_gen,
+                                                       int bump_gen)
+{
+    __shared__ SelSmem sm;
+    const int N = s.N, N2 = 2 * N, R = s.R;
+    const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t gen = *d_gen;
+    if (sc.info[3]) {  // fronts filled N exactly; k_select wrote the survivors
+        if (tid == 0 && bump_gen) *d_gen = gen + 1;
+        return;
+    }
+    const int rc = sc.info[0], count0 = sc.info[5];
     // candidate lists per reference point, ascending position
     if (tid == 0) {
         int acc = 0;
@@ -506,6 +544,11 @@ cudaError_t launch_select(const Shape &s, const float *obj, float *ext, const fl
     e = cudaFuncSetAttribute(k_select, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     k_select<<<1, kSelThreads, smem, st>>>(s, obj, ext, refpts, sc, surv, d_gen, bump_gen);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    const int warps_needed = 2 * s.N;
+    k_assoc<<<std::min((warps_needed + 7) / 8, 148 * 8), 256, 0, st>>>(s, obj, refpts, sc);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    k_niche<<<1, kSelThreads, 0, st>>>(s, sc, surv, d_gen, bump_gen);
     return cudaGetLastError();
 }
 
