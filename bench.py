@@ -36,6 +36,12 @@ WORKLOAD = (f"plain NSGA-III, one synthetic protein L={L_AA} aa (+stop), m={M_CD
             f"4 objectives, Das-Dennis M=4 p={P_REF} (165 points), design job = {G_JOB} generations")
 METRIC = "generations/s"
 L2_FLUSH_BYTES = 256 << 20
+# k_sl at this workload, from one ncu capture (profiles/k_sl_L1000_m8_N1024.md):
+# thread instructions per launch / counted cells per launch, and DRAM bytes per launch
+SL_THREAD_INST_PER_LAUNCH = 42485464361
+SL_DRAM_BYTES_PER_LAUNCH = 6349312
+SL_ALU_PIPE_PCT_NCU = 81.69
+SM_COUNT, LANES_PER_SM_CLK = 148, 128   # 4 schedulers x 32 lanes issue per SM per clock
 
 
 def load_pkg():
@@ -51,6 +57,21 @@ def hairpin_cells_per_cds(n: int) -> int:
     pairs (r, c) with c - r >= 5 over all anti-diagonals."""
     k = n - 5
     return k * (k + 1) // 2 if k > 0 else 0
+
+
+def roofline(cells: int, sl_seconds: float, clocks: dict) -> dict:
+    """Integer-issue roofline of the stem scan: achieved lane-ops/s = counted cells/s x
+    lane instructions per cell (ncu); peak = 148 SMs x 128 lanes x sampled SM clock."""
+    ops_per_cell = SL_THREAD_INST_PER_LAUNCH / cells
+    achieved = cells / sl_seconds * ops_per_cell / 1e9
+    mhz = clocks.get("sm_mhz") or 1965.0
+    peak = SM_COUNT * LANES_PER_SM_CLK * mhz * 1e6 / 1e9
+    return {"bound": "alu", "kernel": "k_sl (hairpin-stem scan)", "unit": "Glane-ops/s", "achieved": achieved,
+            "peak": peak, "frac": achieved / peak, "traffic": SL_DRAM_BYTES_PER_LAUNCH,
+            "peak_source": "issue rate 4x32 lanes/SM/clk x 148 SMs at the sampled SM clock (no measured integer "
+                           "peak exists in MEASURED_PEAKS.json)",
+            "cells_per_launch": cells, "cells_per_s": cells / sl_seconds, "lane_ops_per_cell": ops_per_cell,
+            "alu_pipe_pct_of_peak_ncu": SL_ALU_PIPE_PCT_NCU}
 
 
 class ClockSampler:
@@ -269,9 +290,7 @@ def run_ours(args, world, rank, local):
                        "designs_per_s": value / G_JOB,
                        "stage_ms": {"variation_eval": stage_ms[0], "hairpin_scan": stage_ms[1],
                                     "selection": stage_ms[2]}},
-            "roofline": {"bound": "alu", "kernel": "k_sl (hairpin-stem scan)", "achieved": cells / sl_s / 1e9,
-                         "unit": "Gcells/s", "peak": None, "frac": None, "traffic": None,
-                         "cells_per_launch": cells},
+            "roofline": roofline(cells, sl_s, clocks),
             "clocks": clocks,
             "e2e": {"value": G_E2E / e2e_s, "unit": "generations/s", "h2d_bytes_per_step": h2d / G_E2E,
                     "d2h_bytes_per_step": d2h, "job": f"create + init + {G_E2E} generations + reads"},
@@ -287,8 +306,78 @@ def run_ours(args, world, rank, local):
         torch.distributed.destroy_process_group()
 
 
+def batched_jobs(master_seed: int, count: int = 64):
+    """64 independent proteins: L log-uniform in [100, 3000] aa, m from {2, 4, 8},
+    per-instance seeds from the master seed (SplitMix64)."""
+    x = master_seed
+    jobs = []
+    for j in range(count):
+        x = (x + 0x9E3779B97F4A7C15) & 0xFFFFFFFFFFFFFFFF
+        z = x
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & 0xFFFFFFFFFFFFFFFF
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & 0xFFFFFFFFFFFFFFFF
+        z ^= z >> 31
+        u = ((z >> 11) + 0.5) / float(1 << 53)
+        L = int(round(100 * (3000 / 100) ** u))
+        m = (2, 4, 8)[(z >> 3) % 3]
+        jobs.append((L, m, z))
+    return jobs
+
+
+def run_batched(args):
+    """Config 4: 64 design jobs (N=512, 300 generations) as one batch vs one at a time."""
+    import torch
+    pe = load_pkg()
+    torch.cuda.set_device(0)
+    G = args.generations or 300
+    jobs = batched_jobs(SEED)
+    N, pm = 512, 0.02
+
+    def make(j):
+        L, m, seed = jobs[j]
+        e = pe.Engine(pe.synthetic_protein(L, seed), pe.dirichlet_table(seed), m, N, pm, objectives=pe.OBJ_BASE4,
+                      seed=seed)
+        e.init()
+        return e
+
+    cells = sum(N * m * hairpin_cells_per_cds(3 * (L + 1)) for L, m, _ in jobs) * G
+    # one at a time (the plain per-protein form)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for j in range(len(jobs)):
+        e = make(j)
+        e.step(G)
+        e.synchronize()
+        e.close()
+    t_plain = time.perf_counter() - t0
+    # all together (same accounting: create + init + generations)
+    with ClockSampler(0) as clk:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        engines = [make(j) for j in range(len(jobs))]
+        with pe.Batch(engines) as b:
+            b.step(G)
+            b.synchronize()
+        t_batch = time.perf_counter() - t0
+    for e in engines:
+        e.close()
+    line = {"metric": "designs/s", "value": len(jobs) / t_batch, "unit": "designs/s", "n_gpus": 1,
+            "steps": G, "warmup": 0, "ms_per_step": 1000.0 * t_batch / G, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": f"batched: {len(jobs)} proteins, L log-uniform [100, 3000], m in {{2,4,8}}, "
+                                   f"N={N}, Pm={pm}, 4 objectives, {G} generations, one graph launch per 2 "
+                                   f"generations for all instances",
+                       "plain_designs_per_s": len(jobs) / t_plain, "batched_over_plain": t_plain / t_batch,
+                       "stem_cells_per_s": cells / t_batch,
+                       "timing": "wall clock per mode, each including create + init + all generations"},
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", choices=["plain", "batched", "served"], default="plain")
+    ap.add_argument("--generations", type=int, default=0, help="generations per job (batched / served)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
@@ -297,6 +386,9 @@ def main():
                     help="only build the bench instance, init and run 2 generations (for ncu captures)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
+    if args.workload == "batched":
+        run_batched(args)
+        return
     if args.profile_case:
         pe = load_pkg()
         eng = pe.Engine(pe.synthetic_protein(L_AA, SEED), pe.dirichlet_table(SEED), M_CDS, POP, PM,

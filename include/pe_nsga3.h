@@ -152,6 +152,18 @@ int pe_dirichlet_table(uint64_t seed, pe_codon_table *out);
  * "gc3 <v>", "gc <v>", then optional 61*61 CPS values. */
 int pe_load_codon_table(const char *path, pe_codon_table *out);
 
+/* --- batched design jobs (no counterpart in the reference, which runs one
+ *     protein per process, src/main.cu:467).  count initialised instances, each
+ *     on its own stream (pe_create with cuda_stream = NULL), advance together:
+ *     one CUDA graph launch covers two generations of every instance, with one
+ *     concurrent branch per instance, so the device interleaves their kernels.
+ *     Results equal stepping each instance alone (same seed, same arithmetic). */
+typedef struct pe_batch pe_batch;
+int pe_batch_create(pe_instance *const *instances, int32_t count, pe_batch **out);
+int pe_batch_step(pe_batch *batch, int32_t generations);
+int pe_batch_synchronize(pe_batch *batch);
+int pe_batch_destroy(pe_batch *batch);
+
 /* --- instrumentation (no counterpart in the reference, which only times the
  *     whole loop with cudaEvents, src/main.cu:702-731) --- */
 

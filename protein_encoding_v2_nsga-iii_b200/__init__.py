@@ -116,6 +116,8 @@ def lib() -> C.CDLL:
             "pe_hypervolume": [P, C.c_int32, C.c_int32, P, C.POINTER(C.c_double)],
             "pe_set_profiling": [P, C.c_int32], "pe_stage_times": [P, P],
             "pe_hairpin_noalloc": [P, C.c_int32, C.c_int32, C.c_int32, P, P, P, P],
+            "pe_batch_create": [P, C.c_int32, C.POINTER(P)], "pe_batch_step": [P, C.c_int32],
+            "pe_batch_synchronize": [P], "pe_batch_destroy": [P],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -299,3 +301,38 @@ class Engine:
         info = SelectInfo()
         _ck(lib().pe_select(self._h, generation, _ptr(obj), _ptr(ext), _ptr(surv), _ptr(front), C.byref(info)))
         return surv, front, ext, info
+
+
+class Batch:
+    """Independent design jobs advanced together: one CUDA graph launch per two
+    generations, one concurrent branch per instance (pe_batch_* in the C ABI)."""
+
+    def __init__(self, engines):
+        self.engines = list(engines)
+        arr = (C.c_void_p * len(self.engines))(*[e._h.value for e in self.engines])
+        h = C.c_void_p()
+        _ck(lib().pe_batch_create(arr, len(self.engines), C.byref(h)))
+        self._h = h
+
+    def step(self, generations: int = 1):
+        _ck(lib().pe_batch_step(self._h, generations))
+
+    def synchronize(self):
+        _ck(lib().pe_batch_synchronize(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().pe_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

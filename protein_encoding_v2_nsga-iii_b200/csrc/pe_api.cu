@@ -430,6 +430,138 @@ int pe_create(const pe_config *cfg, const int8_t *aa_idx, int32_t aa_len, const 
     return PE_OK;
 }
 
+// ---------------------------------------------------------------- batches
+
+struct pe_batch {
+    std::vector<pe_instance *> inst;
+    cudaStream_t master = nullptr;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> join;
+    cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};  // [generations] for 1 and 2
+    std::vector<int> parity[3];                                // instance parities the graph was built for
+};
+
+static int batch_capture(pe_batch *b, int gens, cudaGraphExec_t *out)
+{
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(b->master, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = cudaEventRecord(b->fork, b->master);
+    for (size_t i = 0; i < b->inst.size() && e == cudaSuccess; i++) {
+        pe_instance *in = b->inst[i];
+        e = cudaStreamWaitEvent(in->stream, b->fork, 0);
+        int src = in->cur;
+        for (int k = 0; k < gens && e == cudaSuccess; k++) {
+            e = enqueue_generation(in, src);
+            src = 1 - src;
+        }
+        if (e == cudaSuccess) e = cudaEventRecord(b->join[i], in->stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(b->master, b->join[i], 0);
+    }
+    cudaError_t e2 = cudaStreamEndCapture(b->master, &g);
+    if (e != cudaSuccess || e2 != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return fail(PE_ERR_CUDA, "batch capture failed: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
+    }
+    cudaError_t e3 = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    if (e3 != cudaSuccess) return fail(PE_ERR_CUDA, "batch graph instantiate: %s", cudaGetErrorString(e3));
+    return PE_OK;
+}
+
+int pe_batch_create(pe_instance *const *instances, int32_t count, pe_batch **out)
+{
+    if (!instances || count < 1 || !out) return fail(PE_ERR_ARG, "bad batch arguments");
+    *out = nullptr;
+    for (int i = 0; i < count; i++) {
+        pe_instance *in = instances[i];
+        if (!in) return fail(PE_ERR_ARG, "batch member %d is null", i);
+        if (!in->initialized) return fail(PE_ERR_STATE, "batch member %d is not initialised", i);
+        if (!in->own_stream) return fail(PE_ERR_ARG, "batch member %d must own its stream (create with NULL)", i);
+        if (in->profiling) return fail(PE_ERR_STATE, "batch member %d has profiling on", i);
+        for (int j = 0; j < i; j++)
+            if (instances[j] == in) return fail(PE_ERR_ARG, "instance %d appears twice", i);
+        if (in->device != instances[0]->device) return fail(PE_ERR_ARG, "batch members on different devices");
+    }
+    pe_batch *b = new pe_batch();
+    b->inst.assign(instances, instances + count);
+    b->join.resize(count, nullptr);
+    auto bad = [&](cudaError_t e) {
+        pe_batch_destroy(b);
+        return fail(PE_ERR_CUDA, "batch setup: %s", cudaGetErrorString(e));
+    };
+    cudaError_t e = cudaStreamCreateWithFlags(&b->master, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return bad(e);
+    if ((e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming)) != cudaSuccess) return bad(e);
+    for (int i = 0; i < count; i++)
+        if ((e = cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming)) != cudaSuccess) return bad(e);
+    // members' earlier work must be complete before the batch takes over their streams
+    for (pe_instance *in : b->inst)
+        if ((e = cudaStreamSynchronize(in->stream)) != cudaSuccess) return bad(e);
+    *out = b;
+    return PE_OK;
+}
+
+int pe_batch_step(pe_batch *b, int32_t generations)
+{
+    if (!b) return fail(PE_ERR_ARG, "null batch");
+    if (generations < 0) return fail(PE_ERR_ARG, "negative generation count");
+    if (generations == 0) return PE_OK;
+    // order the batch after work already queued on the members' own streams ...
+    for (size_t i = 0; i < b->inst.size(); i++) {
+        CK(cudaEventRecord(b->join[i], b->inst[i]->stream));
+        CK(cudaStreamWaitEvent(b->master, b->join[i], 0));
+    }
+    while (generations > 0) {
+        const int g = generations >= 2 ? 2 : 1;
+        std::vector<int> par(b->inst.size());
+        for (size_t i = 0; i < b->inst.size(); i++) par[i] = b->inst[i]->cur;
+        if (b->graph[g] && b->parity[g] != par) {
+            cudaGraphExecDestroy(b->graph[g]);
+            b->graph[g] = nullptr;
+        }
+        if (!b->graph[g]) {
+            int rc = batch_capture(b, g, &b->graph[g]);
+            if (rc) return rc;
+            b->parity[g] = par;
+        }
+        CK(cudaGraphLaunch(b->graph[g], b->master));
+        for (pe_instance *in : b->inst) {
+            if (g == 1) in->cur = 1 - in->cur;
+            in->generation += g;
+        }
+        generations -= g;
+    }
+    // ... and later calls on a member's stream (reads, pe_step) after the batch
+    CK(cudaEventRecord(b->fork, b->master));
+    for (pe_instance *in : b->inst) CK(cudaStreamWaitEvent(in->stream, b->fork, 0));
+    return PE_OK;
+}
+
+int pe_batch_synchronize(pe_batch *b)
+{
+    if (!b) return fail(PE_ERR_ARG, "null batch");
+    CK(cudaStreamSynchronize(b->master));
+    for (pe_instance *in : b->inst) {
+        int rc = check_status(in);
+        if (rc) return rc;
+    }
+    return PE_OK;
+}
+
+int pe_batch_destroy(pe_batch *b)
+{
+    if (!b) return PE_OK;
+    if (b->master) cudaStreamSynchronize(b->master);
+    for (auto &g : b->graph)
+        if (g) cudaGraphExecDestroy(g);
+    for (cudaEvent_t ev : b->join)
+        if (ev) cudaEventDestroy(ev);
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->master) cudaStreamDestroy(b->master);
+    delete b;
+    return PE_OK;
+}
+
 int pe_set_profiling(pe_instance *in, int32_t enable)
 {
     if (!in) return fail(PE_ERR_ARG, "null instance");
