@@ -374,10 +374,90 @@ def run_batched(args):
     print(json.dumps(line), flush=True)
 
 
+def served_jobs(pe, srv_mod, master_seed: int, count: int, rate: float):
+    """Design requests of the served workload: Poisson arrivals at `rate` jobs/s,
+    L log-uniform in [50, 5000] aa, m uniform in [2, 10], N uniform in
+    {256, 512, 1024, 2048}, generation budget uniform in [200, 1000], stall 50."""
+    rng = np.random.default_rng(master_seed)
+    t, jobs = 0.0, []
+    for j in range(count):
+        t += rng.exponential(1.0 / rate)
+        L = int(round(50 * 100.0 ** rng.random()))
+        m = int(rng.integers(2, 11))
+        N = int(rng.choice([256, 512, 1024, 2048]))
+        G = int(rng.integers(200, 1001))
+        seed = int(rng.integers(1, 1 << 62))
+        jobs.append(srv_mod.Job(pe.synthetic_protein(L, seed), pe.dirichlet_table(seed), m, N, G, seed,
+                                objectives=pe.OBJ_BASE4, mutation_prob=PM, stall=50, arrival=t))
+    return jobs
+
+
+def run_served(args):
+    """Config 5: Poisson arrivals of design jobs, served with continuous batching,
+    against the plain form (one job at a time, in arrival order) on the same jobs."""
+    import copy
+
+    import torch
+    pe = load_pkg()
+    srv_mod = load_pkg_module("server")
+    torch.cuda.set_device(0)
+    count = args.jobs
+    base = served_jobs(pe, srv_mod, SEED, count, 20.0)
+    free, _ = torch.cuda.mem_get_info()
+    budget = int(free * 0.8)
+    lines = {}
+    for mode, max_active in (("served", 64), ("plain", 1)):
+        jobs = [copy.copy(j) for j in base]
+        srv = srv_mod.Server(pe, memory_budget=budget, max_active=max_active, tick=10, hv_every=25)
+        with ClockSampler(0) as clk:
+            done = srv.run(jobs)
+        st = srv_mod.latency_stats(done)
+        st["peak_active"], st["peak_gb"] = srv.peak_active, srv.peak_used / 1e9
+        st["generations"] = sum(j.generations_run for j in done)
+        st["mean_hv"] = float(np.mean([j.hv for j in done if j.hv is not None]))
+        st["clocks"] = clk.summary()
+        st["hv"] = {j.job_id: j.hv for j in done}
+        lines[mode] = st
+        if st["failed"]:
+            raise RuntimeError(f"{st['failed']} jobs failed: " + "; ".join(j.error for j in done if j.error))
+    s, p = lines["served"], lines["plain"]
+    same_hv = all(s["hv"][k] == p["hv"][k] for k in s["hv"])
+    line = {"metric": "designs/s", "value": s["designs_per_s"], "unit": "designs/s", "n_gpus": 1,
+            "steps": count, "warmup": 0, "ms_per_step": 1000.0 * s["span_s"] / count, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": f"served: {count} Poisson arrivals at 20 jobs/s (the first {count} of the "
+                                   "2000-job stream), L log-uniform [50, 5000], m U[2,10], N in "
+                                   "{256,512,1024,2048}, G U[200,1000], stop on hypervolume stall over 50 "
+                                   "generations (checked every 25), 4 objectives, Pm=0.02",
+                       "p50_s": s["p50_s"], "p99_s": s["p99_s"], "mean_s": s["mean_s"],
+                       "plain_p50_s": p["p50_s"], "plain_p99_s": p["p99_s"],
+                       "plain_designs_per_s": p["designs_per_s"],
+                       "served_over_plain": s["designs_per_s"] / p["designs_per_s"],
+                       "stalled_jobs": s["stalled"], "generations": s["generations"],
+                       "mean_final_hv": s["mean_hv"], "same_results_as_plain": same_hv,
+                       "peak_resident_jobs": s["peak_active"], "peak_device_gb": s["peak_gb"],
+                       "memory_budget_gb": budget / 1e9,
+                       "timing": "wall clock from each arrival to its result on the host; "
+                                 "plain = the same server with one resident job"},
+            "clocks": s["clocks"], "plain_clocks": p["clocks"]}
+    print(json.dumps(line), flush=True)
+
+
+def load_pkg_module(stem: str):
+    name = f"pe_b200_{stem}"
+    if name not in sys.modules:
+        spec = importlib.util.spec_from_file_location(name, ROOT / "protein_encoding_v2_nsga-iii_b200" / f"{stem}.py")
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules[name] = mod
+        spec.loader.exec_module(mod)
+    return sys.modules[name]
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--workload", choices=["plain", "batched", "served"], default="plain")
-    ap.add_argument("--generations", type=int, default=0, help="generations per job (batched / served)")
+    ap.add_argument("--generations", type=int, default=0, help="generations per job (batched)")
+    ap.add_argument("--jobs", type=int, default=40, help="design requests in the served workload")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
@@ -388,6 +468,9 @@ def main():
     world, rank, local = dist_setup()
     if args.workload == "batched":
         run_batched(args)
+        return
+    if args.workload == "served":
+        run_served(args)
         return
     if args.profile_case:
         pe = load_pkg()

@@ -80,6 +80,7 @@ typedef struct pe_info {
     int32_t m, N, M, R, p;
     uint32_t generation;    /* generations completed */
     int32_t initialized;
+    uint64_t device_bytes;  /* device memory held by the instance (512 B granules) */
 } pe_info;
 
 typedef struct pe_select_info {
@@ -99,6 +100,9 @@ int pe_create(const pe_config *cfg, const int8_t *aa_idx, int32_t aa_len, const 
               void *cuda_stream, pe_instance **out);
 int pe_destroy(pe_instance *inst);
 int pe_get_info(const pe_instance *inst, pe_info *info);
+/* Device bytes pe_create would allocate for this configuration (for admission
+ * control by memory footprint; no counterpart in the reference). */
+int pe_instance_bytes(const pe_config *cfg, int32_t aa_len, uint64_t *bytes);
 
 /* --- initializationKernel (src/main.cu:26-119): N random solutions (solution 0
  *     = highest-weight codons), evaluated; extreme points seeded. */

@@ -80,7 +80,8 @@ class Config(C.Structure):
 
 class Info(C.Structure):
     _fields_ = [("L", C.c_int32), ("m", C.c_int32), ("N", C.c_int32), ("M", C.c_int32), ("R", C.c_int32),
-                ("p", C.c_int32), ("generation", C.c_uint32), ("initialized", C.c_int32)]
+                ("p", C.c_int32), ("generation", C.c_uint32), ("initialized", C.c_int32),
+                ("device_bytes", C.c_uint64)]
 
 
 class SelectInfo(C.Structure):
@@ -118,6 +119,7 @@ def lib() -> C.CDLL:
             "pe_hairpin_noalloc": [P, C.c_int32, C.c_int32, C.c_int32, P, P, P, P],
             "pe_batch_create": [P, C.c_int32, C.POINTER(P)], "pe_batch_step": [P, C.c_int32],
             "pe_batch_synchronize": [P], "pe_batch_destroy": [P],
+            "pe_instance_bytes": [C.POINTER(Config), C.c_int32, C.POINTER(C.c_uint64)],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -189,6 +191,14 @@ def hairpin_noalloc(d_nt: int, n_solutions: int, m: int, L: int, d_value: int, d
                                  C.c_void_p(d_cds), C.c_void_p(stream) if stream else None))
 
 
+def instance_bytes(aa_len: int, n_cds: int, pop_size: int, objectives: int = OBJ_BASE4, ref_p: int = 0) -> int:
+    """Device bytes an Engine of this shape allocates (admission by memory footprint)."""
+    cfg = Config(n_cds, pop_size, 0.0, objectives, GC3, ref_p, 0)
+    out = C.c_uint64(0)
+    _ck(lib().pe_instance_bytes(C.byref(cfg), aa_len, C.byref(out)))
+    return out.value
+
+
 def hypervolume(points, ref) -> float:
     pts = np.ascontiguousarray(points, np.float64)
     ref = np.ascontiguousarray(ref, np.float64)
@@ -214,6 +224,7 @@ class Engine:
         info = Info()
         _ck(lib().pe_get_info(h, C.byref(info)))
         self.L, self.m, self.N, self.M, self.R, self.p = info.L, info.m, info.N, info.M, info.R, info.p
+        self.device_bytes = int(info.device_bytes)
 
     def close(self):
         if getattr(self, "_h", None):
@@ -270,6 +281,13 @@ class Engine:
         out = np.zeros((2 * self.N, self.M), np.float32) if out is None else out
         _ck(lib().pe_get_objectives(self._h, _ptr(out)))
         return out
+
+    def survivor_objectives(self):
+        """Objectives of the N solutions the last selection kept (the next parents)."""
+        obj = np.zeros((2 * self.N, self.M), np.float32)
+        surv = np.zeros(self.N, np.int32)
+        _ck(lib().pe_get_population(self._h, None, _ptr(obj), None, None, _ptr(surv)))
+        return obj[surv] if self.generation > 0 else obj[: self.N]
 
     def evaluate(self, ids):
         ids = np.ascontiguousarray(ids, np.uint8).reshape(-1, self.m, self.L)

@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -18,6 +19,13 @@ using namespace pe;
 namespace {
 
 thread_local std::string g_err;
+
+// Instances may be driven from different host threads (one thread per instance).
+// cudaMalloc and cudaFree can synchronise implicitly with every stream, which
+// invalidates a stream capture running in another thread; so allocation, free
+// and graph capture never overlap: each holds this lock.
+std::mutex g_cuda_mu;
+using CudaLock = std::lock_guard<std::mutex>;
 
 int fail(int code, const char *fmt, ...)
 {
@@ -127,13 +135,20 @@ struct pe_instance {
     bool profiling = false;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     std::vector<void *> allocs;
+    uint64_t alloc_bytes = 0;  // requested sizes rounded to 512 B (what pe_instance_bytes predicts)
 
     template <class T> int alloc(T **p, size_t count)
     {
         void *v = nullptr;
-        cudaError_t e = cudaMalloc(&v, std::max<size_t>(count, 1) * sizeof(T));
-        if (e != cudaSuccess) return fail(PE_ERR_OOM, "cudaMalloc(%zu bytes): %s", count * sizeof(T), cudaGetErrorString(e));
+        const size_t b = std::max<size_t>(count, 1) * sizeof(T);
+        cudaError_t e;
+        {
+            CudaLock lock(g_cuda_mu);
+            e = cudaMalloc(&v, b);
+        }
+        if (e != cudaSuccess) return fail(PE_ERR_OOM, "cudaMalloc(%zu bytes): %s", b, cudaGetErrorString(e));
         allocs.push_back(v);
+        alloc_bytes += (b + 511) & ~size_t(511);
         *p = (T *)v;
         return PE_OK;
     }
@@ -163,12 +178,17 @@ struct TempBufs {
     std::vector<void *> v;
     ~TempBufs()
     {
+        CudaLock lock(g_cuda_mu);
         for (void *p : v) cudaFree(p);
     }
     template <class T> int get(T **p, size_t count)
     {
         void *q = nullptr;
-        cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
+        cudaError_t e;
+        {
+            CudaLock lock(g_cuda_mu);
+            e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
+        }
         if (e != cudaSuccess) return fail(PE_ERR_OOM, "cudaMalloc: %s", cudaGetErrorString(e));
         v.push_back(q);
         *p = (T *)q;
@@ -221,6 +241,8 @@ cudaError_t enqueue_generation(pe_instance *in, int src)
 
 int build_graphs(pe_instance *in)
 {
+    if (in->graph[0] && in->graph[1]) return PE_OK;
+    CudaLock lock(g_cuda_mu);
     for (int src = 0; src < 2; src++) {
         if (in->graph[src]) continue;
         cudaGraph_t g = nullptr;
@@ -444,6 +466,7 @@ struct pe_batch {
 static int batch_capture(pe_batch *b, int gens, cudaGraphExec_t *out)
 {
     cudaGraph_t g = nullptr;
+    CudaLock lock(g_cuda_mu);
     CK(cudaStreamBeginCapture(b->master, cudaStreamCaptureModeThreadLocal));
     cudaError_t e = cudaEventRecord(b->fork, b->master);
     for (size_t i = 0; i < b->inst.size() && e == cudaSuccess; i++) {
@@ -552,6 +575,7 @@ int pe_batch_destroy(pe_batch *b)
 {
     if (!b) return PE_OK;
     if (b->master) cudaStreamSynchronize(b->master);
+    CudaLock lock(g_cuda_mu);
     for (auto &g : b->graph)
         if (g) cudaGraphExecDestroy(g);
     for (cudaEvent_t ev : b->join)
@@ -587,10 +611,34 @@ int pe_stage_times(pe_instance *in, float *ms3)
     return PE_OK;
 }
 
+int pe_instance_bytes(const pe_config *cfg, int32_t aa_len, uint64_t *bytes)
+{
+    if (!cfg || !bytes || aa_len < 3 || cfg->pop_size < 1 || cfg->n_cds < 2) return fail(PE_ERR_ARG, "bad arguments");
+    const uint64_t L = (uint64_t)aa_len, m = (uint64_t)cfg->n_cds, N = (uint64_t)cfg->pop_size, N2 = 2 * N;
+    const uint64_t M = cfg->objectives == PE_OBJ_BASE4 ? 4 : 6;
+    const uint64_t Lp = (L + 15) & ~uint64_t(15), n = 3 * L, W = (n + 31) / 32, Wp = (W + 2) & ~uint64_t(1);
+    int p = cfg->ref_p;
+    if (p <= 0) {
+        p = 1;
+        while ((int64_t)bincoef((int)M + p - 1, p) <= (int64_t)N) p++;
+        p -= 1;
+        if (p < 1) return fail(PE_ERR_ARG, "pop_size too small for the reference-point rule");
+    }
+    const uint64_t R = bincoef((int)M + p - 1, p), words = (N2 + 31) / 32;
+    auto r = [](uint64_t b) { return (b + 511) & ~uint64_t(511); };  // allocation granularity
+    uint64_t t = r(sizeof(DevTables)) + r(L) + r(R * M * 4);
+    t += 2 * (r(N2 * m * Lp) + r(N2 * m * Wp * 8) + r(N2 * M * 4) + r(N2 * 2 * M) + r(N2 * 12));
+    t += r(N * 4) + r(N2 * words * 4) + 6 * r(N2 * 4) + 3 * r(R * 4) + r((R + 1) * 4) + r(32) + r(72);
+    t += r(N2 * m * 8) + r(N2 * 4) + r(4) + r(M * M * 4) + r(4);
+    *bytes = t;
+    return PE_OK;
+}
+
 int pe_destroy(pe_instance *in)
 {
     if (!in) return PE_OK;
     if (in->stream) cudaStreamSynchronize(in->stream);
+    CudaLock lock(g_cuda_mu);
     for (int i = 0; i < 2; i++)
         if (in->graph[i]) cudaGraphExecDestroy(in->graph[i]);
     for (int k = 0; k < 4; k++)
@@ -612,6 +660,7 @@ int pe_get_info(const pe_instance *in, pe_info *info)
     info->p = in->p;
     info->generation = in->generation;
     info->initialized = in->initialized;
+    info->device_bytes = in->alloc_bytes;
     return PE_OK;
 }
 

@@ -9,6 +9,10 @@
 //                     (calMaximumSL, include/utils.cuh:712-888) on bit planes;
 //                     the last CTA of a solution combines its CDSs.
 #include <cstdint>
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include <cuda_runtime.h>
 
 #include "pe_device.cuh"
@@ -642,9 +646,24 @@ size_t var_smem_bytes(const Shape &s)
            (size_t)((s.L + 15) & ~15);
 }
 
+cudaError_t raise_smem_limit(const void *func, size_t bytes)
+{
+    static std::mutex mu;
+    static std::map<std::pair<int, const void *>, size_t> limit;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(mu);
+    size_t &cur = limit[{dev, func}];
+    if (bytes <= cur) return cudaSuccess;
+    e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) cur = bytes;
+    return e;
+}
+
 template <int MODE> static cudaError_t set_var_attr(size_t smem)
 {
-    return cudaFuncSetAttribute(k_variation<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    return raise_smem_limit((const void *)k_variation<MODE>, smem);
 }
 
 cudaError_t launch_init(const Shape &s, const DevTables *tab, const int8_t *aa, PopBuf dst, int32_t *surv,
@@ -1067,7 +1086,7 @@ cudaError_t launch_sl(const Shape &s, PopBuf buf, int base, int count, int2 *par
 {
     if (count <= 0) return cudaSuccess;
     size_t smem = sl_smem_bytes(s);
-    cudaError_t e = cudaFuncSetAttribute(k_sl, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = raise_smem_limit((const void *)k_sl, smem);
     if (e != cudaSuccess) return e;
     k_sl<<<count * s.m, kSlThreads, smem, st>>>(s, buf, base, part, counter, status);
     return cudaGetLastError();

@@ -91,6 +91,10 @@ cudaError_t launch_mutate(const Shape &s, const DevTables *tab, const int8_t *aa
 cudaError_t launch_sl(const Shape &s, PopBuf buf, int base, int count, int2 *part, int32_t *counter,
                       int32_t *status, cudaStream_t st);
 size_t sl_smem_bytes(const Shape &s);
+// Raise a kernel's dynamic shared-memory limit to at least `bytes` on the current
+// device.  The limit only grows, so launches from different host threads never
+// see it lowered between their own setting and their launch.
+cudaError_t raise_smem_limit(const void *func, size_t bytes);
 size_t var_smem_bytes(const Shape &s);
 
 // records a message for pe_last_error() (pe_api.cu)

@@ -541,7 +541,7 @@ cudaError_t launch_select(const Shape &s, const float *obj, float *ext, const fl
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     size_t smem = select_smem_bytes(s);
-    e = cudaFuncSetAttribute(k_select, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = raise_smem_limit((const void *)k_select, smem);
     if (e != cudaSuccess) return e;
     k_select<<<1, kSelThreads, smem, st>>>(s, obj, ext, refpts, sc, surv, d_gen, bump_gen);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;

@@ -1,0 +1,223 @@
+"""Served design jobs on one GPU: continuous batching.
+
+The reference runs one protein per process (src/main.cu:467-901).  Here design
+requests arrive over time and share the device:
+
+* admission in arrival order, by device footprint (pe_instance_bytes) against a
+  memory budget and by a cap on resident jobs; the head of the queue waits
+  until enough memory is released;
+* every resident job keeps its population on the device, owns a stream and is
+  driven by its own host thread, which replays the job's generation graphs
+  `tick` generations at a time; the blocking calls release the interpreter
+  lock, so the kernels of all resident jobs overlap on the GPU and a long job
+  never holds back a short one;
+* a job retires when it reaches its generation budget, or when the hypervolume
+  of its survivors' normalised objectives (the measure of src/main.cu:789-858)
+  has not improved for `stall` generations, checked every `hv_every`
+  generations; the job waits for each check, so where it stops does not depend
+  on timing;
+* latency = time the result is on the host - arrival time; p50/p99 and designs/s.
+
+A job's result does not depend on what else is resident: every draw is keyed by
+(job seed, generation, individual, position) and each generation runs the same
+kernels as a job alone.
+"""
+from __future__ import annotations
+
+import threading
+import time
+from collections import deque
+from dataclasses import dataclass
+
+import numpy as np
+
+# normalisation constants: six objectives src/main.cu:23-24; four objectives
+# src/auto_execution_experiments.py:47-48 (mCAI, mHD, MGC, MSL)
+IDEAL = {0: np.array([1.0, 0.2, 0.4, 0.5, 0.0, 0.0], np.float32), 1: np.array([1.0, 0.4, 0.0, 0.0], np.float32)}
+NADIR = {0: np.array([0.0, -0.15, 0.0, 0.0, 0.6, 1.0], np.float32), 1: np.array([0.0, 0.0, 0.6, 1.0], np.float32)}
+N_MAXIMISED = {0: 4, 1: 2}
+
+
+def normalised(obj: np.ndarray, objectives: int) -> np.ndarray:
+    """Stored objectives -> the reference's normalised, clamped form."""
+    v = np.array(obj, np.float32, copy=True)
+    v[:, :N_MAXIMISED[objectives]] *= -1.0
+    v = (v - IDEAL[objectives]) / (NADIR[objectives] - IDEAL[objectives])
+    v = np.where(v >= 1.0, np.float32(0.999999), v)
+    return np.where(v < 0.0, np.float32(0.0), v).astype(np.float32)
+
+
+def nondominated(pts: np.ndarray) -> np.ndarray:
+    """Rows of pts (minimisation) that no other row dominates; duplicates kept once."""
+    pts = np.unique(pts, axis=0)
+    keep = np.ones(len(pts), bool)
+    for s in range(0, len(pts), 512):
+        blk = pts[s:s + 512]
+        le = (pts[None, :, :] <= blk[:, None, :]).all(-1)
+        lt = (pts[None, :, :] < blk[:, None, :]).any(-1)
+        keep[s:s + 512] = ~(le & lt).any(1)
+    return pts[keep]
+
+
+def front_hypervolume(pe, obj: np.ndarray, objectives: int) -> float:
+    """Hypervolume of the normalised non-dominated points w.r.t. (1, ..., 1)."""
+    pts = nondominated(normalised(obj, objectives).astype(np.float64))
+    return pe.hypervolume(pts, np.ones(pts.shape[1]))
+
+
+@dataclass(eq=False)
+class Job:
+    aa: np.ndarray
+    table: object
+    n_cds: int
+    pop_size: int
+    generations: int
+    seed: int
+    objectives: int = 1
+    mutation_prob: float = 0.02
+    stall: int = 50                 # 0 disables the stall rule
+    arrival: float = 0.0            # seconds from the start of the run
+    job_id: int = -1
+    # filled by the server
+    start: float | None = None
+    end: float | None = None
+    generations_run: int = 0
+    hv: float | None = None
+    reason: str | None = None       # "budget", "stall" or "error"
+    error: str | None = None
+    survivors: np.ndarray | None = None    # survivors' objectives
+    population: tuple | None = None
+    _best_hv: float = -1.0
+    _best_gen: int = 0
+
+
+class Server:
+    def __init__(self, pe, memory_budget: int, max_active: int = 64, tick: int = 10, hv_every: int = 25,
+                 keep_population: bool = False):
+        self.pe = pe
+        self.memory_budget = int(memory_budget)
+        self.max_active = max_active
+        self.tick = tick
+        self.hv_every = hv_every
+        self.keep_population = keep_population
+        self.queue: deque[Job] = deque()
+        self.active: list[Job] = []
+        self.done: list[Job] = []
+        self.used = 0
+        self.peak_used = 0
+        self.peak_active = 0
+        self._next_id = 0
+        self._cv = threading.Condition()
+        self._threads: list[threading.Thread] = []
+        self.t0 = None
+
+    # ------------------------------------------------------------ bookkeeping
+    def now(self) -> float:
+        return time.perf_counter() - self.t0
+
+    def footprint(self, job: Job) -> int:
+        return self.pe.instance_bytes(len(job.aa), job.n_cds, job.pop_size, job.objectives)
+
+    def submit(self, job: Job) -> int:
+        if self.t0 is None:
+            self.t0 = time.perf_counter()
+        if self.footprint(job) > self.memory_budget:
+            raise ValueError("job needs more device memory than the whole budget")
+        with self._cv:
+            if job.job_id < 0:
+                job.job_id = self._next_id
+                self._next_id += 1
+            self.queue.append(job)
+            self._admit_locked()
+        return job.job_id
+
+    def _admit_locked(self):
+        while self.queue and len(self.active) < self.max_active:
+            job = self.queue[0]
+            need = self.footprint(job)
+            if self.used + need > self.memory_budget:
+                break  # arrival order: the head waits for memory
+            self.queue.popleft()
+            self.used += need
+            self.peak_used = max(self.peak_used, self.used)
+            self.active.append(job)
+            self.peak_active = max(self.peak_active, len(self.active))
+            job.start = self.now()
+            t = threading.Thread(target=self._serve, args=(job,), daemon=True)
+            self._threads.append(t)
+            t.start()
+
+    # ------------------------------------------------------------ one job
+    def _serve(self, job: Job):
+        eng = None
+        try:
+            eng = self.pe.Engine(job.aa, job.table, job.n_cds, job.pop_size, job.mutation_prob,
+                                 objectives=job.objectives, seed=job.seed)
+            eng.init()
+            job.reason = "budget"
+            while job.generations_run < job.generations:
+                g = min(self.tick, job.generations - job.generations_run)
+                if job.stall:
+                    g = min(g, self.hv_every - job.generations_run % self.hv_every)
+                eng.step(g)
+                eng.synchronize()
+                job.generations_run += g
+                if job.stall and job.generations_run % self.hv_every == 0 and job.generations_run < job.generations:
+                    hv = front_hypervolume(self.pe, eng.survivor_objectives(), job.objectives)
+                    if hv > job._best_hv + 1e-12:
+                        job._best_hv, job._best_gen = hv, job.generations_run
+                    elif job.generations_run - job._best_gen >= job.stall:
+                        job.reason = "stall"
+                        break
+            job.survivors = eng.survivor_objectives()
+            if self.keep_population:
+                job.population = eng.population()
+            job.end = self.now()
+        except Exception as exc:  # the job fails alone; the server keeps serving
+            job.reason, job.error, job.end = "error", repr(exc), self.now()
+        finally:
+            if eng is not None:
+                eng.close()
+            with self._cv:
+                self.used -= self.footprint(job)
+                self.active.remove(job)
+                self.done.append(job)
+                self._admit_locked()
+                self._cv.notify_all()
+
+    # ------------------------------------------------------------ driving
+    def run(self, jobs: list[Job]) -> list[Job]:
+        """Serve `jobs` with real-time arrivals (job.arrival seconds after the
+        start); returns the finished jobs in completion order, each with the
+        hypervolume of its final survivors."""
+        pending = deque(sorted(jobs, key=lambda j: j.arrival))
+        self.t0 = time.perf_counter()
+        while pending:
+            wait = pending[0].arrival - self.now()
+            if wait > 0:
+                time.sleep(wait)
+            while pending and pending[0].arrival <= self.now():
+                self.submit(pending.popleft())
+        self.drain()
+        for job in self.done:
+            if job.survivors is not None and job.hv is None:
+                job.hv = front_hypervolume(self.pe, job.survivors, job.objectives)
+        return self.done
+
+    def drain(self):
+        """Block until every submitted job has finished."""
+        with self._cv:
+            while self.queue or self.active:
+                self._cv.wait(timeout=1.0)
+        for t in self._threads:
+            t.join()
+        self._threads.clear()
+
+
+def latency_stats(done: list[Job]) -> dict:
+    lat = np.array([j.end - j.arrival for j in done])
+    span = max(j.end for j in done) - min(j.arrival for j in done)
+    return {"jobs": len(done), "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "mean_s": float(lat.mean()), "designs_per_s": len(done) / span, "span_s": span,
+            "stalled": sum(j.reason == "stall" for j in done), "failed": sum(j.reason == "error" for j in done)}
+

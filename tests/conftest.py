@@ -25,6 +25,18 @@ def _load_pkg():
     return mod
 
 
+def load_pkg_module(stem):
+    """A pure-Python module of the package (server, replicas) under the name pe_b200_<stem>."""
+    name = f"pe_b200_{stem}"
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(name, ROOT / "protein_encoding_v2_nsga-iii_b200" / f"{stem}.py")
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
 @pytest.fixture(scope="session")
 def pe():
     return _load_pkg()

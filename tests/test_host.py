@@ -12,7 +12,7 @@ B7KHU9 = "MIEPLVLGLVMGLVPITLAGLFVAAYLQYKRGNQLNLD"
 
 def test_library_exports_every_declared_symbol(pe):
     names = pe.declared_symbols()
-    assert len(names) == 26 and "pe_step" in names and "pe_batch_step" in names and "pe_hypervolume" in names
+    assert len(names) == 27 and "pe_step" in names and "pe_batch_step" in names and "pe_hypervolume" in names and "pe_instance_bytes" in names
     lib = pe.lib()
     for n in names:
         assert hasattr(lib, n), n
@@ -109,5 +109,29 @@ def test_hypervolume_vs_oracle(pe, orc, d):
         pts[:5] = pts[5:10]  # duplicates
         a, b = pe.hypervolume(pts, np.ones(d)), orc.hypervolume(pts, np.ones(d))
         assert abs(a - b) < 1e-12 * max(1.0, abs(b))
+    # coordinates on a coarse grid: equal x / y / z values, points on the boundary of others' boxes
+    for trial in range(5):
+        pts = rng.integers(0, 6, (60, d)) / 6.0
+        a, b = pe.hypervolume(pts, np.ones(d)), orc.hypervolume(pts, np.ones(d))
+        assert abs(a - b) < 1e-12 * max(1.0, abs(b))
     # single point and box volume
     assert abs(pe.hypervolume(np.full((1, d), 0.5), np.ones(d)) - 0.5 ** d) < 1e-15
+
+
+def test_hypervolume_front_sized(pe, orc):
+    # a 4-objective front of 300 mutually non-dominated points (the served stall check's shape)
+    rng = np.random.default_rng(11)
+    x = rng.random((300, 4))
+    x /= np.linalg.norm(x, axis=1, keepdims=True) * 1.2
+    a, b = pe.hypervolume(x, np.ones(4)), orc.hypervolume(x, np.ones(4))
+    assert abs(a - b) < 1e-12 * b
+
+
+def test_instance_bytes_host(pe):
+    base = pe.instance_bytes(1001, 8, 1024, pe.OBJ_BASE4, ref_p=8)
+    assert base % 512 == 0 and 30 << 20 < base < 200 << 20
+    assert pe.instance_bytes(2001, 8, 1024, pe.OBJ_BASE4, ref_p=8) > base
+    assert pe.instance_bytes(1001, 8, 2048, pe.OBJ_BASE4, ref_p=8) > base
+    assert pe.instance_bytes(1001, 8, 1024, pe.OBJ_REF6) > base          # R = 792 reference points
+    with pytest.raises(pe.PeError):
+        pe.instance_bytes(2, 8, 1024)
