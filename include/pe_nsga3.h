@@ -73,6 +73,9 @@ typedef struct pe_config {
     int32_t gc_mode;        /* pe_gc_mode */
     int32_t ref_p;          /* Das-Dennis partitions; 0 = reference rule (src/main.cu:564-576) */
     uint64_t seed;          /* replaces rand() seeding (src/main.cu:469,525) */
+    int32_t stream_priority;/* priority of the stream pe_create makes when given none:
+                               0 = default, lower = more urgent (clamped to the
+                               device's range); no counterpart in the reference */
 } pe_config;
 
 typedef struct pe_info {

@@ -75,7 +75,8 @@ class CodonTable(C.Structure):
 
 class Config(C.Structure):
     _fields_ = [("n_cds", C.c_int32), ("pop_size", C.c_int32), ("mutation_prob", C.c_float),
-                ("objectives", C.c_int32), ("gc_mode", C.c_int32), ("ref_p", C.c_int32), ("seed", C.c_uint64)]
+                ("objectives", C.c_int32), ("gc_mode", C.c_int32), ("ref_p", C.c_int32), ("seed", C.c_uint64),
+                ("stream_priority", C.c_int32)]
 
 
 class Info(C.Structure):
@@ -213,10 +214,11 @@ class Engine:
     """One protein-design instance resident on the current CUDA device."""
 
     def __init__(self, aa, table: CodonTable, n_cds: int, pop_size: int, mutation_prob: float,
-                 objectives: int = OBJ_BASE4, gc_mode: int = GC3, ref_p: int = 0, seed: int = 0, stream=None):
+                 objectives: int = OBJ_BASE4, gc_mode: int = GC3, ref_p: int = 0, seed: int = 0, stream=None,
+                 stream_priority: int = 0):
         self.aa = np.ascontiguousarray(aa, np.int8)
         self.table = table
-        cfg = Config(n_cds, pop_size, mutation_prob, objectives, gc_mode, ref_p, seed)
+        cfg = Config(n_cds, pop_size, mutation_prob, objectives, gc_mode, ref_p, seed, stream_priority)
         h = C.c_void_p()
         _ck(lib().pe_create(C.byref(cfg), _ptr(self.aa), len(self.aa), C.byref(table),
                             None if stream is None else C.c_void_p(stream), C.byref(h)))

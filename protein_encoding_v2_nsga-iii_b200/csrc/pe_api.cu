@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -21,11 +22,44 @@ namespace {
 thread_local std::string g_err;
 
 // Instances may be driven from different host threads (one thread per instance).
-// cudaMalloc and cudaFree can synchronise implicitly with every stream, which
-// invalidates a stream capture running in another thread; so allocation, free
-// and graph capture never overlap: each holds this lock.
+// Nothing here calls cudaMalloc or cudaFree, which synchronise with the whole
+// device: device memory comes from a stream-ordered pool per device
+// (cudaMallocFromPoolAsync / cudaFreeAsync on the instance's stream), so one
+// instance's create or destroy neither waits for nor disturbs the work and the
+// stream captures of the others.  Captures still take this lock, one at a time.
 std::mutex g_cuda_mu;
 using CudaLock = std::lock_guard<std::mutex>;
+
+// The pool keeps freed memory for the next instance (release threshold
+// unlimited) and lives until the process exits.
+cudaError_t device_pool(int dev, cudaMemPool_t *out)
+{
+    static std::mutex mu;
+    static std::map<int, cudaMemPool_t> pools;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = pools.find(dev);
+    if (it != pools.end()) {
+        *out = it->second;
+        return cudaSuccess;
+    }
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    cudaError_t e = cudaMemPoolCreate(&pool, &props);
+    if (e != cudaSuccess) return e;
+    uint64_t keep = UINT64_MAX;
+    e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    if (e != cudaSuccess) {
+        cudaMemPoolDestroy(pool);
+        return e;
+    }
+    pools[dev] = pool;
+    *out = pool;
+    return cudaSuccess;
+}
 
 int fail(int code, const char *fmt, ...)
 {
@@ -117,6 +151,7 @@ struct pe_instance {
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    cudaMemPool_t pool = nullptr;
     DevTables *d_tab = nullptr;
     int8_t *d_aa = nullptr;
     float *d_ref = nullptr;
@@ -141,12 +176,8 @@ struct pe_instance {
     {
         void *v = nullptr;
         const size_t b = std::max<size_t>(count, 1) * sizeof(T);
-        cudaError_t e;
-        {
-            CudaLock lock(g_cuda_mu);
-            e = cudaMalloc(&v, b);
-        }
-        if (e != cudaSuccess) return fail(PE_ERR_OOM, "cudaMalloc(%zu bytes): %s", b, cudaGetErrorString(e));
+        cudaError_t e = cudaMallocFromPoolAsync(&v, b, pool, stream);
+        if (e != cudaSuccess) return fail(PE_ERR_OOM, "device allocation (%zu bytes): %s", b, cudaGetErrorString(e));
         allocs.push_back(v);
         alloc_bytes += (b + 511) & ~size_t(511);
         *p = (T *)v;
@@ -173,23 +204,21 @@ int alloc_pop(pe_instance *in, PopBuf &b, int nsol)
     return PE_OK;
 }
 
-// temporary device buffers for the operator-level entry points
+// temporary device buffers for the operator-level entry points, stream-ordered
+// on the instance's stream
 struct TempBufs {
+    const pe_instance *in;
     std::vector<void *> v;
+    explicit TempBufs(const pe_instance *in_) : in(in_) {}
     ~TempBufs()
     {
-        CudaLock lock(g_cuda_mu);
-        for (void *p : v) cudaFree(p);
+        for (void *p : v) cudaFreeAsync(p, in->stream);
     }
     template <class T> int get(T **p, size_t count)
     {
         void *q = nullptr;
-        cudaError_t e;
-        {
-            CudaLock lock(g_cuda_mu);
-            e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
-        }
-        if (e != cudaSuccess) return fail(PE_ERR_OOM, "cudaMalloc: %s", cudaGetErrorString(e));
+        cudaError_t e = cudaMallocFromPoolAsync(&q, std::max<size_t>(count, 1) * sizeof(T), in->pool, in->stream);
+        if (e != cudaSuccess) return fail(PE_ERR_OOM, "device allocation: %s", cudaGetErrorString(e));
         v.push_back(q);
         *p = (T *)q;
         return PE_OK;
@@ -362,11 +391,22 @@ int pe_create(const pe_config *cfg, const int8_t *aa_idx, int32_t aa_len, const 
     if (cuda_stream) {
         in->stream = (cudaStream_t)cuda_stream;
     } else {
-        if (cudaStreamCreateWithFlags(&in->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        int least = 0, greatest = 0;
+        if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess) least = greatest = 0;
+        const int prio = std::min(least, std::max(greatest, (int)cfg->stream_priority));
+        if (cudaStreamCreateWithPriority(&in->stream, cudaStreamNonBlocking, prio) != cudaSuccess) {
             delete in;
             return fail(PE_ERR_CUDA, "stream creation failed");
         }
         in->own_stream = true;
+    }
+    {
+        cudaError_t e = device_pool(dev, &in->pool);
+        if (e != cudaSuccess) {
+            if (in->own_stream) cudaStreamDestroy(in->stream);
+            delete in;
+            return fail(PE_ERR_CUDA, "device memory pool: %s", cudaGetErrorString(e));
+        }
     }
     int rc = PE_OK;
     auto cleanup = [&](int code) {
@@ -575,7 +615,6 @@ int pe_batch_destroy(pe_batch *b)
 {
     if (!b) return PE_OK;
     if (b->master) cudaStreamSynchronize(b->master);
-    CudaLock lock(g_cuda_mu);
     for (auto &g : b->graph)
         if (g) cudaGraphExecDestroy(g);
     for (cudaEvent_t ev : b->join)
@@ -638,12 +677,12 @@ int pe_destroy(pe_instance *in)
 {
     if (!in) return PE_OK;
     if (in->stream) cudaStreamSynchronize(in->stream);
-    CudaLock lock(g_cuda_mu);
     for (int i = 0; i < 2; i++)
         if (in->graph[i]) cudaGraphExecDestroy(in->graph[i]);
     for (int k = 0; k < 4; k++)
         if (in->ev[k]) cudaEventDestroy(in->ev[k]);
-    for (void *p : in->allocs) cudaFree(p);
+    for (void *p : in->allocs) cudaFreeAsync(p, in->stream);
+    if (in->stream) cudaStreamSynchronize(in->stream);
     if (in->own_stream && in->stream) cudaStreamDestroy(in->stream);
     delete in;
     return PE_OK;
@@ -740,7 +779,7 @@ int pe_eval_objectives(pe_instance *in, const uint8_t *codon_idx, int32_t n, flo
     const Shape &s = in->s;
     for (size_t i = 0; i < (size_t)n * s.m * s.L; i++)
         if (codon_idx[i] >= PE_NUM_CODON) return fail(PE_ERR_ARG, "codon id out of range at %zu", i);
-    TempBufs t;
+    TempBufs t(in);
     PopBuf b{};
     int2 *part;
     int32_t *counter;
@@ -771,7 +810,7 @@ int pe_mutate(pe_instance *in, uint32_t generation, const int32_t *idx, int32_t 
     const Shape &s = in->s;
     for (size_t i = 0; i < (size_t)n * s.m * s.L; i++)
         if (parents[i] >= PE_NUM_CODON) return fail(PE_ERR_ARG, "codon id out of range at %zu", i);
-    TempBufs t;
+    TempBufs t(in);
     PopBuf src{}, dst{};
     int32_t *d_par, *d_idx, *d_ops;
     uint32_t *d_g;
@@ -808,7 +847,7 @@ int pe_select(pe_instance *in, uint32_t generation, const float *obj, float *ext
     if (!in || !obj || !extremes) return fail(PE_ERR_ARG, "bad arguments");
     const Shape &s = in->s;
     const int N2 = 2 * s.N;
-    TempBufs t;
+    TempBufs t(in);
     float *d_obj, *d_ext;
     int32_t *d_sv;
     uint32_t *d_g;

@@ -3,9 +3,10 @@
 The reference runs one protein per process (src/main.cu:467-901).  Here design
 requests arrive over time and share the device:
 
-* admission in arrival order, by device footprint (pe_instance_bytes) against a
-  memory budget and by a cap on resident jobs; the head of the queue waits
-  until enough memory is released;
+* admission by device footprint (pe_instance_bytes) against a memory budget and
+  by a cap on resident jobs, in arrival order or shortest estimated work first
+  (a job that has waited longer than `max_wait` seconds goes ahead of both); the
+  chosen job waits until enough memory is released;
 * every resident job keeps its population on the device, owns a stream and is
   driven by its own host thread, which replays the job's generation graphs
   `tick` generations at a time; the blocking calls release the interpreter
@@ -16,6 +17,11 @@ requests arrive over time and share the device:
   has not improved for `stall` generations, checked every `hv_every`
   generations; the job waits for each check, so where it stops does not depend
   on timing;
+* each job's stream gets a priority from its estimated work (counted cells of
+  the stem scan over its generation budget): the block scheduler then serves
+  the kernels of short jobs first and fills the rest of the GPU with long ones
+  (shortest-job-first at CTA granularity), instead of slowing every job down
+  equally;
 * latency = time the result is on the host - arrival time; p50/p99 and designs/s.
 
 A job's result does not depend on what else is resident: every draw is keyed by
@@ -47,21 +53,24 @@ def normalised(obj: np.ndarray, objectives: int) -> np.ndarray:
     return np.where(v < 0.0, np.float32(0.0), v).astype(np.float32)
 
 
-def nondominated(pts: np.ndarray) -> np.ndarray:
-    """Rows of pts (minimisation) that no other row dominates; duplicates kept once."""
-    pts = np.unique(pts, axis=0)
-    keep = np.ones(len(pts), bool)
-    for s in range(0, len(pts), 512):
-        blk = pts[s:s + 512]
-        le = (pts[None, :, :] <= blk[:, None, :]).all(-1)
-        lt = (pts[None, :, :] < blk[:, None, :]).any(-1)
-        keep[s:s + 512] = ~(le & lt).any(1)
-    return pts[keep]
+def estimated_cells(job) -> float:
+    """Counted cells of the stem scan over the job's whole generation budget (the
+    scan dominates a generation's device time)."""
+    k = 3 * len(job.aa) - 5
+    return float(job.pop_size) * job.n_cds * k * (k + 1) / 2 * job.generations
+
+
+def work_priority(job, levels: int = 6) -> int:
+    """Stream priority by estimated work: one level per decade of counted cells
+    from 1e10 up; -(levels-1) (most urgent) for the smallest jobs, 0 for the largest."""
+    decade = int(np.floor(np.log10(max(estimated_cells(job), 1.0)))) - 10
+    return -(levels - 1) + min(max(decade, 0), levels - 1)
 
 
 def front_hypervolume(pe, obj: np.ndarray, objectives: int) -> float:
-    """Hypervolume of the normalised non-dominated points w.r.t. (1, ..., 1)."""
-    pts = nondominated(normalised(obj, objectives).astype(np.float64))
+    """Hypervolume of the normalised points w.r.t. (1, ..., 1) (pe_hypervolume drops
+    the dominated ones itself)."""
+    pts = normalised(obj, objectives).astype(np.float64)
     return pe.hypervolume(pts, np.ones(pts.shape[1]))
 
 
@@ -79,6 +88,7 @@ class Job:
     arrival: float = 0.0            # seconds from the start of the run
     job_id: int = -1
     # filled by the server
+    submitted: float | None = None
     start: float | None = None
     end: float | None = None
     generations_run: int = 0
@@ -87,14 +97,24 @@ class Job:
     error: str | None = None
     survivors: np.ndarray | None = None    # survivors' objectives
     population: tuple | None = None
+    priority: int = 0
+    gpu_s: float = 0.0              # host time in generation launches + waits
+    read_s: float = 0.0             # host time reading survivors for stall checks
+    hv_s: float = 0.0               # host time computing their hypervolume
     _best_hv: float = -1.0
     _best_gen: int = 0
 
 
 class Server:
     def __init__(self, pe, memory_budget: int, max_active: int = 64, tick: int = 10, hv_every: int = 25,
-                 keep_population: bool = False):
+                 keep_population: bool = False, priority=work_priority, order: str = "arrival",
+                 max_wait: float | None = None):
+        if order not in ("arrival", "shortest"):
+            raise ValueError("order must be 'arrival' or 'shortest'")
         self.pe = pe
+        self.priority = priority      # job -> stream priority, or None for equal priorities
+        self.order = order
+        self.max_wait = max_wait
         self.memory_budget = int(memory_budget)
         self.max_active = max_active
         self.tick = tick
@@ -127,17 +147,28 @@ class Server:
             if job.job_id < 0:
                 job.job_id = self._next_id
                 self._next_id += 1
+            job.submitted = self.now()
             self.queue.append(job)
             self._admit_locked()
         return job.job_id
 
+    def _next_locked(self) -> Job:
+        if self.max_wait is not None:
+            now = self.now()
+            for job in self.queue:  # arrival order
+                if now - job.submitted > self.max_wait:
+                    return job
+        if self.order == "shortest":
+            return min(self.queue, key=estimated_cells)
+        return self.queue[0]
+
     def _admit_locked(self):
         while self.queue and len(self.active) < self.max_active:
-            job = self.queue[0]
+            job = self._next_locked()
             need = self.footprint(job)
             if self.used + need > self.memory_budget:
-                break  # arrival order: the head waits for memory
-            self.queue.popleft()
+                break  # the chosen job waits for memory
+            self.queue.remove(job)
             self.used += need
             self.peak_used = max(self.peak_used, self.used)
             self.active.append(job)
@@ -151,19 +182,27 @@ class Server:
     def _serve(self, job: Job):
         eng = None
         try:
+            job.priority = self.priority(job) if self.priority else 0
             eng = self.pe.Engine(job.aa, job.table, job.n_cds, job.pop_size, job.mutation_prob,
-                                 objectives=job.objectives, seed=job.seed)
+                                 objectives=job.objectives, seed=job.seed, stream_priority=job.priority)
             eng.init()
             job.reason = "budget"
             while job.generations_run < job.generations:
                 g = min(self.tick, job.generations - job.generations_run)
                 if job.stall:
                     g = min(g, self.hv_every - job.generations_run % self.hv_every)
+                t0 = time.perf_counter()
                 eng.step(g)
                 eng.synchronize()
+                t1 = time.perf_counter()
+                job.gpu_s += t1 - t0
                 job.generations_run += g
                 if job.stall and job.generations_run % self.hv_every == 0 and job.generations_run < job.generations:
-                    hv = front_hypervolume(self.pe, eng.survivor_objectives(), job.objectives)
+                    surv = eng.survivor_objectives()
+                    t2 = time.perf_counter()
+                    hv = front_hypervolume(self.pe, surv, job.objectives)
+                    job.read_s += t2 - t1
+                    job.hv_s += time.perf_counter() - t2
                     if hv > job._best_hv + 1e-12:
                         job._best_hv, job._best_gen = hv, job.generations_run
                     elif job.generations_run - job._best_gen >= job.stall:
@@ -219,5 +258,7 @@ def latency_stats(done: list[Job]) -> dict:
     span = max(j.end for j in done) - min(j.arrival for j in done)
     return {"jobs": len(done), "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
             "mean_s": float(lat.mean()), "designs_per_s": len(done) / span, "span_s": span,
-            "stalled": sum(j.reason == "stall" for j in done), "failed": sum(j.reason == "error" for j in done)}
+            "stalled": sum(j.reason == "stall" for j in done), "failed": sum(j.reason == "error" for j in done),
+"host_hv_s": float(sum(j.hv_s for j in done)), "host_read_s": float(sum(j.read_s for j in done)),
+            "gpu_wait_s": float(sum(j.gpu_s for j in done))}
 

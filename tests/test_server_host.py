@@ -15,7 +15,7 @@ class FakeEngine:
     live = 0
     peak = 0
 
-    def __init__(self, aa, table, m, N, pm, objectives=1, seed=0):
+    def __init__(self, aa, table, m, N, pm, objectives=1, seed=0, stream_priority=0):
         self.gen, self.N, self.seed = 0, N, seed
         with FakeEngine.lock:
             FakeEngine.live += 1
@@ -105,13 +105,45 @@ def test_failed_job_does_not_stop_server():
     assert done[0].reason == "error" and "device error" in done[0].error and srv.used == 0 and FakeEngine.live == 0
 
 
-def test_nondominated_and_normalisation():
+def test_normalisation():
     srv_mod = _server_mod()
-    pts = np.array([[0.1, 0.5], [0.2, 0.2], [0.3, 0.3], [0.1, 0.5], [0.6, 0.1]])
-    nd = srv_mod.nondominated(pts)
-    assert sorted(map(tuple, nd)) == [(0.1, 0.5), (0.2, 0.2), (0.6, 0.1)]
     obj = np.array([[-0.8, -0.3, 0.1, 0.2], [-1.2, 0.1, 0.9, -0.1]], np.float32)
     v = srv_mod.normalised(obj, 1)
     # mCAI 0.8 -> (0.8-1)/(0-1) = 0.2; mHD 0.3 -> (0.3-0.4)/(0-0.4) = 0.25; MGC 0.1/0.6; MSL 0.2
     assert np.allclose(v[0], [0.2, 0.25, 0.1 / 0.6, 0.2], atol=1e-6)
     assert v[1, 0] == 0.0 and v[1, 1] == np.float32(0.999999) and v[1, 2] == np.float32(0.999999) and v[1, 3] == 0.0
+
+
+def test_work_priority_orders_by_size():
+    srv_mod = _server_mod()
+    small = srv_mod.Job(np.zeros(51, np.int8), None, 2, 256, 200, 1)
+    mid = srv_mod.Job(np.zeros(1001, np.int8), None, 8, 1024, 500, 1)
+    big = srv_mod.Job(np.zeros(5001, np.int8), None, 10, 2048, 1000, 1)
+    pr = [srv_mod.work_priority(j) for j in (small, mid, big)]
+    assert pr[0] == -5 and pr[0] < pr[1] < pr[2] and pr[2] == 0
+    assert srv_mod.estimated_cells(mid) == 1024 * 8 * 2998 * 2999 / 2 * 500
+
+
+def test_shortest_first_admission_and_max_wait():
+    srv_mod = _server_mod()
+    srv = srv_mod.Server(FakePe, memory_budget=1 << 20, max_active=1, order="shortest")
+    sizes = [400, 60, 200, 60]
+    jobs = [srv_mod.Job(np.zeros(L, np.int8), None, 2, 8, 10, 1, stall=0) for L in sizes]
+    import time
+    srv.t0 = time.perf_counter()
+    with srv._cv:   # queue all four before any is admitted
+        for j in jobs:
+            j.job_id = srv._next_id
+            srv._next_id += 1
+            j.submitted = srv.now()
+            srv.queue.append(j)
+        first = srv._next_locked()
+    assert first is jobs[1]                      # smallest, earliest of the two smallest
+    srv.max_wait = 0.0                           # everything has waited: arrival order wins
+    with srv._cv:
+        assert srv._next_locked() is jobs[0]
+        srv.max_wait = None
+        srv._admit_locked()
+    srv.drain()
+    order = [j.job_id for j in sorted(srv.done, key=lambda j: j.start)]
+    assert order == [1, 3, 2, 0]
