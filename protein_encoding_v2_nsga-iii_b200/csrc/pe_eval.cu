@@ -8,6 +8,7 @@
 //  k_sl               one CTA per (solution, CDS): the hairpin-stem scan
 //                     (calMaximumSL, include/utils.cuh:712-888) on bit planes;
 //                     the last CTA of a solution combines its CDSs.
+#include <algorithm>
 #include <cstdint>
 #include <map>
 #include <mutex>
@@ -719,16 +720,21 @@ cudaError_t launch_mutate(const Shape &s, const DevTables *tab, const int8_t *aa
 // anti-diagonal d = r+c are r in [max(0, d-n+1), floor((d-5)/2)] (upper
 // triangle, loop of >= 4 nucleotides); their longest run of pairing cells is
 // that anti-diagonal's stem length, and the lower triangle never exceeds it
-// (include/utils.cuh:743-774).  Each lane owns one shift delta and walks its
-// cells 32 at a time:
-//     match word = ~((S.lo ^ T.lo) | (S.hi ^ T.hi))
-// with runs carried across words by ffs/clz and long interior runs caught by
-// an AND-shift tower.  T is kept as 32 pre-shifted copies, transposed so that
-// the 32 lanes of a warp read 32 consecutive 8-byte words.
+// (include/utils.cuh:743-774).
+//
+// Two passes.  The band scan (below) finds every run of >= 8 pairing cells and
+// measures those exactly; for random-like sequences of a few hundred
+// nucleotides or more the longest stem is >= 8 and that pass is the whole scan.
+// Otherwise the exact word scan runs: each lane owns one shift delta and walks
+// its cells 32 at a time,
+//     match word = ~((S.lo ^ T.lo) | (S.hi ^ T.hi)),
+// with runs carried across words by ffs/clz and the longest run inside each
+// word counted; T is then kept as 32 pre-shifted copies, transposed so that the
+// 32 lanes of a warp read 32 consecutive 8-byte words.
 
 __device__ __forceinline__ uint32_t fshr(uint32_t lo, uint32_t hi, int sh) { return __funnelshift_r(lo, hi, sh); }
 
-template <bool MASKED, bool EXACT>
+template <bool MASKED>
 __device__ __forceinline__ void sl_word(uint2 sv, uint2 tv, int k, int r_lo, int r_hi, int &cur, int &dbest)
 {
     uint32_t m = ~((sv.x ^ tv.x) | (sv.y ^ tv.y));
@@ -745,23 +751,16 @@ __device__ __forceinline__ void sl_word(uint2 sv, uint2 tv, int k, int r_lo, int
         const uint32_t z = ~m;
         dbest = max(dbest, cur + __ffs(z) - 1);  // run carried in + ones at the low end
         cur = __clz(z);                          // ones at the high end carry out
-        // starts of 8 consecutive ones inside the word (rare: exact length below)
-        uint32_t x = m & (m >> 1);
-        x &= x >> 2;
-        x &= x >> 4;
-        if (EXACT || x) {
-            uint32_t y = m;
-            int len = 0;
-            while (y) {
-                y &= y >> 1;
-                len++;
-            }
-            dbest = max(dbest, len);
+        uint32_t y = m;                          // longest run inside the word
+        int len = 0;
+        while (y) {
+            y &= y >> 1;
+            len++;
         }
+        dbest = max(dbest, len);
     }
 }
 
-template <bool EXACT>
 __device__ void sl_scan(const uint2 *__restrict__ S, const uint2 *__restrict__ Tc, int n, int *next_chunk, int lane,
                         int &best, int &bestd)
 {
@@ -798,10 +797,10 @@ __device__ void sl_scan(const uint2 *__restrict__ S, const uint2 *__restrict__ T
         const uint2 *trow = Tc + (ptrdiff_t)((delta >> 5) + kSlGuardRows) * 32 + (delta & 31);
         int cur = 0, dbest = 0;
         int k = kmin;
-        for (; k < kf_lo; k++) sl_word<true, EXACT>(S[k], trow[k * 32], k, r_lo, r_hi, cur, dbest);
+        for (; k < kf_lo; k++) sl_word<true>(S[k], trow[k * 32], k, r_lo, r_hi, cur, dbest);
 #pragma unroll 4
-        for (; k <= kf_hi; k++) sl_word<false, EXACT>(S[k], trow[k * 32], k, r_lo, r_hi, cur, dbest);
-        for (; k <= kmax; k++) sl_word<true, EXACT>(S[k], trow[k * 32], k, r_lo, r_hi, cur, dbest);
+        for (; k <= kf_hi; k++) sl_word<false>(S[k], trow[k * 32], k, r_lo, r_hi, cur, dbest);
+        for (; k <= kmax; k++) sl_word<true>(S[k], trow[k * 32], k, r_lo, r_hi, cur, dbest);
         dbest = max(dbest, cur);
         if (valid) {
             int d = n - 1 - delta;
@@ -815,6 +814,207 @@ __device__ void sl_scan(const uint2 *__restrict__ S, const uint2 *__restrict__ T
     }
 }
 
+// ---------------------------------------------------------------------------
+// Band scan: the first pass, which finds every run of >= 8 pairing cells.
+//
+// A lane takes one item = (band of 32 consecutive shifts delta0..delta0+31,
+// delta0 a multiple of 32; segment of 32 consecutive rows r = 32s..32s+31).
+// Row r's match word over the band (bit j: s[r] pairs with t[r + delta0 + j])
+// is a window of T's equality plane for the nucleotide s[r]:
+//     m_r = E_{s[r]} bits [r + delta0, r + delta0 + 32),
+// at bit offset r mod 32, a constant of the unrolled step.  Going down the
+// rows, A2 = m_r & m_{r-1}, A4 = A2_r & A2_{r-2} and A8 = A4_r & A4_{r-4} mark
+// the diagonals whose run reaches 8 at row r, and A8 & ~A8_{r-1} the runs that
+// have just reached 8; eight rows of the previous segment rebuild the history
+// first.  Those rising edges are rare: the lane ORs them into one mask per item
+// and queues (mask, band, segment); each warp measures its queued runs exactly,
+// 32 at a time, one per lane (sl_band_entry).
+//
+// Cells outside a diagonal's counted range: rows below it read T outside
+// [0, n) (zero planes) or a row outside [0, n) (the zero plane 4), so they
+// never match; rows past its top end may match, which only extends a run
+// beyond the range, and sl_band_entry clips every run to the range.  So every
+// counted run of length >= 8 is measured exactly once, and runs that are
+// shorter inside the range never win against it.
+constexpr int kEqGuard = 4;   // guard words on each side of the equality planes
+constexpr int kSegPitch = 33; // row-offset table: 32 rows per segment + 1 (bank spread)
+constexpr int kBandQueue = 64;
+
+__host__ __device__ __forceinline__ int sl_plane_stride(int W) { return (W + 2 * kEqGuard + 2 + 31) & ~31; }
+__host__ __device__ __forceinline__ int sl_band_base(int n) { return -(((n - 6) + 31) & ~31); }
+__host__ __device__ __forceinline__ int sl_num_bands(int n) { return n - 6 >= 0 ? ((n - 6) - sl_band_base(n)) / 32 + 1 : 0; }
+
+// First row of band b's items and its last segment (rows of the counted
+// triangle: r >= -delta, 2r + delta <= n - 6).
+__device__ __forceinline__ void sl_band_segments(int n, int d0, int &s_lo, int &s_hi)
+{
+    s_lo = max(0, -d0 - 31) >> 5;
+    s_hi = ((n - 6 - d0) >> 1) >> 5;
+}
+
+// Exact measurement of the runs queued for one item: for each diagonal j of
+// the mask, the rows where its run reached 8 inside segment s are found again
+// from 64 rows of match bits (same cells as the band scan), and each run is
+// followed to its end and clipped to the diagonal's counted range.
+__device__ void sl_band_entry(uint32_t mask, int d0, int s, int n, const uint2 *__restrict__ S,
+                              const uint32_t *__restrict__ Tlo, const uint32_t *__restrict__ Thi, int &best, int &bestd)
+{
+    const int dmax = n - 6;
+    const int R0 = 32 * (s - 1);
+    const uint2 SA = s >= 1 ? S[s - 1] : make_uint2(0u, 0u), SB = S[s];
+    while (mask) {
+        const int j = __ffs(mask) - 1;
+        mask &= mask - 1;
+        const int delta = d0 + j;
+        if (delta < -dmax || delta > dmax) continue;
+        const int r_hi = (n - 6 - delta) >> 1;
+        // match bits of rows R0 .. R0+63 on this diagonal, zero where the row or
+        // its T index falls outside [0, n)
+        const int i0 = R0 + delta, w0 = (i0 >> 5) + kSlGuardRows, sh = i0 & 31;
+        const uint32_t tlA = fshr(Tlo[w0], Tlo[w0 + 1], sh), thA = fshr(Thi[w0], Thi[w0 + 1], sh);
+        const uint32_t tlB = fshr(Tlo[w0 + 1], Tlo[w0 + 2], sh), thB = fshr(Thi[w0 + 1], Thi[w0 + 2], sh);
+        const uint32_t eA = ~((SA.x ^ tlA) | (SA.y ^ thA)), eB = ~((SB.x ^ tlB) | (SB.y ^ thB));
+        const int lo = max(max(0, -delta), R0) - R0, hi = min(min(n, n - delta) - 1, R0 + 63) - R0;
+        if (lo > hi) continue;
+        const uint64_t valid = (~0ull >> (63 - hi)) & (~0ull << lo);
+        const uint64_t X = (((uint64_t)eB << 32) | eA) & valid;
+        uint64_t R8 = X & (X >> 1);
+        R8 &= R8 >> 2;
+        R8 &= R8 >> 4;
+        // runs starting at bit b reach 8 at row R0 + b + 7, inside segment s for b in [25, 56]
+        uint64_t edges = R8 & ~(R8 << 1) & (((1ull << 32) - 1) << 25);
+        while (edges) {
+            const int b = __ffsll((long long)edges) - 1;
+            edges &= edges - 1;
+            const int a = R0 + b;  // first row of the run
+            if (a > r_hi) continue;
+            int e = a + 7;         // last row known to pair
+            while (e < r_hi) {
+                const int p = e + 1, i = p + delta;
+                const int ws = p >> 5, wt = (i >> 5) + kSlGuardRows;
+                const uint32_t sl = fshr(S[ws].x, S[ws + 1].x, p & 31), sh2 = fshr(S[ws].y, S[ws + 1].y, p & 31);
+                const uint32_t tl = fshr(Tlo[wt], Tlo[wt + 1], i & 31), th = fshr(Thi[wt], Thi[wt + 1], i & 31);
+                const uint32_t mm = ~((sl ^ tl) | (sh2 ^ th));
+                if (mm == 0xffffffffu) {
+                    e += 32;
+                    continue;
+                }
+                e += __ffs(~mm) - 1;
+                break;
+            }
+            const int L = min(e, r_hi) - a + 1;
+            const int d = n - 1 - delta;
+            if (L > best || (L == best && d < bestd)) {
+                best = L;
+                bestd = d;
+            }
+        }
+    }
+}
+
+// read-only table loads from the shared window (free to reorder: nothing
+// writes the tables during the scan)
+__device__ __forceinline__ uint32_t lds_u32(uint32_t a)
+{
+    uint32_t v;
+    asm("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(a));
+    return v;
+}
+__device__ __forceinline__ uint2 lds_v2(uint32_t a)
+{
+    uint2 v;
+    asm("ld.shared.v2.u32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "r"(a));
+    return v;
+}
+
+__device__ void sl_band_scan(const uint2 *__restrict__ E2, const int *__restrict__ poffT,
+                             const int *__restrict__ bstart, int nb, const uint2 *__restrict__ S,
+                             const uint32_t *__restrict__ Tlo, const uint32_t *__restrict__ Thi, int n,
+                             int2 *__restrict__ queue, int *next_chunk, int lane, int &best, int &bestd)
+{
+    if (nb <= 0) return;
+    const int D0 = sl_band_base(n);
+    const int nitems = bstart[nb];
+    const int nchunks = (nitems + 31) >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    int qn = 0;  // entries in this warp's queue (warp-uniform)
+    for (;;) {
+        int ch = 0;
+        if (lane == 0) ch = atomicAdd(next_chunk, 1);
+        ch = __shfl_sync(0xffffffffu, ch, 0);
+        if (ch >= nchunks) break;
+        const int item = ch * 32 + lane;
+        uint32_t pend = 0;
+        int b = 0, s = 0;
+        if (item < nitems) {
+            int lo = 0, hi = nb - 1;  // band: bstart[b] <= item < bstart[b + 1]
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (bstart[mid] <= item) lo = mid;
+                else hi = mid - 1;
+            }
+            b = lo;
+            const int d0 = D0 + 32 * b;
+            int s_lo, s_hi;
+            sl_band_segments(n, d0, s_lo, s_hi);
+            s = s_lo + (item - bstart[b]);
+            // E2 entry x holds T words x - kEqGuard, x + 1 - kEqGuard; row 32u + t of band
+            // d0 reads entry u + d0/32 + kEqGuard of the row's plane, at bit offset t
+            // 32-bit shared-window addresses; poffT holds byte offsets into E2
+            const uint32_t qa = (uint32_t)__cvta_generic_to_shared(E2 + (d0 / 32 + kEqGuard));
+            const uint32_t pa = (uint32_t)__cvta_generic_to_shared(poffT + s * kSegPitch);
+            uint32_t m1 = 0, a8p = 0, a2h[2] = {0, 0}, a4h[4] = {0, 0, 0, 0};
+#pragma unroll
+            for (int k = 0; k < 40; k++) {
+                // steps 0..7: rows 24..31 of segment s-1; steps 8..39: rows 0..31 of segment s
+                const int t = k < 8 ? k + 24 : k - 8;
+                const uint32_t pv = lds_u32(pa + 4 * (k < 8 ? t : kSegPitch + t));
+                const uint2 w = lds_v2(qa + pv);
+                const uint32_t m = fshr(w.x, w.y, t);
+                const uint32_t A2 = m & m1;
+                const uint32_t A4 = A2 & a2h[k & 1];
+                const uint32_t A8 = A4 & a4h[k & 3];
+                if (k >= 8) pend |= A8 & ~a8p;
+                a2h[k & 1] = A2;
+                a4h[k & 3] = A4;
+                m1 = m;
+                a8p = A8;
+            }
+        }
+        // queue the items with rising edges; measure 32 of them at a time
+        const unsigned has = __ballot_sync(0xffffffffu, pend != 0);
+        if (has) {
+            if (pend) queue[qn + __popc(has & lt)] = make_int2((int)pend, (b << 16) | s);
+            qn += __popc(has);
+            __syncwarp();
+            if (qn >= 32) {
+                const int2 q = queue[lane];
+                sl_band_entry((uint32_t)q.x, D0 + 32 * (q.y >> 16), q.y & 0xffff, n, S, Tlo, Thi, best, bestd);
+                __syncwarp();
+                if (lane < qn - 32) queue[lane] = queue[32 + lane];
+                qn -= 32;
+                __syncwarp();
+            }
+        }
+    }
+    if (lane < qn) {
+        const int2 q = queue[lane];
+        sl_band_entry((uint32_t)q.x, D0 + 32 * (q.y >> 16), q.y & 0xffff, n, S, Tlo, Thi, best, bestd);
+    }
+    __syncwarp();
+}
+
+// T's equality plane for nucleotide v (4 = the zero plane) at T word w, zero
+// outside [0, n)
+__device__ __forceinline__ uint32_t eq_word(const uint32_t *Tlo, const uint32_t *Thi, int W, int n, int v, int w)
+{
+    if (v > 3 || w < 0 || w >= W) return 0u;
+    const uint32_t lo = Tlo[w + kSlGuardRows], hi = Thi[w + kSlGuardRows];
+    const uint32_t valid = n - 32 * w >= 32 ? 0xffffffffu : ((1u << (n - 32 * w)) - 1u);
+    const uint32_t x = (v & 1) ? lo : ~lo, y = (v & 2) ? hi : ~hi;
+    return x & y & valid;
+}
+
 __device__ __forceinline__ void pair_reduce(int &best, int &bestd, int ob, int od)
 {
     if (ob > best || (ob == best && od < bestd)) {
@@ -824,6 +1024,7 @@ __device__ __forceinline__ void pair_reduce(int &best, int &bestd, int ob, int o
 }
 
 struct SlSmem {
+    int2 queue[kSlThreads / 32][kBandQueue];  // band-scan items waiting for exact measurement
     int wbest[kSlThreads / 32];
     int wbestd[kSlThreads / 32];
     int last;
@@ -920,17 +1121,48 @@ __global__ void __launch_bounds__(kSlThreads) k_sl(Shape s, PopBuf buf, int base
         Thi[e] = hi;
     }
     __syncthreads();
-    // 32 shifted copies, transposed: Tc[row][sh] = T bits [32(row-G)+sh, +31]
-    const int rows = W + 2 * G;
-    for (int e = tid; e < rows * 32; e += nth) {
-        int row = e >> 5, sh = e & 31;
-        Tc[e] = make_uint2(fshr(Tlo[row], Tlo[row + 1], sh), fshr(Thi[row], Thi[row + 1], sh));
+    // band-scan tables, in the space the shifted copies of T take later:
+    //   E2[v][x]      (E_v word x-kEqGuard, E_v word x+1-kEqGuard), v = 0..3 nucleotides, 4 zero
+    //   poffT[sp][t]  row r = 32(sp-1)+t: 8 (v(r)*PS + sp-1) bytes, v(r) = 4 outside [0, n); pitch 33
+    //   bstart[b]     first item of band b (items of band b: its 32-row segments)
+    const int PS = sl_plane_stride(W), NSP = W + 2;
+    const int nb = sl_num_bands(n), D0 = sl_band_base(n);
+    uint2 *E2 = Tc;
+    int *poffT = reinterpret_cast<int *>(E2 + 5 * PS);
+    int *bstart = poffT + kSegPitch * NSP;
+    for (int e = tid; e < 5 * PS; e += nth) {
+        const int v = e / PS, x = e - v * PS - kEqGuard;
+        E2[e] = make_uint2(eq_word(Tlo, Thi, W, n, v, x), eq_word(Tlo, Thi, W, n, v, x + 1));
+    }
+    for (int e = tid; e < kSegPitch * NSP; e += nth) {
+        const int sp = e / kSegPitch, t = e - sp * kSegPitch, r = 32 * (sp - 1) + t;
+        const int v = (t < 32 && r >= 0 && r < n) ? plane_nt(S, r) : 4;
+        poffT[e] = (v * PS + (sp - 1)) * (int)sizeof(uint2);  // byte offset into E2
+    }
+    if (warp == 0) {
+        int carry = 0;
+        for (int b0 = 0; b0 < nb; b0 += 32) {
+            const int b = b0 + lane;
+            int x = 0;
+            if (b < nb) {
+                int s_lo, s_hi;
+                sl_band_segments(n, D0 + 32 * b, s_lo, s_hi);
+                x = s_hi - s_lo + 1;
+            }
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
+            }
+            if (b < nb) bstart[b + 1] = carry + x;
+            carry += __shfl_sync(0xffffffffu, x, 31);
+        }
+        if (lane == 0) bstart[0] = 0;
     }
     if (tid == 0) sm.next_chunk = 0;
     __syncthreads();
 
     int best = 0, bestd = 0x7fffffff;
-    sl_scan<false>(S, Tc, n, &sm.next_chunk, lane, best, bestd);
+    sl_band_scan(E2, poffT, bstart, nb, S, Tlo, Thi, n, sm.queue[warp], &sm.next_chunk, lane, best, bestd);
     // CTA reduction of (best, smallest anti-diagonal)
     for (int o = 16; o > 0; o >>= 1) {
         int ob = __shfl_xor_sync(0xffffffffu, best, o), od = __shfl_xor_sync(0xffffffffu, bestd, o);
@@ -950,10 +1182,18 @@ __global__ void __launch_bounds__(kSlThreads) k_sl(Shape s, PopBuf buf, int base
     }
     __syncthreads();
     if (sm.res[0] < 8) {
-        // short maxima may hide inside a word: rescan with exact per-word runs
+        // no run reaches 8: exact per-word runs over 32 shifted copies of T,
+        // transposed (Tc[row][sh] = T bits [32(row-G)+sh, +31]), which replace
+        // the band-scan tables
+        const int rows = W + 2 * G;
+        for (int e = tid; e < rows * 32; e += nth) {
+            int row = e >> 5, sh = e & 31;
+            Tc[e] = make_uint2(fshr(Tlo[row], Tlo[row + 1], sh), fshr(Thi[row], Thi[row + 1], sh));
+        }
+        __syncthreads();
         best = 0;
         bestd = 0x7fffffff;
-        sl_scan<true>(S, Tc, n, &sm.next_chunk, lane, best, bestd);
+        sl_scan(S, Tc, n, &sm.next_chunk, lane, best, bestd);
         for (int o = 16; o > 0; o >>= 1) {
             int ob = __shfl_xor_sync(0xffffffffu, best, o), od = __shfl_xor_sync(0xffffffffu, bestd, o);
             pair_reduce(best, bestd, ob, od);
@@ -1077,7 +1317,11 @@ size_t sl_smem_bytes(const Shape &s)
     b += (size_t)(W + 2) * sizeof(uint2);
     b += 2 * (size_t)(W + 2 * G + 1) * sizeof(uint32_t);
     b += 16;  // alignment of Tc
-    b += (size_t)(W + 2 * G) * 32 * sizeof(uint2);
+    // Tc (32 shifted copies of T) or, before it, the band-scan tables
+    const size_t tc = (size_t)(W + 2 * G) * 32 * sizeof(uint2);
+    const size_t band = (size_t)5 * sl_plane_stride(W) * sizeof(uint2) + (size_t)kSegPitch * (W + 2) * sizeof(int) +
+                        (size_t)(sl_num_bands(s.n) + 1) * sizeof(int);
+    b += std::max(tc, band);
     return b;
 }
 
