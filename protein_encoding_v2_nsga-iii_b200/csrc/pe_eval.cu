@@ -817,18 +817,20 @@ __device__ void sl_scan(const uint2 *__restrict__ S, const uint2 *__restrict__ T
 // ---------------------------------------------------------------------------
 // Band scan: the first pass, which finds every run of >= 8 pairing cells.
 //
-// A lane takes one item = (band of 32 consecutive shifts delta0..delta0+31,
-// delta0 a multiple of 32; segment of 32 consecutive rows r = 32s..32s+31).
-// Row r's match word over the band (bit j: s[r] pairs with t[r + delta0 + j])
-// is a window of T's equality plane for the nucleotide s[r]:
+// Shifts are grouped in bands of 32 (delta0 .. delta0+31, delta0 a multiple of
+// 32).  A lane takes one item = (group of kBandGroup adjacent bands, segment of
+// 32 consecutive rows r = 32s..32s+31).  Row r's match word over a band (bit j:
+// s[r] pairs with t[r + delta0 + j]) is a window of T's equality plane for the
+// nucleotide s[r]:
 //     m_r = E_{s[r]} bits [r + delta0, r + delta0 + 32),
-// at bit offset r mod 32, a constant of the unrolled step.  Going down the
-// rows, A2 = m_r & m_{r-1}, A4 = A2_r & A2_{r-2} and A8 = A4_r & A4_{r-4} mark
-// the diagonals whose run reaches 8 at row r, and A8 & ~A8_{r-1} the runs that
-// have just reached 8; eight rows of the previous segment rebuild the history
-// first.  Those rising edges are rare: the lane ORs them into one mask per item
-// and queues (mask, band, segment); each warp measures its queued runs exactly,
-// 32 at a time, one per lane (sl_band_entry).
+// at bit offset r mod 32, a constant of the unrolled step; one 16-byte load of
+// four consecutive plane words gives the windows of all bands of the group.
+// Going down the rows, A2 = m_r & m_{r-1}, A4 = A2_r & A2_{r-2} and
+// A8 = A4_r & A4_{r-4} mark the diagonals whose run reaches 8 at row r, and
+// A8 & ~A8_{r-1} the runs that have just reached 8; eight rows of the previous
+// segment rebuild the history first.  Those rising edges are rare: the lane ORs
+// them into one mask per band and queues (mask, band, segment); each warp
+// measures its queued runs exactly, 32 at a time, one per lane (sl_band_entry).
 //
 // Cells outside a diagonal's counted range: rows below it read T outside
 // [0, n) (zero planes) or a row outside [0, n) (the zero plane 4), so they
@@ -836,26 +838,29 @@ __device__ void sl_scan(const uint2 *__restrict__ S, const uint2 *__restrict__ T
 // beyond the range, and sl_band_entry clips every run to the range.  So every
 // counted run of length >= 8 is measured exactly once, and runs that are
 // shorter inside the range never win against it.
-constexpr int kEqGuard = 4;   // guard words on each side of the equality planes
-constexpr int kSegPitch = 33; // row-offset table: 32 rows per segment + 1 (bank spread)
+constexpr int kBandGroup = 3;            // bands per item (one 4-word load)
+constexpr int kEqGuard = kBandGroup + 3; // guard words on each side of the equality planes
+constexpr int kSegPitch = 33;            // row-offset table: 32 rows per segment + 1 (bank spread)
 constexpr int kBandQueue = 64;
 
-__host__ __device__ __forceinline__ int sl_plane_stride(int W) { return (W + 2 * kEqGuard + 2 + 31) & ~31; }
+__host__ __device__ __forceinline__ int sl_plane_stride(int W) { return (W + 2 * kEqGuard + 4 + 31) & ~31; }
 __host__ __device__ __forceinline__ int sl_band_base(int n) { return -(((n - 6) + 31) & ~31); }
 __host__ __device__ __forceinline__ int sl_num_bands(int n) { return n - 6 >= 0 ? ((n - 6) - sl_band_base(n)) / 32 + 1 : 0; }
+__host__ __device__ __forceinline__ int sl_num_groups(int n) { return (sl_num_bands(n) + kBandGroup - 1) / kBandGroup; }
 
-// First row of band b's items and its last segment (rows of the counted
-// triangle: r >= -delta, 2r + delta <= n - 6).
-__device__ __forceinline__ void sl_band_segments(int n, int d0, int &s_lo, int &s_hi)
+// Segments of the rows a group of bands starting at shift d0 covers (rows of
+// the counted triangle: r >= -delta, 2r + delta <= n - 6): from the lowest
+// first row of its bands (the last band) to the highest last row (the first).
+__device__ __forceinline__ void sl_group_segments(int n, int d0, int &s_lo, int &s_hi)
 {
-    s_lo = max(0, -d0 - 31) >> 5;
+    s_lo = max(0, -(d0 + 32 * (kBandGroup - 1)) - 31) >> 5;
     s_hi = ((n - 6 - d0) >> 1) >> 5;
 }
 
-// Exact measurement of the runs queued for one item: for each diagonal j of
-// the mask, the rows where its run reached 8 inside segment s are found again
-// from 64 rows of match bits (same cells as the band scan), and each run is
-// followed to its end and clipped to the diagonal's counted range.
+// Exact measurement of the runs queued for one (band, segment): for each
+// diagonal j of the mask, the rows where its run reached 8 inside segment s are
+// found again from 64 rows of match bits (same cells as the band scan), and
+// each run is followed to its end and clipped to the diagonal's counted range.
 __device__ void sl_band_entry(uint32_t mask, int d0, int s, int n, const uint2 *__restrict__ S,
                               const uint32_t *__restrict__ Tlo, const uint32_t *__restrict__ Thi, int &best, int &bestd)
 {
@@ -920,21 +925,25 @@ __device__ __forceinline__ uint32_t lds_u32(uint32_t a)
     asm("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(a));
     return v;
 }
-__device__ __forceinline__ uint2 lds_v2(uint32_t a)
+__device__ __forceinline__ uint4 lds_v4(uint32_t a)
 {
-    uint2 v;
-    asm("ld.shared.v2.u32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "r"(a));
+    uint4 v;
+    asm("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "r"(a));
     return v;
 }
+__device__ __forceinline__ uint32_t word_of(const uint4 &w, int i)
+{
+    return i == 0 ? w.x : i == 1 ? w.y : i == 2 ? w.z : w.w;
+}
 
-__device__ void sl_band_scan(const uint2 *__restrict__ E2, const int *__restrict__ poffT,
-                             const int *__restrict__ bstart, int nb, const uint2 *__restrict__ S,
+__device__ void sl_band_scan(const uint4 *__restrict__ E4, const int *__restrict__ poffT,
+                             const int *__restrict__ gstart, int ng, const uint2 *__restrict__ S,
                              const uint32_t *__restrict__ Tlo, const uint32_t *__restrict__ Thi, int n,
                              int2 *__restrict__ queue, int *next_chunk, int lane, int &best, int &bestd)
 {
-    if (nb <= 0) return;
+    if (ng <= 0) return;
     const int D0 = sl_band_base(n);
-    const int nitems = bstart[nb];
+    const int nitems = gstart[ng];
     const int nchunks = (nitems + 31) >> 5;
     const unsigned lt = (1u << lane) - 1u;
     int qn = 0;  // entries in this warp's queue (warp-uniform)
@@ -944,56 +953,69 @@ __device__ void sl_band_scan(const uint2 *__restrict__ E2, const int *__restrict
         ch = __shfl_sync(0xffffffffu, ch, 0);
         if (ch >= nchunks) break;
         const int item = ch * 32 + lane;
-        uint32_t pend = 0;
-        int b = 0, s = 0;
+        uint32_t pend[kBandGroup];
+#pragma unroll
+        for (int g = 0; g < kBandGroup; g++) pend[g] = 0;
+        int grp = 0, s = 0;
         if (item < nitems) {
-            int lo = 0, hi = nb - 1;  // band: bstart[b] <= item < bstart[b + 1]
+            int lo = 0, hi = ng - 1;  // group: gstart[grp] <= item < gstart[grp + 1]
             while (lo < hi) {
                 const int mid = (lo + hi + 1) >> 1;
-                if (bstart[mid] <= item) lo = mid;
+                if (gstart[mid] <= item) lo = mid;
                 else hi = mid - 1;
             }
-            b = lo;
-            const int d0 = D0 + 32 * b;
+            grp = lo;
+            const int d0 = D0 + 32 * kBandGroup * grp;
             int s_lo, s_hi;
-            sl_band_segments(n, d0, s_lo, s_hi);
-            s = s_lo + (item - bstart[b]);
-            // E2 entry x holds T words x - kEqGuard, x + 1 - kEqGuard; row 32u + t of band
-            // d0 reads entry u + d0/32 + kEqGuard of the row's plane, at bit offset t
-            // 32-bit shared-window addresses; poffT holds byte offsets into E2
-            const uint32_t qa = (uint32_t)__cvta_generic_to_shared(E2 + (d0 / 32 + kEqGuard));
+            sl_group_segments(n, d0, s_lo, s_hi);
+            s = s_lo + (item - gstart[grp]);
+            // E4 entry x holds T words x-kEqGuard .. x+3-kEqGuard; row 32u + t reads entry
+            // u + d0/32 + kEqGuard of the row's plane, words g, g+1 for band g, at bit offset t
+            const uint32_t qa = (uint32_t)__cvta_generic_to_shared(E4 + (d0 / 32 + kEqGuard));
             const uint32_t pa = (uint32_t)__cvta_generic_to_shared(poffT + s * kSegPitch);
-            uint32_t m1 = 0, a8p = 0, a2h[2] = {0, 0}, a4h[4] = {0, 0, 0, 0};
+            uint32_t m1[kBandGroup], a8p[kBandGroup], a2h[kBandGroup][2], a4h[kBandGroup][4];
+#pragma unroll
+            for (int g = 0; g < kBandGroup; g++) {
+                m1[g] = a8p[g] = 0;
+                a2h[g][0] = a2h[g][1] = 0;
+                a4h[g][0] = a4h[g][1] = a4h[g][2] = a4h[g][3] = 0;
+            }
 #pragma unroll
             for (int k = 0; k < 40; k++) {
                 // steps 0..7: rows 24..31 of segment s-1; steps 8..39: rows 0..31 of segment s
                 const int t = k < 8 ? k + 24 : k - 8;
                 const uint32_t pv = lds_u32(pa + 4 * (k < 8 ? t : kSegPitch + t));
-                const uint2 w = lds_v2(qa + pv);
-                const uint32_t m = fshr(w.x, w.y, t);
-                const uint32_t A2 = m & m1;
-                const uint32_t A4 = A2 & a2h[k & 1];
-                const uint32_t A8 = A4 & a4h[k & 3];
-                if (k >= 8) pend |= A8 & ~a8p;
-                a2h[k & 1] = A2;
-                a4h[k & 3] = A4;
-                m1 = m;
-                a8p = A8;
+                const uint4 w = lds_v4(qa + pv);
+#pragma unroll
+                for (int g = 0; g < kBandGroup; g++) {
+                    const uint32_t m = fshr(word_of(w, g), word_of(w, g + 1), t);
+                    const uint32_t A2 = m & m1[g];
+                    const uint32_t A4 = A2 & a2h[g][k & 1];
+                    const uint32_t A8 = A4 & a4h[g][k & 3];
+                    if (k >= 8) pend[g] |= A8 & ~a8p[g];
+                    a2h[g][k & 1] = A2;
+                    a4h[g][k & 3] = A4;
+                    m1[g] = m;
+                    a8p[g] = A8;
+                }
             }
         }
-        // queue the items with rising edges; measure 32 of them at a time
-        const unsigned has = __ballot_sync(0xffffffffu, pend != 0);
-        if (has) {
-            if (pend) queue[qn + __popc(has & lt)] = make_int2((int)pend, (b << 16) | s);
-            qn += __popc(has);
-            __syncwarp();
-            if (qn >= 32) {
-                const int2 q = queue[lane];
-                sl_band_entry((uint32_t)q.x, D0 + 32 * (q.y >> 16), q.y & 0xffff, n, S, Tlo, Thi, best, bestd);
+        // queue the (band, segment) pairs with rising edges; measure 32 at a time
+#pragma unroll
+        for (int g = 0; g < kBandGroup; g++) {
+            const unsigned has = __ballot_sync(0xffffffffu, pend[g] != 0);
+            if (has) {
+                if (pend[g]) queue[qn + __popc(has & lt)] = make_int2((int)pend[g], ((kBandGroup * grp + g) << 16) | s);
+                qn += __popc(has);
                 __syncwarp();
-                if (lane < qn - 32) queue[lane] = queue[32 + lane];
-                qn -= 32;
-                __syncwarp();
+                if (qn >= 32) {
+                    const int2 q = queue[lane];
+                    sl_band_entry((uint32_t)q.x, D0 + 32 * (q.y >> 16), q.y & 0xffff, n, S, Tlo, Thi, best, bestd);
+                    __syncwarp();
+                    if (lane < qn - 32) queue[lane] = queue[32 + lane];
+                    qn -= 32;
+                    __syncwarp();
+                }
             }
         }
     }
@@ -1122,47 +1144,48 @@ __global__ void __launch_bounds__(kSlThreads) k_sl(Shape s, PopBuf buf, int base
     }
     __syncthreads();
     // band-scan tables, in the space the shifted copies of T take later:
-    //   E2[v][x]      (E_v word x-kEqGuard, E_v word x+1-kEqGuard), v = 0..3 nucleotides, 4 zero
-    //   poffT[sp][t]  row r = 32(sp-1)+t: 8 (v(r)*PS + sp-1) bytes, v(r) = 4 outside [0, n); pitch 33
-    //   bstart[b]     first item of band b (items of band b: its 32-row segments)
+    //   E4[v][x]      E_v words x-kEqGuard .. x+3-kEqGuard, v = 0..3 nucleotides, 4 the zero plane
+    //   poffT[sp][t]  row r = 32(sp-1)+t: 16 (v(r)*PS + sp-1) bytes, v(r) = 4 outside [0, n); pitch 33
+    //   gstart[g]     first item of band group g (items: the group's 32-row segments)
     const int PS = sl_plane_stride(W), NSP = W + 2;
-    const int nb = sl_num_bands(n), D0 = sl_band_base(n);
-    uint2 *E2 = Tc;
-    int *poffT = reinterpret_cast<int *>(E2 + 5 * PS);
-    int *bstart = poffT + kSegPitch * NSP;
+    const int ng = sl_num_groups(n), D0 = sl_band_base(n);
+    uint4 *E4 = reinterpret_cast<uint4 *>(Tc);
+    int *poffT = reinterpret_cast<int *>(E4 + 5 * PS);
+    int *gstart = poffT + kSegPitch * NSP;
     for (int e = tid; e < 5 * PS; e += nth) {
         const int v = e / PS, x = e - v * PS - kEqGuard;
-        E2[e] = make_uint2(eq_word(Tlo, Thi, W, n, v, x), eq_word(Tlo, Thi, W, n, v, x + 1));
+        E4[e] = make_uint4(eq_word(Tlo, Thi, W, n, v, x), eq_word(Tlo, Thi, W, n, v, x + 1),
+                           eq_word(Tlo, Thi, W, n, v, x + 2), eq_word(Tlo, Thi, W, n, v, x + 3));
     }
     for (int e = tid; e < kSegPitch * NSP; e += nth) {
         const int sp = e / kSegPitch, t = e - sp * kSegPitch, r = 32 * (sp - 1) + t;
         const int v = (t < 32 && r >= 0 && r < n) ? plane_nt(S, r) : 4;
-        poffT[e] = (v * PS + (sp - 1)) * (int)sizeof(uint2);  // byte offset into E2
+        poffT[e] = (v * PS + (sp - 1)) * (int)sizeof(uint4);  // byte offset into E4
     }
     if (warp == 0) {
         int carry = 0;
-        for (int b0 = 0; b0 < nb; b0 += 32) {
-            const int b = b0 + lane;
+        for (int g0 = 0; g0 < ng; g0 += 32) {
+            const int g = g0 + lane;
             int x = 0;
-            if (b < nb) {
+            if (g < ng) {
                 int s_lo, s_hi;
-                sl_band_segments(n, D0 + 32 * b, s_lo, s_hi);
+                sl_group_segments(n, D0 + 32 * kBandGroup * g, s_lo, s_hi);
                 x = s_hi - s_lo + 1;
             }
             for (int o = 1; o < 32; o <<= 1) {
                 const int y = __shfl_up_sync(0xffffffffu, x, o);
                 if (lane >= o) x += y;
             }
-            if (b < nb) bstart[b + 1] = carry + x;
+            if (g < ng) gstart[g + 1] = carry + x;
             carry += __shfl_sync(0xffffffffu, x, 31);
         }
-        if (lane == 0) bstart[0] = 0;
+        if (lane == 0) gstart[0] = 0;
     }
     if (tid == 0) sm.next_chunk = 0;
     __syncthreads();
 
     int best = 0, bestd = 0x7fffffff;
-    sl_band_scan(E2, poffT, bstart, nb, S, Tlo, Thi, n, sm.queue[warp], &sm.next_chunk, lane, best, bestd);
+    sl_band_scan(E4, poffT, gstart, ng, S, Tlo, Thi, n, sm.queue[warp], &sm.next_chunk, lane, best, bestd);
     // CTA reduction of (best, smallest anti-diagonal)
     for (int o = 16; o > 0; o >>= 1) {
         int ob = __shfl_xor_sync(0xffffffffu, best, o), od = __shfl_xor_sync(0xffffffffu, bestd, o);
@@ -1319,8 +1342,8 @@ size_t sl_smem_bytes(const Shape &s)
     b += 16;  // alignment of Tc
     // Tc (32 shifted copies of T) or, before it, the band-scan tables
     const size_t tc = (size_t)(W + 2 * G) * 32 * sizeof(uint2);
-    const size_t band = (size_t)5 * sl_plane_stride(W) * sizeof(uint2) + (size_t)kSegPitch * (W + 2) * sizeof(int) +
-                        (size_t)(sl_num_bands(s.n) + 1) * sizeof(int);
+    const size_t band = (size_t)5 * sl_plane_stride(W) * sizeof(uint4) + (size_t)kSegPitch * (W + 2) * sizeof(int) +
+                        (size_t)(sl_num_groups(s.n) + 1) * sizeof(int);
     b += std::max(tc, band);
     return b;
 }
