@@ -826,11 +826,12 @@ __device__ void sl_scan(const uint2 *__restrict__ S, const uint2 *__restrict__ T
 // at bit offset r mod 32, a constant of the unrolled step; one 16-byte load of
 // four consecutive plane words gives the windows of all bands of the group.
 // Going down the rows, A2 = m_r & m_{r-1}, A4 = A2_r & A2_{r-2} and
-// A8 = A4_r & A4_{r-4} mark the diagonals whose run reaches 8 at row r, and
-// A8 & ~A8_{r-1} the runs that have just reached 8; eight rows of the previous
-// segment rebuild the history first.  Those rising edges are rare: the lane ORs
-// them into one mask per band and queues (mask, band, segment); each warp
-// measures its queued runs exactly, 32 at a time, one per lane (sl_band_entry).
+// A4_r & A4_{r-4} mark the diagonals with a run of 8 ending at row r; eight
+// rows of the previous segment rebuild the history first.  Such runs are rare:
+// the lane ORs those marks into one mask per band (a single 3-input logic op
+// per row) and queues (mask, band, segment); each warp measures its queued runs
+// exactly, 32 at a time, one per lane (sl_band_entry), which keeps the runs
+// that reach 8 inside the segment, so each run is measured once.
 //
 // Cells outside a diagonal's counted range: rows below it read T outside
 // [0, n) (zero planes) or a row outside [0, n) (the zero plane 4), so they
@@ -851,7 +852,7 @@ __host__ __device__ __forceinline__ int sl_num_groups(int n) { return (sl_num_ba
 // Segments of the rows a group of bands starting at shift d0 covers (rows of
 // the counted triangle: r >= -delta, 2r + delta <= n - 6): from the lowest
 // first row of its bands (the last band) to the highest last row (the first).
-__device__ __forceinline__ void sl_group_segments(int n, int d0, int &s_lo, int &s_hi)
+__host__ __device__ __forceinline__ void sl_group_segments(int n, int d0, int &s_lo, int &s_hi)
 {
     s_lo = max(0, -(d0 + 32 * (kBandGroup - 1)) - 31) >> 5;
     s_hi = ((n - 6 - d0) >> 1) >> 5;
@@ -973,10 +974,10 @@ __device__ void sl_band_scan(const uint4 *__restrict__ E4, const int *__restrict
             // u + d0/32 + kEqGuard of the row's plane, words g, g+1 for band g, at bit offset t
             const uint32_t qa = (uint32_t)__cvta_generic_to_shared(E4 + (d0 / 32 + kEqGuard));
             const uint32_t pa = (uint32_t)__cvta_generic_to_shared(poffT + s * kSegPitch);
-            uint32_t m1[kBandGroup], a8p[kBandGroup], a2h[kBandGroup][2], a4h[kBandGroup][4];
+            uint32_t m1[kBandGroup], a2h[kBandGroup][2], a4h[kBandGroup][4];
 #pragma unroll
             for (int g = 0; g < kBandGroup; g++) {
-                m1[g] = a8p[g] = 0;
+                m1[g] = 0;
                 a2h[g][0] = a2h[g][1] = 0;
                 a4h[g][0] = a4h[g][1] = a4h[g][2] = a4h[g][3] = 0;
             }
@@ -991,12 +992,10 @@ __device__ void sl_band_scan(const uint4 *__restrict__ E4, const int *__restrict
                     const uint32_t m = fshr(word_of(w, g), word_of(w, g + 1), t);
                     const uint32_t A2 = m & m1[g];
                     const uint32_t A4 = A2 & a2h[g][k & 1];
-                    const uint32_t A8 = A4 & a4h[g][k & 3];
-                    if (k >= 8) pend[g] |= A8 & ~a8p[g];
+                    if (k >= 8) pend[g] |= A4 & a4h[g][k & 3];
                     a2h[g][k & 1] = A2;
                     a4h[g][k & 3] = A4;
                     m1[g] = m;
-                    a8p[g] = A8;
                 }
             }
         }
