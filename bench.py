@@ -36,12 +36,14 @@ WORKLOAD = (f"plain NSGA-III, one synthetic protein L={L_AA} aa (+stop), m={M_CD
             f"4 objectives, Das-Dennis M=4 p={P_REF} (165 points), design job = {G_JOB} generations")
 METRIC = "generations/s"
 L2_FLUSH_BYTES = 256 << 20
-# k_sl at this workload, from one ncu capture (profiles/k_sl_L1000_m8_N1024.md):
-# thread instructions per launch / counted cells per launch, and DRAM bytes per launch
-SL_THREAD_INST_PER_LAUNCH = 42485464361
-SL_DRAM_BYTES_PER_LAUNCH = 6349312
-SL_ALU_PIPE_PCT_NCU = 81.69
-SM_COUNT, LANES_PER_SM_CLK = 148, 128   # 4 schedulers x 32 lanes issue per SM per clock
+# k_sl at this workload, from ncu captures of one launch (profiles/k_sl_L1000_m8_N1024.md):
+# ALU-pipe warp instructions, all thread instructions and DRAM bytes per launch; the ALU
+# pipe's peak (sm__inst_executed_pipe_alu.avg.peak_sustained) and its utilisation
+SL_ALU_WARP_INST_PER_LAUNCH = 240743253
+SL_THREAD_INST_PER_LAUNCH = 10823598092
+SL_DRAM_BYTES_PER_LAUNCH = 6364928
+SL_ALU_PIPE_PCT_NCU = 74.06
+SM_COUNT, ALU_WARP_INST_PER_SM_CLK = 148, 2
 
 
 def load_pkg():
@@ -60,18 +62,20 @@ def hairpin_cells_per_cds(n: int) -> int:
 
 
 def roofline(cells: int, sl_seconds: float, clocks: dict) -> dict:
-    """Integer-issue roofline of the stem scan: achieved lane-ops/s = counted cells/s x
-    lane instructions per cell (ncu); peak = 148 SMs x 128 lanes x sampled SM clock."""
-    ops_per_cell = SL_THREAD_INST_PER_LAUNCH / cells
-    achieved = cells / sl_seconds * ops_per_cell / 1e9
+    """Integer-pipe roofline of the stem scan, the binding unit (bit-logic and shifts
+    on the ALU pipe): achieved = ALU-pipe warp instructions per launch (ncu) / the
+    launch time measured here; peak = 2 ALU warp instructions per SM per clock x 148
+    SMs x the SM clock sampled during the timed region."""
+    achieved = SL_ALU_WARP_INST_PER_LAUNCH / sl_seconds / 1e9
     mhz = clocks.get("sm_mhz") or 1965.0
-    peak = SM_COUNT * LANES_PER_SM_CLK * mhz * 1e6 / 1e9
-    return {"bound": "alu", "kernel": "k_sl (hairpin-stem scan)", "unit": "Glane-ops/s", "achieved": achieved,
+    peak = SM_COUNT * ALU_WARP_INST_PER_SM_CLK * mhz * 1e6 / 1e9
+    return {"bound": "alu", "kernel": "k_sl (hairpin-stem scan)", "unit": "G ALU warp-inst/s", "achieved": achieved,
             "peak": peak, "frac": achieved / peak, "traffic": SL_DRAM_BYTES_PER_LAUNCH,
-            "peak_source": "issue rate 4x32 lanes/SM/clk x 148 SMs at the sampled SM clock (no measured integer "
-                           "peak exists in MEASURED_PEAKS.json)",
-            "cells_per_launch": cells, "cells_per_s": cells / sl_seconds, "lane_ops_per_cell": ops_per_cell,
-            "alu_pipe_pct_of_peak_ncu": SL_ALU_PIPE_PCT_NCU}
+            "peak_source": "ALU pipe 2 warp-inst/SM/clk (ncu peak_sustained) x 148 SMs at the sampled SM clock; "
+                           "MEASURED_PEAKS.json has no integer peak",
+            "algorithmic_bytes_per_launch": SL_DRAM_BYTES_PER_LAUNCH,
+            "cells_per_launch": cells, "cells_per_s": cells / sl_seconds,
+            "lane_ops_per_cell": SL_THREAD_INST_PER_LAUNCH / cells, "alu_pipe_pct_of_peak_ncu": SL_ALU_PIPE_PCT_NCU}
 
 
 class ClockSampler:

@@ -380,7 +380,7 @@ int pe_create(const pe_config *cfg, const int8_t *aa_idx, int32_t aa_len, const 
     int smem_optin = 0;
     CK(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     if (sl_smem_bytes(s) > (size_t)smem_optin || var_smem_bytes(s) > (size_t)smem_optin ||
-        select_smem_bytes(s) > (size_t)smem_optin)
+        select_smem_bytes(s) > (size_t)smem_optin || niche_smem_bytes(s) > (size_t)smem_optin)
         return fail(PE_ERR_ARG, "problem too large for one CTA (L=%d m=%d N=%d)", L, m, N);
 
     pe_instance *in = new pe_instance();

@@ -826,7 +826,7 @@ __device__ void sl_scan(const uint2 *__restrict__ S, const uint2 *__restrict__ T
 // at bit offset r mod 32, a constant of the unrolled step; one 16-byte load of
 // four consecutive plane words gives the windows of all bands of the group.
 // Going down the rows, A2 = m_r & m_{r-1}, A4 = A2_r & A2_{r-2} and
-// A4_r & A4_{r-4} mark the diagonals with a run of 8 ending at row r; eight
+// A4_r & A4_{r-4} mark the diagonals with a run of 8 ending at row r; seven
 // rows of the previous segment rebuild the history first.  Such runs are rare:
 // the lane ORs those marks into one mask per band (a single 3-input logic op
 // per row) and queues (mask, band, segment); each warp measures its queued runs
@@ -982,17 +982,18 @@ __device__ void sl_band_scan(const uint4 *__restrict__ E4, const int *__restrict
                 a4h[g][0] = a4h[g][1] = a4h[g][2] = a4h[g][3] = 0;
             }
 #pragma unroll
-            for (int k = 0; k < 40; k++) {
-                // steps 0..7: rows 24..31 of segment s-1; steps 8..39: rows 0..31 of segment s
-                const int t = k < 8 ? k + 24 : k - 8;
-                const uint32_t pv = lds_u32(pa + 4 * (k < 8 ? t : kSegPitch + t));
+            for (int k = 0; k < 39; k++) {
+                // steps 0..6: rows 25..31 of segment s-1 (the runs of 8 ending at rows 0..31
+                // of segment s start there at the earliest); steps 7..38: rows 0..31 of segment s
+                const int t = k < 7 ? k + 25 : k - 7;
+                const uint32_t pv = lds_u32(pa + 4 * (k < 7 ? t : kSegPitch + t));
                 const uint4 w = lds_v4(qa + pv);
 #pragma unroll
                 for (int g = 0; g < kBandGroup; g++) {
                     const uint32_t m = fshr(word_of(w, g), word_of(w, g + 1), t);
                     const uint32_t A2 = m & m1[g];
                     const uint32_t A4 = A2 & a2h[g][k & 1];
-                    if (k >= 8) pend[g] |= A4 & a4h[g][k & 3];
+                    if (k >= 7) pend[g] |= A4 & a4h[g][k & 3];
                     a2h[g][k & 1] = A2;
                     a4h[g][k & 3] = A4;
                     m1[g] = m;

@@ -104,5 +104,6 @@ void set_error_text(const char *msg);
 cudaError_t launch_select(const Shape &s, const float *obj, float *ext, const float *refpts, SelectScratch sc,
                           int32_t *surv, uint32_t *d_gen, int bump_gen, cudaStream_t st);
 size_t select_smem_bytes(const Shape &s);
+size_t niche_smem_bytes(const Shape &s);
 
 }  // namespace pe

@@ -439,92 +439,202 @@ __global__ void __launch_bounds__(256) k_assoc(Shape s, const float *__restrict_
     }
 }
 
-// referenceBasedSorting phase 2 (:1182-1279): candidate lists and niche levels
+// exclusive block scan of an int over the CTA; returns the prefix and leaves
+// the total in *total (all threads)
+__device__ __forceinline__ int block_scan_value(int v, SelSmem &sm, int *total)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+    int inc = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+    }
+    if (lane == 31) sm.warp_tot[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        const int w = lane < nwarps ? sm.warp_tot[lane] : 0;
+        int x = w;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane < nwarps) sm.warp_tot[lane] = x - w;
+        if (lane == 31) sm.warp_tot[32] = x;
+    }
+    __syncthreads();
+    const int r = sm.warp_tot[warp] + inc - v;
+    *total = sm.warp_tot[32];
+    __syncthreads();
+    return r;
+}
+
+// referenceBasedSorting phase 2 (:1182-1279): candidate lists and niche levels.
+//
+// The reference visits levels 0, 1, 2, ... and, within a level, the reference
+// points in ascending index; point j takes one candidate at every level from
+// its niche count c_j on while it has candidates (n_j of them), until N are
+// chosen.  So j picks at levels c_j .. c_j + n_j - 1, every level before the
+// level L* at which the N-th pick falls is complete, and at L* the first K
+// active points pick.  This kernel computes L* and K from a histogram over
+// levels, lets every point draw its own picks (the draws of point j depend
+// only on j, its levels and its list), and writes each level's picks to their
+// positions with one warp per level: the same survivors, in the same order,
+// as the level-by-level loop, in a fixed number of steps.
 __global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc, int32_t *surv, uint32_t *d_gen,
                                                        int bump_gen)
 {
-    __shared__ SelSmem sm;
-    const int N = s.N, N2 = 2 * N, R = s.R;
-    const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SelSmem &sm = *reinterpret_cast<SelSmem *>(smem_raw);
+    const int N = s.N, N2 = 2 * N, R = s.R, Lsz = N2 + 4;
+    int *cj = reinterpret_cast<int *>(smem_raw + ((sizeof(SelSmem) + 15) & ~size_t(15)));
+    int *nj = cj + R;
+    int *coff = nj + R;    // R + 1
+    int *kq = coff + R + 1;
+    int *lv = kq + R;      // Lsz: level histogram, then picks before each level
+    const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarps = nth >> 5;
     const uint32_t gen = *d_gen;
     if (sc.info[3]) {  // fronts filled N exactly; k_select wrote the survivors
         if (tid == 0 && bump_gen) *d_gen = gen + 1;
         return;
     }
-    const int rc = sc.info[0], count0 = sc.info[5];
-    // candidate lists per reference point, ascending position
-    if (tid == 0) {
-        int acc = 0;
-        for (int j = 0; j < R; j++) {
-            sc.coff[j] = acc;
-            acc += sc.ncand[j];
-        }
-        sc.coff[R] = acc;
+    const int rc = sc.info[0], count0 = sc.info[5], need = N - count0;
+    for (int j = tid; j < R; j += nth) {
+        cj[j] = sc.rho[j];
+        nj[j] = sc.ncand[j];
+        kq[j] = 0;
     }
+    for (int l = tid; l < Lsz; l += nth) lv[l] = 0;
+    if (tid == 0) sm.i0 = 0;
     __syncthreads();
-    int32_t *fill = sc.fill;
-    for (int j = tid; j < R; j += nth) fill[j] = 0;
-    __syncthreads();
-    if (warp == 0) {
-        for (int base = count0; base < rc; base += 32) {
-            int t = base + lane;
-            bool act = t < rc;
-            int j = act ? sc.assoc[t] : -1 - lane;
-            uint32_t peers = __match_any_sync(0xffffffffu, j);
-            int rank = __popc(peers & ((1u << lane) - 1u));
-            int f0v = act ? fill[j] : 0;
-            __syncwarp();
-            if (act) sc.cand[sc.coff[j] + f0v + rank] = sc.sorted[t];
-            __syncwarp();
-            if (act && rank == 0) fill[j] = f0v + __popc(peers);
-            __syncwarp();
-        }
-    }
-    __syncthreads();
-    // ---------------- niching (phase 2, :1182-1279), exactly N survivors
-    for (int t = tid; t < count0; t += nth) surv[t] = sc.sorted[t];
-    if (tid == 0) {
-        sm.count = count0;
-        sm.level = 0;
-    }
-    __syncthreads();
-    while (sm.count < N && sm.level <= N2 + 2) {
-        const int level = sm.level;
-        for (int jb = 0; jb < R; jb += nth) {
-            int j = jb + tid;
-            int flag = (j < R) && sc.rho[j] == level && sc.ncand[j] > 0;
-            int tot;
-            int pos = block_scan_flag(flag, sm, &tot);
-            int out = sm.count + pos;
-            if (flag && out < N) {
-                int *cl = sc.cand + sc.coff[j];
-                int nc = sc.ncand[j];
-                int slot = 0;
-                if (level == 0) {
-                    float bd = sc.dist[cl[0]];
-                    for (int u = 1; u < nc; u++) {
-                        float dv = sc.dist[cl[u]];
-                        if (dv < bd) {
-                            bd = dv;
-                            slot = u;
-                        }
-                    }
-                } else {
-                    slot = (int)rng_uint(draw(s.seed, TAG_NICHE, gen, (uint32_t)j, (uint32_t)level, 0), (uint32_t)nc);
-                }
-                surv[out] = cl[slot];
-                sc.rho[j] = level + 1;
-                sc.ncand[j] = nc - 1;
-                cl[slot] = cl[nc - 1];
+    // CSR offsets of the candidate lists; level histogram (+1 at c_j, -1 at c_j + n_j)
+    for (int base = 0; base < R; base += nth) {
+        const int j = base + tid;
+        const int v = j < R ? nj[j] : 0;
+        int tot;
+        const int pos = block_scan_value(v, sm, &tot);
+        if (j < R) {
+            coff[j] = sm.i0 + pos;
+            if (v > 0) {
+                atomicAdd(&lv[min(cj[j], Lsz - 1)], 1);
+                atomicAdd(&lv[min(cj[j] + v, Lsz - 1)], -1);
             }
-            __syncthreads();
-            if (tid == 0) sm.count = min(N, sm.count + tot);
-            __syncthreads();
         }
-        if (tid == 0) sm.level = level + 1;
+        __syncthreads();
+        if (tid == 0) sm.i0 += tot;
         __syncthreads();
     }
+    if (tid == 0) coff[R] = sm.i0;
+    // candidate lists in ascending position (kq counts the fill)
+    if (warp == 0) {
+        for (int base = count0; base < rc; base += 32) {
+            const int t = base + lane;
+            const bool act = t < rc;
+            const int j = act ? sc.assoc[t] : -1 - lane;
+            const uint32_t peers = __match_any_sync(0xffffffffu, j);
+            const int rank = __popc(peers & ((1u << lane) - 1u));
+            const int f0v = act ? kq[j] : 0;
+            __syncwarp();
+            if (act) sc.cand[coff[j] + f0v + rank] = sc.sorted[t];
+            __syncwarp();
+            if (act && rank == 0) kq[j] = f0v + __popc(peers);
+            __syncwarp();
+        }
+    }
+    // active points per level, then picks before each level: lv[l] = picks at levels < l
+    if (tid == 0) {
+        sm.i0 = 0;
+        sm.i1 = 0;
+    }
+    __syncthreads();
+    for (int base = 0; base < Lsz; base += nth) {
+        const int l = base + tid;
+        const int d = l < Lsz ? lv[l] : 0;
+        int tot;
+        const int act = sm.i0 + block_scan_value(d, sm, &tot) + d;  // active points at level l
+        int tot2;
+        const int before = sm.i1 + block_scan_value(l < Lsz ? act : 0, sm, &tot2);
+        if (l < Lsz) lv[l] = before;
+        __syncthreads();
+        if (tid == 0) {
+            sm.i0 += tot;
+            sm.i1 += tot2;
+        }
+        __syncthreads();
+    }
+    // L*: the level of the last pick; K: picks at L*
+    if (tid == 0) {
+        sm.i2 = Lsz;
+        sm.i3 = 0;
+    }
+    __syncthreads();
+    for (int l = tid; l + 1 < Lsz; l += nth)
+        if (lv[l] < need && lv[l + 1] >= need) {
+            sm.i2 = l;
+            sm.i3 = need - lv[l];
+        }
+    __syncthreads();
+    const int Ls = sm.i2, K = sm.i3;
+    // picks per point: every level in [c_j, min(c_j + n_j, L*)), plus L* for the first K active there
+    if (tid == 0) sm.i0 = 0;
+    __syncthreads();
+    for (int base = 0; base < R; base += nth) {
+        const int j = base + tid;
+        const bool on = j < R && nj[j] > 0 && cj[j] <= Ls && Ls < cj[j] + nj[j];
+        int tot;
+        const int pos = sm.i0 + block_scan_flag(on, sm, &tot);
+        if (j < R) kq[j] = (nj[j] > 0 ? max(0, min(cj[j] + nj[j], Ls) - cj[j]) : 0) + (on && pos < K ? 1 : 0);
+        __syncthreads();
+        if (tid == 0) sm.i0 += tot;
+        __syncthreads();
+    }
+    // each point draws its picks; the q-th pick ends at list position n_j - 1 - q
+    for (int j = tid; j < R; j += nth) {
+        int *cl = sc.cand + coff[j];
+        int nc = nj[j];
+        for (int q = 0; q < kq[j]; q++) {
+            const int level = cj[j] + q;
+            int slot = 0;
+            if (level == 0) {
+                float bd = sc.dist[cl[0]];
+                for (int u = 1; u < nc; u++) {
+                    const float dv = sc.dist[cl[u]];
+                    if (dv < bd) {
+                        bd = dv;
+                        slot = u;
+                    }
+                }
+            } else {
+                slot = (int)rng_uint(draw(s.seed, TAG_NICHE, gen, (uint32_t)j, (uint32_t)level, 0), (uint32_t)nc);
+            }
+            const int pick = cl[slot];
+            cl[slot] = cl[nc - 1];
+            cl[nc - 1] = pick;
+            nc--;
+        }
+    }
+    for (int t = tid; t < count0; t += nth) surv[t] = sc.sorted[t];
+    __syncthreads();
+    // positions: level l's picks follow the picks of earlier levels, in ascending point index
+    const int lmax = min(Ls, Lsz - 1);
+    for (int l = warp; l <= lmax; l += nwarps) {
+        int run = 0;
+        for (int jb = 0; jb < R; jb += 32) {
+            const int j = jb + lane;
+            const bool act = j < R && nj[j] > 0 && cj[j] <= l && l < cj[j] + nj[j];
+            const uint32_t bal = __ballot_sync(0xffffffffu, act);
+            const int rank = run + __popc(bal & ((1u << lane) - 1u));
+            if (act && (l < Ls || rank < K))
+                surv[count0 + lv[l] + rank] = sc.cand[coff[j] + nj[j] - 1 - (l - cj[j])];
+            run += __popc(bal);
+        }
+    }
+    __syncthreads();
     if (tid == 0 && bump_gen) *d_gen = gen + 1;
+}
+
+size_t niche_smem_bytes(const Shape &s)
+{
+    return ((sizeof(SelSmem) + 15) & ~size_t(15)) + (size_t)(4 * s.R + 1 + 2 * s.N + 4) * sizeof(int);
 }
 
 size_t select_smem_bytes(const Shape &s)
@@ -548,7 +658,9 @@ cudaError_t launch_select(const Shape &s, const float *obj, float *ext, const fl
     const int warps_needed = 2 * s.N;
     k_assoc<<<std::min((warps_needed + 7) / 8, 148 * 8), 256, 0, st>>>(s, obj, refpts, sc);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    k_niche<<<1, kSelThreads, 0, st>>>(s, sc, surv, d_gen, bump_gen);
+    const size_t nsm = niche_smem_bytes(s);
+    if ((e = raise_smem_limit((const void *)k_niche, nsm)) != cudaSuccess) return e;
+    k_niche<<<1, kSelThreads, nsm, st>>>(s, sc, surv, d_gen, bump_gen);
     return cudaGetLastError();
 }
 
