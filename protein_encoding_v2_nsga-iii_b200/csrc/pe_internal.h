@@ -13,7 +13,7 @@ enum Kind { K_CAI = 0, K_CBP = 1, K_HSC = 2, K_HD = 3, K_GC = 4, K_SL = 5 };
 
 constexpr int kMaxObj = 6;
 constexpr int kMaxCds = 64;          // objidx stores CDS indices as int8
-constexpr int kSlThreads = 256;      // SL scan CTA
+constexpr int kSlThreads = 128;      // SL scan CTA (4 warps: less idle time at the end of a CDS)
 constexpr int kVarThreads = 256;     // variation / light-eval CTA
 constexpr int kSelThreads = 1024;    // selection CTA
 constexpr int kSlGuardRows = 8;      // zero guard rows around the shifted T copies
