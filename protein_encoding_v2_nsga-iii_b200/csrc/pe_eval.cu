@@ -761,7 +761,8 @@ __device__ __forceinline__ void sl_word(uint2 sv, uint2 tv, int k, int r_lo, int
     }
 }
 
-__device__ void sl_scan(const uint2 *__restrict__ S, const uint2 *__restrict__ Tc, int n, int *next_chunk, int lane,
+__device__ void sl_scan(const uint2 *__restrict__ S, const uint32_t *__restrict__ Tlo, const uint32_t *__restrict__ Thi,
+                        int n, int *next_chunk, int lane,
                         int &best, int &bestd)
 {
     const int dmax = n - 6;
@@ -794,13 +795,17 @@ __device__ void sl_scan(const uint2 *__restrict__ S, const uint2 *__restrict__ T
         }
         kf_lo = max(kf_lo, kmin);
         kf_hi = min(kf_hi, kmax);
-        const uint2 *trow = Tc + (ptrdiff_t)((delta >> 5) + kSlGuardRows) * 32 + (delta & 31);
+        // T bits [32k + delta, +31]: words row, row + 1 of T at bit offset delta mod 32
+        const int row = (delta >> 5) + kSlGuardRows, sh = delta & 31;
+        auto tw = [&](int k) {
+            return make_uint2(fshr(Tlo[row + k], Tlo[row + k + 1], sh), fshr(Thi[row + k], Thi[row + k + 1], sh));
+        };
         int cur = 0, dbest = 0;
         int k = kmin;
-        for (; k < kf_lo; k++) sl_word<true>(S[k], trow[k * 32], k, r_lo, r_hi, cur, dbest);
+        for (; k < kf_lo; k++) sl_word<true>(S[k], tw(k), k, r_lo, r_hi, cur, dbest);
 #pragma unroll 4
-        for (; k <= kf_hi; k++) sl_word<false>(S[k], trow[k * 32], k, r_lo, r_hi, cur, dbest);
-        for (; k <= kmax; k++) sl_word<true>(S[k], trow[k * 32], k, r_lo, r_hi, cur, dbest);
+        for (; k <= kf_hi; k++) sl_word<false>(S[k], tw(k), k, r_lo, r_hi, cur, dbest);
+        for (; k <= kmax; k++) sl_word<true>(S[k], tw(k), k, r_lo, r_hi, cur, dbest);
         dbest = max(dbest, cur);
         if (valid) {
             int d = n - 1 - delta;
@@ -1071,8 +1076,8 @@ __global__ void __launch_bounds__(kSlThreads) k_sl(Shape s, PopBuf buf, int base
     uint2 *S = reinterpret_cast<uint2 *>(smem_raw + ((sizeof(SlSmem) + 15) & ~size_t(15)));  // W + 2
     uint32_t *Tlo = reinterpret_cast<uint32_t *>(S + (W + 2));                               // W + 2G + 1
     uint32_t *Thi = Tlo + (W + 2 * G + 1);
-    uint2 *Tc = reinterpret_cast<uint2 *>(Thi + (W + 2 * G + 1));
-    Tc = reinterpret_cast<uint2 *>((reinterpret_cast<uintptr_t>(Tc) + 15) & ~uintptr_t(15));
+    unsigned char *tab = reinterpret_cast<unsigned char *>(Thi + (W + 2 * G + 1));
+    tab = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(tab) + 15) & ~uintptr_t(15));
 
     const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarps = nth >> 5;
     const int sol = blockIdx.x / s.m, c = blockIdx.x - sol * s.m;
@@ -1149,7 +1154,7 @@ __global__ void __launch_bounds__(kSlThreads) k_sl(Shape s, PopBuf buf, int base
     //   gstart[g]     first item of band group g (items: the group's 32-row segments)
     const int PS = sl_plane_stride(W), NSP = W + 2;
     const int ng = sl_num_groups(n), D0 = sl_band_base(n);
-    uint4 *E4 = reinterpret_cast<uint4 *>(Tc);
+    uint4 *E4 = reinterpret_cast<uint4 *>(tab);
     int *poffT = reinterpret_cast<int *>(E4 + 5 * PS);
     int *gstart = poffT + kSegPitch * NSP;
     for (int e = tid; e < 5 * PS; e += nth) {
@@ -1205,18 +1210,10 @@ __global__ void __launch_bounds__(kSlThreads) k_sl(Shape s, PopBuf buf, int base
     }
     __syncthreads();
     if (sm.res[0] < 8) {
-        // no run reaches 8: exact per-word runs over 32 shifted copies of T,
-        // transposed (Tc[row][sh] = T bits [32(row-G)+sh, +31]), which replace
-        // the band-scan tables
-        const int rows = W + 2 * G;
-        for (int e = tid; e < rows * 32; e += nth) {
-            int row = e >> 5, sh = e & 31;
-            Tc[e] = make_uint2(fshr(Tlo[row], Tlo[row + 1], sh), fshr(Thi[row], Thi[row + 1], sh));
-        }
-        __syncthreads();
+        // no run reaches 8: exact per-word runs
         best = 0;
         bestd = 0x7fffffff;
-        sl_scan(S, Tc, n, &sm.next_chunk, lane, best, bestd);
+        sl_scan(S, Tlo, Thi, n, &sm.next_chunk, lane, best, bestd);
         for (int o = 16; o > 0; o >>= 1) {
             int ob = __shfl_xor_sync(0xffffffffu, best, o), od = __shfl_xor_sync(0xffffffffu, bestd, o);
             pair_reduce(best, bestd, ob, od);
@@ -1339,12 +1336,10 @@ size_t sl_smem_bytes(const Shape &s)
     size_t b = (sizeof(SlSmem) + 15) & ~size_t(15);
     b += (size_t)(W + 2) * sizeof(uint2);
     b += 2 * (size_t)(W + 2 * G + 1) * sizeof(uint32_t);
-    b += 16;  // alignment of Tc
-    // Tc (32 shifted copies of T) or, before it, the band-scan tables
-    const size_t tc = (size_t)(W + 2 * G) * 32 * sizeof(uint2);
+    b += 16;  // alignment of the band-scan tables
     const size_t band = (size_t)5 * sl_plane_stride(W) * sizeof(uint4) + (size_t)kSegPitch * (W + 2) * sizeof(int) +
                         (size_t)(sl_num_groups(s.n) + 1) * sizeof(int);
-    b += std::max(tc, band);
+    b += band;
     return b;
 }
 
