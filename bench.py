@@ -21,6 +21,7 @@ import csv
 import importlib.util
 import io
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -32,8 +33,34 @@ import numpy as np
 
 ROOT = Path(__file__).resolve().parent
 L_AA, M_CDS, POP, PM, P_REF, G_JOB, SEED = 1000, 8, 1024, 0.02, 8, 500, 2024
+# objective set of the plain workload: 1 = the four objectives (default), 0 = the reference's six
+# (then p follows the reference's rule from N: p = 7, 792 points); set by --objectives
+OBJ_SET, P_USE, M_OBJ = 1, P_REF, 4
 WORKLOAD = (f"plain NSGA-III, one synthetic protein L={L_AA} aa (+stop), m={M_CDS} CDSs, N={POP}, Pm={PM}, "
             f"4 objectives, Das-Dennis M=4 p={P_REF} (165 points), design job = {G_JOB} generations")
+
+
+def set_workload(shape: str | None, six: bool):
+    """Plain workload other than the default: --shape L,m,N,p (p = 0: the reference's rule
+    from N) and/or the reference's six objectives."""
+    global L_AA, M_CDS, POP, P_REF, G_JOB, OBJ_SET, P_USE, M_OBJ, WORKLOAD
+    if shape:
+        v = [int(x) for x in shape.split(",")]
+        L_AA, M_CDS, POP, P_REF = v[:4]
+        if len(v) > 4:
+            G_JOB = v[4]
+    OBJ_SET, M_OBJ = (0, 6) if six else (1, 4)
+    P_USE = 0 if six and not shape else P_REF
+    p, R = P_USE, None
+    if p <= 0:   # the reference's rule (src/main.cu:564-576): largest p with C(M+p-1, p) <= N
+        p = 1
+        while math.comb(M_OBJ + p - 1, p) <= POP:
+            p += 1
+        p -= 1
+    R = math.comb(M_OBJ + p - 1, p)
+    WORKLOAD = (f"plain NSGA-III, one synthetic protein L={L_AA} aa (+stop), m={M_CDS} CDSs, N={POP}, Pm={PM}, "
+                f"{'the reference' + chr(39) + 's 6' if six else '4'} objectives, Das-Dennis M={M_OBJ} p={p} "
+                f"({R} points), design job = {G_JOB} generations")
 METRIC = "generations/s"
 L2_FLUSH_BYTES = 256 << 20
 # k_sl at this workload, from ncu captures of one launch (profiles/k_sl_L1000_m8_N1024.md):
@@ -43,7 +70,11 @@ SL_ALU_WARP_INST_PER_LAUNCH = 240743253
 SL_THREAD_INST_PER_LAUNCH = 10823598092
 SL_DRAM_BYTES_PER_LAUNCH = 6364928
 SL_ALU_PIPE_PCT_NCU = 74.06
+SL_CELLS_PER_LAUNCH = 36827144192      # 1024 x 8 CDSs of 3003 nucleotides
 SM_COUNT, ALU_WARP_INST_PER_SM_CLK = 148, 2
+# kernels one generation launches (one CUDA graph replay): k_variation, k_sl, k_dominance,
+# k_select, k_assoc, k_niche
+KERNELS_PER_GENERATION = 6
 
 
 def load_pkg():
@@ -66,7 +97,9 @@ def roofline(cells: int, sl_seconds: float, clocks: dict) -> dict:
     on the ALU pipe): achieved = ALU-pipe warp instructions per launch (ncu) / the
     launch time measured here; peak = 2 ALU warp instructions per SM per clock x 148
     SMs x the SM clock sampled during the timed region."""
-    achieved = SL_ALU_WARP_INST_PER_LAUNCH / sl_seconds / 1e9
+    # the ncu count is for the default shape; other shapes scale it by counted cells
+    alu_inst = SL_ALU_WARP_INST_PER_LAUNCH * cells / SL_CELLS_PER_LAUNCH
+    achieved = alu_inst / sl_seconds / 1e9
     mhz = clocks.get("sm_mhz") or 1965.0
     peak = SM_COUNT * ALU_WARP_INST_PER_SM_CLK * mhz * 1e6 / 1e9
     return {"bound": "alu", "kernel": "k_sl (hairpin-stem scan)", "unit": "G ALU warp-inst/s", "achieved": achieved,
@@ -75,11 +108,13 @@ def roofline(cells: int, sl_seconds: float, clocks: dict) -> dict:
                            "MEASURED_PEAKS.json has no integer peak",
             "algorithmic_bytes_per_launch": SL_DRAM_BYTES_PER_LAUNCH,
             "cells_per_launch": cells, "cells_per_s": cells / sl_seconds,
-            "lane_ops_per_cell": SL_THREAD_INST_PER_LAUNCH / cells, "alu_pipe_pct_of_peak_ncu": SL_ALU_PIPE_PCT_NCU}
+            "lane_ops_per_cell": SL_THREAD_INST_PER_LAUNCH / SL_CELLS_PER_LAUNCH,
+            "alu_pipe_pct_of_peak_ncu": SL_ALU_PIPE_PCT_NCU,
+            "instruction_count": "ncu, L=1000 m=8 N=1024" + ("" if cells == SL_CELLS_PER_LAUNCH else "; scaled by cells")}
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 100 ms while timing."""
+    """nvidia-smi clocks / throttle reasons sampled every 20 ms while timing."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -92,7 +127,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
@@ -141,7 +176,7 @@ def cpu_reference(pe, orc, pop, aa, table, steps: int, threads: int):
     restricted to every 16th anti-diagonal (rotating), (3) selection on the full 2N set.
     seconds/generation = t1*N/S + t2*16*(N*m)/threads + t3."""
     ids, obj, objidx, pql, surv = pop
-    prob = orc.Problem(aa, table.arrays(), M_CDS, POP, PM, objset=1, p=P_REF, seed=SEED)
+    prob = orc.Problem(aa, table.arrays(), M_CDS, POP, PM, objset=OBJ_SET, p=P_USE, seed=SEED)
     S = min(len(surv), max(8, threads))
     par = surv[:S]
     nt = np.asarray(table.arrays()["nt"])
@@ -154,7 +189,7 @@ def cpu_reference(pe, orc, pop, aa, table, steps: int, threads: int):
         t1 = time.perf_counter()
         orc.sl_sample(cds, k % SL_STRIDE, SL_STRIDE, threads=threads)
         t2 = time.perf_counter()
-        ext = obj[:4].copy()
+        ext = obj[:M_OBJ].copy()
         prob.select(k, obj, ext)
         t3 = time.perf_counter()
         sec_per_gen = (t1 - t0) * POP / S + (t2 - t1) * SL_STRIDE * (POP * M_CDS) / threads + (t3 - t2)
@@ -175,7 +210,7 @@ def run_reference(args, world, rank):
     threads = os.cpu_count() or 1
     aa = pe.synthetic_protein(L_AA, SEED)
     table = pe.dirichlet_table(SEED)
-    prob = orc.Problem(aa, table.arrays(), M_CDS, POP, PM, objset=1, p=P_REF, seed=SEED)
+    prob = orc.Problem(aa, table.arrays(), M_CDS, POP, PM, objset=OBJ_SET, p=P_USE, seed=SEED)
     # parents: a population generated and evaluated by the oracle itself (bounded: `threads` solutions)
     S = max(8, threads)
     ids = np.stack([prob.gen_solution(i) for i in range(S)])
@@ -213,7 +248,7 @@ def run_ours(args, world, rank, local):
     stream = torch.cuda.Stream(device=dev)
     aa = pe.synthetic_protein(L_AA, SEED)
     table = pe.dirichlet_table(SEED)
-    eng = pe.Engine(aa, table, M_CDS, POP, PM, objectives=pe.OBJ_BASE4, ref_p=P_REF, seed=SEED + rank,
+    eng = pe.Engine(aa, table, M_CDS, POP, PM, objectives=OBJ_SET, ref_p=P_USE, seed=SEED + rank,
                     stream=stream.cuda_stream)
     eng.init()
     eng.set_profiling(True)
@@ -255,11 +290,11 @@ def run_ours(args, world, rank, local):
     line = None
     if rank == 0:
         # end-to-end through the public API with host buffers: a design job of G_E2E generations
-        G_E2E = 20
-        obj_host = np.zeros((2 * POP, 4), np.float32)
+        G_E2E = 100
+        obj_host = np.zeros((2 * POP, M_OBJ), np.float32)
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
-        e2 = pe.Engine(aa, table, M_CDS, POP, PM, objectives=pe.OBJ_BASE4, ref_p=P_REF, seed=SEED + 7)
+        e2 = pe.Engine(aa, table, M_CDS, POP, PM, objectives=OBJ_SET, ref_p=P_USE, seed=SEED + 7)
         e2.init()
         for _ in range(G_E2E):
             e2.step(1)
@@ -298,7 +333,7 @@ def run_ours(args, world, rank, local):
             "clocks": clocks,
             "e2e": {"value": G_E2E / e2e_s, "unit": "generations/s", "h2d_bytes_per_step": h2d / G_E2E,
                     "d2h_bytes_per_step": d2h, "job": f"create + init + {G_E2E} generations + reads"},
-            "gpu_launches": 4 * args.steps,
+            "gpu_launches": KERNELS_PER_GENERATION * args.steps,
             "wall_s": t_wall,
             "peaks_file": {k: peaks.get(k) for k in ("hbm_gbs", "bf16_tflops", "sm_max_mhz")},
         }
@@ -471,13 +506,19 @@ def main():
     ap.add_argument("--workload", choices=["plain", "batched", "served"], default="plain")
     ap.add_argument("--generations", type=int, default=0, help="generations per job (batched)")
     ap.add_argument("--jobs", type=int, default=40, help="design requests in the served workload")
+    ap.add_argument("--shape", default=None, help="plain workload L,m,N,p[,G] instead of 1000,8,1024,8,500 "
+                    "(p=0: the reference's rule from N; G: generations of a design job)")
+    ap.add_argument("--objectives", choices=["base4", "ref6"], default="base4",
+                    help="objective set of the plain workload (ref6: the reference's six, p by its rule)")
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--profile-case", action="store_true",
                     help="only build the bench instance, init and run 2 generations (for ncu captures)")
     args = ap.parse_args()
+    if args.objectives == "ref6" or args.shape:
+        set_workload(args.shape, args.objectives == "ref6")
     world, rank, local = dist_setup()
     if args.workload == "batched":
         run_batched(args)
