@@ -91,7 +91,8 @@ __device__ bool cta_full_hairpin(const Shape &s, const SmemTab &st, const uint8_
     const int n = s.n, K = s.K;
     if (K <= 0) return false;
     bool found = false;
-    for (int ri = K - 1; ri < n && !found; ri++) {
+    // (ri, ci) pairs exist only for ri <= n - K - 5 (ci in [ri + 5, n - K])
+    for (int ri = K - 1; ri <= n - K - 5 && !found; ri++) {
         for (int ci = ri + 5; ci + K - 1 <= n - 1 && !found; ci++) {
             int ok = 1;
             for (int u = tid; u < K; u += nth) ok &= (nt_at(st, row, ri - u) ^ nt_at(st, row, ci + u)) == 3;
