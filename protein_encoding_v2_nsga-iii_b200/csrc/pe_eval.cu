@@ -831,13 +831,16 @@ __device__ void sl_scan(const uint2 *__restrict__ S, const uint32_t *__restrict_
 //     m_r = E_{s[r]} bits [r + delta0, r + delta0 + 32),
 // at bit offset r mod 32, a constant of the unrolled step; one 16-byte load of
 // four consecutive plane words gives the windows of all bands of the group.
-// Going down the rows, A2 = m_r & m_{r-1}, A4 = A2_r & A2_{r-2} and
-// A4_r & A4_{r-4} mark the diagonals with a run of 8 ending at row r; seven
-// rows of the previous segment rebuild the history first.  Such runs are rare:
-// the lane ORs those marks into one mask per band (a single 3-input logic op
-// per row) and queues (mask, band, segment); each warp measures its queued runs
-// exactly, 32 at a time, one per lane (sl_band_entry), which keeps the runs
-// that reach 8 inside the segment, so each run is measured once.
+// Every fourth row r (r = 3 mod 4) the AND of the match words of rows r-4 .. r
+// marks the diagonals pairing on those 5 rows: a run of >= 8 rows always covers
+// such a window, at the row ((start + 4) | 3) at the latest, so the marks catch
+// every run of 8 or more (plus some shorter ones).  Per band and row that is one
+// funnel shift and 3/4 of a 3-input logic op; one row of the previous segment
+// gives the first window.  Marked diagonals are rare: the lane ORs the marks
+// into one mask per band and queues (mask, band, segment); each warp measures
+// its queued runs exactly, 32 at a time, one per lane (sl_band_entry), which
+// keeps the runs that start at rows 32s-4 .. 32s+27, the ones whose first tested
+// row lies in segment s, so each run is measured once.
 //
 // Cells outside a diagonal's counted range: rows below it read T outside
 // [0, n) (zero planes) or a row outside [0, n) (the zero plane 4), so they
@@ -893,14 +896,26 @@ __device__ void sl_band_entry(uint32_t mask, int d0, int s, int n, const uint2 *
         uint64_t R8 = X & (X >> 1);
         R8 &= R8 >> 2;
         R8 &= R8 >> 4;
-        // runs starting at bit b reach 8 at row R0 + b + 7, inside segment s for b in [25, 56]
-        uint64_t edges = R8 & ~(R8 << 1) & (((1ull << 32) - 1) << 25);
+        // segment s owns the runs of >= 8 that start at rows 32s-4 .. 32s+27 (bits 28 .. 59):
+        // the first tested row of such a run, ((start + 4) | 3), lies in segment s.  Runs
+        // starting at bits 57 .. 59 reach past the window when all their bits up to 63 pair.
+        const uint64_t starts = X & ~(X << 1) & (((1ull << 32) - 1) << 28);
+        uint64_t open_end = 0;
+#pragma unroll
+        for (int b = 57; b <= 59; b++)
+            if ((X >> b) == (~0ull >> b)) open_end |= 1ull << b;
+        uint64_t edges = starts & (R8 | open_end);
         while (edges) {
             const int b = __ffsll((long long)edges) - 1;
             edges &= edges - 1;
             const int a = R0 + b;  // first row of the run
             if (a > r_hi) continue;
-            int e = a + 7;         // last row known to pair
+            int e;                 // last row known to pair
+            if ((R8 >> b) & 1) {
+                e = a + 7;
+            } else {               // a run from bit b to bit 63 at least; shorter than 8 so far
+                e = R0 + 63;
+            }
             while (e < r_hi) {
                 const int p = e + 1, i = p + delta;
                 const int ws = p >> 5, wt = (i >> 5) + kSlGuardRows;
@@ -980,29 +995,32 @@ __device__ void sl_band_scan(const uint4 *__restrict__ E4, const int *__restrict
             // u + d0/32 + kEqGuard of the row's plane, words g, g+1 for band g, at bit offset t
             const uint32_t qa = (uint32_t)__cvta_generic_to_shared(E4 + (d0 / 32 + kEqGuard));
             const uint32_t pa = (uint32_t)__cvta_generic_to_shared(poffT + s * kSegPitch);
-            uint32_t m1[kBandGroup], a2h[kBandGroup][2], a4h[kBandGroup][4];
-#pragma unroll
-            for (int g = 0; g < kBandGroup; g++) {
-                m1[g] = 0;
-                a2h[g][0] = a2h[g][1] = 0;
-                a4h[g][0] = a4h[g][1] = a4h[g][2] = a4h[g][3] = 0;
-            }
-#pragma unroll
-            for (int k = 0; k < 39; k++) {
-                // steps 0..6: rows 25..31 of segment s-1 (the runs of 8 ending at rows 0..31
-                // of segment s start there at the earliest); steps 7..38: rows 0..31 of segment s
-                const int t = k < 7 ? k + 25 : k - 7;
-                const uint32_t pv = lds_u32(pa + 4 * (k < 7 ? t : kSegPitch + t));
+            // m4[g]: the match word of the row before the current 4-row block
+            uint32_t m4[kBandGroup];
+            {
+                const uint32_t pv = lds_u32(pa + 4 * 31);  // row 31 of segment s-1
                 const uint4 w = lds_v4(qa + pv);
 #pragma unroll
+                for (int g = 0; g < kBandGroup; g++) m4[g] = fshr(word_of(w, g), word_of(w, g + 1), 31);
+            }
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                // rows 4q .. 4q+3 of segment s; the 5 rows 4q-1 .. 4q+3 all pairing on a
+                // diagonal mark it
+                uint32_t mm[4][kBandGroup];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int t = 4 * q + u;
+                    const uint32_t pv = lds_u32(pa + 4 * (kSegPitch + t));
+                    const uint4 w = lds_v4(qa + pv);
+#pragma unroll
+                    for (int g = 0; g < kBandGroup; g++) mm[u][g] = fshr(word_of(w, g), word_of(w, g + 1), t);
+                }
+#pragma unroll
                 for (int g = 0; g < kBandGroup; g++) {
-                    const uint32_t m = fshr(word_of(w, g), word_of(w, g + 1), t);
-                    const uint32_t A2 = m & m1[g];
-                    const uint32_t A4 = A2 & a2h[g][k & 1];
-                    if (k >= 7) pend[g] |= A4 & a4h[g][k & 3];
-                    a2h[g][k & 1] = A2;
-                    a4h[g][k & 3] = A4;
-                    m1[g] = m;
+                    const uint32_t x = m4[g] & mm[0][g] & mm[1][g];
+                    pend[g] |= x & mm[2][g] & mm[3][g];
+                    m4[g] = mm[3][g];
                 }
             }
         }

@@ -75,6 +75,7 @@ struct SelSmem {
     int rc, fstart, fsize, cut, nfront, count, level, hyp;
     float ideal[kMaxObj], worst[kMaxObj], nadir[kMaxObj];
     float red[64 * kMaxObj];
+    float ext[kMaxObj * kMaxObj];  // extreme points while they are updated
 };
 
 // exclusive block scan of a 0/1 flag over kSelThreads threads; returns the
@@ -247,45 +248,72 @@ __global__ void __launch_bounds__(kSelThreads) k_select(Shape s, const float *__
     // ---------------- extreme points (findExtremePoints, :601-683), tree order of findMinValue
     {
         const int B = N2 + M;
+        for (int e = tid; e < M * M; e += nth) sm.ext[e] = ext[e];
+        __syncthreads();
+        auto value = [&](int t, int i, int &ix) {
+            if (t < f0) {
+                const int sol = sc.sorted[t];
+                ix = sol;
+                return asf_val(obj + (size_t)sol * M, sm.ideal, i, M);
+            }
+            if (t < f0 + M) {
+                ix = N2 + (t - f0);
+                return asf_val(sm.ext + (t - f0) * M, sm.ideal, i, M);
+            }
+            ix = -1;
+            return FLT_MAX;
+        };
+        // tbuf[t] < tbuf[u] replaces t by u (strict: the lower position keeps ties)
+        auto pair = [&](int t, int u) {
+            if (tbuf[u] < tbuf[t]) {
+                tbuf[t] = tbuf[u];
+                tix[t] = tix[u];
+            }
+        };
         for (int i = 0; i < M; i++) {
-            for (int t = tid; t < B; t += nth) {
-                float v = FLT_MAX;
-                int ix = -1;
-                if (t < f0) {
-                    int sol = sc.sorted[t];
-                    v = asf_val(obj + (size_t)sol * M, sm.ideal, i, M);
-                    ix = sol;
-                } else if (t < f0 + M) {
-                    v = asf_val(ext + (size_t)(t - f0) * M, sm.ideal, i, M);
-                    ix = N2 + (t - f0);
-                }
-                tbuf[t] = v;
-                tix[t] = ix;
+            // first level fused with the ASF values: position t against t + B/2
+            int h = B / 2;
+            for (int t = tid; t < h; t += nth) {
+                int i0, i1;
+                const float v0 = value(t, i, i0), v1 = value(t + h, i, i1);
+                tbuf[t] = v1 < v0 ? v1 : v0;
+                tix[t] = v1 < v0 ? i1 : i0;
             }
             __syncthreads();
-            for (int half = B / 2;; half /= 2) {
-                for (int t = tid; t < half; t += nth)
-                    if (tbuf[t + half] < tbuf[t]) {
-                        tbuf[t] = tbuf[t + half];
-                        tix[t] = tix[t + half];
+            // later levels; after an odd level its last position joins position 0,
+            // done by the thread that handles position 0 next; levels of at most 32
+            // pairs run in warp 0 alone
+            while (h > 1) {
+                const bool odd = h & 1;
+                const int hp = h - 1;
+                h >>= 1;
+                if (h > 32) {
+                    for (int t = tid; t < h; t += nth) {
+                        if (t == 0 && odd) pair(0, hp);
+                        pair(t, t + h);
                     }
-                __syncthreads();
-                if (half == 1) break;
-                if ((half & 1) && tid == 0 && tbuf[half - 1] < tbuf[0]) {
-                    tbuf[0] = tbuf[half - 1];
-                    tix[0] = tix[half - 1];
+                    __syncthreads();
+                } else if (warp == 0) {
+                    if (lane < h) {
+                        if (lane == 0 && odd) pair(0, hp);
+                        pair(lane, lane + h);
+                    }
+                    __syncwarp();
                 }
-                __syncthreads();
             }
             if (tid == 0) {
-                int sel = tix[0];
+                const int sel = tix[0];
                 float tmp[kMaxObj];
                 if (sel >= N2) {
-                    for (int k = 0; k < M; k++) tmp[k] = ext[(sel - N2) * M + k];
-                    for (int k = 0; k < M; k++) ext[i * M + k] = tmp[k];
+                    for (int k = 0; k < M; k++) tmp[k] = sm.ext[(sel - N2) * M + k];
                 } else if (sel >= 0) {
-                    for (int k = 0; k < M; k++) ext[i * M + k] = obj[(size_t)sel * M + k];
+                    for (int k = 0; k < M; k++) tmp[k] = obj[(size_t)sel * M + k];
                 }
+                if (sel >= 0)
+                    for (int k = 0; k < M; k++) {
+                        sm.ext[i * M + k] = tmp[k];
+                        ext[i * M + k] = tmp[k];
+                    }
             }
             __syncthreads();
         }
@@ -295,7 +323,7 @@ __global__ void __launch_bounds__(kSelThreads) k_select(Shape s, const float *__
     if (tid == 0) {
         float AB[kMaxObj][kMaxObj + 1], x[kMaxObj];
         for (int i = 0; i < M; i++) {
-            for (int j = 0; j < M; j++) AB[i][j] = ext[i * M + j];
+            for (int j = 0; j < M; j++) AB[i][j] = sm.ext[i * M + j];
             AB[i][M] = 1.0f;
         }
         for (int c = 0; c < M; c++) {
@@ -318,7 +346,7 @@ __global__ void __launch_bounds__(kSelThreads) k_select(Shape s, const float *__
         int exc = 0;
         for (int k = 0; k < M; k++) {
             float res = 0.0f;
-            for (int i = 0; i < M; i++) res = __fadd_rn(res, __fmul_rn(x[i], __fsub_rn(ext[k * M + i], sm.ideal[i])));
+            for (int i = 0; i < M; i++) res = __fadd_rn(res, __fmul_rn(x[i], __fsub_rn(sm.ext[k * M + i], sm.ideal[i])));
             if (fabsf(__fsub_rn(res, 1.0f)) > 1e-6f || isnan(res) || isinf(res)) exc = 1;
             float icp = __fdiv_rn(1.0f, x[k]);
             if (icp <= 1e-6f || isnan(icp) || isinf(icp)) exc = 1;
@@ -491,6 +519,9 @@ __global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc
     int *coff = nj + R;    // R + 1
     int *kq = coff + R + 1;
     int *lv = kq + R;      // Lsz: level histogram, then picks before each level
+    int *las = lv + Lsz;   // 2N: reference point of each last-front member (position count0 + t)
+    int *lsol = las + N2;  // 2N: the member itself
+    int *cand = lsol + N2; // 2N: candidate lists (CSR by reference point)
     const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarps = nth >> 5;
     const uint32_t gen = *d_gen;
     if (sc.info[3]) {  // fronts filled N exactly; k_select wrote the survivors
@@ -504,6 +535,10 @@ __global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc
         kq[j] = 0;
     }
     for (int l = tid; l < Lsz; l += nth) lv[l] = 0;
+    for (int t = count0 + tid; t < rc; t += nth) {
+        las[t - count0] = sc.assoc[t];
+        lsol[t - count0] = sc.sorted[t];
+    }
     if (tid == 0) sm.i0 = 0;
     __syncthreads();
     // CSR offsets of the candidate lists; level histogram (+1 at c_j, -1 at c_j + n_j)
@@ -529,12 +564,12 @@ __global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc
         for (int base = count0; base < rc; base += 32) {
             const int t = base + lane;
             const bool act = t < rc;
-            const int j = act ? sc.assoc[t] : -1 - lane;
+            const int j = act ? las[t - count0] : -1 - lane;
             const uint32_t peers = __match_any_sync(0xffffffffu, j);
             const int rank = __popc(peers & ((1u << lane) - 1u));
             const int f0v = act ? kq[j] : 0;
             __syncwarp();
-            if (act) sc.cand[coff[j] + f0v + rank] = sc.sorted[t];
+            if (act) cand[coff[j] + f0v + rank] = lsol[t - count0];
             __syncwarp();
             if (act && rank == 0) kq[j] = f0v + __popc(peers);
             __syncwarp();
@@ -589,7 +624,7 @@ __global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc
     }
     // each point draws its picks; the q-th pick ends at list position n_j - 1 - q
     for (int j = tid; j < R; j += nth) {
-        int *cl = sc.cand + coff[j];
+        int *cl = cand + coff[j];
         int nc = nj[j];
         for (int q = 0; q < kq[j]; q++) {
             const int level = cj[j] + q;
@@ -624,7 +659,7 @@ __global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc
             const uint32_t bal = __ballot_sync(0xffffffffu, act);
             const int rank = run + __popc(bal & ((1u << lane) - 1u));
             if (act && (l < Ls || rank < K))
-                surv[count0 + lv[l] + rank] = sc.cand[coff[j] + nj[j] - 1 - (l - cj[j])];
+                surv[count0 + lv[l] + rank] = cand[coff[j] + nj[j] - 1 - (l - cj[j])];
             run += __popc(bal);
         }
     }
@@ -634,7 +669,7 @@ __global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc
 
 size_t niche_smem_bytes(const Shape &s)
 {
-    return ((sizeof(SelSmem) + 15) & ~size_t(15)) + (size_t)(4 * s.R + 1 + 2 * s.N + 4) * sizeof(int);
+    return ((sizeof(SelSmem) + 15) & ~size_t(15)) + (size_t)(4 * s.R + 1 + 2 * s.N + 4 + 3 * 2 * s.N) * sizeof(int);
 }
 
 size_t select_smem_bytes(const Shape &s)
