@@ -831,16 +831,18 @@ __device__ void sl_scan(const uint2 *__restrict__ S, const uint32_t *__restrict_
 //     m_r = E_{s[r]} bits [r + delta0, r + delta0 + 32),
 // at bit offset r mod 32, a constant of the unrolled step; one 16-byte load of
 // four consecutive plane words gives the windows of all bands of the group.
-// Every fourth row r (r = 3 mod 4) the AND of the match words of rows r-4 .. r
-// marks the diagonals pairing on those 5 rows: a run of >= 8 rows always covers
-// such a window, at the row ((start + 4) | 3) at the latest, so the marks catch
-// every run of 8 or more (plus some shorter ones).  Per band and row that is one
-// funnel shift and 3/4 of a 3-input logic op; one row of the previous segment
-// gives the first window.  Marked diagonals are rare: the lane ORs the marks
-// into one mask per band and queues (mask, band, segment); each warp measures
-// its queued runs exactly, 32 at a time, one per lane (sl_band_entry), which
-// keeps the runs that start at rows 32s-4 .. 32s+27, the ones whose first tested
-// row lies in segment s, so each run is measured once.
+// The rows are cut into blocks: rows 29..31 of the previous segment, then
+// 3k..3k+2 (k = 0..9) and 30..31 of the segment.  The AND of two consecutive
+// blocks' match words marks the diagonals pairing on those 6 (or 5) rows.  Window
+// starts are never more than 3 rows apart, so a run of >= 8 rows always covers
+// one window, first the one starting at the run's start or within 2 rows after:
+// the marks catch every run of 8 or more (plus some shorter ones).  Per band and
+// row that is one funnel shift and 2/3 of a 3-input logic op.  Marked diagonals
+// are rare: the lane ORs the marks into one mask per band and queues (mask,
+// band, segment); each warp measures its queued runs exactly, 32 at a time, one
+// per lane (sl_band_entry), which keeps the runs that start at rows
+// 32s-4 .. 32s+27, the ones whose first covering window lies in segment s, so
+// each run is measured once.
 //
 // Cells outside a diagonal's counted range: rows below it read T outside
 // [0, n) (zero planes) or a row outside [0, n) (the zero plane 4), so they
@@ -897,8 +899,9 @@ __device__ void sl_band_entry(uint32_t mask, int d0, int s, int n, const uint2 *
         R8 &= R8 >> 2;
         R8 &= R8 >> 4;
         // segment s owns the runs of >= 8 that start at rows 32s-4 .. 32s+27 (bits 28 .. 59):
-        // the first tested row of such a run, ((start + 4) | 3), lies in segment s.  Runs
-        // starting at bits 57 .. 59 reach past the window when all their bits up to 63 pair.
+        // the first window covering such a run (window starts ... 32s-5 | 32s-3, 32s, ...,
+        // 32s+24, 32s+27 | 32s+29 ...) belongs to segment s.  Runs starting at bits 57 .. 59
+        // reach past the 64 rows when all their bits up to 63 pair.
         const uint64_t starts = X & ~(X << 1) & (((1ull << 32) - 1) << 28);
         uint64_t open_end = 0;
 #pragma unroll
@@ -995,32 +998,28 @@ __device__ void sl_band_scan(const uint4 *__restrict__ E4, const int *__restrict
             // u + d0/32 + kEqGuard of the row's plane, words g, g+1 for band g, at bit offset t
             const uint32_t qa = (uint32_t)__cvta_generic_to_shared(E4 + (d0 / 32 + kEqGuard));
             const uint32_t pa = (uint32_t)__cvta_generic_to_shared(poffT + s * kSegPitch);
-            // m4[g]: the match word of the row before the current 4-row block
-            uint32_t m4[kBandGroup];
-            {
-                const uint32_t pv = lds_u32(pa + 4 * 31);  // row 31 of segment s-1
-                const uint4 w = lds_v4(qa + pv);
+            // blocks of rows: 29..31 of segment s-1, then 3k..3k+2 (k = 0..9) and 30..31
+            // of segment s; two consecutive blocks pairing on a diagonal mark it
+            uint32_t bprev[kBandGroup];
 #pragma unroll
-                for (int g = 0; g < kBandGroup; g++) m4[g] = fshr(word_of(w, g), word_of(w, g + 1), 31);
-            }
+            for (int k = -1; k <= 10; k++) {
+                const int r0 = k < 0 ? 29 : 3 * k, nr = k == 10 ? 2 : 3;
+                uint32_t b[kBandGroup];
 #pragma unroll
-            for (int q = 0; q < 8; q++) {
-                // rows 4q .. 4q+3 of segment s; the 5 rows 4q-1 .. 4q+3 all pairing on a
-                // diagonal mark it
-                uint32_t mm[4][kBandGroup];
-#pragma unroll
-                for (int u = 0; u < 4; u++) {
-                    const int t = 4 * q + u;
-                    const uint32_t pv = lds_u32(pa + 4 * (kSegPitch + t));
+                for (int u = 0; u < nr; u++) {
+                    const int t = r0 + u;
+                    const uint32_t pv = lds_u32(pa + 4 * (k < 0 ? t : kSegPitch + t));
                     const uint4 w = lds_v4(qa + pv);
 #pragma unroll
-                    for (int g = 0; g < kBandGroup; g++) mm[u][g] = fshr(word_of(w, g), word_of(w, g + 1), t);
+                    for (int g = 0; g < kBandGroup; g++) {
+                        const uint32_t m = fshr(word_of(w, g), word_of(w, g + 1), t);
+                        b[g] = u == 0 ? m : (b[g] & m);
+                    }
                 }
 #pragma unroll
                 for (int g = 0; g < kBandGroup; g++) {
-                    const uint32_t x = m4[g] & mm[0][g] & mm[1][g];
-                    pend[g] |= x & mm[2][g] & mm[3][g];
-                    m4[g] = mm[3][g];
+                    if (k >= 0) pend[g] |= bprev[g] & b[g];
+                    bprev[g] = b[g];
                 }
             }
         }
