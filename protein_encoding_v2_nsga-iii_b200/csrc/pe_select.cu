@@ -522,6 +522,8 @@ __global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc
     int *las = lv + Lsz;   // 2N: reference point of each last-front member (position count0 + t)
     int *lsol = las + N2;  // 2N: the member itself
     int *cand = lsol + N2; // 2N: candidate lists (CSR by reference point)
+    int *pofs = cand + N2; // R + 1: first pick of each point
+    uint32_t *rnd = reinterpret_cast<uint32_t *>(pofs + R + 1);  // N: the raw draw of every pick
     const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarps = nth >> 5;
     const uint32_t gen = *d_gen;
     if (sc.info[3]) {  // fronts filled N exactly; k_select wrote the survivors
@@ -622,7 +624,32 @@ __global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc
         if (tid == 0) sm.i0 += tot;
         __syncthreads();
     }
-    // each point draws its picks; the q-th pick ends at list position n_j - 1 - q
+    // the raw draws of all picks, computed in parallel (each is keyed by its point and level)
+    if (tid == 0) sm.i0 = 0;
+    __syncthreads();
+    for (int base = 0; base < R; base += nth) {
+        const int j = base + tid;
+        int tot;
+        const int pos = sm.i0 + block_scan_value(j < R ? kq[j] : 0, sm, &tot);
+        if (j < R) pofs[j] = pos;
+        __syncthreads();
+        if (tid == 0) sm.i0 += tot;
+        __syncthreads();
+    }
+    if (tid == 0) pofs[R] = sm.i0;
+    __syncthreads();
+    for (int pk = tid; pk < pofs[R]; pk += nth) {
+        int lo = 0, hi = R - 1;  // point: pofs[lo] <= pk < pofs[lo + 1]
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (pofs[mid] <= pk) lo = mid;
+            else hi = mid - 1;
+        }
+        const int level = cj[lo] + (pk - pofs[lo]);
+        rnd[pk] = level == 0 ? 0u : draw(s.seed, TAG_NICHE, gen, (uint32_t)lo, (uint32_t)level, 0);
+    }
+    __syncthreads();
+    // each point takes its picks; the q-th pick ends at list position n_j - 1 - q
     for (int j = tid; j < R; j += nth) {
         int *cl = cand + coff[j];
         int nc = nj[j];
@@ -639,7 +666,7 @@ __global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc
                     }
                 }
             } else {
-                slot = (int)rng_uint(draw(s.seed, TAG_NICHE, gen, (uint32_t)j, (uint32_t)level, 0), (uint32_t)nc);
+                slot = (int)rng_uint(rnd[pofs[j] + q], (uint32_t)nc);
             }
             const int pick = cl[slot];
             cl[slot] = cl[nc - 1];
@@ -669,7 +696,8 @@ __global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc
 
 size_t niche_smem_bytes(const Shape &s)
 {
-    return ((sizeof(SelSmem) + 15) & ~size_t(15)) + (size_t)(4 * s.R + 1 + 2 * s.N + 4 + 3 * 2 * s.N) * sizeof(int);
+    return ((sizeof(SelSmem) + 15) & ~size_t(15)) +
+           (size_t)(4 * s.R + 1 + 2 * s.N + 4 + 3 * 2 * s.N + s.R + 1 + s.N) * sizeof(int);
 }
 
 size_t select_smem_bytes(const Shape &s)
