@@ -64,14 +64,16 @@ def set_workload(shape: str | None, six: bool):
 METRIC = "generations/s"
 L2_FLUSH_BYTES = 256 << 20
 # k_sl at this workload, from ncu captures of one launch (profiles/k_sl_L1000_m8_N1024.md):
-# ALU-pipe warp instructions, all thread instructions and DRAM bytes per launch; the ALU
-# pipe's peak (sm__inst_executed_pipe_alu.avg.peak_sustained) and its utilisation
-SL_ALU_WARP_INST_PER_LAUNCH = 240743253
-SL_THREAD_INST_PER_LAUNCH = 10823598092
-SL_DRAM_BYTES_PER_LAUNCH = 6364928
-SL_ALU_PIPE_PCT_NCU = 74.06
+# shared-memory data-pipe wavefronts (the binding unit: 76 % of its peak of 1 per SM per
+# clock), ALU-pipe warp instructions (61 % of 2 per SM per clock), thread instructions and
+# DRAM bytes per launch
+SL_SMEM_WAVEFRONTS_PER_LAUNCH = 110211502
+SL_ALU_WARP_INST_PER_LAUNCH = 155447588
+SL_THREAD_INST_PER_LAUNCH = 8194283402
+SL_DRAM_BYTES_PER_LAUNCH = 6365952
+SL_SMEM_PCT_NCU, SL_ALU_PIPE_PCT_NCU = 76.36, 61.44
+SM_COUNT, SMEM_WAVEFRONTS_PER_SM_CLK, ALU_WARP_INST_PER_SM_CLK = 148, 1, 2
 SL_CELLS_PER_LAUNCH = 36827144192      # 1024 x 8 CDSs of 3003 nucleotides
-SM_COUNT, ALU_WARP_INST_PER_SM_CLK = 148, 2
 # kernels one generation launches (one CUDA graph replay): k_variation, k_sl, k_dominance,
 # k_select, k_assoc, k_niche
 KERNELS_PER_GENERATION = 6
@@ -93,23 +95,26 @@ def hairpin_cells_per_cds(n: int) -> int:
 
 
 def roofline(cells: int, sl_seconds: float, clocks: dict) -> dict:
-    """Integer-pipe roofline of the stem scan, the binding unit (bit-logic and shifts
-    on the ALU pipe): achieved = ALU-pipe warp instructions per launch (ncu) / the
-    launch time measured here; peak = 2 ALU warp instructions per SM per clock x 148
-    SMs x the SM clock sampled during the timed region."""
-    # the ncu count is for the default shape; other shapes scale it by counted cells
-    alu_inst = SL_ALU_WARP_INST_PER_LAUNCH * cells / SL_CELLS_PER_LAUNCH
-    achieved = alu_inst / sl_seconds / 1e9
+    """Roofline of the stem scan on its binding unit, the shared-memory data pipe (table
+    loads of the band scan): achieved = wavefronts per launch (ncu) / the launch time
+    measured here; peak = 1 wavefront per SM per clock x 148 SMs x the SM clock sampled
+    during the timed region.  The ALU pipe (2 warp instructions per SM per clock) is
+    reported beside it."""
+    scale = cells / SL_CELLS_PER_LAUNCH   # the ncu counts are for the default shape
     mhz = clocks.get("sm_mhz") or 1965.0
-    peak = SM_COUNT * ALU_WARP_INST_PER_SM_CLK * mhz * 1e6 / 1e9
-    return {"bound": "alu", "kernel": "k_sl (hairpin-stem scan)", "unit": "G ALU warp-inst/s", "achieved": achieved,
-            "peak": peak, "frac": achieved / peak, "traffic": SL_DRAM_BYTES_PER_LAUNCH,
-            "peak_source": "ALU pipe 2 warp-inst/SM/clk (ncu peak_sustained) x 148 SMs at the sampled SM clock; "
-                           "MEASURED_PEAKS.json has no integer peak",
-            "algorithmic_bytes_per_launch": SL_DRAM_BYTES_PER_LAUNCH,
+    achieved = SL_SMEM_WAVEFRONTS_PER_LAUNCH * scale / sl_seconds / 1e9
+    peak = SM_COUNT * SMEM_WAVEFRONTS_PER_SM_CLK * mhz * 1e6 / 1e9
+    alu = SL_ALU_WARP_INST_PER_LAUNCH * scale / sl_seconds / 1e9
+    alu_peak = SM_COUNT * ALU_WARP_INST_PER_SM_CLK * mhz * 1e6 / 1e9
+    return {"bound": "smem", "kernel": "k_sl (hairpin-stem scan)", "unit": "G wavefronts/s", "achieved": achieved,
+            "peak": peak, "frac": achieved / peak, "traffic": SL_DRAM_BYTES_PER_LAUNCH * scale,
+            "peak_source": "shared-memory data pipe 1 wavefront/SM/clk (ncu peak_sustained) x 148 SMs at the "
+                           "sampled SM clock; MEASURED_PEAKS.json has no integer or shared-memory peak",
+            "alu": {"achieved": alu, "peak": alu_peak, "frac": alu / alu_peak, "unit": "G ALU warp-inst/s"},
+            "algorithmic_bytes_per_launch": SL_DRAM_BYTES_PER_LAUNCH * scale,
             "cells_per_launch": cells, "cells_per_s": cells / sl_seconds,
             "lane_ops_per_cell": SL_THREAD_INST_PER_LAUNCH / SL_CELLS_PER_LAUNCH,
-            "alu_pipe_pct_of_peak_ncu": SL_ALU_PIPE_PCT_NCU,
+            "ncu_pct_of_peak": {"smem_wavefronts": SL_SMEM_PCT_NCU, "alu_pipe": SL_ALU_PIPE_PCT_NCU},
             "instruction_count": "ncu, L=1000 m=8 N=1024" + ("" if cells == SL_CELLS_PER_LAUNCH else "; scaled by cells")}
 
 
