@@ -26,6 +26,7 @@ enum { MODE_INIT = 0, MODE_EVAL = 1, MODE_MUTATE = 2 };
 // small per-CTA copies of the codon tables
 struct SmemTab {
     uint8_t nt[64][4];
+    uint8_t pat[64];  // the codon's three nucleotides as plane bits: lo bits 0..2, hi bits 4..6
     int64_t lw[64];
     uint8_t wzero[64];
     uint8_t gc3[64];
@@ -39,6 +40,9 @@ __device__ __forceinline__ void load_tab(SmemTab &st, const DevTables *gt, int t
 {
     for (int i = tid; i < 64; i += nth) {
         *(uint32_t *)st.nt[i] = *(const uint32_t *)gt->nt[i];
+        uint32_t pt = 0;
+        for (int b = 0; b < 3; b++) pt |= ((gt->nt[i][b] & 1u) << b) | ((gt->nt[i][b] >> 1) << (4 + b));
+        st.pat[i] = (uint8_t)pt;
         st.lw[i] = gt->lw[i];
         st.wzero[i] = gt->wzero[i];
         st.gc3[i] = gt->gc3[i];
@@ -60,23 +64,22 @@ __device__ __forceinline__ int nt_at(const SmemTab &st, const uint8_t *row, int 
 // bit b of word w holds nucleotide 32w+b (A=00, C=01, G=10, U=11).
 __device__ void pack_planes(const Shape &s, const SmemTab &st, const uint8_t *ids, uint2 *planes, int tid, int nth)
 {
+    // word w holds nucleotides 32w .. 32w+31: the codons a0 = floor(32w/3) .. that
+    // overlap it contribute their 3-bit patterns at bit offset 3a - 32w
     const int total = s.m * s.Wp;
     for (int e = tid; e < total; e += nth) {
         int c = e / s.Wp, w = e - c * s.Wp;
         uint32_t lo = 0, hi = 0;
         if (w < s.W) {
             const uint8_t *row = ids + c * s.Lp;
-            int base = 32 * w;
-            int a = base / 3, b = base - 3 * a;
-            int lim = min(32, s.n - base);
-            for (int i = 0; i < lim; i++) {
-                uint32_t code = st.nt[row[a]][b];
-                lo |= (code & 1u) << i;
-                hi |= (code >> 1) << i;
-                if (++b == 3) {
-                    b = 0;
-                    a++;
-                }
+            const int base = 32 * w;
+            const int a0 = base / 3, a1 = min((base + 31) / 3, s.L - 1);
+            for (int a = a0; a <= a1; a++) {
+                const uint32_t pt = st.pat[row[a]];
+                const int off = 3 * a - base;  // -2 .. 31
+                const uint32_t l3 = pt & 7u, h3 = (pt >> 4) & 7u;
+                lo |= off >= 0 ? (l3 << off) : (l3 >> -off);
+                hi |= off >= 0 ? (h3 << off) : (h3 >> -off);
             }
         }
         planes[e] = make_uint2(lo, hi);
