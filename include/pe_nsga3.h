@@ -76,6 +76,10 @@ typedef struct pe_config {
     int32_t stream_priority;/* priority of the stream pe_create makes when given none:
                                0 = default, lower = more urgent (clamped to the
                                device's range); no counterpart in the reference */
+    int32_t sl_threads;     /* hairpin-scan CTA size: 64, 128 or 256, or 0 to let
+                               pe_init_population time the three on the initial
+                               population and keep the fastest (results do not
+                               depend on it); no counterpart in the reference */
 } pe_config;
 
 typedef struct pe_info {
@@ -84,6 +88,7 @@ typedef struct pe_info {
     uint32_t generation;    /* generations completed */
     int32_t initialized;
     uint64_t device_bytes;  /* device memory held by the instance (512 B granules) */
+    int32_t sl_threads;     /* hairpin-scan CTA size in use */
 } pe_info;
 
 typedef struct pe_select_info {
@@ -108,7 +113,9 @@ int pe_get_info(const pe_instance *inst, pe_info *info);
 int pe_instance_bytes(const pe_config *cfg, int32_t aa_len, uint64_t *bytes);
 
 /* --- initializationKernel (src/main.cu:26-119): N random solutions (solution 0
- *     = highest-weight codons), evaluated; extreme points seeded. */
+ *     = highest-weight codons), evaluated; extreme points seeded.  With
+ *     cfg.sl_threads = 0 the first call also picks the hairpin-scan CTA size by
+ *     timing (a few extra scans of the initial population). */
 int pe_init_population(pe_instance *inst);
 
 /* --- the generation loop (src/main.cu:708-728): mutationKernel + sortingKernel,

@@ -76,13 +76,13 @@ class CodonTable(C.Structure):
 class Config(C.Structure):
     _fields_ = [("n_cds", C.c_int32), ("pop_size", C.c_int32), ("mutation_prob", C.c_float),
                 ("objectives", C.c_int32), ("gc_mode", C.c_int32), ("ref_p", C.c_int32), ("seed", C.c_uint64),
-                ("stream_priority", C.c_int32)]
+                ("stream_priority", C.c_int32), ("sl_threads", C.c_int32)]
 
 
 class Info(C.Structure):
     _fields_ = [("L", C.c_int32), ("m", C.c_int32), ("N", C.c_int32), ("M", C.c_int32), ("R", C.c_int32),
                 ("p", C.c_int32), ("generation", C.c_uint32), ("initialized", C.c_int32),
-                ("device_bytes", C.c_uint64)]
+                ("device_bytes", C.c_uint64), ("sl_threads", C.c_int32)]
 
 
 class SelectInfo(C.Structure):
@@ -215,10 +215,10 @@ class Engine:
 
     def __init__(self, aa, table: CodonTable, n_cds: int, pop_size: int, mutation_prob: float,
                  objectives: int = OBJ_BASE4, gc_mode: int = GC3, ref_p: int = 0, seed: int = 0, stream=None,
-                 stream_priority: int = 0):
+                 stream_priority: int = 0, sl_threads: int = 0):
         self.aa = np.ascontiguousarray(aa, np.int8)
         self.table = table
-        cfg = Config(n_cds, pop_size, mutation_prob, objectives, gc_mode, ref_p, seed, stream_priority)
+        cfg = Config(n_cds, pop_size, mutation_prob, objectives, gc_mode, ref_p, seed, stream_priority, sl_threads)
         h = C.c_void_p()
         _ck(lib().pe_create(C.byref(cfg), _ptr(self.aa), len(self.aa), C.byref(table),
                             None if stream is None else C.c_void_p(stream), C.byref(h)))
@@ -250,6 +250,13 @@ class Engine:
         info = Info()
         _ck(lib().pe_get_info(self._h, C.byref(info)))
         return info.generation
+
+    @property
+    def sl_threads(self) -> int:
+        """Hairpin-scan CTA size in use (picked by timing at init unless forced)."""
+        info = Info()
+        _ck(lib().pe_get_info(self._h, C.byref(info)))
+        return info.sl_threads
 
     def init(self):
         _ck(lib().pe_init_population(self._h))

@@ -319,6 +319,8 @@ int pe_create(const pe_config *cfg, const int8_t *aa_idx, int32_t aa_len, const 
         return fail(PE_ERR_ARG, "mutation_prob must be in [0,1]");
     if (cfg->objectives != PE_OBJ_REF6 && cfg->objectives != PE_OBJ_BASE4) return fail(PE_ERR_ARG, "bad objective set");
     if (cfg->gc_mode != PE_GC3 && cfg->gc_mode != PE_GC_ALL) return fail(PE_ERR_ARG, "bad gc mode");
+    if (cfg->sl_threads != 0 && cfg->sl_threads != 64 && cfg->sl_threads != 128 && cfg->sl_threads != 256)
+        return fail(PE_ERR_ARG, "sl_threads must be 0, 64, 128 or 256, got %d", cfg->sl_threads);
     // table validation
     {
         int expect = 0;
@@ -353,6 +355,7 @@ int pe_create(const pe_config *cfg, const int8_t *aa_idx, int32_t aa_len, const 
     s.K = (s.n - 4) / 2;
     s.pm = cfg->mutation_prob;
     s.seed = cfg->seed;
+    s.sl_threads = cfg->sl_threads;
     {
         static const int ref6[6] = {K_CAI, K_CBP, K_HSC, K_HD, K_GC, K_SL};
         static const int base4[4] = {K_CAI, K_HD, K_GC, K_SL};
@@ -700,14 +703,52 @@ int pe_get_info(const pe_instance *in, pe_info *info)
     info->generation = in->generation;
     info->initialized = in->initialized;
     info->device_bytes = in->alloc_bytes;
+    info->sl_threads = in->s.sl_threads > 0 ? in->s.sl_threads : 128;
     return PE_OK;
 }
 
 int pe_init_population(pe_instance *in)
 {
     if (!in) return fail(PE_ERR_ARG, "null instance");
-    const Shape &s = in->s;
+    Shape &s = in->s;
     CK(launch_init(s, in->d_tab, in->d_aa, in->buf[0], in->d_surv, in->stream));
+    if (in->cfg.sl_threads == 0 && s.sl_threads == 0) {
+        // pick the hairpin-scan CTA size: time a warm scan of the initial population
+        // with each size (they all give the same result) and keep the fastest
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        CK(cudaEventCreate(&e0));
+        if (cudaEventCreate(&e1) != cudaSuccess) {
+            cudaEventDestroy(e0);
+            return fail(PE_ERR_CUDA, "event creation failed");
+        }
+        const int sizes[3] = {64, 128, 256};
+        float best_ms = 0.0f;
+        int best = 128;
+        cudaError_t e = cudaSuccess;
+        for (int k = 0; k < 3 && e == cudaSuccess; k++) {
+            s.sl_threads = sizes[k];
+            float ms = 0.0f;
+            e = launch_sl(s, in->buf[0], 0, s.N, in->d_part, in->d_counter, in->d_status, in->stream);
+            if (e == cudaSuccess) e = cudaEventRecord(e0, in->stream);
+            if (e == cudaSuccess) e = launch_sl(s, in->buf[0], 0, s.N, in->d_part, in->d_counter, in->d_status, in->stream);
+            if (e == cudaSuccess) e = cudaEventRecord(e1, in->stream);
+            if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+            if (e == cudaSuccess && (k == 0 || ms < best_ms)) {
+                best_ms = ms;
+                best = sizes[k];
+            }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        s.sl_threads = best;
+        if (e != cudaSuccess) return fail(PE_ERR_CUDA, "hairpin-scan tuning: %s", cudaGetErrorString(e));
+        for (int i = 0; i < 2; i++)
+            if (in->graph[i]) {
+                cudaGraphExecDestroy(in->graph[i]);
+                in->graph[i] = nullptr;
+            }
+    }
     CK(launch_sl(s, in->buf[0], 0, s.N, in->d_part, in->d_counter, in->d_status, in->stream));
     // extreme points start as the objective vectors of solutions 0..M-1
     // (initializationKernel, src/main.cu:106-109)

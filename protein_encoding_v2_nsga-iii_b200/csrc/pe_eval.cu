@@ -1071,10 +1071,10 @@ __device__ __forceinline__ void pair_reduce(int &best, int &bestd, int ob, int o
     }
 }
 
-struct SlSmem {
-    int2 queue[kSlThreads / 32][kBandQueue];  // band-scan items waiting for exact measurement
-    int wbest[kSlThreads / 32];
-    int wbestd[kSlThreads / 32];
+template <int NT> struct SlSmem {
+    int2 queue[NT / 32][kBandQueue];  // band-scan items waiting for exact measurement
+    int wbest[NT / 32];
+    int wbestd[NT / 32];
     int last;
     int res[3];
     int next_chunk;
@@ -1087,14 +1087,15 @@ __device__ __forceinline__ int plane_nt(const uint2 *P, int x)
     return (int)(((w.x >> b) & 1u) | (((w.y >> b) & 1u) << 1));
 }
 
-__global__ void __launch_bounds__(kSlThreads) k_sl(Shape s, PopBuf buf, int base, int2 *part, int32_t *counter,
+template <int NT>
+__global__ void __launch_bounds__(NT) k_sl(Shape s, PopBuf buf, int base, int2 *part, int32_t *counter,
                                                  int32_t *status)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    SlSmem &sm = *reinterpret_cast<SlSmem *>(smem_raw);
+    SlSmem<NT> &sm = *reinterpret_cast<SlSmem<NT> *>(smem_raw);
     const int G = kSlGuardRows;
     const int W = s.W, n = s.n;
-    uint2 *S = reinterpret_cast<uint2 *>(smem_raw + ((sizeof(SlSmem) + 15) & ~size_t(15)));  // W + 2
+    uint2 *S = reinterpret_cast<uint2 *>(smem_raw + ((sizeof(SlSmem<NT>) + 15) & ~size_t(15)));  // W + 2
     uint32_t *Tlo = reinterpret_cast<uint32_t *>(S + (W + 2));                               // W + 2G + 1
     uint32_t *Thi = Tlo + (W + 2 * G + 1);
     unsigned char *tab = reinterpret_cast<unsigned char *>(Thi + (W + 2 * G + 1));
@@ -1351,10 +1352,10 @@ __global__ void __launch_bounds__(kSlThreads) k_sl(Shape s, PopBuf buf, int base
     }
 }
 
-size_t sl_smem_bytes(const Shape &s)
+static size_t sl_smem_bytes_nt(const Shape &s, size_t head)
 {
     const int G = kSlGuardRows, W = s.W;
-    size_t b = (sizeof(SlSmem) + 15) & ~size_t(15);
+    size_t b = (head + 15) & ~size_t(15);
     b += (size_t)(W + 2) * sizeof(uint2);
     b += 2 * (size_t)(W + 2 * G + 1) * sizeof(uint32_t);
     b += 16;  // alignment of the band-scan tables
@@ -1364,15 +1365,28 @@ size_t sl_smem_bytes(const Shape &s)
     return b;
 }
 
+size_t sl_smem_bytes(const Shape &s) { return sl_smem_bytes_nt(s, sizeof(SlSmem<kSlThreadsMax>)); }
+
+template <int NT>
+static cudaError_t launch_sl_nt(const Shape &s, PopBuf buf, int base, int count, int2 *part, int32_t *counter,
+                                int32_t *status, cudaStream_t st)
+{
+    const size_t smem = sl_smem_bytes_nt(s, sizeof(SlSmem<NT>));
+    cudaError_t e = raise_smem_limit((const void *)k_sl<NT>, smem);
+    if (e != cudaSuccess) return e;
+    k_sl<NT><<<count * s.m, NT, smem, st>>>(s, buf, base, part, counter, status);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_sl(const Shape &s, PopBuf buf, int base, int count, int2 *part, int32_t *counter, int32_t *status,
                       cudaStream_t st)
 {
     if (count <= 0) return cudaSuccess;
-    size_t smem = sl_smem_bytes(s);
-    cudaError_t e = raise_smem_limit((const void *)k_sl, smem);
-    if (e != cudaSuccess) return e;
-    k_sl<<<count * s.m, kSlThreads, smem, st>>>(s, buf, base, part, counter, status);
-    return cudaGetLastError();
+    switch (s.sl_threads) {
+    case 64: return launch_sl_nt<64>(s, buf, base, count, part, counter, status, st);
+    case 256: return launch_sl_nt<256>(s, buf, base, count, part, counter, status, st);
+    default: return launch_sl_nt<128>(s, buf, base, count, part, counter, status, st);
+    }
 }
 
 }  // namespace pe

@@ -13,7 +13,7 @@ enum Kind { K_CAI = 0, K_CBP = 1, K_HSC = 2, K_HD = 3, K_GC = 4, K_SL = 5 };
 
 constexpr int kMaxObj = 6;
 constexpr int kMaxCds = 64;          // objidx stores CDS indices as int8
-constexpr int kSlThreads = 128;      // SL scan CTA (4 warps: less idle time at the end of a CDS)
+constexpr int kSlThreadsMax = 256;   // largest stem-scan CTA (sizes 64, 128, 256)
 constexpr int kVarThreads = 256;     // variation / light-eval CTA
 constexpr int kSelThreads = 1024;    // selection CTA
 constexpr int kSlGuardRows = 8;      // zero guard rows around the shifted T copies
@@ -37,6 +37,7 @@ struct Shape {
     float pm;
     uint64_t seed;
     int slot[6];  // slot of each Kind or -1
+    int sl_threads;  // stem-scan CTA size (64, 128 or 256; 0 = 128), picked per instance by timing
 };
 
 // Device-resident tables derived from pe_codon_table.

@@ -83,3 +83,19 @@ def test_stem_near_every_edge(pe, orc, gpu):
         ids[:, :, aa == K] = aaa
         ids[:, :, aa == F] = uuu
         check(pe, orc, aa, tabc, ids)
+
+
+def test_cta_size_does_not_change_results(pe, gpu):
+    """The hairpin-scan CTA size (forced, or picked by timing at init) changes speed only."""
+    aa = pe.synthetic_protein(400, 12)
+    tab = pe.dirichlet_table(12)
+    pops = []
+    for nt in (0, 64, 128, 256):
+        with pe.Engine(aa, tab, 4, 96, 0.05, seed=12, sl_threads=nt) as e:
+            e.init()
+            assert e.sl_threads in (64, 128, 256) and (nt == 0 or e.sl_threads == nt)
+            e.step(4)
+            pops.append(e.population())
+    for p in pops[1:]:
+        for x, y in zip(p, pops[0]):
+            assert np.array_equal(np.asarray(x).view(np.uint8), np.asarray(y).view(np.uint8))

@@ -135,3 +135,8 @@ def test_instance_bytes_host(pe):
     assert pe.instance_bytes(1001, 8, 1024, pe.OBJ_REF6) > base          # R = 792 reference points
     with pytest.raises(pe.PeError):
         pe.instance_bytes(2, 8, 1024)
+
+
+def test_sl_threads_must_be_a_supported_size(pe):
+    with pytest.raises(pe.PeError):
+        pe.Engine(pe.synthetic_protein(40, 1), pe.dirichlet_table(1), 2, 8, 0.05, sl_threads=96)
