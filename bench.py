@@ -292,24 +292,31 @@ def run_ours(args, world, rank, local):
     cells = POP * M_CDS * hairpin_cells_per_cds(n_nt)
     sl_s = stage_ms[1] / 1000.0
 
+    # end-to-end through the public API with host buffers: every rank runs a design job of
+    # G_E2E generations on its GPU; the whole-job rate uses the slowest rank
+    G_E2E = 100
+    obj_host = np.zeros((2 * POP, M_OBJ), np.float32)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    e2 = pe.Engine(aa, table, M_CDS, POP, PM, objectives=OBJ_SET, ref_p=P_USE, seed=SEED + 7 + rank)
+    e2.init()
+    for _ in range(G_E2E):
+        e2.step(1)
+        e2.objectives(obj_host)                 # per-generation device->host read of the objective block
+    final = e2.population()
+    e2.close()
+    e2e_s = time.perf_counter() - t0
+    te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
+    e2e_s = float(te.item())
+    h2d = aa.nbytes + 4 * (64 * 4 + 61 * 61 + 12)
+    d2h = obj_host.nbytes + sum(a.nbytes for a in final) / G_E2E
+
     line = None
     if rank == 0:
-        # end-to-end through the public API with host buffers: a design job of G_E2E generations
-        G_E2E = 100
-        obj_host = np.zeros((2 * POP, M_OBJ), np.float32)
-        torch.cuda.synchronize(dev)
-        t0 = time.perf_counter()
-        e2 = pe.Engine(aa, table, M_CDS, POP, PM, objectives=OBJ_SET, ref_p=P_USE, seed=SEED + 7)
-        e2.init()
-        for _ in range(G_E2E):
-            e2.step(1)
-            e2.objectives(obj_host)                 # per-generation device->host read of the objective block
-        final = e2.population()
-        e2.close()
-        e2e_s = time.perf_counter() - t0
-        h2d = aa.nbytes + 4 * (64 * 4 + 61 * 61 + 12)
-        d2h = obj_host.nbytes + sum(a.nbytes for a in final) / G_E2E
-
         # CPU baseline: the oracle on this host, bounded sample (N=1 only)
         cpu = None
         if world == 1:
@@ -336,8 +343,9 @@ def run_ours(args, world, rank, local):
                                     "selection": stage_ms[2]}},
             "roofline": roofline(cells, sl_s, clocks),
             "clocks": clocks,
-            "e2e": {"value": G_E2E / e2e_s, "unit": "generations/s", "h2d_bytes_per_step": h2d / G_E2E,
-                    "d2h_bytes_per_step": d2h, "job": f"create + init + {G_E2E} generations + reads"},
+            "e2e": {"value": world * G_E2E / e2e_s, "unit": "generations/s", "h2d_bytes_per_step": world * h2d / G_E2E,
+                    "d2h_bytes_per_step": world * d2h,
+                    "job": f"per rank: create + init + {G_E2E} generations + reads; all ranks / slowest rank"},
             "gpu_launches": KERNELS_PER_GENERATION * args.steps,
             "wall_s": t_wall,
             "peaks_file": {k: peaks.get(k) for k in ("hbm_gbs", "bf16_tflops", "sm_max_mhz")},
