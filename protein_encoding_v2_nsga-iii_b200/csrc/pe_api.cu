@@ -9,6 +9,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -287,6 +288,31 @@ int build_graphs(pe_instance *in)
         if (e3 != cudaSuccess) return fail(PE_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e3));
     }
     return PE_OK;
+}
+
+// Hairpin-scan CTA sizes chosen at init, per (device, L, m, N): instances of a shape
+// already tuned in this process skip the timing.
+struct SlTuneKey {
+    int dev, L, m, N;
+    bool operator<(const SlTuneKey &o) const
+    {
+        return std::tie(dev, L, m, N) < std::tie(o.dev, o.L, o.m, o.N);
+    }
+};
+std::mutex g_tune_mu;
+std::map<SlTuneKey, int> g_tuned;
+
+int sl_tuned(const SlTuneKey &k)
+{
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tuned.find(k);
+    return it == g_tuned.end() ? 0 : it->second;
+}
+
+void sl_remember(const SlTuneKey &k, int threads)
+{
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tuned[k] = threads;
 }
 
 }  // namespace
@@ -712,44 +738,52 @@ int pe_init_population(pe_instance *in)
     if (!in) return fail(PE_ERR_ARG, "null instance");
     Shape &s = in->s;
     CK(launch_init(s, in->d_tab, in->d_aa, in->buf[0], in->d_surv, in->stream));
+    bool scanned = false;
     if (in->cfg.sl_threads == 0 && s.sl_threads == 0) {
-        // pick the hairpin-scan CTA size: time a warm scan of the initial population
-        // with each size (they all give the same result) and keep the fastest
-        cudaEvent_t e0 = nullptr, e1 = nullptr;
-        CK(cudaEventCreate(&e0));
-        if (cudaEventCreate(&e1) != cudaSuccess) {
-            cudaEventDestroy(e0);
-            return fail(PE_ERR_CUDA, "event creation failed");
-        }
-        const int sizes[3] = {64, 128, 256};
-        float best_ms = 0.0f;
-        int best = 128;
-        cudaError_t e = cudaSuccess;
-        for (int k = 0; k < 3 && e == cudaSuccess; k++) {
-            s.sl_threads = sizes[k];
-            float ms = 0.0f;
-            e = launch_sl(s, in->buf[0], 0, s.N, in->d_part, in->d_counter, in->d_status, in->stream);
-            if (e == cudaSuccess) e = cudaEventRecord(e0, in->stream);
+        const SlTuneKey key{in->device, s.L, s.m, s.N};
+        s.sl_threads = sl_tuned(key);
+        if (s.sl_threads == 0) {
+            // pick the hairpin-scan CTA size: after one warm scan of the initial population,
+            // time one scan with each size (they all give the same result) and keep the
+            // fastest; the choice is remembered for this shape on this device
+            cudaEvent_t ev[4] = {};
+            cudaError_t e = cudaSuccess;
+            for (int k = 0; k < 4 && e == cudaSuccess; k++) e = cudaEventCreate(&ev[k]);
+            const int sizes[3] = {64, 128, 256};
+            s.sl_threads = 128;
             if (e == cudaSuccess) e = launch_sl(s, in->buf[0], 0, s.N, in->d_part, in->d_counter, in->d_status, in->stream);
-            if (e == cudaSuccess) e = cudaEventRecord(e1, in->stream);
-            if (e == cudaSuccess) e = cudaEventSynchronize(e1);
-            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
-            if (e == cudaSuccess && (k == 0 || ms < best_ms)) {
-                best_ms = ms;
-                best = sizes[k];
+            for (int k = 0; k < 3 && e == cudaSuccess; k++) {
+                s.sl_threads = sizes[k];
+                e = cudaEventRecord(ev[k], in->stream);
+                if (e == cudaSuccess)
+                    e = launch_sl(s, in->buf[0], 0, s.N, in->d_part, in->d_counter, in->d_status, in->stream);
             }
+            if (e == cudaSuccess) e = cudaEventRecord(ev[3], in->stream);
+            if (e == cudaSuccess) e = cudaEventSynchronize(ev[3]);
+            float best_ms = 0.0f;
+            int best = 128;
+            for (int k = 0; k < 3 && e == cudaSuccess; k++) {
+                float ms = 0.0f;
+                e = cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
+                if (e == cudaSuccess && (k == 0 || ms < best_ms)) {
+                    best_ms = ms;
+                    best = sizes[k];
+                }
+            }
+            for (int k = 0; k < 4; k++)
+                if (ev[k]) cudaEventDestroy(ev[k]);
+            s.sl_threads = best;
+            if (e != cudaSuccess) return fail(PE_ERR_CUDA, "hairpin-scan tuning: %s", cudaGetErrorString(e));
+            sl_remember(key, best);
+            scanned = true;   // the timed scans left the initial population's stems in place
         }
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
-        s.sl_threads = best;
-        if (e != cudaSuccess) return fail(PE_ERR_CUDA, "hairpin-scan tuning: %s", cudaGetErrorString(e));
         for (int i = 0; i < 2; i++)
             if (in->graph[i]) {
                 cudaGraphExecDestroy(in->graph[i]);
                 in->graph[i] = nullptr;
             }
     }
-    CK(launch_sl(s, in->buf[0], 0, s.N, in->d_part, in->d_counter, in->d_status, in->stream));
+    if (!scanned) CK(launch_sl(s, in->buf[0], 0, s.N, in->d_part, in->d_counter, in->d_status, in->stream));
     // extreme points start as the objective vectors of solutions 0..M-1
     // (initializationKernel, src/main.cu:106-109)
     CK(cudaMemsetAsync(in->d_ext, 0, (size_t)s.M * s.M * sizeof(float), in->stream));
@@ -781,8 +815,7 @@ int pe_step(pe_instance *in, int32_t generations)
 int pe_synchronize(pe_instance *in)
 {
     if (!in) return fail(PE_ERR_ARG, "null instance");
-    CK(cudaStreamSynchronize(in->stream));
-    return check_status(in);
+    return check_status(in);   // queues the status read behind the stream's work and waits for it
 }
 
 int pe_get_population(pe_instance *in, uint8_t *codon_idx, float *obj, int8_t *objidx, int32_t *pql,
@@ -796,16 +829,27 @@ int pe_get_population(pe_instance *in, uint8_t *codon_idx, float *obj, int8_t *o
     const int nsol = in->generation == 0 ? s.N : 2 * s.N;
     if (codon_idx) {
         if (in->generation == 0) memset(codon_idx, 0, (size_t)2 * s.N * s.m * s.L);
-        CK(cudaMemcpy2DAsync(codon_idx, (size_t)s.L, b.ids, (size_t)s.Lp, (size_t)s.L, (size_t)nsol * s.m,
-                             cudaMemcpyDeviceToHost, in->stream));
+        // rows are padded to Lp on the device: pack them there (a pitched device copy),
+        // then make one contiguous copy to the host (a pitched copy into pageable host
+        // memory goes row by row and is several times slower).  The packed rows go to
+        // the codon ids of the other ping-pong buffer: between generations nothing
+        // reads it, and the next generation writes all of it before reading any.
+        const size_t rows = (size_t)nsol * s.m;
+        const uint8_t *src = b.ids;
+        if (s.Lp != s.L) {
+            uint8_t *packed = in->buf[1 - in->cur].ids;
+            CK(cudaMemcpy2DAsync(packed, (size_t)s.L, b.ids, (size_t)s.Lp, (size_t)s.L, rows, cudaMemcpyDeviceToDevice,
+                                 in->stream));
+            src = packed;
+        }
+        CK(cudaMemcpyAsync(codon_idx, src, rows * s.L, cudaMemcpyDeviceToHost, in->stream));
     }
     if (obj) CK(cudaMemcpyAsync(obj, b.obj, (size_t)2 * s.N * s.M * sizeof(float), cudaMemcpyDeviceToHost, in->stream));
     if (objidx) CK(cudaMemcpyAsync(objidx, b.objidx, (size_t)2 * s.N * 2 * s.M, cudaMemcpyDeviceToHost, in->stream));
     if (pql) CK(cudaMemcpyAsync(pql, b.pql, (size_t)2 * s.N * 3 * sizeof(int32_t), cudaMemcpyDeviceToHost, in->stream));
     if (survivors)
         CK(cudaMemcpyAsync(survivors, in->d_surv, (size_t)s.N * sizeof(int32_t), cudaMemcpyDeviceToHost, in->stream));
-    CK(cudaStreamSynchronize(in->stream));
-    return check_status(in);
+    return check_status(in);   // the status read queues behind the copies; one synchronisation
 }
 
 int pe_get_objectives(pe_instance *in, float *obj)
