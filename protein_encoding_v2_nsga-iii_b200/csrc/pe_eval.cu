@@ -836,14 +836,21 @@ __device__ void sl_scan(const uint2 *__restrict__ S, const uint32_t *__restrict_
 // four consecutive plane words gives the windows of all bands of the group.
 // The rows are cut into blocks: rows 29..31 of the previous segment, then
 // 3k..3k+2 (k = 0..9) and 30..31 of the segment.  The AND of two consecutive
-// blocks' match words marks the diagonals pairing on those 6 (or 5) rows.  Window
-// starts are never more than 3 rows apart, so a run of >= 8 rows always covers
-// one window, first the one starting at the run's start or within 2 rows after:
-// the marks catch every run of 8 or more (plus some shorter ones).  Per band and
-// row that is one funnel shift and 2/3 of a 3-input logic op.  Marked diagonals
-// are rare: the lane ORs the marks into one mask per band and queues (mask,
-// band, segment); each warp measures its queued runs exactly, 32 at a time, one
-// per lane (sl_band_entry), which keeps the runs that start at rows
+// blocks' match words gives the diagonals pairing on those 6 (or 5) rows: a
+// window.  Window starts are never more than 3 rows apart, so a run of >= 8 rows
+// always covers one window, first the one starting at the run's start or within
+// 2 rows after.  Such a run is longer than its 6-row window, so it also pairs on
+// the row just before or just after the window: a diagonal is marked when a
+// 6-row window and one of its two neighbouring rows pair (the row before the
+// first window, in the previous segment, is not needed: the runs this segment
+// owns that cover that window reach the row after it), and on the last, 5-row
+// window alone.  The marks catch every run of 8 or more; the neighbour test
+// drops the exact 6-row runs, two thirds of the shorter runs the windows alone
+// would mark.  Per band and row that is one funnel shift and 4/3 of a 3-input
+// logic op.  Marked diagonals are rare: the lane ORs the marks into one mask
+// per band and queues (mask, band, segment); each warp measures its queued
+// runs exactly, 32 at a time, one per lane (sl_band_entry), which keeps the
+// runs that start at rows
 // 32s-4 .. 32s+27, the ones whose first covering window lies in segment s, so
 // each run is measured once.
 //
@@ -855,7 +862,7 @@ __device__ void sl_scan(const uint2 *__restrict__ S, const uint32_t *__restrict_
 // shorter inside the range never win against it.
 constexpr int kBandGroup = 3;            // bands per item (one 4-word load)
 constexpr int kEqGuard = kBandGroup + 3; // guard words on each side of the equality planes
-constexpr int kSegPitch = 33;            // row-offset table: 32 rows per segment + 1 (bank spread)
+constexpr int kSegPitch = 17;            // row-entry table: 16 words (two rows each) per segment + 1 (bank spread)
 constexpr int kBandQueue = 64;
 
 __host__ __device__ __forceinline__ int sl_plane_stride(int W) { return (W + 2 * kEqGuard + 4 + 31) & ~31; }
@@ -998,30 +1005,47 @@ __device__ void sl_band_scan(const uint4 *__restrict__ E4, const int *__restrict
             sl_group_segments(n, d0, s_lo, s_hi);
             s = s_lo + (item - gstart[grp]);
             // E4 entry x holds T words x-kEqGuard .. x+3-kEqGuard; row 32u + t reads entry
-            // u + d0/32 + kEqGuard of the row's plane, words g, g+1 for band g, at bit offset t
+            // u + d0/32 + kEqGuard of the row's plane, words g, g+1 for band g, at bit offset t;
+            // the row-entry table gives the entry of two rows per 32-bit word
             const uint32_t qa = (uint32_t)__cvta_generic_to_shared(E4 + (d0 / 32 + kEqGuard));
             const uint32_t pa = (uint32_t)__cvta_generic_to_shared(poffT + s * kSegPitch);
             // blocks of rows: 29..31 of segment s-1, then 3k..3k+2 (k = 0..9) and 30..31
-            // of segment s; two consecutive blocks pairing on a diagonal mark it
-            uint32_t bprev[kBandGroup];
+            // of segment s; two consecutive blocks and a neighbouring row pairing on a
+            // diagonal mark it
+            uint32_t bprev[kBandGroup], win[kBandGroup], l1[kBandGroup], l2[kBandGroup];
+            uint32_t pw = 0;  // the table word holding the current row's entry (two rows per word)
 #pragma unroll
             for (int k = -1; k <= 10; k++) {
                 const int r0 = k < 0 ? 29 : 3 * k, nr = k == 10 ? 2 : 3;
-                uint32_t b[kBandGroup];
+                uint32_t b[kBandGroup], f[kBandGroup], l[kBandGroup];
 #pragma unroll
                 for (int u = 0; u < nr; u++) {
                     const int t = r0 + u;
-                    const uint32_t pv = lds_u32(pa + 4 * (k < 0 ? t : kSegPitch + t));
+                    if (k < 0 ? (t == 29 || t == 30) : (t & 1) == 0)
+                        pw = lds_u32(pa + 4 * ((k < 0 ? 0 : kSegPitch) + (t >> 1)));
+                    const uint32_t pv = ((t & 1) ? (pw >> 16) : (pw & 0xffffu)) * 16u;
                     const uint4 w = lds_v4(qa + pv);
 #pragma unroll
                     for (int g = 0; g < kBandGroup; g++) {
                         const uint32_t m = fshr(word_of(w, g), word_of(w, g + 1), t);
                         b[g] = u == 0 ? m : (b[g] & m);
+                        if (u == 0) f[g] = m;
+                        l[g] = m;
                     }
                 }
+                // window (k-2, k-1) closes with the first row of block k; window (k-1, k)
+                // opens with the last row of block k-2 (none for k = 0); the last window
+                // (rows 27..31) is kept as it is
 #pragma unroll
                 for (int g = 0; g < kBandGroup; g++) {
-                    if (k >= 0) pend[g] |= bprev[g] & b[g];
+                    if (k >= 1) pend[g] |= win[g] & f[g];
+                    if (k >= 0) {
+                        win[g] = bprev[g] & b[g];
+                        if (k == 10) pend[g] |= win[g];
+                        else if (k >= 1) pend[g] |= win[g] & l2[g];
+                    }
+                    l2[g] = l1[g];
+                    l1[g] = l[g];
                     bprev[g] = b[g];
                 }
             }
@@ -1172,7 +1196,9 @@ __global__ void __launch_bounds__(NT) k_sl(Shape s, PopBuf buf, int base, int2 *
     __syncthreads();
     // band-scan tables, in the space the shifted copies of T take later:
     //   E4[v][x]      E_v words x-kEqGuard .. x+3-kEqGuard, v = 0..3 nucleotides, 4 the zero plane
-    //   poffT[sp][t]  row r = 32(sp-1)+t: 16 (v(r)*PS + sp-1) bytes, v(r) = 4 outside [0, n); pitch 33
+    //   poffT[sp][i]  rows r = 32(sp-1)+2i, r+1: E4 entries v(r)*PS + sp-1 in the low and high
+    //                 16 bits (v(r) = 4 outside [0, n); 5*PS < 65536 since E4's 80*PS bytes fit in
+    //                 shared memory); pitch 17 words
     //   gstart[g]     first item of band group g (items: the group's 32-row segments)
     const int PS = sl_plane_stride(W), NSP = W + 2;
     const int ng = sl_num_groups(n), D0 = sl_band_base(n);
@@ -1185,9 +1211,10 @@ __global__ void __launch_bounds__(NT) k_sl(Shape s, PopBuf buf, int base, int2 *
                            eq_word(Tlo, Thi, W, n, v, x + 2), eq_word(Tlo, Thi, W, n, v, x + 3));
     }
     for (int e = tid; e < kSegPitch * NSP; e += nth) {
-        const int sp = e / kSegPitch, t = e - sp * kSegPitch, r = 32 * (sp - 1) + t;
-        const int v = (t < 32 && r >= 0 && r < n) ? plane_nt(S, r) : 4;
-        poffT[e] = (v * PS + (sp - 1)) * (int)sizeof(uint4);  // byte offset into E4
+        const int sp = e / kSegPitch, i = e - sp * kSegPitch, r = 32 * (sp - 1) + 2 * i;
+        const int v0 = (i < 16 && r >= 0 && r < n) ? plane_nt(S, r) : 4;
+        const int v1 = (i < 16 && r + 1 >= 0 && r + 1 < n) ? plane_nt(S, r + 1) : 4;
+        poffT[e] = (v0 * PS + (sp - 1)) | ((v1 * PS + (sp - 1)) << 16);  // E4 entries of rows r, r + 1
     }
     if (warp == 0) {
         int carry = 0;
