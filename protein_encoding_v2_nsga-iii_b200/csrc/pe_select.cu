@@ -69,6 +69,90 @@ __global__ void __launch_bounds__(256) k_dominance(Shape s, const float *__restr
     }
 }
 
+// Across the lanes of a warp, lane w holding v: the smallest (largest) value, the
+// lowest lane among equal ones -- what a loop over w = 0, 1, ... keeping the first
+// strictly better value returns (including which of -0 / +0).
+__device__ __forceinline__ float warp_first_min(float v, int lane)
+{
+    int w = lane;
+    for (int o = 16; o > 0; o >>= 1) {
+        const float u = __shfl_xor_sync(0xffffffffu, v, o);
+        const int x = __shfl_xor_sync(0xffffffffu, w, o);
+        if (u < v || (u == v && x < w)) {
+            v = u;
+            w = x;
+        }
+    }
+    return v;
+}
+__device__ __forceinline__ float warp_first_max(float v, int lane)
+{
+    int w = lane;
+    for (int o = 16; o > 0; o >>= 1) {
+        const float u = __shfl_xor_sync(0xffffffffu, v, o);
+        const int x = __shfl_xor_sync(0xffffffffu, w, o);
+        if (u > v || (u == v && x < w)) {
+            v = u;
+            w = x;
+        }
+    }
+    return v;
+}
+
+// Extreme points: the reference finds, for each axis, the lowest ASF value with a
+// tree reduction (findMinValue) over positions 0 .. B-1, B = 2N + M: front-0
+// solutions first, then the current extreme points, then FLT_MAX fillers.  Level 1
+// pairs position t with t + B/2; each later level, of h slots, pairs slot t with
+// t + h/2 (h even) or, for odd h, slot 0 first with slot h-1 and then with (h-1)/2;
+// a pair keeps its first slot on equal values.  So the winner is the lowest value,
+// and among equal values the position first in a fixed order: the order of the
+// merged lists, each merge listing its first slot, then (odd h) slot h-1, then the
+// other.  tree_key gives a position's place in that order, the choice made at
+// every level (0 first, 1 the odd slot, 2 the other), root level in the highest
+// bits; positions that level 1 leaves out (odd B) never win and get ~0.
+__device__ __forceinline__ uint64_t tree_key(int p, int B)
+{
+    int h = B >> 1;
+    if (p >= 2 * h) return ~0ull;
+    int slot = p < h ? p : p - h;
+    uint64_t key = p < h ? 0u : 2u;
+    int lvl = 1;
+    while (h > 1) {
+        const int hn = h >> 1;
+        uint64_t d;
+        if (slot < hn) {
+            d = 0;
+        } else if (slot < 2 * hn) {
+            d = 2;
+            slot -= hn;
+        } else {  // odd h: the last slot joins slot 0 before slot hn does
+            d = 1;
+            slot = 0;
+        }
+        key |= d << (2 * lvl);
+        lvl++;
+        h = hn;
+    }
+    return key;
+}
+
+// candidate of the extreme-point search: ASF value bits (values are >= +0, so their
+// bits order as the values do) and position (kNoPos: none yet).  Tree keys are only
+// needed between equal values, so they are computed then.
+constexpr uint32_t kNoPos = 0xffffffffu;
+static_assert(kSelThreads == 1024, "the selection CTA's cross-warp steps use one lane per warp");
+struct ExtCand {
+    uint32_t v;
+    uint32_t pos;
+};
+
+__device__ __forceinline__ bool ext_before(uint32_t v, uint32_t pos, const ExtCand &c, int B)
+{
+    if (v != c.v) return v < c.v;
+    if (c.pos == kNoPos) return true;
+    return tree_key((int)pos, B) < tree_key((int)c.pos, B);
+}
+
 struct SelSmem {
     int warp_tot[33];
     int i0, i1, i2, i3, i4;
@@ -76,6 +160,13 @@ struct SelSmem {
     float ideal[kMaxObj], worst[kMaxObj], nadir[kMaxObj];
     float red[64 * kMaxObj];
     float ext[kMaxObj * kMaxObj];  // extreme points while they are updated
+    ExtCand xc[32][kMaxObj];       // per-warp extreme-point candidates
+    uint64_t xck[32][kMaxObj];     // their tree keys
+    float xa[kMaxObj * kMaxObj];   // ASF of last generation's extreme points, per axis
+    float xf[kMaxObj * kMaxObj];   // ASF of each axis' front-0 winner, per axis
+    uint64_t xkey[kMaxObj];        // tree keys of the extreme-point positions
+    uint64_t xfkey[kMaxObj];       // tree keys of the front-0 winners
+    int xsrc[kMaxObj];             // source of each new extreme point
 };
 
 // exclusive block scan of a 0/1 flag over kSelThreads threads; returns the
@@ -104,20 +195,120 @@ __device__ __forceinline__ int block_scan_flag(int flag, SelSmem &sm, int *total
     return res;
 }
 
-__device__ __forceinline__ float asf_val(const float *x, const float *ideal, int i, int M)
+// ASF (include/sorting.cuh:428-449) of point x for every axis i: the largest of
+// tmp_k / w_k with tmp_k = x_k - ideal_k (0 below 0.001), w_i = 1 and the other
+// weights 1e-6.  Every tmp_k is >= 0 and a correctly rounded division is monotone in
+// its dividend, so the largest tmp_k / 1e-6 over k != i is (the largest tmp_k over
+// k != i) / 1e-6, and tmp_i / 1 is tmp_i: two divisions give all M values, equal to
+// the reference's M * M.
+__device__ __forceinline__ void asf_all(const float *x, const float *ideal, int M, float *out)
 {
-    // ASF (include/sorting.cuh:428-449) with weights 1 (objective i) / 1e-6
-    float mx = -FLT_MAX;
+    float tmp[kMaxObj];
+    float m1 = -1.0f, m2 = -1.0f;  // largest and second largest tmp_k
+    int a1 = -1;
     for (int k = 0; k < M; k++) {
-        float tmp = __fsub_rn(x[k], ideal[k]);
-        if ((double)tmp < 0.001) tmp = 0.0f;
-        float q = __fdiv_rn(tmp, k == i ? 1.0f : 1e-6f);
-        if (q > mx) mx = q;
+        float t = __fsub_rn(x[k], ideal[k]);
+        if ((double)t < 0.001) t = 0.0f;
+        tmp[k] = t;
+        if (t > m1) {
+            m2 = m1;
+            m1 = t;
+            a1 = k;
+        } else if (t > m2) {
+            m2 = t;
+        }
     }
-    return mx;
+    const float q1 = m1 >= 0.0f ? __fdiv_rn(m1, 1e-6f) : -FLT_MAX;
+    const float q2 = m2 >= 0.0f ? __fdiv_rn(m2, 1e-6f) : -FLT_MAX;
+    for (int i = 0; i < M; i++) {
+        const float q = i == a1 ? q2 : q1;  // largest over k != i
+        out[i] = tmp[i] > q ? tmp[i] : q;
+    }
 }
 
-__global__ void __launch_bounds__(kSelThreads) k_select(Shape s, const float *__restrict__ obj, float *ext,
+// the same for one axis i: one division
+__device__ __forceinline__ float asf_axis(const float *x, const float *ideal, int i, int M)
+{
+    float ti = 0.0f, m = -1.0f;  // tmp_i and the largest tmp_k over k != i
+    for (int k = 0; k < M; k++) {
+        float t = __fsub_rn(x[k], ideal[k]);
+        if ((double)t < 0.001) t = 0.0f;
+        if (k == i) ti = t;
+        else if (t > m) m = t;
+    }
+    const float q = m >= 0.0f ? __fdiv_rn(m, 1e-6f) : -FLT_MAX;
+    return ti > q ? ti : q;
+}
+
+// element j of a row held in registers (j known only at run time)
+__device__ __forceinline__ float row_at(const float (&row)[kMaxObj + 1], int j)
+{
+    float v = row[0];
+#pragma unroll
+    for (int q = 1; q <= kMaxObj; q++)
+        if (j == q) v = row[q];
+    return v;
+}
+
+// Hyperplane through the extreme points by Gaussian elimination
+// (GaussianElimination, include/sorting.cuh:555-599) and its check (:929-956), by
+// one warp: lane r < M holds row r of [ext | 1] and does that row's share of every
+// step, with the same operations in the same order as the serial loops.  Writes
+// nadir = ideal + intercepts; returns 1 (all lanes) when the hyperplane is unusable.
+__device__ int hyperplane_nadir(int M, const float *ext, const float *ideal, float *nadir, int lane)
+{
+    const unsigned full = 0xffffffffu;
+    const bool mine = lane < M;
+    float row[kMaxObj + 1];
+#pragma unroll
+    for (int j = 0; j <= kMaxObj; j++) row[j] = (mine && j < M) ? ext[lane * M + j] : (j == M ? 1.0f : 0.0f);
+    for (int c = 0; c < M; c++) {
+        const float pcc = __shfl_sync(full, row_at(row, c), c);
+        if ((double)fabsf(pcc) <= 1e-6) {
+            // add the first later row with a usable entry in column c
+            const unsigned cand = __ballot_sync(full, mine && lane > c && (double)fabsf(row_at(row, c)) > 1e-6);
+            if (cand) {
+                const int r = __ffs(cand) - 1;
+#pragma unroll
+                for (int j = 0; j <= kMaxObj; j++) {
+                    const float vr = __shfl_sync(full, row[j], r);
+                    if (lane == c && j >= c && j <= M) row[j] = __fadd_rn(row[j], vr);
+                }
+            }
+        }
+        const float pc = __shfl_sync(full, row_at(row, c), c);
+        const float f = __fdiv_rn(row_at(row, c), pc);
+        const bool elim = mine && lane > c;
+#pragma unroll
+        for (int j = 0; j <= kMaxObj; j++) {
+            const float vc = __shfl_sync(full, row[j], c);
+            if (elim && j >= c && j <= M) row[j] = __fsub_rn(row[j], __fmul_rn(f, vc));
+        }
+    }
+    // back substitution: lane r finds x[r] once x[r+1 .. M-1] are known
+    float xr = 0.0f;
+    for (int r = M - 1; r >= 0; r--) {
+        float sacc = 0.0f;
+        for (int j = r + 1; j < M; j++) sacc = __fadd_rn(sacc, __fmul_rn(row_at(row, j), __shfl_sync(full, xr, j)));
+        const float xv = __fdiv_rn(__fsub_rn(row_at(row, M), sacc), row_at(row, r));
+        if (lane == r) xr = xv;
+    }
+    int exc = 0;
+    float res = 0.0f;
+    for (int i = 0; i < M; i++) {
+        const float xi = __shfl_sync(full, xr, i);
+        if (mine) res = __fadd_rn(res, __fmul_rn(xi, __fsub_rn(ext[lane * M + i], ideal[i])));
+    }
+    if (mine) {
+        if (fabsf(__fsub_rn(res, 1.0f)) > 1e-6f || isnan(res) || isinf(res)) exc = 1;
+        const float icp = __fdiv_rn(1.0f, xr);
+        if (icp <= 1e-6f || isnan(icp) || isinf(icp)) exc = 1;
+        nadir[lane] = __fadd_rn(ideal[lane], icp);
+    }
+    return __any_sync(full, exc) ? 1 : 0;
+}
+
+__global__ void __launch_bounds__(kSelThreads, 1) k_select(Shape s, const float *__restrict__ obj, float *ext,
                                                         const float *__restrict__ refpts, SelectScratch sc,
                                                         int32_t *surv, uint32_t *d_gen, int bump_gen)
 {
@@ -126,8 +317,6 @@ __global__ void __launch_bounds__(kSelThreads) k_select(Shape s, const float *__
     const int N = s.N, N2 = 2 * N, M = s.M, R = s.R;
     const int words = (N2 + 31) >> 5;
     uint32_t *fmask = reinterpret_cast<uint32_t *>(smem_raw + ((sizeof(SelSmem) + 15) & ~size_t(15)));
-    float *tbuf = reinterpret_cast<float *>(fmask + ((words + 3) & ~3));
-    int32_t *tix = reinterpret_cast<int32_t *>(tbuf + ((N2 + M + 3) & ~3));
     const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5;
     (void)d_gen;
     (void)bump_gen;
@@ -206,185 +395,176 @@ __global__ void __launch_bounds__(kSelThreads) k_select(Shape s, const float *__
     const int rc = sm.rc;
     const int last_size = sm.fsize;
 
-    // ---------------- ideal / worst (exact min / max)
-    {
-        float mn[kMaxObj], mx[kMaxObj];
-        for (int k = 0; k < M; k++) {
-            mn[k] = FLT_MAX;
-            mx[k] = -FLT_MAX;
+    // ---------------- ideal / worst (exact min / max), objective by objective
+    for (int k = 0; k < M; k++) {
+        float mn = FLT_MAX, mx = -FLT_MAX;
+        for (int i = tid; i < N2; i += nth) {
+            const float v = obj[(size_t)i * M + k];
+            if (v < mn) mn = v;
+            if (v > mx) mx = v;
         }
-        for (int i = tid; i < N2; i += nth)
-            for (int k = 0; k < M; k++) {
-                float v = obj[(size_t)i * M + k];
-                if (v < mn[k]) mn[k] = v;
-                if (v > mx[k]) mx[k] = v;
-            }
-        for (int k = 0; k < M; k++) {
-            for (int o = 16; o > 0; o >>= 1) {
-                float a = __shfl_xor_sync(0xffffffffu, mn[k], o), b = __shfl_xor_sync(0xffffffffu, mx[k], o);
-                if (a < mn[k]) mn[k] = a;
-                if (b > mx[k]) mx[k] = b;
-            }
+        for (int o = 16; o > 0; o >>= 1) {
+            const float a = __shfl_xor_sync(0xffffffffu, mn, o), b = __shfl_xor_sync(0xffffffffu, mx, o);
+            if (a < mn) mn = a;
+            if (b > mx) mx = b;
         }
-        if (lane == 0)
-            for (int k = 0; k < M; k++) {
-                sm.red[warp * kMaxObj + k] = mn[k];
-                sm.red[32 * kMaxObj + warp * kMaxObj + k] = mx[k];
-            }
-        __syncthreads();
-        if (tid < M) {
-            float a = FLT_MAX, b = -FLT_MAX;
-            for (int w = 0; w < (nth >> 5); w++) {
-                float u = sm.red[w * kMaxObj + tid], v = sm.red[32 * kMaxObj + w * kMaxObj + tid];
-                if (u < a) a = u;
-                if (v > b) b = v;
-            }
-            sm.ideal[tid] = a;
-            sm.worst[tid] = b;
+        if (lane == 0) {
+            sm.red[warp * kMaxObj + k] = mn;
+            sm.red[32 * kMaxObj + warp * kMaxObj + k] = mx;
         }
-        __syncthreads();
     }
+    __syncthreads();
+    if (warp < M) {  // warp k: objective k over the per-warp results, in warp order
+        const float a = warp_first_min(sm.red[lane * kMaxObj + warp], lane);
+        const float b = warp_first_max(sm.red[32 * kMaxObj + lane * kMaxObj + warp], lane);
+        if (lane == 0) {
+            sm.ideal[warp] = a;
+            sm.worst[warp] = b;
+        }
+    }
+    __syncthreads();
 
     // ---------------- extreme points (findExtremePoints, :601-683), tree order of findMinValue
+    // Front 0 does not change between axes: a parallel pass finds, axis by axis, its
+    // first solution in (value, tree order).  The current extreme points, which change
+    // as the axes are done in turn, and the FLT_MAX fillers are then weighed against
+    // it axis by axis.  The pass also takes the maximum of front 0 (MNDF nadir).
     {
         const int B = N2 + M;
         for (int e = tid; e < M * M; e += nth) sm.ext[e] = ext[e];
-        __syncthreads();
-        auto value = [&](int t, int i, int &ix) {
-            if (t < f0) {
-                const int sol = sc.sorted[t];
-                ix = sol;
-                return asf_val(obj + (size_t)sol * M, sm.ideal, i, M);
-            }
-            if (t < f0 + M) {
-                ix = N2 + (t - f0);
-                return asf_val(sm.ext + (t - f0) * M, sm.ideal, i, M);
-            }
-            ix = -1;
-            return FLT_MAX;
-        };
-        // tbuf[t] < tbuf[u] replaces t by u (strict: the lower position keeps ties)
-        auto pair = [&](int t, int u) {
-            if (tbuf[u] < tbuf[t]) {
-                tbuf[t] = tbuf[u];
-                tix[t] = tix[u];
-            }
-        };
         for (int i = 0; i < M; i++) {
-            // first level fused with the ASF values: position t against t + B/2
-            int h = B / 2;
-            for (int t = tid; t < h; t += nth) {
-                int i0, i1;
-                const float v0 = value(t, i, i0), v1 = value(t + h, i, i1);
-                tbuf[t] = v1 < v0 ? v1 : v0;
-                tix[t] = v1 < v0 ? i1 : i0;
+            ExtCand best{0xffffffffu, kNoPos};
+            float fmx = -FLT_MAX;
+            for (int t = tid; t < f0; t += nth) {
+                const float *x = obj + (size_t)sc.sorted[t] * M;
+                const uint32_t v = __float_as_uint(asf_axis(x, sm.ideal, i, M));
+                if (ext_before(v, (uint32_t)t, best, B)) best = ExtCand{v, (uint32_t)t};
+                const float xi = x[i];
+                if (xi > fmx) fmx = xi;
             }
-            __syncthreads();
-            // later levels; after an odd level its last position joins position 0,
-            // done by the thread that handles position 0 next; levels of at most 32
-            // pairs run in warp 0 alone
-            while (h > 1) {
-                const bool odd = h & 1;
-                const int hp = h - 1;
-                h >>= 1;
-                if (h > 32) {
-                    for (int t = tid; t < h; t += nth) {
-                        if (t == 0 && odd) pair(0, hp);
-                        pair(t, t + h);
-                    }
-                    __syncthreads();
-                } else if (warp == 0) {
-                    if (lane < h) {
-                        if (lane == 0 && odd) pair(0, hp);
-                        pair(lane, lane + h);
-                    }
-                    __syncwarp();
+            uint64_t bkey = best.pos != kNoPos ? tree_key((int)best.pos, B) : ~0ull;
+            for (int o = 16; o > 0; o >>= 1) {
+                const uint32_t v2 = __shfl_xor_sync(0xffffffffu, best.v, o), p2 = __shfl_xor_sync(0xffffffffu, best.pos, o);
+                const uint64_t k2 = __shfl_xor_sync(0xffffffffu, bkey, o);
+                if (v2 < best.v || (v2 == best.v && k2 < bkey)) {
+                    best = ExtCand{v2, p2};
+                    bkey = k2;
                 }
+                const float b = __shfl_xor_sync(0xffffffffu, fmx, o);
+                if (b > fmx) fmx = b;
             }
-            if (tid == 0) {
-                const int sel = tix[0];
-                float tmp[kMaxObj];
-                if (sel >= N2) {
-                    for (int k = 0; k < M; k++) tmp[k] = sm.ext[(sel - N2) * M + k];
-                } else if (sel >= 0) {
-                    for (int k = 0; k < M; k++) tmp[k] = obj[(size_t)sel * M + k];
-                }
-                if (sel >= 0)
-                    for (int k = 0; k < M; k++) {
-                        sm.ext[i * M + k] = tmp[k];
-                        ext[i * M + k] = tmp[k];
-                    }
+            if (lane == 0) {
+                sm.xc[warp][i] = best;
+                sm.xck[warp][i] = bkey;
+                sm.red[warp * kMaxObj + i] = fmx;
             }
-            __syncthreads();
         }
+        __syncthreads();
+        if (warp < M) {  // warp i: axis i over the per-warp candidates
+            const ExtCand d = sm.xc[lane][warp];
+            uint32_t v = d.v, pos = d.pos;
+            uint64_t key = sm.xck[lane][warp];
+            for (int o = 16; o > 0; o >>= 1) {
+                const uint32_t v2 = __shfl_xor_sync(0xffffffffu, v, o), p2 = __shfl_xor_sync(0xffffffffu, pos, o);
+                const uint64_t k2 = __shfl_xor_sync(0xffffffffu, key, o);
+                if (v2 < v || (v2 == v && k2 < key)) {
+                    v = v2;
+                    pos = p2;
+                    key = k2;
+                }
+            }
+            const float b = warp_first_max(sm.red[lane * kMaxObj + warp], lane);
+            if (lane == 0) {
+                sm.xc[0][warp] = ExtCand{v, pos};
+                sm.xfkey[warp] = key;
+                sm.red[32 * kMaxObj + warp] = b;  // max of front 0 (MNDF)
+            }
+            if (lane == 1) sm.xkey[warp] = tree_key(f0 + warp, B);
+        }
+        __syncthreads();
+        // The current extreme point r, as the axes are done in turn, is a copy of an
+        // extreme point of the last generation (source r' < M) or of the front-0 winner
+        // of an earlier axis j (source M + j): its ASF values come from two small tables.
+        if (tid < 2 * M) {
+            const int r = tid % M;
+            float a[kMaxObj];
+            if (tid < M) {
+                asf_all(sm.ext + r * M, sm.ideal, M, a);
+                for (int i = 0; i < M; i++) sm.xa[r * M + i] = a[i];
+            } else {
+                const uint32_t pos = sm.xc[0][r].pos;
+                if (pos < (uint32_t)f0) asf_all(obj + (size_t)sc.sorted[pos] * M, sm.ideal, M, a);
+                for (int i = 0; i < M; i++) sm.xf[r * M + i] = pos < (uint32_t)f0 ? a[i] : 0.0f;
+            }
+        }
+        __syncthreads();
+        if (warp == 0) {  // the axes in turn; lane r < M holds extreme point r's source
+            const uint32_t vmax = __float_as_uint(FLT_MAX);
+            // the FLT_MAX fillers can only come first on an axis whose front-0 value is
+            // not below FLT_MAX: the first filler in tree order, only then
+            uint64_t fkey = ~0ull;
+            if (__any_sync(0xffffffffu, lane < M && sm.xc[0][lane].v >= vmax)) {
+                for (int t = f0 + M + lane; t < B; t += 32) fkey = min(fkey, tree_key(t, B));
+                for (int o = 16; o > 0; o >>= 1) fkey = min(fkey, __shfl_xor_sync(0xffffffffu, fkey, o));
+            }
+            int src = lane;
+            const uint64_t rkey = lane < M ? sm.xkey[lane] : ~0ull;
+            for (int i = 0; i < M; i++) {
+                uint32_t cv = sm.xc[0][i].v;
+                uint64_t ck = sm.xfkey[i];
+                int win = ck != ~0ull ? M + i : -1;  // -1: a filler, the point stays
+                if (fkey != ~0ull && (vmax < cv || (vmax == cv && fkey < ck))) {
+                    cv = vmax;
+                    ck = fkey;
+                    win = -1;
+                }
+                // the extreme points as they stand, lowest (value, key) over the lanes
+                uint32_t v = 0xffffffffu;
+                uint64_t key = ~0ull;
+                int q = src;
+                if (lane < M && rkey != ~0ull) {
+                    v = __float_as_uint(src < M ? sm.xa[src * M + i] : sm.xf[(src - M) * M + i]);
+                    key = rkey;
+                }
+                for (int o = 16; o > 0; o >>= 1) {
+                    const uint32_t v2 = __shfl_xor_sync(0xffffffffu, v, o);
+                    const uint64_t k2 = __shfl_xor_sync(0xffffffffu, key, o);
+                    const int q2 = __shfl_xor_sync(0xffffffffu, q, o);
+                    if (v2 < v || (v2 == v && k2 < key)) {
+                        v = v2;
+                        key = k2;
+                        q = q2;
+                    }
+                }
+                if (key != ~0ull && (v < cv || (v == cv && key < ck))) win = q;
+                if (win >= 0 && lane == i) src = win;
+            }
+            if (lane < M) sm.xsrc[lane] = src;
+        }
+        __syncthreads();
+        for (int e = tid; e < M * M; e += nth) {
+            const int i = e / M, k = e - i * M, q = sm.xsrc[i];
+            sm.xa[e] = q < M ? sm.ext[q * M + k] : obj[(size_t)sc.sorted[sm.xc[0][q - M].pos] * M + k];
+        }
+        __syncthreads();
+        for (int e = tid; e < M * M; e += nth) {
+            sm.ext[e] = sm.xa[e];
+            ext[e] = sm.xa[e];
+        }
+        __syncthreads();
     }
 
     // ---------------- hyperplane intercepts (GaussianElimination :555-599, check :929-956)
-    if (tid == 0) {
-        float AB[kMaxObj][kMaxObj + 1], x[kMaxObj];
-        for (int i = 0; i < M; i++) {
-            for (int j = 0; j < M; j++) AB[i][j] = sm.ext[i * M + j];
-            AB[i][M] = 1.0f;
+    if (warp == 0) {
+        const int exc = hyperplane_nadir(M, sm.ext, sm.ideal, sm.nadir, lane);
+        if (lane == 0) sm.hyp = exc;
+        if (exc && lane < M) {
+            // updateNadirValue_MNDF (:685-884): max over front 0, worst when too close to ideal
+            const float b = sm.red[32 * kMaxObj + lane];
+            sm.nadir[lane] = __fsub_rn(b, sm.ideal[lane]) > 1e-6f ? b : sm.worst[lane];
         }
-        for (int c = 0; c < M; c++) {
-            if ((double)fabsf(AB[c][c]) <= 1e-6) {
-                int r = c;
-                while (r < M && !((double)fabsf(AB[r][c]) > 1e-6)) r++;
-                if (r < M)
-                    for (int j = c; j <= M; j++) AB[c][j] = __fadd_rn(AB[c][j], AB[r][j]);
-            }
-            for (int r = c + 1; r < M; r++) {
-                float f = __fdiv_rn(AB[r][c], AB[c][c]);
-                for (int j = c; j <= M; j++) AB[r][j] = __fsub_rn(AB[r][j], __fmul_rn(f, AB[c][j]));
-            }
-        }
-        for (int r = M - 1; r >= 0; r--) {
-            float sacc = 0.0f;
-            for (int j = r + 1; j < M; j++) sacc = __fadd_rn(sacc, __fmul_rn(AB[r][j], x[j]));
-            x[r] = __fdiv_rn(__fsub_rn(AB[r][M], sacc), AB[r][r]);
-        }
-        int exc = 0;
-        for (int k = 0; k < M; k++) {
-            float res = 0.0f;
-            for (int i = 0; i < M; i++) res = __fadd_rn(res, __fmul_rn(x[i], __fsub_rn(sm.ext[k * M + i], sm.ideal[i])));
-            if (fabsf(__fsub_rn(res, 1.0f)) > 1e-6f || isnan(res) || isinf(res)) exc = 1;
-            float icp = __fdiv_rn(1.0f, x[k]);
-            if (icp <= 1e-6f || isnan(icp) || isinf(icp)) exc = 1;
-            sm.nadir[k] = __fadd_rn(sm.ideal[k], icp);
-        }
-        sm.hyp = exc;
     }
     __syncthreads();
-    if (sm.hyp) {
-        // updateNadirValue_MNDF (:685-884): max over front 0, worst when too close to ideal
-        float mx[kMaxObj];
-        for (int k = 0; k < M; k++) mx[k] = -FLT_MAX;
-        for (int t = tid; t < f0; t += nth) {
-            int sol = sc.sorted[t];
-            for (int k = 0; k < M; k++) {
-                float v = obj[(size_t)sol * M + k];
-                if (v > mx[k]) mx[k] = v;
-            }
-        }
-        for (int k = 0; k < M; k++)
-            for (int o = 16; o > 0; o >>= 1) {
-                float b = __shfl_xor_sync(0xffffffffu, mx[k], o);
-                if (b > mx[k]) mx[k] = b;
-            }
-        __syncthreads();
-        if (lane == 0)
-            for (int k = 0; k < M; k++) sm.red[warp * kMaxObj + k] = mx[k];
-        __syncthreads();
-        if (tid < M) {
-            float b = -FLT_MAX;
-            for (int w = 0; w < (nth >> 5); w++) {
-                float v = sm.red[w * kMaxObj + tid];
-                if (v > b) b = v;
-            }
-            sm.nadir[tid] = __fsub_rn(b, sm.ideal[tid]) > 1e-6f ? b : sm.worst[tid];
-        }
-        __syncthreads();
-    }
     if (tid == 0) {
         sc.info[0] = rc;
         sc.info[1] = last_size;
@@ -703,8 +883,7 @@ size_t niche_smem_bytes(const Shape &s)
 size_t select_smem_bytes(const Shape &s)
 {
     const int N2 = 2 * s.N, words = (N2 + 31) >> 5;
-    return ((sizeof(SelSmem) + 15) & ~size_t(15)) + (size_t)((words + 3) & ~3) * 4 +
-           (size_t)((N2 + s.M + 3) & ~3) * 4 + (size_t)(N2 + s.M) * 4;
+    return ((sizeof(SelSmem) + 15) & ~size_t(15)) + (size_t)((words + 3) & ~3) * 4;
 }
 
 cudaError_t launch_select(const Shape &s, const float *obj, float *ext, const float *refpts, SelectScratch sc,
