@@ -694,7 +694,8 @@ __global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SelSmem &sm = *reinterpret_cast<SelSmem *>(smem_raw);
     const int N = s.N, N2 = 2 * N, R = s.R, Lsz = N2 + 4;
-    int *cj = reinterpret_cast<int *>(smem_raw + ((sizeof(SelSmem) + 15) & ~size_t(15)));
+    unsigned long long *amin = reinterpret_cast<unsigned long long *>(smem_raw + ((sizeof(SelSmem) + 15) & ~size_t(15)));
+    int *cj = reinterpret_cast<int *>(amin + R);  // amin: R level-0 picks (distance bits, list index)
     int *nj = cj + R;
     int *coff = nj + R;    // R + 1
     int *kq = coff + R + 1;
@@ -715,6 +716,7 @@ __global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc
         cj[j] = sc.rho[j];
         nj[j] = sc.ncand[j];
         kq[j] = 0;
+        amin[j] = ~0ull;
     }
     for (int l = tid; l < Lsz; l += nth) lv[l] = 0;
     for (int t = count0 + tid; t < rc; t += nth) {
@@ -741,22 +743,26 @@ __global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc
         __syncthreads();
     }
     if (tid == 0) coff[R] = sm.i0;
-    // candidate lists in ascending position (kq counts the fill)
-    if (warp == 0) {
-        for (int base = count0; base < rc; base += 32) {
-            const int t = base + lane;
-            const bool act = t < rc;
-            const int j = act ? las[t - count0] : -1 - lane;
-            const uint32_t peers = __match_any_sync(0xffffffffu, j);
-            const int rank = __popc(peers & ((1u << lane) - 1u));
-            const int f0v = act ? kq[j] : 0;
-            __syncwarp();
-            if (act) cand[coff[j] + f0v + rank] = lsol[t - count0];
-            __syncwarp();
-            if (act && rank == 0) kq[j] = f0v + __popc(peers);
-            __syncwarp();
-        }
+    // candidate lists in ascending position: each member takes a slot in its point's
+    // range (kq counts the fill), then finds its place by counting the members of
+    // that range before it; the nearest member of each point (the first in list order
+    // among equal distances, the level-0 pick) comes out on the way
+    const int nm = rc - count0;
+    for (int t = tid; t < nm; t += nth) {
+        const int j = las[t];
+        cand[coff[j] + atomicAdd(&kq[j], 1)] = t;
     }
+    __syncthreads();
+    for (int t = tid; t < nm; t += nth) {
+        const int j = las[t], b = coff[j], e = b + nj[j];
+        int r = 0;
+        for (int u = b; u < e; u++) r += cand[u] < t;
+        las[t] = b + r;  // only this thread reads las[t]
+        // distances are >= +0 (or FLT_MAX), so their bits order as the values do
+        atomicMin(&amin[j], ((unsigned long long)__float_as_uint(sc.dist[lsol[t]]) << 32) | (uint32_t)r);
+    }
+    __syncthreads();
+    for (int t = tid; t < nm; t += nth) cand[las[t]] = lsol[t];
     // active points per level, then picks before each level: lv[l] = picks at levels < l
     if (tid == 0) {
         sm.i0 = 0;
@@ -837,14 +843,7 @@ __global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc
             const int level = cj[j] + q;
             int slot = 0;
             if (level == 0) {
-                float bd = sc.dist[cl[0]];
-                for (int u = 1; u < nc; u++) {
-                    const float dv = sc.dist[cl[u]];
-                    if (dv < bd) {
-                        bd = dv;
-                        slot = u;
-                    }
-                }
+                slot = (int)(uint32_t)amin[j];  // the first pick: the list is as built
             } else {
                 slot = (int)rng_uint(rnd[pofs[j] + q], (uint32_t)nc);
             }
@@ -876,7 +875,7 @@ __global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc
 
 size_t niche_smem_bytes(const Shape &s)
 {
-    return ((sizeof(SelSmem) + 15) & ~size_t(15)) +
+    return ((sizeof(SelSmem) + 15) & ~size_t(15)) + (size_t)s.R * sizeof(unsigned long long) +
            (size_t)(4 * s.R + 1 + 2 * s.N + 4 + 3 * 2 * s.N + s.R + 1 + s.N) * sizeof(int);
 }
 
