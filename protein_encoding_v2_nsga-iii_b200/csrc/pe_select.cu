@@ -160,6 +160,10 @@ struct SelSmem {
     float ideal[kMaxObj], worst[kMaxObj], nadir[kMaxObj];
     float red[64 * kMaxObj];
     float ext[kMaxObj * kMaxObj];  // extreme points while they are updated
+};
+
+// k_select's extreme-point workspace (after the front mask in its dynamic shared memory)
+struct ExtSmem {
     ExtCand xc[32][kMaxObj];       // per-warp extreme-point candidates
     uint64_t xck[32][kMaxObj];     // their tree keys
     float xa[kMaxObj * kMaxObj];   // ASF of last generation's extreme points, per axis
@@ -317,6 +321,7 @@ __global__ void __launch_bounds__(kSelThreads, 1) k_select(Shape s, const float 
     const int N = s.N, N2 = 2 * N, M = s.M, R = s.R;
     const int words = (N2 + 31) >> 5;
     uint32_t *fmask = reinterpret_cast<uint32_t *>(smem_raw + ((sizeof(SelSmem) + 15) & ~size_t(15)));
+    ExtSmem &xs = *reinterpret_cast<ExtSmem *>(fmask + (((N2 + 31) / 32 + 3) & ~3));
     const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5;
     (void)d_gen;
     (void)bump_gen;
@@ -454,16 +459,16 @@ __global__ void __launch_bounds__(kSelThreads, 1) k_select(Shape s, const float 
                 if (b > fmx) fmx = b;
             }
             if (lane == 0) {
-                sm.xc[warp][i] = best;
-                sm.xck[warp][i] = bkey;
+                xs.xc[warp][i] = best;
+                xs.xck[warp][i] = bkey;
                 sm.red[warp * kMaxObj + i] = fmx;
             }
         }
         __syncthreads();
         if (warp < M) {  // warp i: axis i over the per-warp candidates
-            const ExtCand d = sm.xc[lane][warp];
+            const ExtCand d = xs.xc[lane][warp];
             uint32_t v = d.v, pos = d.pos;
-            uint64_t key = sm.xck[lane][warp];
+            uint64_t key = xs.xck[lane][warp];
             for (int o = 16; o > 0; o >>= 1) {
                 const uint32_t v2 = __shfl_xor_sync(0xffffffffu, v, o), p2 = __shfl_xor_sync(0xffffffffu, pos, o);
                 const uint64_t k2 = __shfl_xor_sync(0xffffffffu, key, o);
@@ -475,11 +480,11 @@ __global__ void __launch_bounds__(kSelThreads, 1) k_select(Shape s, const float 
             }
             const float b = warp_first_max(sm.red[lane * kMaxObj + warp], lane);
             if (lane == 0) {
-                sm.xc[0][warp] = ExtCand{v, pos};
-                sm.xfkey[warp] = key;
+                xs.xc[0][warp] = ExtCand{v, pos};
+                xs.xfkey[warp] = key;
                 sm.red[32 * kMaxObj + warp] = b;  // max of front 0 (MNDF)
             }
-            if (lane == 1) sm.xkey[warp] = tree_key(f0 + warp, B);
+            if (lane == 1) xs.xkey[warp] = tree_key(f0 + warp, B);
         }
         __syncthreads();
         // The current extreme point r, as the axes are done in turn, is a copy of an
@@ -490,11 +495,11 @@ __global__ void __launch_bounds__(kSelThreads, 1) k_select(Shape s, const float 
             float a[kMaxObj];
             if (tid < M) {
                 asf_all(sm.ext + r * M, sm.ideal, M, a);
-                for (int i = 0; i < M; i++) sm.xa[r * M + i] = a[i];
+                for (int i = 0; i < M; i++) xs.xa[r * M + i] = a[i];
             } else {
-                const uint32_t pos = sm.xc[0][r].pos;
+                const uint32_t pos = xs.xc[0][r].pos;
                 if (pos < (uint32_t)f0) asf_all(obj + (size_t)sc.sorted[pos] * M, sm.ideal, M, a);
-                for (int i = 0; i < M; i++) sm.xf[r * M + i] = pos < (uint32_t)f0 ? a[i] : 0.0f;
+                for (int i = 0; i < M; i++) xs.xf[r * M + i] = pos < (uint32_t)f0 ? a[i] : 0.0f;
             }
         }
         __syncthreads();
@@ -503,15 +508,15 @@ __global__ void __launch_bounds__(kSelThreads, 1) k_select(Shape s, const float 
             // the FLT_MAX fillers can only come first on an axis whose front-0 value is
             // not below FLT_MAX: the first filler in tree order, only then
             uint64_t fkey = ~0ull;
-            if (__any_sync(0xffffffffu, lane < M && sm.xc[0][lane].v >= vmax)) {
+            if (__any_sync(0xffffffffu, lane < M && xs.xc[0][lane].v >= vmax)) {
                 for (int t = f0 + M + lane; t < B; t += 32) fkey = min(fkey, tree_key(t, B));
                 for (int o = 16; o > 0; o >>= 1) fkey = min(fkey, __shfl_xor_sync(0xffffffffu, fkey, o));
             }
             int src = lane;
-            const uint64_t rkey = lane < M ? sm.xkey[lane] : ~0ull;
+            const uint64_t rkey = lane < M ? xs.xkey[lane] : ~0ull;
             for (int i = 0; i < M; i++) {
-                uint32_t cv = sm.xc[0][i].v;
-                uint64_t ck = sm.xfkey[i];
+                uint32_t cv = xs.xc[0][i].v;
+                uint64_t ck = xs.xfkey[i];
                 int win = ck != ~0ull ? M + i : -1;  // -1: a filler, the point stays
                 if (fkey != ~0ull && (vmax < cv || (vmax == cv && fkey < ck))) {
                     cv = vmax;
@@ -523,7 +528,7 @@ __global__ void __launch_bounds__(kSelThreads, 1) k_select(Shape s, const float 
                 uint64_t key = ~0ull;
                 int q = src;
                 if (lane < M && rkey != ~0ull) {
-                    v = __float_as_uint(src < M ? sm.xa[src * M + i] : sm.xf[(src - M) * M + i]);
+                    v = __float_as_uint(src < M ? xs.xa[src * M + i] : xs.xf[(src - M) * M + i]);
                     key = rkey;
                 }
                 for (int o = 16; o > 0; o >>= 1) {
@@ -539,17 +544,17 @@ __global__ void __launch_bounds__(kSelThreads, 1) k_select(Shape s, const float 
                 if (key != ~0ull && (v < cv || (v == cv && key < ck))) win = q;
                 if (win >= 0 && lane == i) src = win;
             }
-            if (lane < M) sm.xsrc[lane] = src;
+            if (lane < M) xs.xsrc[lane] = src;
         }
         __syncthreads();
         for (int e = tid; e < M * M; e += nth) {
-            const int i = e / M, k = e - i * M, q = sm.xsrc[i];
-            sm.xa[e] = q < M ? sm.ext[q * M + k] : obj[(size_t)sc.sorted[sm.xc[0][q - M].pos] * M + k];
+            const int i = e / M, k = e - i * M, q = xs.xsrc[i];
+            xs.xa[e] = q < M ? sm.ext[q * M + k] : obj[(size_t)sc.sorted[xs.xc[0][q - M].pos] * M + k];
         }
         __syncthreads();
         for (int e = tid; e < M * M; e += nth) {
-            sm.ext[e] = sm.xa[e];
-            ext[e] = sm.xa[e];
+            sm.ext[e] = xs.xa[e];
+            ext[e] = xs.xa[e];
         }
         __syncthreads();
     }
@@ -694,8 +699,7 @@ __global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SelSmem &sm = *reinterpret_cast<SelSmem *>(smem_raw);
     const int N = s.N, N2 = 2 * N, R = s.R, Lsz = N2 + 4;
-    unsigned long long *amin = reinterpret_cast<unsigned long long *>(smem_raw + ((sizeof(SelSmem) + 15) & ~size_t(15)));
-    int *cj = reinterpret_cast<int *>(amin + R);  // amin: R level-0 picks (distance bits, list index)
+    int *cj = reinterpret_cast<int *>(smem_raw + ((sizeof(SelSmem) + 15) & ~size_t(15)));
     int *nj = cj + R;
     int *coff = nj + R;    // R + 1
     int *kq = coff + R + 1;
@@ -716,7 +720,6 @@ __global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc
         cj[j] = sc.rho[j];
         nj[j] = sc.ncand[j];
         kq[j] = 0;
-        amin[j] = ~0ull;
     }
     for (int l = tid; l < Lsz; l += nth) lv[l] = 0;
     for (int t = count0 + tid; t < rc; t += nth) {
@@ -745,24 +748,47 @@ __global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc
     if (tid == 0) coff[R] = sm.i0;
     // candidate lists in ascending position: each member takes a slot in its point's
     // range (kq counts the fill), then finds its place by counting the members of
-    // that range before it; the nearest member of each point (the first in list order
-    // among equal distances, the level-0 pick) comes out on the way
+    // that range before it.  On the way, the nearest member of each point (the first
+    // in list order among equal distances) is found -- the pick at level 0, which is a
+    // point's first pick whenever it has one, so it is made here for every point with
+    // niche count 0 (a point that ends up picking nothing never reads its list).
+    // pofs and kq serve as scratch: the least distance bits, then the least rank.
     const int nm = rc - count0;
     for (int t = tid; t < nm; t += nth) {
         const int j = las[t];
         cand[coff[j] + atomicAdd(&kq[j], 1)] = t;
     }
     __syncthreads();
+    for (int j = tid; j < R; j += nth) {
+        pofs[j] = 0x7fffffff;
+        kq[j] = 0x7fffffff;
+    }
     for (int t = tid; t < nm; t += nth) {
         const int j = las[t], b = coff[j], e = b + nj[j];
         int r = 0;
         for (int u = b; u < e; u++) r += cand[u] < t;
         las[t] = b + r;  // only this thread reads las[t]
-        // distances are >= +0 (or FLT_MAX), so their bits order as the values do
-        atomicMin(&amin[j], ((unsigned long long)__float_as_uint(sc.dist[lsol[t]]) << 32) | (uint32_t)r);
     }
     __syncthreads();
-    for (int t = tid; t < nm; t += nth) cand[las[t]] = lsol[t];
+    for (int t = tid; t < nm; t += nth) {
+        cand[las[t]] = lsol[t];
+        const int j = sc.assoc[count0 + t];
+        // distances are >= +0 (or FLT_MAX), so their bits order as the values do
+        if (cj[j] == 0) atomicMin(&pofs[j], __float_as_int(sc.dist[lsol[t]]));
+    }
+    __syncthreads();
+    for (int t = tid; t < nm; t += nth) {
+        const int j = sc.assoc[count0 + t];
+        if (cj[j] == 0 && __float_as_int(sc.dist[lsol[t]]) == pofs[j]) atomicMin(&kq[j], las[t] - coff[j]);
+    }
+    __syncthreads();
+    for (int j = tid; j < R; j += nth)
+        if (cj[j] == 0 && nj[j] > 0) {
+            int *cl = cand + coff[j];
+            const int slot = kq[j], last = nj[j] - 1, pick = cl[slot];
+            cl[slot] = cl[last];
+            cl[last] = pick;
+        }
     // active points per level, then picks before each level: lv[l] = picks at levels < l
     if (tid == 0) {
         sm.i0 = 0;
@@ -843,7 +869,7 @@ __global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc
             const int level = cj[j] + q;
             int slot = 0;
             if (level == 0) {
-                slot = (int)(uint32_t)amin[j];  // the first pick: the list is as built
+                slot = nc - 1;  // made while the lists were built: already at the end
             } else {
                 slot = (int)rng_uint(rnd[pofs[j] + q], (uint32_t)nc);
             }
@@ -875,14 +901,14 @@ __global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc
 
 size_t niche_smem_bytes(const Shape &s)
 {
-    return ((sizeof(SelSmem) + 15) & ~size_t(15)) + (size_t)s.R * sizeof(unsigned long long) +
+    return ((sizeof(SelSmem) + 15) & ~size_t(15)) +
            (size_t)(4 * s.R + 1 + 2 * s.N + 4 + 3 * 2 * s.N + s.R + 1 + s.N) * sizeof(int);
 }
 
 size_t select_smem_bytes(const Shape &s)
 {
     const int N2 = 2 * s.N, words = (N2 + 31) >> 5;
-    return ((sizeof(SelSmem) + 15) & ~size_t(15)) + (size_t)((words + 3) & ~3) * 4;
+    return ((sizeof(SelSmem) + 15) & ~size_t(15)) + (size_t)((words + 3) & ~3) * 4 + sizeof(ExtSmem);
 }
 
 cudaError_t launch_select(const Shape &s, const float *obj, float *ext, const float *refpts, SelectScratch sc,

@@ -109,7 +109,8 @@ def select_inputs(rng, N, M):
     return obj
 
 
-@pytest.mark.parametrize("N,M,p", [(32, 4, 4), (64, 4, 6), (100, 6, 3), (512, 4, 8), (1024, 4, 8)])
+@pytest.mark.parametrize("N,M,p", [(32, 4, 4), (64, 4, 6), (100, 6, 3), (512, 4, 8), (1024, 4, 8),
+                                   (2048, 6, 0), (4096, 4, 0)])
 def test_selection_matches_oracle(pe, orc, gpu, N, M, p):
     objset = 0 if M == 6 else 1
     tabc = pe.dirichlet_table(3)
@@ -184,6 +185,20 @@ def test_full_size_generation(pe, orc, gpu):
     o = prob.evaluate(ids[pick])
     for a, b in zip((obj[pick], objidx[pick], pql[pick]), o):
         assert same(a, b)
+
+
+def test_long_protein_large_population_fits(pe, gpu):
+    """L=3000, m=4, N=4096 with the reference's p rule (4060 reference points): the
+    selection and stem-scan kernels' shared memory still fits one CTA, and a
+    generation keeps N distinct survivors."""
+    tabc = pe.dirichlet_table(4)
+    aa = pe.synthetic_protein(3000, 5)
+    with pe.Engine(aa, tabc, 4, 4096, 0.02, objectives=1, ref_p=0, seed=3) as eng:
+        assert eng.R == 4060
+        eng.init()
+        eng.step(2)
+        surv = eng.population()[4]
+        assert len(set(surv.tolist())) == 4096
 
 
 def test_population_of_one_and_errors(pe, gpu):
