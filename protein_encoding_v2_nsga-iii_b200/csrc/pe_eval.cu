@@ -1205,16 +1205,29 @@ __global__ void __launch_bounds__(NT) k_sl(Shape s, PopBuf buf, int base, int2 *
     uint4 *E4 = reinterpret_cast<uint4 *>(tab);
     int *poffT = reinterpret_cast<int *>(E4 + 5 * PS);
     int *gstart = poffT + kSegPitch * NSP;
-    for (int e = tid; e < 5 * PS; e += nth) {
-        const int v = e / PS, x = e - v * PS - kEqGuard;
-        E4[e] = make_uint4(eq_word(Tlo, Thi, W, n, v, x), eq_word(Tlo, Thi, W, n, v, x + 1),
-                           eq_word(Tlo, Thi, W, n, v, x + 2), eq_word(Tlo, Thi, W, n, v, x + 3));
+    // each equality word once, stored into the four entries that hold it (entry x holds
+    // words x - kEqGuard .. x + 3 - kEqGuard, word j of the entry being word x - kEqGuard + j)
+    uint32_t *E4w = reinterpret_cast<uint32_t *>(E4);
+    for (int e = tid; e < 5 * (PS + 3); e += nth) {
+        const int v = e / (PS + 3), w = e - v * (PS + 3) - kEqGuard;
+        const uint32_t word = eq_word(Tlo, Thi, W, n, v, w);
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int x = w + kEqGuard - j;
+            if (x >= 0 && x < PS) E4w[(v * PS + x) * 4 + j] = word;
+        }
     }
     for (int e = tid; e < kSegPitch * NSP; e += nth) {
-        const int sp = e / kSegPitch, i = e - sp * kSegPitch, r = 32 * (sp - 1) + 2 * i;
-        const int v0 = (i < 16 && r >= 0 && r < n) ? plane_nt(S, r) : 4;
-        const int v1 = (i < 16 && r + 1 >= 0 && r + 1 < n) ? plane_nt(S, r + 1) : 4;
-        poffT[e] = (v0 * PS + (sp - 1)) | ((v1 * PS + (sp - 1)) << 16);  // E4 entries of rows r, r + 1
+        const int sp = e / kSegPitch, i = e - sp * kSegPitch;
+        int word = (4 * PS + sp - 1) * 0x10001;  // both rows outside [0, n): the zero plane
+        if (i < 16 && sp >= 1 && sp - 1 < W) {   // rows r = 32(sp-1) + 2i and r + 1
+            const uint2 sw = S[sp - 1];
+            const int b = 2 * i, r = 32 * (sp - 1) + b;
+            const int v0 = r < n ? (int)(((sw.x >> b) & 1u) | (((sw.y >> b) & 1u) << 1)) : 4;
+            const int v1 = r + 1 < n ? (int)(((sw.x >> (b + 1)) & 1u) | (((sw.y >> (b + 1)) & 1u) << 1)) : 4;
+            word = (v0 * PS + sp - 1) | ((v1 * PS + sp - 1) << 16);  // E4 entries of rows r, r + 1
+        }
+        poffT[e] = word;
     }
     if (warp == 0) {
         int carry = 0;
