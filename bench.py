@@ -64,14 +64,14 @@ def set_workload(shape: str | None, six: bool):
 METRIC = "generations/s"
 L2_FLUSH_BYTES = 256 << 20
 # k_sl at this workload, from ncu captures of one launch (profiles/k_sl_L1000_m8_N1024.md):
-# ALU-pipe warp instructions (75 % of its peak of 2 per SM per clock: the binding unit),
-# shared-memory data-pipe wavefronts (71 % of 1 per SM per clock), thread instructions and
+# ALU-pipe warp instructions (74 % of its peak of 2 per SM per clock, of active cycles),
+# shared-memory data-pipe wavefronts (73 % of 1 per SM per clock), thread instructions and
 # DRAM bytes per launch
-SL_SMEM_WAVEFRONTS_PER_LAUNCH = 96928102
-SL_ALU_WARP_INST_PER_LAUNCH = 180148993
-SL_THREAD_INST_PER_LAUNCH = 8941359021
-SL_DRAM_BYTES_PER_LAUNCH = 6366976
-SL_SMEM_PCT_NCU, SL_ALU_PIPE_PCT_NCU = 70.65, 75.01
+SL_SMEM_WAVEFRONTS_PER_LAUNCH = 97926106
+SL_ALU_WARP_INST_PER_LAUNCH = 174395757
+SL_THREAD_INST_PER_LAUNCH = 8717690016
+SL_DRAM_BYTES_PER_LAUNCH = 6365952
+SL_SMEM_PCT_NCU, SL_ALU_PIPE_PCT_NCU = 72.73, 74.38
 SM_COUNT, SMEM_WAVEFRONTS_PER_SM_CLK, ALU_WARP_INST_PER_SM_CLK = 148, 1, 2
 SL_CELLS_PER_LAUNCH = 36827144192      # 1024 x 8 CDSs of 3003 nucleotides
 # kernels one generation launches (one CUDA graph replay): k_variation, k_sl, k_dominance,
