@@ -62,12 +62,16 @@ __device__ __forceinline__ int nt_at(const SmemTab &st, const uint8_t *row, int 
 
 // Pack codon ids of every CDS into (lo, hi) nucleotide bit planes:
 // bit b of word w holds nucleotide 32w+b (A=00, C=01, G=10, U=11).
-__device__ void pack_planes(const Shape &s, const SmemTab &st, const uint8_t *ids, uint2 *planes, int tid, int nth)
+__device__ void pack_planes(const Shape &s, const SmemTab &st, const uint8_t *ids, uint2 *planes, int tid, int nth,
+                            const uint32_t *only = nullptr)
 {
     // word w holds nucleotides 32w .. 32w+31: the codons a0 = floor(32w/3) .. that
-    // overlap it contribute their 3-bit patterns at bit offset 3a - 32w
+    // overlap it contribute their 3-bit patterns at bit offset 3a - 32w.  With
+    // `only`, just the words whose bit is set there are packed (the others hold
+    // their values already).
     const int total = s.m * s.Wp;
     for (int e = tid; e < total; e += nth) {
+        if (only && !((only[e >> 5] >> (e & 31)) & 1u)) continue;
         int c = e / s.Wp, w = e - c * s.Wp;
         uint32_t lo = 0, hi = 0;
         if (w < s.W) {
@@ -562,6 +566,8 @@ __global__ void __launch_bounds__(kVarThreads) k_variation(Shape s, const DevTab
     uint8_t *ids = smem_raw + ((sizeof(VarSmem) + 15) & ~size_t(15));
     uint2 *planes = reinterpret_cast<uint2 *>(ids + (size_t)s.m * s.Lp);
     int8_t *aa = reinterpret_cast<int8_t *>(planes + (size_t)s.m * s.Wp);
+    // MODE_MUTATE: plane words the mutation touched (bit c * Wp + w)
+    uint32_t *dirty = reinterpret_cast<uint32_t *>(aa + ((s.L + 15) & ~15));
 
     const int tid = threadIdx.x, nth = blockDim.x;
     const int i = blockIdx.x;
@@ -596,6 +602,13 @@ __global__ void __launch_bounds__(kVarThreads) k_variation(Shape s, const DevTab
         const uint4 *g = reinterpret_cast<const uint4 *>(src.ids + (size_t)par * sol_bytes);
         uint4 *d = reinterpret_cast<uint4 *>(ids);
         for (size_t e = tid; e < sol_bytes / 16; e += nth) d[e] = g[e];
+        // the parent's planes: the child's differ only in the words its mutation touches
+        {
+            const uint4 *ps = reinterpret_cast<const uint4 *>(src.planes + (size_t)par * sol_words);
+            uint4 *pd = reinterpret_cast<uint4 *>(planes);
+            for (size_t e = tid; e < sol_words / 2; e += nth) pd[e] = ps[e];
+            for (int e = tid; e < (int)((sol_words + 31) / 32); e += nth) dirty[e] = 0u;
+        }
         if (tid < s.M) sm.pobj[tid] = src.obj[(size_t)par * s.M + tid];
         if (tid < 2 * s.M) sm.pobjidx[tid] = src.objidx[(size_t)par * 2 * s.M + tid];
         if (tid < 3) sm.ppql[tid] = src.pql[(size_t)par * 3 + tid];
@@ -626,9 +639,26 @@ __global__ void __launch_bounds__(kVarThreads) k_variation(Shape s, const DevTab
         }
         __syncthreads();
         mutate_solution(s, gt, sm, aa, ids, gen, ridx, tid, nth);
+        __syncthreads();
+        // mark the plane words of every 4-codon group that differs from the parent
+        // (codons a .. a+3 are nucleotides 3a .. 3a+11: one or two words)
+        for (size_t e = tid; e < sol_bytes / 16; e += nth) {
+            const uint4 pv = g[e], cv = reinterpret_cast<const uint4 *>(ids)[e];
+            const uint32_t pw[4] = {pv.x, pv.y, pv.z, pv.w}, cw[4] = {cv.x, cv.y, cv.z, cv.w};
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                if (pw[k] == cw[k]) continue;
+                const int q = 16 * (int)e + 4 * k, c = q / s.Lp, a = q - c * s.Lp;
+                const int w0 = (3 * a) >> 5, w1 = min((3 * a + 11) >> 5, s.W - 1);
+                for (int w = w0; w <= w1; w++) {
+                    const int bit = c * s.Wp + w;
+                    atomicOr(&dirty[bit >> 5], 1u << (bit & 31));
+                }
+            }
+        }
     }
     __syncthreads();
-    pack_planes(s, sm.tab, ids, planes, tid, nth);
+    pack_planes(s, sm.tab, ids, planes, tid, nth, MODE == MODE_MUTATE ? dirty : nullptr);
     __syncthreads();
     // write the (new) solution
     if (MODE != MODE_EVAL) {
@@ -648,7 +678,7 @@ __global__ void __launch_bounds__(kVarThreads) k_variation(Shape s, const DevTab
 size_t var_smem_bytes(const Shape &s)
 {
     return ((sizeof(VarSmem) + 15) & ~size_t(15)) + (size_t)s.m * s.Lp + (size_t)s.m * s.Wp * sizeof(uint2) +
-           (size_t)((s.L + 15) & ~15);
+           (size_t)((s.L + 15) & ~15) + (size_t)((s.m * s.Wp + 31) / 32) * sizeof(uint32_t);
 }
 
 cudaError_t raise_smem_limit(const void *func, size_t bytes)
