@@ -124,7 +124,9 @@ int pe_step(pe_instance *inst, int32_t generations);
 int pe_synchronize(pe_instance *inst);
 
 /* Current 2N set (parents then offspring of the last generation) and survivors
- * (src/main.cu:772-787).  Any pointer may be NULL. */
+ * (src/main.cu:772-787).  Any pointer may be NULL.  Waits for the instance's
+ * stream; call it between pe_step calls (the codon ids are packed on the device in
+ * the buffer the next generation overwrites). */
 int pe_get_population(pe_instance *inst, uint8_t *codon_idx, float *obj, int8_t *objidx, int32_t *pql,
                       int32_t *survivors);
 /* Objectives only (2N*M floats): the per-generation progress read. */
