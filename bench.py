@@ -64,16 +64,19 @@ def set_workload(shape: str | None, six: bool):
 METRIC = "generations/s"
 L2_FLUSH_BYTES = 256 << 20
 # k_sl at this workload, from ncu captures of one launch (profiles/k_sl_L1000_m8_N1024.md):
-# ALU-pipe warp instructions (74 % of its peak of 2 per SM per clock, of active cycles),
-# shared-memory data-pipe wavefronts (73 % of 1 per SM per clock), thread instructions and
+# ALU-pipe warp instructions (57 % of its peak of 2 per SM per clock, of active cycles),
+# shared-memory data-pipe wavefronts (45 % of 1 per SM per clock), thread instructions and
 # DRAM bytes per launch
-SL_SMEM_WAVEFRONTS_PER_LAUNCH = 97926106
-SL_ALU_WARP_INST_PER_LAUNCH = 174395757
-SL_THREAD_INST_PER_LAUNCH = 8717690016
-SL_DRAM_BYTES_PER_LAUNCH = 6365952
-SL_SMEM_PCT_NCU, SL_ALU_PIPE_PCT_NCU = 72.73, 74.38
+SL_SMEM_WAVEFRONTS_PER_LAUNCH = 27719685
+SL_ALU_WARP_INST_PER_LAUNCH = 56379096
+SL_THREAD_INST_PER_LAUNCH = 2542106810
+SL_DRAM_BYTES_PER_LAUNCH = 2310912
+SL_SMEM_PCT_NCU, SL_ALU_PIPE_PCT_NCU = 45.36, 57.09
 SM_COUNT, SMEM_WAVEFRONTS_PER_SM_CLK, ALU_WARP_INST_PER_SM_CLK = 148, 1, 2
-SL_CELLS_PER_LAUNCH = 36827144192      # 1024 x 8 CDSs of 3003 nucleotides
+# CDSs the captured launch scanned (of 1024 x 8: the others kept their parents' results)
+# and its counted cells (4495501 per CDS of 3003 nucleotides)
+SL_CDS_PER_LAUNCH = 2311
+SL_CELLS_PER_LAUNCH = SL_CDS_PER_LAUNCH * 4495501
 # kernels one generation launches (one CUDA graph replay): k_variation, k_sl, k_dominance,
 # k_select, k_assoc, k_niche
 KERNELS_PER_GENERATION = 6
@@ -101,7 +104,7 @@ def roofline(cells: int, sl_seconds: float, clocks: dict) -> dict:
     during the timed region) and the shared-memory data pipe (wavefronts per launch
     against 1 per SM per clock).  The headline figures are those of the unit with the
     larger fraction; the other is reported beside them."""
-    scale = cells / SL_CELLS_PER_LAUNCH   # the ncu counts are for the default shape
+    scale = cells / SL_CELLS_PER_LAUNCH   # the ncu counts are for one launch of the default shape
     mhz = clocks.get("sm_mhz") or 1965.0
     smem = SL_SMEM_WAVEFRONTS_PER_LAUNCH * scale / sl_seconds / 1e9
     smem_peak = SM_COUNT * SMEM_WAVEFRONTS_PER_SM_CLK * mhz * 1e6 / 1e9
@@ -123,6 +126,7 @@ def roofline(cells: int, sl_seconds: float, clocks: dict) -> dict:
             other: {k: v for k, v in units[other].items() if k != "peak_source"},
             "algorithmic_bytes_per_launch": SL_DRAM_BYTES_PER_LAUNCH * scale,
             "cells_per_launch": cells, "cells_per_s": cells / sl_seconds,
+            "counted_cells": "cells of the CDSs scanned (unchanged CDSs keep their parents' results)",
             "lane_ops_per_cell": SL_THREAD_INST_PER_LAUNCH / SL_CELLS_PER_LAUNCH,
             "ncu_pct_of_peak": {"smem_wavefronts": SL_SMEM_PCT_NCU, "alu_pipe": SL_ALU_PIPE_PCT_NCU},
             "instruction_count": "ncu, L=1000 m=8 N=1024" + ("" if cells == SL_CELLS_PER_LAUNCH else "; scaled by cells")}
@@ -270,6 +274,7 @@ def run_ours(args, world, rank, local):
     for _ in range(args.warmup):
         eng.step(1)
     eng.synchronize()
+    scans0 = eng.scan_count()
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     stage = np.zeros(3)
@@ -299,7 +304,10 @@ def run_ours(args, world, rank, local):
     value = world * args.steps / max_s
     stage_ms = stage / args.steps
     n_nt = 3 * (L_AA + 1)
-    cells = POP * M_CDS * hairpin_cells_per_cds(n_nt)
+    # a child's CDS that its mutation left unchanged keeps its parent's stem result:
+    # the stem-scan work is the CDSs actually scanned
+    scans_per_gen = (eng.scan_count() - scans0) / args.steps
+    cells = scans_per_gen * hairpin_cells_per_cds(n_nt)
     sl_s = stage_ms[1] / 1000.0
 
     # end-to-end through the public API with host buffers: every rank runs a design job of
@@ -427,6 +435,7 @@ def run_batched(args):
             b.step(G)
             b.synchronize()
         t_batch = time.perf_counter() - t0
+    scanned_cells = sum(e.scan_count() * hairpin_cells_per_cds(3 * (L + 1)) for e, (L, _, _) in zip(engines, jobs))
     for e in engines:
         e.close()
     line = {"metric": "designs/s", "value": len(jobs) / t_batch, "unit": "designs/s", "n_gpus": 1,
@@ -436,7 +445,8 @@ def run_batched(args):
                                    f"N={N}, Pm={pm}, 4 objectives, {G} generations, one graph launch per 2 "
                                    f"generations for all instances",
                        "plain_designs_per_s": len(jobs) / t_plain, "batched_over_plain": t_plain / t_batch,
-                       "stem_cells_per_s": cells / t_batch,
+                       "stem_cells_per_s": scanned_cells / t_batch,
+                       "stem_cells_scanned_of_all": scanned_cells / cells,
                        "timing": "wall clock per mode, each including create + init + all generations"},
             "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
@@ -566,9 +576,12 @@ def main():
         eng = pe.Engine(pe.synthetic_protein(L_AA, SEED), pe.dirichlet_table(SEED), M_CDS, POP, PM,
                         objectives=pe.OBJ_BASE4, ref_p=P_REF, seed=SEED, sl_threads=128)
         eng.init()
-        eng.step(2)
-        eng.synchronize()
+        scans = [eng.scan_count()]
+        for _ in range(2):
+            eng.step(1)
+            scans.append(eng.scan_count())
         eng.close()
+        print(json.dumps({"cds_scans_per_launch": [scans[0]] + [b - a for a, b in zip(scans, scans[1:])]}))
         return
     if args.impl == "reference":
         run_reference(args, world, rank)

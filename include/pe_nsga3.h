@@ -189,6 +189,10 @@ int pe_set_profiling(pe_instance *inst, int32_t enable);
 /* Device milliseconds of those stages in the last completed generation
  * (call after pe_synchronize). */
 int pe_stage_times(pe_instance *inst, float *ms3);
+/* CDS stem scans run since pe_create (no reference counterpart): a child's CDS
+ * that its mutation left unchanged keeps its parent's stem result and is not
+ * scanned again.  Waits for the instance's stream. */
+int pe_scan_count(pe_instance *inst, uint64_t *count);
 
 /* --- allocation-free hairpin-stem evaluation (no counterpart in the reference).
  *

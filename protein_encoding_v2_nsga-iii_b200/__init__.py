@@ -116,7 +116,7 @@ def lib() -> C.CDLL:
             "pe_dirichlet_table": [C.c_uint64, C.POINTER(CodonTable)],
             "pe_load_codon_table": [C.c_char_p, C.POINTER(CodonTable)],
             "pe_hypervolume": [P, C.c_int32, C.c_int32, P, C.POINTER(C.c_double)],
-            "pe_set_profiling": [P, C.c_int32], "pe_stage_times": [P, P],
+            "pe_set_profiling": [P, C.c_int32], "pe_stage_times": [P, P], "pe_scan_count": [P, P],
             "pe_hairpin_noalloc": [P, C.c_int32, C.c_int32, C.c_int32, P, P, P, P],
             "pe_batch_create": [P, C.c_int32, C.POINTER(P)], "pe_batch_step": [P, C.c_int32],
             "pe_batch_synchronize": [P], "pe_batch_destroy": [P],
@@ -275,6 +275,12 @@ class Engine:
         out = np.zeros(3, np.float32)
         _ck(lib().pe_stage_times(self._h, _ptr(out)))
         return out
+
+    def scan_count(self) -> int:
+        """CDS stem scans run so far (a child's unchanged CDS keeps its parent's result)."""
+        v = C.c_uint64(0)
+        _ck(lib().pe_scan_count(self._h, C.byref(v)))
+        return v.value
 
     def population(self):
         N2 = 2 * self.N

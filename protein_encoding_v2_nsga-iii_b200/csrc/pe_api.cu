@@ -162,6 +162,7 @@ struct pe_instance {
     int2 *d_part = nullptr;
     int32_t *d_counter = nullptr;
     int32_t *d_status = nullptr;
+    unsigned long long *d_scanned = nullptr;  // CDS stem scans run
     float *d_ext = nullptr;
     uint32_t *d_gen = nullptr;
     int cur = 0;
@@ -197,11 +198,13 @@ int alloc_pop(pe_instance *in, PopBuf &b, int nsol)
     if ((rc = in->alloc(&b.obj, (size_t)nsol * s.M))) return rc;
     if ((rc = in->alloc(&b.objidx, (size_t)nsol * 2 * s.M))) return rc;
     if ((rc = in->alloc(&b.pql, (size_t)nsol * 3))) return rc;
+    if ((rc = in->alloc(&b.cds, (size_t)nsol * s.m))) return rc;
     CK(cudaMemsetAsync(b.ids, 0, (size_t)nsol * s.m * s.Lp, in->stream));
     CK(cudaMemsetAsync(b.planes, 0, (size_t)nsol * s.m * s.Wp * sizeof(uint2), in->stream));
     CK(cudaMemsetAsync(b.obj, 0, (size_t)nsol * s.M * sizeof(float), in->stream));
     CK(cudaMemsetAsync(b.objidx, 0, (size_t)nsol * 2 * s.M, in->stream));
     CK(cudaMemsetAsync(b.pql, 0, (size_t)nsol * 3 * sizeof(int32_t), in->stream));
+    CK(cudaMemsetAsync(b.cds, 0xff, (size_t)nsol * s.m * sizeof(int2), in->stream));  // x = -1: to scan
     return PE_OK;
 }
 
@@ -261,7 +264,7 @@ cudaError_t enqueue_generation(pe_instance *in, int src)
                       nullptr, in->stream);
     if (e != cudaSuccess) return e;
     if ((e = mark(in, 1)) != cudaSuccess) return e;
-    e = launch_sl(s, in->buf[dst], s.N, s.N, in->d_part, in->d_counter, in->d_status, in->stream);
+    e = launch_sl(s, in->buf[dst], s.N, s.N, in->d_part, in->d_counter, in->d_status, in->stream, in->d_scanned);
     if (e != cudaSuccess) return e;
     if ((e = mark(in, 2)) != cudaSuccess) return e;
     e = launch_select(s, in->buf[dst].obj, in->d_ext, in->d_ref, in->sc, in->d_surv, in->d_gen, 1, in->stream);
@@ -497,6 +500,7 @@ int pe_create(const pe_config *cfg, const int8_t *aa_idx, int32_t aa_len, const 
     if ((rc = in->alloc(&in->sc.finfo, 3 * PE_MAX_OBJ))) return cleanup(rc);
     if ((rc = in->alloc(&in->d_part, (size_t)N2 * m))) return cleanup(rc);
     if ((rc = in->alloc(&in->d_counter, (size_t)N2))) return cleanup(rc);
+    if ((rc = in->alloc(&in->d_scanned, 1))) return cleanup(rc);
     if ((rc = in->alloc(&in->d_status, 1))) return cleanup(rc);
     if ((rc = in->alloc(&in->d_ext, (size_t)s.M * s.M))) return cleanup(rc);
     if ((rc = in->alloc(&in->d_gen, 1))) return cleanup(rc);
@@ -512,6 +516,7 @@ int pe_create(const pe_config *cfg, const int8_t *aa_idx, int32_t aa_len, const 
     CKC(cudaMemcpyAsync(in->d_aa, aa_idx, (size_t)L, cudaMemcpyHostToDevice, st));
     CKC(cudaMemcpyAsync(in->d_ref, ref.data(), ref.size() * sizeof(float), cudaMemcpyHostToDevice, st));
     CKC(cudaMemsetAsync(in->d_counter, 0, (size_t)N2 * sizeof(int32_t), st));
+    CKC(cudaMemsetAsync(in->d_scanned, 0, sizeof(unsigned long long), st));
     CKC(cudaMemsetAsync(in->d_status, 0, sizeof(int32_t), st));
     CKC(cudaMemsetAsync(in->d_ext, 0, (size_t)s.M * s.M * sizeof(float), st));
     CKC(cudaMemsetAsync(in->d_gen, 0, sizeof(uint32_t), st));
@@ -679,6 +684,16 @@ int pe_stage_times(pe_instance *in, float *ms3)
     return PE_OK;
 }
 
+int pe_scan_count(pe_instance *in, uint64_t *count)
+{
+    if (!in || !count) return fail(PE_ERR_ARG, "null argument");
+    unsigned long long v = 0;
+    CK(cudaMemcpyAsync(&v, in->d_scanned, sizeof v, cudaMemcpyDeviceToHost, in->stream));
+    CK(cudaStreamSynchronize(in->stream));
+    *count = (uint64_t)v;
+    return PE_OK;
+}
+
 int pe_instance_bytes(const pe_config *cfg, int32_t aa_len, uint64_t *bytes)
 {
     if (!cfg || !bytes || aa_len < 3 || cfg->pop_size < 1 || cfg->n_cds < 2) return fail(PE_ERR_ARG, "bad arguments");
@@ -698,6 +713,7 @@ int pe_instance_bytes(const pe_config *cfg, int32_t aa_len, uint64_t *bytes)
     t += 2 * (r(N2 * m * Lp) + r(N2 * m * Wp * 8) + r(N2 * M * 4) + r(N2 * 2 * M) + r(N2 * 12));
     t += r(N * 4) + r(N2 * words * 4) + 6 * r(N2 * 4) + 3 * r(R * 4) + r((R + 1) * 4) + r(32) + r(72);
     t += r(N2 * m * 8) + r(N2 * 4) + r(4) + r(M * M * 4) + r(4);
+    t += 2 * r(N2 * m * 8) + r(8);  // per-CDS stem results of both buffers, scan count
     *bytes = t;
     return PE_OK;
 }
@@ -751,12 +767,17 @@ int pe_init_population(pe_instance *in)
             for (int k = 0; k < 4 && e == cudaSuccess; k++) e = cudaEventCreate(&ev[k]);
             const int sizes[3] = {64, 128, 256};
             s.sl_threads = 128;
-            if (e == cudaSuccess) e = launch_sl(s, in->buf[0], 0, s.N, in->d_part, in->d_counter, in->d_status, in->stream);
+            // the warm scan stores the per-CDS results; the timed ones scan every CDS
+            // (no carried results) and rewrite the same objectives
+            PopBuf full = in->buf[0];
+            full.cds = nullptr;
+            if (e == cudaSuccess)
+                e = launch_sl(s, in->buf[0], 0, s.N, in->d_part, in->d_counter, in->d_status, in->stream,
+                              in->d_scanned);
             for (int k = 0; k < 3 && e == cudaSuccess; k++) {
                 s.sl_threads = sizes[k];
                 e = cudaEventRecord(ev[k], in->stream);
-                if (e == cudaSuccess)
-                    e = launch_sl(s, in->buf[0], 0, s.N, in->d_part, in->d_counter, in->d_status, in->stream);
+                if (e == cudaSuccess) e = launch_sl(s, full, 0, s.N, in->d_part, in->d_counter, in->d_status, in->stream);
             }
             if (e == cudaSuccess) e = cudaEventRecord(ev[3], in->stream);
             if (e == cudaSuccess) e = cudaEventSynchronize(ev[3]);
@@ -783,7 +804,8 @@ int pe_init_population(pe_instance *in)
                 in->graph[i] = nullptr;
             }
     }
-    if (!scanned) CK(launch_sl(s, in->buf[0], 0, s.N, in->d_part, in->d_counter, in->d_status, in->stream));
+    if (!scanned)
+        CK(launch_sl(s, in->buf[0], 0, s.N, in->d_part, in->d_counter, in->d_status, in->stream, in->d_scanned));
     // extreme points start as the objective vectors of solutions 0..M-1
     // (initializationKernel, src/main.cu:106-109)
     CK(cudaMemsetAsync(in->d_ext, 0, (size_t)s.M * s.M * sizeof(float), in->stream));

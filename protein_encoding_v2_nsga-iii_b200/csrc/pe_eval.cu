@@ -591,10 +591,14 @@ __global__ void __launch_bounds__(kVarThreads) k_variation(Shape s, const DevTab
         for (int c = 0; c < s.m; c++)
             for (int a = s.L + tid; a < s.Lp; a += nth) ids[c * s.Lp + a] = 0;
         if (tid == 0 && surv) surv[i] = i;
+        if (dst.cds)
+            for (int c = tid; c < s.m; c += nth) dst.cds[(size_t)i * s.m + c] = make_int2(-1, 0);
     } else if (MODE == MODE_EVAL) {
         const uint4 *g = reinterpret_cast<const uint4 *>(dst.ids + (size_t)i * sol_bytes);
         uint4 *d = reinterpret_cast<uint4 *>(ids);
         for (size_t e = tid; e < sol_bytes / 16; e += nth) d[e] = g[e];
+        if (dst.cds)
+            for (int c = tid; c < s.m; c += nth) dst.cds[(size_t)i * s.m + c] = make_int2(-1, 0);
     } else {  // MODE_MUTATE
         gen = *d_gen;
         ridx = rng_idx ? (uint32_t)rng_idx[i] : (uint32_t)i;
@@ -623,6 +627,9 @@ __global__ void __launch_bounds__(kVarThreads) k_variation(Shape s, const DevTab
             if (tid < s.M) dst.obj[dslot * s.M + tid] = src.obj[(size_t)par * s.M + tid];
             if (tid < 2 * s.M) dst.objidx[dslot * 2 * s.M + tid] = src.objidx[(size_t)par * 2 * s.M + tid];
             if (tid < 3) dst.pql[dslot * 3 + tid] = src.pql[(size_t)par * 3 + tid];
+            if (dst.cds)
+                for (int c = tid; c < s.m; c += nth)
+                    dst.cds[dslot * s.m + c] = src.cds ? src.cds[(size_t)par * s.m + c] : make_int2(-1, 0);
         }
         out_slot = child_base + i;
         if (tid == 0) {
@@ -659,6 +666,20 @@ __global__ void __launch_bounds__(kVarThreads) k_variation(Shape s, const DevTab
     }
     __syncthreads();
     pack_planes(s, sm.tab, ids, planes, tid, nth, MODE == MODE_MUTATE ? dirty : nullptr);
+    if (MODE == MODE_MUTATE && dst.cds) {
+        // a CDS none of whose plane words changed keeps its parent's hairpin result
+        const int par = parent_of[i];
+        for (int c = tid; c < s.m; c += nth) {
+            bool changed = src.cds == nullptr;
+            const int b0 = c * s.Wp, b1 = b0 + s.Wp;  // this CDS's bits [b0, b1)
+            for (int wd = b0 >> 5; wd <= (b1 - 1) >> 5 && !changed; wd++) {
+                const int lo = max(b0, 32 * wd) - 32 * wd, hi = min(b1, 32 * wd + 32) - 32 * wd;
+                const uint32_t mask = hi - lo == 32 ? ~0u : ((1u << (hi - lo)) - 1u) << lo;
+                changed = (dirty[wd] & mask) != 0u;
+            }
+            dst.cds[(size_t)out_slot * s.m + c] = changed ? make_int2(-1, 0) : src.cds[(size_t)par * s.m + c];
+        }
+    }
     __syncthreads();
     // write the (new) solution
     if (MODE != MODE_EVAL) {
@@ -1143,7 +1164,7 @@ __device__ __forceinline__ int plane_nt(const uint2 *P, int x)
 
 template <int NT>
 __global__ void __launch_bounds__(NT) k_sl(Shape s, PopBuf buf, int base, int2 *part, int32_t *counter,
-                                                 int32_t *status)
+                                                 int32_t *status, unsigned long long *scanned)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SlSmem<NT> &sm = *reinterpret_cast<SlSmem<NT> *>(smem_raw);
@@ -1160,40 +1181,32 @@ __global__ void __launch_bounds__(NT) k_sl(Shape s, PopBuf buf, int base, int2 *
     const size_t gsol = (size_t)(base + sol);
     const uint2 *P = buf.planes + (gsol * s.m + c) * s.Wp;
 
-    // stage S (the CDS planes) with one bulk async copy (TMA engine)
-    {
-        __shared__ __align__(8) uint64_t bar;
-        const uint32_t bytes = (uint32_t)(s.Wp * sizeof(uint2));
-        uint32_t bar_a = (uint32_t)__cvta_generic_to_shared(&bar);
-        if (tid == 0) {
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a));
-            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        }
-        __syncthreads();
-        if (tid == 0) {
-            uint32_t dst_a = (uint32_t)__cvta_generic_to_shared(S);
-            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a), "r"(bytes) : "memory");
-            asm volatile(
-                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst_a),
-                "l"(P), "r"(bytes), "r"(bar_a)
-                : "memory");
-        }
-        // bounded wait on phase 0
-        int done = 0;
-        for (int it = 0; it < (1 << 22) && !done; it++) {
-            uint32_t ok;
-            asm volatile(
-                "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
-                : "=r"(ok)
-                : "r"(bar_a), "r"(0u)
-                : "memory");
-            done = (int)ok;
-        }
-        // the copy engine never completed: flag it, give the copy a second
-        // bounded window to land, and leave this CTA (the host reports PE_ERR_TIMEOUT)
-        if (__syncthreads_or(!done)) {
-            if (tid == 0) atomicOr(status, 1);
-            for (int it = 0; it < (1 << 20) && !done; it++) {
+    // this CDS's result: carried over from the parent when the mutation left the CDS
+    // as it was, else found by the scan below
+    int2 *res = buf.cds ? buf.cds + gsol * s.m : part + (size_t)sol * s.m;
+    const bool reuse = buf.cds != nullptr && res[c].x >= 0;
+    if (!reuse) {
+        // stage S (the CDS planes) with one bulk async copy (TMA engine)
+        {
+            __shared__ __align__(8) uint64_t bar;
+            const uint32_t bytes = (uint32_t)(s.Wp * sizeof(uint2));
+            uint32_t bar_a = (uint32_t)__cvta_generic_to_shared(&bar);
+            if (tid == 0) {
+                asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a));
+                asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            }
+            __syncthreads();
+            if (tid == 0) {
+                uint32_t dst_a = (uint32_t)__cvta_generic_to_shared(S);
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a), "r"(bytes) : "memory");
+                asm volatile(
+                    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst_a),
+                    "l"(P), "r"(bytes), "r"(bar_a)
+                    : "memory");
+            }
+            // bounded wait on phase 0
+            int done = 0;
+            for (int it = 0; it < (1 << 22) && !done; it++) {
                 uint32_t ok;
                 asm volatile(
                     "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
@@ -1202,115 +1215,105 @@ __global__ void __launch_bounds__(NT) k_sl(Shape s, PopBuf buf, int base, int2 *
                     : "memory");
                 done = (int)ok;
             }
-            return;
-        }
-        if (tid == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(bar_a));
-        for (int w = s.Wp + tid; w < W + 2; w += nth) S[w] = make_uint2(0u, 0u);
-    }
-    __syncthreads();
-    // reverse complement planes, zero outside [0, W)
-    for (int e = tid; e < W + 2 * G + 1; e += nth) {
-        int w = e - G;
-        uint32_t lo = 0, hi = 0;
-        if (w >= 0 && w < W) {
-            int start = n - 32 - 32 * w;  // source bit of T bit 31 ... bit 0 is source n-1-32w
-            int q = start >> 5, sh = start & 31;
-            uint32_t a0 = (q >= 0 && q < W) ? S[q].x : 0u, a1 = (q + 1 >= 0 && q + 1 < W) ? S[q + 1].x : 0u;
-            uint32_t b0 = (q >= 0 && q < W) ? S[q].y : 0u, b1 = (q + 1 >= 0 && q + 1 < W) ? S[q + 1].y : 0u;
-            lo = ~__brev(fshr(a0, a1, sh));
-            hi = ~__brev(fshr(b0, b1, sh));
-        }
-        Tlo[e] = lo;
-        Thi[e] = hi;
-    }
-    __syncthreads();
-    // band-scan tables, in the space the shifted copies of T take later:
-    //   E4[v][x]      E_v words x-kEqGuard .. x+3-kEqGuard, v = 0..3 nucleotides, 4 the zero plane
-    //   poffT[sp][i]  rows r = 32(sp-1)+2i, r+1: E4 entries v(r)*PS + sp-1 in the low and high
-    //                 16 bits (v(r) = 4 outside [0, n); 5*PS < 65536 since E4's 80*PS bytes fit in
-    //                 shared memory); pitch 17 words
-    //   gstart[g]     first item of band group g (items: the group's 32-row segments)
-    const int PS = sl_plane_stride(W), NSP = W + 2;
-    const int ng = sl_num_groups(n), D0 = sl_band_base(n);
-    uint4 *E4 = reinterpret_cast<uint4 *>(tab);
-    int *poffT = reinterpret_cast<int *>(E4 + 5 * PS);
-    int *gstart = poffT + kSegPitch * NSP;
-    // each equality word once, stored into the four entries that hold it (entry x holds
-    // words x - kEqGuard .. x + 3 - kEqGuard, word j of the entry being word x - kEqGuard + j)
-    uint32_t *E4w = reinterpret_cast<uint32_t *>(E4);
-    for (int e = tid; e < 5 * (PS + 3); e += nth) {
-        const int v = e / (PS + 3), w = e - v * (PS + 3) - kEqGuard;
-        const uint32_t word = eq_word(Tlo, Thi, W, n, v, w);
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const int x = w + kEqGuard - j;
-            if (x >= 0 && x < PS) E4w[(v * PS + x) * 4 + j] = word;
-        }
-    }
-    for (int e = tid; e < kSegPitch * NSP; e += nth) {
-        const int sp = e / kSegPitch, i = e - sp * kSegPitch;
-        int word = (4 * PS + sp - 1) * 0x10001;  // both rows outside [0, n): the zero plane
-        if (i < 16 && sp >= 1 && sp - 1 < W) {   // rows r = 32(sp-1) + 2i and r + 1
-            const uint2 sw = S[sp - 1];
-            const int b = 2 * i, r = 32 * (sp - 1) + b;
-            const int v0 = r < n ? (int)(((sw.x >> b) & 1u) | (((sw.y >> b) & 1u) << 1)) : 4;
-            const int v1 = r + 1 < n ? (int)(((sw.x >> (b + 1)) & 1u) | (((sw.y >> (b + 1)) & 1u) << 1)) : 4;
-            word = (v0 * PS + sp - 1) | ((v1 * PS + sp - 1) << 16);  // E4 entries of rows r, r + 1
-        }
-        poffT[e] = word;
-    }
-    if (warp == 0) {
-        int carry = 0;
-        for (int g0 = 0; g0 < ng; g0 += 32) {
-            const int g = g0 + lane;
-            int x = 0;
-            if (g < ng) {
-                int s_lo, s_hi;
-                sl_group_segments(n, D0 + 32 * kBandGroup * g, s_lo, s_hi);
-                x = s_hi - s_lo + 1;
+            // the copy engine never completed: flag it, give the copy a second
+            // bounded window to land, and leave this CTA (the host reports PE_ERR_TIMEOUT)
+            if (__syncthreads_or(!done)) {
+                if (tid == 0) atomicOr(status, 1);
+                for (int it = 0; it < (1 << 20) && !done; it++) {
+                    uint32_t ok;
+                    asm volatile(
+                        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+                        : "=r"(ok)
+                        : "r"(bar_a), "r"(0u)
+                        : "memory");
+                    done = (int)ok;
+                }
+                return;
             }
-            for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(0xffffffffu, x, o);
-                if (lane >= o) x += y;
-            }
-            if (g < ng) gstart[g + 1] = carry + x;
-            carry += __shfl_sync(0xffffffffu, x, 31);
+            if (tid == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(bar_a));
+            for (int w = s.Wp + tid; w < W + 2; w += nth) S[w] = make_uint2(0u, 0u);
         }
-        if (lane == 0) gstart[0] = 0;
-    }
-    if (tid == 0) sm.next_chunk = 0;
-    __syncthreads();
+        __syncthreads();
+        // reverse complement planes, zero outside [0, W)
+        for (int e = tid; e < W + 2 * G + 1; e += nth) {
+            int w = e - G;
+            uint32_t lo = 0, hi = 0;
+            if (w >= 0 && w < W) {
+                int start = n - 32 - 32 * w;  // source bit of T bit 31 ... bit 0 is source n-1-32w
+                int q = start >> 5, sh = start & 31;
+                uint32_t a0 = (q >= 0 && q < W) ? S[q].x : 0u, a1 = (q + 1 >= 0 && q + 1 < W) ? S[q + 1].x : 0u;
+                uint32_t b0 = (q >= 0 && q < W) ? S[q].y : 0u, b1 = (q + 1 >= 0 && q + 1 < W) ? S[q + 1].y : 0u;
+                lo = ~__brev(fshr(a0, a1, sh));
+                hi = ~__brev(fshr(b0, b1, sh));
+            }
+            Tlo[e] = lo;
+            Thi[e] = hi;
+        }
+        __syncthreads();
+        // band-scan tables, in the space the shifted copies of T take later:
+        //   E4[v][x]      E_v words x-kEqGuard .. x+3-kEqGuard, v = 0..3 nucleotides, 4 the zero plane
+        //   poffT[sp][i]  rows r = 32(sp-1)+2i, r+1: E4 entries v(r)*PS + sp-1 in the low and high
+        //                 16 bits (v(r) = 4 outside [0, n); 5*PS < 65536 since E4's 80*PS bytes fit in
+        //                 shared memory); pitch 17 words
+        //   gstart[g]     first item of band group g (items: the group's 32-row segments)
+        const int PS = sl_plane_stride(W), NSP = W + 2;
+        const int ng = sl_num_groups(n), D0 = sl_band_base(n);
+        uint4 *E4 = reinterpret_cast<uint4 *>(tab);
+        int *poffT = reinterpret_cast<int *>(E4 + 5 * PS);
+        int *gstart = poffT + kSegPitch * NSP;
+        // each equality word once, stored into the four entries that hold it (entry x holds
+        // words x - kEqGuard .. x + 3 - kEqGuard, word j of the entry being word x - kEqGuard + j)
+        uint32_t *E4w = reinterpret_cast<uint32_t *>(E4);
+        for (int e = tid; e < 5 * (PS + 3); e += nth) {
+            const int v = e / (PS + 3), w = e - v * (PS + 3) - kEqGuard;
+            const uint32_t word = eq_word(Tlo, Thi, W, n, v, w);
+    #pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int x = w + kEqGuard - j;
+                if (x >= 0 && x < PS) E4w[(v * PS + x) * 4 + j] = word;
+            }
+        }
+        for (int e = tid; e < kSegPitch * NSP; e += nth) {
+            const int sp = e / kSegPitch, i = e - sp * kSegPitch;
+            int word = (4 * PS + sp - 1) * 0x10001;  // both rows outside [0, n): the zero plane
+            if (i < 16 && sp >= 1 && sp - 1 < W) {   // rows r = 32(sp-1) + 2i and r + 1
+                const uint2 sw = S[sp - 1];
+                const int b = 2 * i, r = 32 * (sp - 1) + b;
+                const int v0 = r < n ? (int)(((sw.x >> b) & 1u) | (((sw.y >> b) & 1u) << 1)) : 4;
+                const int v1 = r + 1 < n ? (int)(((sw.x >> (b + 1)) & 1u) | (((sw.y >> (b + 1)) & 1u) << 1)) : 4;
+                word = (v0 * PS + sp - 1) | ((v1 * PS + sp - 1) << 16);  // E4 entries of rows r, r + 1
+            }
+            poffT[e] = word;
+        }
+        if (warp == 0) {
+            int carry = 0;
+            for (int g0 = 0; g0 < ng; g0 += 32) {
+                const int g = g0 + lane;
+                int x = 0;
+                if (g < ng) {
+                    int s_lo, s_hi;
+                    sl_group_segments(n, D0 + 32 * kBandGroup * g, s_lo, s_hi);
+                    x = s_hi - s_lo + 1;
+                }
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, x, o);
+                    if (lane >= o) x += y;
+                }
+                if (g < ng) gstart[g + 1] = carry + x;
+                carry += __shfl_sync(0xffffffffu, x, 31);
+            }
+            if (lane == 0) gstart[0] = 0;
+        }
+        if (tid == 0) sm.next_chunk = 0;
+        __syncthreads();
 
-    int best = 0, bestd = 0x7fffffff;
-    sl_band_scan(E4, poffT, gstart, ng, S, Tlo, Thi, n, sm.queue[warp], &sm.next_chunk, lane, best, bestd);
-    // CTA reduction of (best, smallest anti-diagonal)
-    for (int o = 16; o > 0; o >>= 1) {
-        int ob = __shfl_xor_sync(0xffffffffu, best, o), od = __shfl_xor_sync(0xffffffffu, bestd, o);
-        pair_reduce(best, bestd, ob, od);
-    }
-    if (lane == 0) {
-        sm.wbest[warp] = best;
-        sm.wbestd[warp] = bestd;
-    }
-    __syncthreads();
-    if (tid == 0) {
-        int b = sm.wbest[0], d = sm.wbestd[0];
-        for (int w = 1; w < nwarps; w++) pair_reduce(b, d, sm.wbest[w], sm.wbestd[w]);
-        sm.res[0] = b;
-        sm.res[1] = d;
-        sm.next_chunk = 0;
-    }
-    __syncthreads();
-    if (sm.res[0] < 8) {
-        // no run reaches 8: exact per-word runs
-        best = 0;
-        bestd = 0x7fffffff;
-        sl_scan(S, Tlo, Thi, n, &sm.next_chunk, lane, best, bestd);
+        int best = 0, bestd = 0x7fffffff;
+        sl_band_scan(E4, poffT, gstart, ng, S, Tlo, Thi, n, sm.queue[warp], &sm.next_chunk, lane, best, bestd);
+        // CTA reduction of (best, smallest anti-diagonal)
         for (int o = 16; o > 0; o >>= 1) {
             int ob = __shfl_xor_sync(0xffffffffu, best, o), od = __shfl_xor_sync(0xffffffffu, bestd, o);
             pair_reduce(best, bestd, ob, od);
         }
-        __syncthreads();
         if (lane == 0) {
             sm.wbest[warp] = best;
             sm.wbestd[warp] = bestd;
@@ -1321,11 +1324,38 @@ __global__ void __launch_bounds__(NT) k_sl(Shape s, PopBuf buf, int base, int2 *
             for (int w = 1; w < nwarps; w++) pair_reduce(b, d, sm.wbest[w], sm.wbestd[w]);
             sm.res[0] = b;
             sm.res[1] = d;
+            sm.next_chunk = 0;
         }
         __syncthreads();
+        if (sm.res[0] < 8) {
+            // no run reaches 8: exact per-word runs
+            best = 0;
+            bestd = 0x7fffffff;
+            sl_scan(S, Tlo, Thi, n, &sm.next_chunk, lane, best, bestd);
+            for (int o = 16; o > 0; o >>= 1) {
+                int ob = __shfl_xor_sync(0xffffffffu, best, o), od = __shfl_xor_sync(0xffffffffu, bestd, o);
+                pair_reduce(best, bestd, ob, od);
+            }
+            __syncthreads();
+            if (lane == 0) {
+                sm.wbest[warp] = best;
+                sm.wbestd[warp] = bestd;
+            }
+            __syncthreads();
+            if (tid == 0) {
+                int b = sm.wbest[0], d = sm.wbestd[0];
+                for (int w = 1; w < nwarps; w++) pair_reduce(b, d, sm.wbest[w], sm.wbestd[w]);
+                sm.res[0] = b;
+                sm.res[1] = d;
+            }
+            __syncthreads();
+        }
     }
     if (tid == 0) {
-        part[(size_t)sol * s.m + c] = make_int2(sm.res[0], sm.res[1]);
+        if (!reuse) {
+            res[c] = make_int2(sm.res[0], sm.res[1]);
+            if (scanned) atomicAdd(scanned, 1ull);
+        }
         __threadfence();
         int old = atomicAdd(&counter[sol], 1);
         sm.last = (old == s.m - 1);
@@ -1337,7 +1367,7 @@ __global__ void __launch_bounds__(NT) k_sl(Shape s, PopBuf buf, int base, int2 *
     if (tid == 0) {
         int Lb = -1, cb = 0, db = 0;
         for (int cc = 0; cc < s.m; cc++) {
-            int2 v = __ldcg(&part[(size_t)sol * s.m + cc]);
+            int2 v = __ldcg(&res[cc]);
             if (v.x >= Lb) {
                 Lb = v.x;
                 cb = cc;
@@ -1439,23 +1469,23 @@ size_t sl_smem_bytes(const Shape &s) { return sl_smem_bytes_nt(s, sizeof(SlSmem<
 
 template <int NT>
 static cudaError_t launch_sl_nt(const Shape &s, PopBuf buf, int base, int count, int2 *part, int32_t *counter,
-                                int32_t *status, cudaStream_t st)
+                                int32_t *status, cudaStream_t st, unsigned long long *scanned)
 {
     const size_t smem = sl_smem_bytes_nt(s, sizeof(SlSmem<NT>));
     cudaError_t e = raise_smem_limit((const void *)k_sl<NT>, smem);
     if (e != cudaSuccess) return e;
-    k_sl<NT><<<count * s.m, NT, smem, st>>>(s, buf, base, part, counter, status);
+    k_sl<NT><<<count * s.m, NT, smem, st>>>(s, buf, base, part, counter, status, scanned);
     return cudaGetLastError();
 }
 
 cudaError_t launch_sl(const Shape &s, PopBuf buf, int base, int count, int2 *part, int32_t *counter, int32_t *status,
-                      cudaStream_t st)
+                      cudaStream_t st, unsigned long long *scanned)
 {
     if (count <= 0) return cudaSuccess;
     switch (s.sl_threads) {
-    case 64: return launch_sl_nt<64>(s, buf, base, count, part, counter, status, st);
-    case 256: return launch_sl_nt<256>(s, buf, base, count, part, counter, status, st);
-    default: return launch_sl_nt<128>(s, buf, base, count, part, counter, status, st);
+    case 64: return launch_sl_nt<64>(s, buf, base, count, part, counter, status, st, scanned);
+    case 256: return launch_sl_nt<256>(s, buf, base, count, part, counter, status, st, scanned);
+    default: return launch_sl_nt<128>(s, buf, base, count, part, counter, status, st, scanned);
     }
 }
 

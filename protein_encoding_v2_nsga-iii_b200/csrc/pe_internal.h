@@ -63,6 +63,10 @@ struct PopBuf {
     float *obj;        // [2N][M]
     int8_t *objidx;    // [2N][2M]
     int32_t *pql;      // [2N][3]
+    // [2N][m] hairpin scan of each CDS: (longest stem, its anti-diagonal); x = -1 marks a
+    // CDS to scan.  A child's unchanged CDSs carry their parent's result, so only the
+    // CDSs its mutation touched are scanned.  nullptr: every CDS is scanned.
+    int2 *cds;
 };
 
 struct SelectScratch {
@@ -90,7 +94,7 @@ cudaError_t launch_mutate(const Shape &s, const DevTables *tab, const int8_t *aa
                           const int32_t *parent_of, const int32_t *rng_idx, int count, int copy_base, int child_base,
                           const uint32_t *d_gen, int32_t *ops, cudaStream_t st);
 cudaError_t launch_sl(const Shape &s, PopBuf buf, int base, int count, int2 *part, int32_t *counter,
-                      int32_t *status, cudaStream_t st);
+                      int32_t *status, cudaStream_t st, unsigned long long *scanned = nullptr);
 size_t sl_smem_bytes(const Shape &s);
 // Raise a kernel's dynamic shared-memory limit to at least `bytes` on the current
 // device.  The limit only grows, so launches from different host threads never

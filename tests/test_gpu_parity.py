@@ -187,6 +187,26 @@ def test_full_size_generation(pe, orc, gpu):
         assert same(a, b)
 
 
+def test_unchanged_cds_keeps_parent_stem(pe, orc, gpu):
+    """A child's CDS that its mutation left unchanged keeps its parent's stem result
+    instead of being scanned again: fewer scans than CDSs, and every solution's
+    objectives still equal a fresh evaluation by the oracle."""
+    tabc = pe.dirichlet_table(6)
+    tab = tabc.arrays()
+    aa = pe.synthetic_protein(119, 8)
+    N, m, G = 64, 8, 6
+    with pe.Engine(aa, tabc, m, N, 0.02, objectives=1, ref_p=4, seed=11, sl_threads=128) as eng:
+        eng.init()
+        assert eng.scan_count() == N * m
+        eng.step(G)
+        per_gen = (eng.scan_count() - N * m) / G
+        ids, obj, objidx, pql, surv = eng.population()
+    assert 0 < per_gen < 0.7 * N * m
+    o = orc.Problem(aa, tab, m, N, 0.02, objset=1, p=4).evaluate(ids)
+    for a, b in zip((obj, objidx, pql), o):
+        assert same(a, b)
+
+
 def test_long_protein_large_population_fits(pe, gpu):
     """L=3000, m=4, N=4096 with the reference's p rule (4060 reference points): the
     selection and stem-scan kernels' shared memory still fits one CTA, and a
