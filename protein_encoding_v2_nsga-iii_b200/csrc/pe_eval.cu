@@ -1399,37 +1399,82 @@ __global__ void __launch_bounds__(NT) k_sl(Shape s, PopBuf buf, int base, int2 *
     // sides inside the counted cells (recorded again, later, from the lower
     // triangle), else the run cut at the loop limit.
     if (warp == 0) {
-        const uint2 *Q = buf.planes + (gsol * s.m + cb) * s.Wp;
+        // the winning CDS's planes, staged in shared memory (the tables' space is free)
+        uint2 *Q = reinterpret_cast<uint2 *>(tab);
+        const uint2 *Qg = buf.planes + (gsol * s.m + cb) * s.Wp;
+        for (int w = lane; w < s.Wp; w += 32) Q[w] = Qg[w];
+        __syncwarp();
         const int r_lo = max(0, d - (n - 1)), r_hi = (d - 5) >> 1;
-        int run = 0, first = -1, typeII = 0;
-        for (int r0 = r_lo; r0 <= r_hi + 1; r0 += 32) {
-            int r = r0 + lane;
-            int bit = 0;
-            if (r <= r_hi + 1) bit = ((plane_nt(Q, r) ^ plane_nt(Q, d - r)) == 3);
-            uint32_t word = __ballot_sync(0xffffffffu, bit);
-            if (lane == 0) {
-                int lim = min(32, r_hi + 2 - r0);
-                for (int b = 0; b < lim; b++) {
-                    int rr = r0 + b, on = (word >> b) & 1u;
-                    if (rr <= r_hi) {
-                        if (on) {
-                            run++;
-                        } else {
-                            if (run == Lb && first < 0) first = rr - run;
-                            run = 0;
-                        }
-                    } else {
-                        if (run == Lb) {
-                            if (!on) {
-                                if (first < 0) first = rr - run;
-                            } else {
-                                typeII = 1;
-                            }
-                        }
-                    }
+        // Pairing rows r_lo .. r_hi of anti-diagonal d, 32 per lane: every counted run
+        // on d is at most Lb long (Lb is the CDS's longest), so a run of Lb starts
+        // wherever Lb consecutive rows pair.  Each lane takes the runs whose last row
+        // lies in its word; a run that enters from the words below carries their
+        // length (a scan over the lanes).  The first run of Lb closed by a row that
+        // does not pair gives (p, q); one ending at r_hi is closed by row r_hi + 1
+        // (outside the counted range), and if that row pairs too the stem is cut at
+        // the loop limit (typeII).
+        const int nwords = (r_hi - r_lo + 1 + 31) >> 5;
+        const int beyond = ((plane_nt(Q, r_hi + 1) ^ plane_nt(Q, d - r_hi - 1)) == 3);
+        // rows r .. r+31 of diagonal d: s[r+b] against s[d-r-b]
+        auto diag_word = [&](int r) -> uint32_t {
+            const int ws = r >> 5, bs = r & 31;
+            const uint32_t slo = fshr(Q[ws].x, Q[ws + 1].x, bs), shi = fshr(Q[ws].y, Q[ws + 1].y, bs);
+            const int t0 = d - r - 31;  // partner of row r + 31; bit 31 - b of the window is s[d - r - b]
+            const int wt = t0 >> 5, bt = t0 & 31;  // wt may be -1 when high rows fall outside
+            const uint2 qa = wt >= 0 ? Q[wt] : make_uint2(0u, 0u), qb = Q[wt + 1];
+            const uint32_t tlo = __brev(fshr(qa.x, qb.x, bt)), thi = __brev(fshr(qa.y, qb.y, bt));
+            return (slo ^ tlo) & (shi ^ thi);  // complementary in both bits
+        };
+        int first = 0x7fffffff, typeII = 0;
+        uint32_t carry = 0;  // run length ending at the last row of the previous pass
+        for (int k0 = 0; k0 < nwords; k0 += 32) {
+            const int k = k0 + lane, r0 = r_lo + 32 * k;
+            uint32_t X = 0u, nb = 0u;  // this word's in-range bits; bit 0 of the next word
+            if (k < nwords) {
+                X = diag_word(r0);
+                const int rows = r_hi - r0 + 1;
+                if (rows < 32) X &= (1u << rows) - 1u;
+                if (lane == 31 && r0 + 32 <= r_hi)
+                    nb = (plane_nt(Q, r0 + 32) ^ plane_nt(Q, d - r0 - 32)) == 3;
+            }
+            const uint32_t nb_lane = __shfl_down_sync(0xffffffffu, X & 1u, 1);
+            if (lane < 31) nb = nb_lane;
+            // run length ending at this word's top: all ones ? 32 + previous : trailing ones
+            uint32_t A = X == 0xffffffffu, Bv = A ? 32u : (uint32_t)__clz((int)~X);
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t A2 = __shfl_up_sync(0xffffffffu, A, o), B2 = __shfl_up_sync(0xffffffffu, Bv, o);
+                if (lane >= o) {
+                    Bv = A * B2 + Bv;
+                    A &= A2;
                 }
             }
+            const uint32_t E = A * carry + Bv;
+            uint32_t cin = __shfl_up_sync(0xffffffffu, E, 1);
+            if (lane == 0) cin = carry;
+            carry = __shfl_sync(0xffffffffu, E, 31);
+            // runs ending in this word: a one followed by a zero (or by the range's end)
+            const uint32_t ends = X & ~((X >> 1) | (nb << 31));
+            const uint32_t starts = X & ~((X << 1) | (cin ? 1u : 0u));
+            int cand = 0x7fffffff, cand2 = 0;
+            uint32_t e_bits = ends;
+            while (e_bits && cand == 0x7fffffff) {
+                const int e = __ffs((int)e_bits) - 1;
+                e_bits &= e_bits - 1;
+                const uint32_t sm_ = starts & (e == 31 ? ~0u : ((2u << e) - 1u));
+                const int len = sm_ ? e - (31 - __clz((int)sm_)) + 1 : e + 1 + (int)cin;
+                if (len >= Lb) {
+                    const int pstart = r0 + e - len + 1;
+                    if (r0 + e == r_hi && beyond) cand2 = 1;  // cut at the loop limit
+                    else cand = pstart;
+                }
+            }
+            // lowest lane with a closed run of Lb holds the first one
+            const unsigned has = __ballot_sync(0xffffffffu, cand != 0x7fffffff);
+            if (has && first == 0x7fffffff) first = __shfl_sync(0xffffffffu, cand, __ffs((int)has) - 1);
+            if (__any_sync(0xffffffffu, cand2)) typeII = 1;
+            if (first != 0x7fffffff) break;
         }
+        if (first == 0x7fffffff) first = -1;
         if (lane == 0) {
             int p, q;
             if (first >= 0) {
