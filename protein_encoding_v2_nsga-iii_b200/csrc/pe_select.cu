@@ -28,7 +28,9 @@ __device__ __forceinline__ bool dominates(const float *a, const float *b, int M)
     // dominate (include/sorting.cuh:94-130): |a-b| <= 1e-6 counts as equal
     int eq = 0;
     bool worse = false;
-    for (int k = 0; k < M; k++) {
+#pragma unroll
+    for (int k = 0; k < kMaxObj; k++) {
+        if (k >= M) break;
         float d = fabsf(__fsub_rn(a[k], b[k]));
         if (d > 1e-6f) {
             if (a[k] > b[k]) worse = true;
@@ -39,22 +41,31 @@ __device__ __forceinline__ bool dominates(const float *a, const float *b, int M)
     return eq != M && !worse;
 }
 
+// MM: the objective count when known at compile time (4 or 6; 0: s.M at run time),
+// so the two objective vectors stay in registers
+template <int MM>
 __global__ void __launch_bounds__(256) k_dominance(Shape s, const float *__restrict__ obj, uint32_t *__restrict__ dom,
                                                    int32_t *__restrict__ np)
 {
     __shared__ int wsum[8];
+    const int M = MM > 0 ? MM : s.M;
     const int N2 = 2 * s.N, words = (N2 + 31) >> 5;
     const int i = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     float oi[kMaxObj];
-    for (int k = 0; k < s.M; k++) oi[k] = obj[(size_t)i * s.M + k];
+#pragma unroll
+    for (int k = 0; k < (MM > 0 ? MM : kMaxObj); k++)
+        if (k < M) oi[k] = obj[(size_t)i * M + k];
     int cnt = 0;
+#pragma unroll 2
     for (int w = warp; w < words; w += 8) {
         int j = 32 * w + lane;
         bool bit = false;
         if (j < N2 && j != i) {
             float oj[kMaxObj];
-            for (int k = 0; k < s.M; k++) oj[k] = __ldg(&obj[(size_t)j * s.M + k]);
-            bit = dominates(oj, oi, s.M);
+#pragma unroll
+            for (int k = 0; k < (MM > 0 ? MM : kMaxObj); k++)
+                if (k < M) oj[k] = __ldg(&obj[(size_t)j * M + k]);
+            bit = dominates(oj, oi, M);
         }
         uint32_t word = __ballot_sync(0xffffffffu, bit);
         if (lane == 0) dom[(size_t)i * words + w] = word;
@@ -598,35 +609,48 @@ __global__ void __launch_bounds__(kSelThreads, 1) k_select(Shape s, const float 
 // referenceBasedSorting phase 1 (:1105-1180) on the whole grid: one warp per
 // solution of fronts 0..last, lanes over reference points; perpendicular
 // distance (include/utils.cuh:1149-1171), argmin with the lowest index on ties.
+// MM: the objective count when known at compile time (0: s.M at run time)
+template <int MM>
 __global__ void __launch_bounds__(256) k_assoc(Shape s, const float *__restrict__ obj,
                                                const float *__restrict__ refpts, SelectScratch sc)
 {
     if (sc.info[3]) return;  // fronts filled N exactly: no niching
-    const int M = s.M, R = s.R;
+    const int M = MM > 0 ? MM : s.M, R = s.R;
+    constexpr int KU = MM > 0 ? MM : kMaxObj;  // unrolled loop bound (k < M guards the rest)
     const int rc = sc.info[0], count0 = sc.info[5];
     const int lane = threadIdx.x & 31;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
     float ideal[kMaxObj], span[kMaxObj];
-    for (int k = 0; k < M; k++) {
+#pragma unroll
+    for (int k = 0; k < KU; k++) {
+        if (k >= M) break;
         ideal[k] = sc.finfo[k];
         span[k] = __fsub_rn(sc.finfo[2 * M + k], ideal[k]);
     }
     for (int t = gw; t < rc; t += nw) {
         const int sol = sc.sorted[t];
         float f[kMaxObj];
-        for (int k = 0; k < M; k++) f[k] = __fdiv_rn(__fsub_rn(obj[(size_t)sol * M + k], ideal[k]), span[k]);
+#pragma unroll
+        for (int k = 0; k < KU; k++) {
+            if (k >= M) break;
+            f[k] = __fdiv_rn(__fsub_rn(obj[(size_t)sol * M + k], ideal[k]), span[k]);
+        }
         float best = FLT_MAX;
         int bj = 0;
         for (int j = lane; j < R; j += 32) {
             const float *w = refpts + (size_t)j * M;
             float num = 0.0f, den = 0.0f;
-            for (int k = 0; k < M; k++) {
+#pragma unroll
+            for (int k = 0; k < KU; k++) {
+                if (k >= M) break;
                 num = __fadd_rn(num, __fmul_rn(w[k], f[k]));
                 den = __fadd_rn(den, __fmul_rn(w[k], w[k]));
             }
             float kk = __fdiv_rn(num, den);
             float d2 = 0.0f;
-            for (int k = 0; k < M; k++) {
+#pragma unroll
+            for (int k = 0; k < KU; k++) {
+                if (k >= M) break;
                 float e = __fsub_rn(__fmul_rn(kk, w[k]), f[k]);
                 d2 = __fadd_rn(d2, __fmul_rn(e, e));
             }
@@ -914,7 +938,9 @@ size_t select_smem_bytes(const Shape &s)
 cudaError_t launch_select(const Shape &s, const float *obj, float *ext, const float *refpts, SelectScratch sc,
                           int32_t *surv, uint32_t *d_gen, int bump_gen, cudaStream_t st)
 {
-    k_dominance<<<2 * s.N, 256, 0, st>>>(s, obj, sc.dom, sc.np);
+    if (s.M == 4) k_dominance<4><<<2 * s.N, 256, 0, st>>>(s, obj, sc.dom, sc.np);
+    else if (s.M == 6) k_dominance<6><<<2 * s.N, 256, 0, st>>>(s, obj, sc.dom, sc.np);
+    else k_dominance<0><<<2 * s.N, 256, 0, st>>>(s, obj, sc.dom, sc.np);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     size_t smem = select_smem_bytes(s);
@@ -923,7 +949,10 @@ cudaError_t launch_select(const Shape &s, const float *obj, float *ext, const fl
     k_select<<<1, kSelThreads, smem, st>>>(s, obj, ext, refpts, sc, surv, d_gen, bump_gen);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     const int warps_needed = 2 * s.N;
-    k_assoc<<<std::min((warps_needed + 7) / 8, 148 * 8), 256, 0, st>>>(s, obj, refpts, sc);
+    const int ag = std::min((warps_needed + 7) / 8, 148 * 8);
+    if (s.M == 4) k_assoc<4><<<ag, 256, 0, st>>>(s, obj, refpts, sc);
+    else if (s.M == 6) k_assoc<6><<<ag, 256, 0, st>>>(s, obj, refpts, sc);
+    else k_assoc<0><<<ag, 256, 0, st>>>(s, obj, refpts, sc);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     const size_t nsm = niche_smem_bytes(s);
     if ((e = raise_smem_limit((const void *)k_niche, nsm)) != cudaSuccess) return e;
