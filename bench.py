@@ -64,14 +64,14 @@ def set_workload(shape: str | None, six: bool):
 METRIC = "generations/s"
 L2_FLUSH_BYTES = 256 << 20
 # k_sl at this workload, from ncu captures of one launch (profiles/k_sl_L1000_m8_N1024.md):
-# ALU-pipe warp instructions (57 % of its peak of 2 per SM per clock, of active cycles),
-# shared-memory data-pipe wavefronts (45 % of 1 per SM per clock), thread instructions and
+# ALU-pipe warp instructions (69 % of its peak of 2 per SM per clock, of active cycles),
+# shared-memory data-pipe wavefronts (73 % of 1 per SM per clock), thread instructions and
 # DRAM bytes per launch
-SL_SMEM_WAVEFRONTS_PER_LAUNCH = 27719685
-SL_ALU_WARP_INST_PER_LAUNCH = 56379096
-SL_THREAD_INST_PER_LAUNCH = 2542106810
-SL_DRAM_BYTES_PER_LAUNCH = 2310912
-SL_SMEM_PCT_NCU, SL_ALU_PIPE_PCT_NCU = 45.36, 57.09
+SL_SMEM_WAVEFRONTS_PER_LAUNCH = 27776979
+SL_ALU_WARP_INST_PER_LAUNCH = 46420822
+SL_THREAD_INST_PER_LAUNCH = 2483621141
+SL_DRAM_BYTES_PER_LAUNCH = 2475520
+SL_SMEM_PCT_NCU, SL_ALU_PIPE_PCT_NCU = 73.22, 69.25
 SM_COUNT, SMEM_WAVEFRONTS_PER_SM_CLK, ALU_WARP_INST_PER_SM_CLK = 148, 1, 2
 # CDSs the captured launch scanned (of 1024 x 8: the others kept their parents' results)
 # and its counted cells (4495501 per CDS of 3003 nucleotides)
