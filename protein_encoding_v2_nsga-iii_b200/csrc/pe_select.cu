@@ -5,9 +5,12 @@
 //               and np[i] = popc(row) -- replaces the reference's two (2N)^2
 //               bool matrices (include/sorting.cuh:974-1089).
 //  k_select     one CTA: front peeling on the bit matrix, ideal / worst,
-//               extreme points, hyperplane (Gaussian elimination) or MNDF nadir,
-//               reference-point association and niche selection, stopping at
-//               exactly N survivors (include/sorting.cuh:94-1282).
+//               extreme points, hyperplane (Gaussian elimination) or MNDF nadir
+//               (include/sorting.cuh:94-972).
+//  k_assoc      the whole grid, a warp per solution of fronts 0..last: nearest
+//               reference point and its perpendicular distance (:1105-1180).
+//  k_niche      one CTA: niche counts, candidate lists and the closed form of the
+//               level-by-level niching, stopping at exactly N survivors (:1182-1279).
 //
 // Deterministic rules (the reference decides these by atomic order):
 // fronts are listed in ascending solution index; each niche level visits
