@@ -11,8 +11,9 @@ job is 500 generations (designs/s = generations/s / 500).
 
 Multi-GPU: one independent replica per rank (its own seed, no data-path
 collective); `value` = generations of all ranks / the slowest rank's time.
-The reference arm times the CPU restatement of the reference algorithm on the
-host cores (the reference itself has no CPU implementation).
+The reference arm times whole generations of the CPU restatement of the
+reference algorithm (the oracle; the reference itself has no CPU
+implementation) on all host threads, with inputs the oracle generates itself.
 """
 from __future__ import annotations
 
@@ -63,7 +64,7 @@ def set_workload(shape: str | None, six: bool):
                 f"({R} points), design job = {G_JOB} generations")
 METRIC = "generations/s"
 L2_FLUSH_BYTES = 256 << 20
-# k_sl at this workload, from ncu captures of one launch (profiles/k_sl_L1000_m8_N1024.md):
+# k_sl at this workload, from ncu captures of one launch (the committed k_sl profile summary):
 # ALU-pipe warp instructions (69 % of its peak of 2 per SM per clock, of active cycles),
 # shared-memory data-pipe wavefronts (73 % of 1 per SM per clock), thread instructions and
 # DRAM bytes per launch
@@ -185,74 +186,139 @@ def dist_setup():
     return world, rank, local
 
 
-SL_STRIDE = 16
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
 
 
-def cpu_reference(pe, orc, pop, aa, table, steps: int, threads: int):
-    """Time the CPU restatement of one generation on bounded samples, scaled to the
-    full workload.  Per step: (1) mutation + every objective but the stem for S
-    offspring, (2) the reference's serial anti-diagonal stem sweep of `threads` CDSs
-    restricted to every 16th anti-diagonal (rotating), (3) selection on the full 2N set.
-    seconds/generation = t1*N/S + t2*16*(N*m)/threads + t3."""
-    ids, obj, objidx, pql, surv = pop
-    prob = orc.Problem(aa, table.arrays(), M_CDS, POP, PM, objset=OBJ_SET, p=P_USE, seed=SEED)
-    S = min(len(surv), max(8, threads))
-    par = surv[:S]
-    nt = np.asarray(table.arrays()["nt"])
-    cds = np.stack([nt[ids[par[i % S], i % M_CDS]].reshape(-1) for i in range(threads)]).astype(np.uint8)
-    rates = []
-    for k in range(steps):
+# the same dict in both arms: the workload, not how an arm times it
+def config_dict(world: int) -> dict:
+    return {"workload": WORKLOAD, "global_batch": POP * world, "parallelism": f"replicas{world}",
+            "l2": "GPU arm: L2 flushed between timed steps (256 MiB write, untimed); CPU arm: no device cache"}
+
+
+def oracle_problem(orc):
+    """The plain workload's protein, codon table and problem, built by the oracle alone
+    (the engine library is not loaded)."""
+    aa = orc.synthetic_protein(L_AA, SEED)
+    table = orc.dirichlet_table(SEED)
+    return orc.Problem(aa, table, M_CDS, POP, PM, objset=OBJ_SET, p=P_USE, seed=SEED)
+
+
+def time_oracle_generations(run, steps: int, threads: int) -> list[float]:
+    """Seconds of each of `steps` whole oracle generations (mutation + evaluation of all N
+    offspring with every objective, then selection on the 2N set; src/main.cu:708-728)."""
+    out = []
+    for _ in range(steps):
         t0 = time.perf_counter()
-        prob.mutate_light(k, np.arange(S, dtype=np.int32), ids[par], obj[par], objidx[par], pql[par],
-                          threads=threads)
-        t1 = time.perf_counter()
-        orc.sl_sample(cds, k % SL_STRIDE, SL_STRIDE, threads=threads)
-        t2 = time.perf_counter()
-        ext = obj[:M_OBJ].copy()
-        prob.select(k, obj, ext)
-        t3 = time.perf_counter()
-        sec_per_gen = (t1 - t0) * POP / S + (t2 - t1) * SL_STRIDE * (POP * M_CDS) / threads + (t3 - t2)
-        rates.append(1.0 / sec_per_gen)
-    sample = (f"per step: mutation + non-stem objectives of {S} offspring, the serial stem sweep of {threads} CDSs "
-              f"on every {SL_STRIDE}th anti-diagonal, selection on the full 2N={2 * POP} set; "
-              f"{threads} threads; scaled to N={POP}, m={M_CDS}")
-    return rates, sample
+        run.generation(threads)
+        out.append(time.perf_counter() - t0)
+    return out
 
 
 def run_reference(args, world, rank):
-    """The reference arm: the CPU restatement of the reference algorithm on host cores."""
+    """The reference arm: whole generations of the CPU restatement of the reference
+    algorithm on all host threads.  Rank 0 alone runs it."""
     if rank != 0:
         return
-    pe = load_pkg()
     sys.path.insert(0, str(ROOT / "oracle"))
     import pe_oracle as orc
-    threads = os.cpu_count() or 1
-    aa = pe.synthetic_protein(L_AA, SEED)
-    table = pe.dirichlet_table(SEED)
-    prob = orc.Problem(aa, table.arrays(), M_CDS, POP, PM, objset=OBJ_SET, p=P_USE, seed=SEED)
-    # parents: a population generated and evaluated by the oracle itself (bounded: `threads` solutions)
-    S = max(8, threads)
-    ids = np.stack([prob.gen_solution(i) for i in range(S)])
-    obj, objidx, pql = prob.evaluate(ids, threads=threads)
-    fake_obj = np.concatenate([obj] * ((2 * POP + S - 1) // S))[:2 * POP]
-    fake_obj = fake_obj + np.random.default_rng(0).random(fake_obj.shape).astype(np.float32) * 1e-3
-    pop = (ids, fake_obj, np.concatenate([objidx] * ((2 * POP + S - 1) // S))[:2 * POP],
-           np.concatenate([pql] * ((2 * POP + S - 1) // S))[:2 * POP], np.arange(S, dtype=np.int32))
-    for _ in range(max(0, args.warmup > 0)):
-        cpu_reference(pe, orc, pop, aa, table, 1, threads)
+    threads = host_threads()
+    prob = oracle_problem(orc)
+    run = orc.Run(prob)
+    t_init = time.perf_counter()
+    run.init(threads)
+    t_init = time.perf_counter() - t_init
+    time_oracle_generations(run, args.warmup, threads)
     t0 = time.perf_counter()
-    rates, sample = cpu_reference(pe, orc, pop, aa, table, args.steps, threads)
+    secs = time_oracle_generations(run, args.steps, threads)
     wall = time.perf_counter() - t0
-    value = statistics.median(rates)
+    run.close()
+    total = sum(secs)
+    value = args.steps / total
+    sample = (f"{args.steps} whole generations of the workload (after {args.warmup} untimed ones and the "
+              f"initial population, {t_init:.1f} s): mutation and full evaluation of all {POP} offspring, "
+              f"selection on the {2 * POP}-solution set; {threads} threads")
     line = {"metric": METRIC, "value": value, "unit": "generations/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u32", "data": "synthetic", "impl": "reference",
-            "config": {"workload": WORKLOAD, "designs_per_s": value / G_JOB},
+            "warmup": args.warmup, "ms_per_step": 1000.0 * total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic", "impl": "reference",
+            "config": config_dict(world), "designs_per_s": value / G_JOB,
             "cpu_baseline": {"value": value, "unit": "generations/s", "cores": threads, "kind": "port",
                              "sample": sample},
             "e2e": {"value": value, "unit": "generations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "wall_s": wall}
+            "step_s": [round(x, 3) for x in secs], "wall_s": wall}
     print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_one_generation(pe_state, extremes, generation: int) -> dict:
+    """The oracle on this host: one whole generation started from the engine's current
+    population (bit-identical to the oracle's own state at that generation)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pe_oracle as orc
+    threads = host_threads()
+    run = orc.Run(oracle_problem(orc))
+    ids, obj, objidx, pql, surv = pe_state
+    run.set_state(ids, obj, objidx, pql, surv, extremes, generation)
+    sec = time_oracle_generations(run, 1, threads)[0]
+    run.close()
+    return {"value": 1.0 / sec, "unit": "generations/s", "cores": threads, "kind": "port",
+            "sample": f"one whole generation (mutation and full evaluation of all {POP} offspring, selection on "
+                      f"the {2 * POP}-solution set) started from the GPU run's population at generation "
+                      f"{generation}; {threads} threads; {sec:.1f} s"}
+
+
+def reference_cuda_build(pe, seconds_limit: float = 90.0, G: int = 10) -> dict:
+    """The reference's own CUDA build (oracle/_ref/Protein_NSGA3, compiled unmodified from
+    its sources) on this GPU at the plain workload's shape with its own settings (six
+    objectives, its codon table, p by its rule), timed by its own `Generation cycles time`
+    print (src/main.cu:702-731, 862); beside it this engine at the same settings and
+    generation count, timed with CUDA events around the back-to-back generations."""
+    import shutil
+    import tempfile
+
+    import torch
+    exe, hv = ROOT / "oracle" / "_ref" / "Protein_NSGA3", ROOT / "oracle" / "_ref" / "hv"
+    if not exe.exists() or not hv.exists():
+        return {"unavailable": "oracle/_ref/Protein_NSGA3 not built (make -C oracle ref needs the reference sources)"}
+    aa = pe.synthetic_protein(L_AA, SEED)
+    letters = "".join(pe.AMINO[int(x)] for x in aa[:-1])
+    res = {"shape": f"L={L_AA} (+stop), N={POP}, m={M_CDS}, Pm={PM}, {G} generations; the reference's six "
+                    f"objectives, its codon table, p by its rule"}
+    with tempfile.TemporaryDirectory() as d:
+        (Path(d) / "p.fasta.txt").write_text(">synthetic\n" + letters + "\n")
+        shutil.copy(hv, Path(d) / "hv")
+        try:
+            out = subprocess.run([str(exe), "p.fasta.txt", str(POP), str(G), str(M_CDS), str(PM)], cwd=d,
+                                 capture_output=True, text=True, timeout=seconds_limit)
+        except subprocess.TimeoutExpired:
+            res["unavailable"] = f"the reference build did not finish within {seconds_limit:.0f} s"
+            return res
+        import re
+        m = re.search(r"Generation cycles time\s*:\s*([0-9.eE+-]+)", out.stdout)
+        if out.returncode != 0 or not m:
+            res["unavailable"] = f"reference build exit {out.returncode}: {out.stdout[-200:]} {out.stderr[-200:]}"
+            return res
+        gen_s = float(m.group(1))
+        res["reference_generations_per_s"] = G / gen_s
+        res["reference_generation_cycles_s"] = gen_s
+    table = pe.load_codon_table(ROOT / "protein_encoding_v2_nsga-iii_b200" / "data" / "ref_codon_table.txt")
+    stream = torch.cuda.Stream()
+    with pe.Engine(aa, table, M_CDS, POP, PM, objectives=pe.OBJ_REF6, ref_p=0, seed=SEED,
+                   stream=stream.cuda_stream) as eng:
+        eng.init()
+        eng.step(3)
+        eng.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        eng.step(G)
+        b.record(stream)
+        eng.synchronize()
+        ours = G / (a.elapsed_time(b) / 1000.0)
+    res["engine_generations_per_s"] = ours
+    res["engine_over_reference"] = ours / res["reference_generations_per_s"]
+    return res
 
 
 def run_ours(args, world, rank, local):
@@ -277,7 +343,7 @@ def run_ours(args, world, rank, local):
     scans0 = eng.scan_count()
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    stage = np.zeros(3)
+    stage = np.zeros((args.steps, 3))
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize(dev)
@@ -290,7 +356,7 @@ def run_ours(args, world, rank, local):
                 eng.step(1)
                 ev[k][1].record(stream)
             eng.synchronize()
-            stage += eng.stage_times()
+            stage[k] = eng.stage_times()
         torch.cuda.synchronize(dev)
         t_wall = time.perf_counter() - t_wall
     if world > 1:
@@ -302,7 +368,11 @@ def run_ours(args, world, rank, local):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
     max_s = float(t.item())
     value = world * args.steps / max_s
-    stage_ms = stage / args.steps
+    stage_ms = stage.mean(axis=0)
+    # stage times per window of 5 timed generations (early generations are front-heavy)
+    windows = [{"generations": [args.warmup + w, args.warmup + min(w + 5, args.steps) - 1],
+                "variation_eval": float(stage[w:w + 5, 0].mean()), "hairpin_scan": float(stage[w:w + 5, 1].mean()),
+                "selection": float(stage[w:w + 5, 2].mean())} for w in range(0, args.steps, 5)]
     n_nt = 3 * (L_AA + 1)
     # a child's CDS that its mutation left unchanged keeps its parent's stem result:
     # the stem-scan work is the CDSs actually scanned
@@ -310,10 +380,9 @@ def run_ours(args, world, rank, local):
     cells = scans_per_gen * hairpin_cells_per_cds(n_nt)
     sl_s = stage_ms[1] / 1000.0
 
-    # end-to-end through the public API with host buffers: every rank runs a design job of
-    # G_E2E generations on its GPU; the whole-job rate uses the slowest rank
-    # (three jobs, the median: one 100-generation job is ~0.07 s of wall clock)
-    G_E2E, E2E_JOBS = 100, 3
+    # end-to-end through the public API with host buffers: every rank runs whole design jobs
+    # (G_JOB generations) on its GPU; the whole-job rate uses the slowest rank (three jobs, the median)
+    G_E2E, E2E_JOBS = G_JOB, 3
     obj_host = np.zeros((2 * POP, M_OBJ), np.float32)
     if world > 1:
         torch.distributed.barrier()
@@ -341,13 +410,15 @@ def run_ours(args, world, rank, local):
     line = None
     if rank == 0:
         # CPU baseline: the oracle on this host, bounded sample (N=1 only)
-        cpu = None
+        cpu, ref_cuda = None, None
         if world == 1:
-            sys.path.insert(0, str(ROOT / "oracle"))
-            import pe_oracle as orc
-            threads = os.cpu_count() or 1
-            rates, sample = cpu_reference(pe, orc, eng.population(), aa, table, 1, threads)
-            cpu = {"value": rates[0], "unit": "generations/s", "cores": threads, "kind": "port", "sample": sample}
+            # extreme points only steer the normalisation: the survivors' first M objective
+            # vectors give the timed generation the same work
+            state = eng.population()
+            ext = state[1][state[4][:M_OBJ]]
+            cpu = cpu_baseline_one_generation(state, ext, eng.generation)
+            if not args.skip_reference_cuda:
+                ref_cuda = reference_cuda_build(pe)
 
         peaks = {}
         try:
@@ -359,23 +430,26 @@ def run_ours(args, world, rank, local):
             "metric": METRIC, "value": value, "unit": "generations/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 * max_s / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "global_batch": POP * world, "parallelism": f"replicas{world}",
-                       "l2": "flushed between timed steps (256 MiB write, untimed)",
-                       "designs_per_s": value / G_JOB,
-                       "stage_ms": {"variation_eval": stage_ms[0], "hairpin_scan": stage_ms[1],
-                                    "selection": stage_ms[2]}},
+            "config": config_dict(world),
+            "designs_per_s": value / G_JOB,
+            "stage_ms": {"variation_eval": stage_ms[0], "hairpin_scan": stage_ms[1], "selection": stage_ms[2]},
+            "stage_ms_windows": windows,
             "roofline": roofline(cells, sl_s, clocks),
             "clocks": clocks,
             "e2e": {"value": world * G_E2E / e2e_s, "unit": "generations/s", "h2d_bytes_per_step": world * h2d / G_E2E,
                     "d2h_bytes_per_step": world * d2h,
-                    "job": f"per rank: create + init + {G_E2E} generations + reads, median of {E2E_JOBS} jobs; "
-                           "all ranks / slowest rank", "rank0_job_s": [round(x, 5) for x in job_s]},
+                    "designs_per_s": world / e2e_s,
+                    "job": f"per rank: create + init + {G_E2E} generations (a whole design job) + per-generation "
+                           f"objective reads + final population read, median of {E2E_JOBS} jobs; all ranks / "
+                           "slowest rank", "rank0_job_s": [round(x, 5) for x in job_s]},
             "gpu_launches": KERNELS_PER_GENERATION * args.steps,
             "wall_s": t_wall,
             "peaks_file": {k: peaks.get(k) for k in ("hbm_gbs", "bf16_tflops", "sm_max_mhz")},
         }
         if cpu:
             line["cpu_baseline"] = cpu
+        if ref_cuda:
+            line["ref_cuda"] = ref_cuda
         print(json.dumps(line), flush=True)
     eng.close()
     if world > 1:
@@ -550,8 +624,11 @@ def main():
     ap.add_argument("--objectives", choices=["base4", "ref6"], default="base4",
                     help="objective set of the plain workload (ref6: the reference's six, p by its rule)")
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed generations (default 500; 3 for --impl reference, whose CPU generations take ~20 s)")
     ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--skip-reference-cuda", action="store_true",
+                    help="do not run the reference's own CUDA build beside the bench")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--sl-threads", type=int, default=0, choices=[0, 64, 128, 256],
                     help="stem-scan CTA size (0: timed per instance at init); a fixed size keeps a run "
@@ -559,6 +636,8 @@ def main():
     ap.add_argument("--profile-case", action="store_true",
                     help="only build the bench instance, init and run 2 generations (for ncu captures)")
     args = ap.parse_args()
+    if args.steps is None:
+        args.steps = 3 if args.impl == "reference" else 500
     if args.objectives == "ref6" or args.shape:
         set_workload(args.shape, args.objectives == "ref6")
     world, rank, local = dist_setup()

@@ -201,15 +201,19 @@ int pe_scan_count(pe_instance *inst, uint64_t *count);
  * cudaMalloc/cudaFree): the longest-stem objective of n solutions already on the
  * device, computed with no allocation.  All pointers are device pointers:
  *   d_nt     uint8 [n][m][3L]  nucleotide codes (A=0 C=1 G=2 U=3)
- *   d_value  float [n]         stem length / ((3L-4)/2)  (NaN if a scan did not finish)
+ *   d_value  float [n]         stem length / ((3L-4)/2)
  *   d_pql    int32 [n][3]      stem p, q, length
  *   d_cds    int8  [n]         CDS holding the stem
- * Scratch is one fixed 8 MiB device array held by every GPU that loads the
- * library until exit; calls needing more (roughly n*m*3L/4 bytes) return
- * PE_ERR_ARG.  The first call on a device looks the array up (no allocation);
- * make that call before capturing work on the stream.  Asynchronous on
- * cuda_stream (NULL = default stream).  Every call shares the array, so calls
- * that overlap on the GPU race and give wrong results. */
+ * A solution whose scan did not finish (a bounded device wait gave up) reads
+ * NaN, (-1, -1, -1) and -1.  Scratch is one fixed 8 MiB device array; calls
+ * needing more (roughly n*m*3L/4 bytes) return PE_ERR_ARG.  The array is taken
+ * from the device's memory when this code is first used on that device (CUDA
+ * loads device code lazily by default): a call with n_solutions = 0 (pointers
+ * may be NULL) does only that set-up, so make it while setting up, before the
+ * application's memory manager takes the device's memory and before any stream
+ * capture; after it the array stays reserved until the process exits and no call
+ * allocates.  Asynchronous on cuda_stream (NULL = default stream).  Every call
+ * shares the array, so calls that overlap on the GPU race and give wrong results. */
 int pe_hairpin_noalloc(const uint8_t *d_nt, int32_t n_solutions, int32_t m, int32_t L, float *d_value,
                        int32_t *d_pql, int8_t *d_cds, void *cuda_stream);
 

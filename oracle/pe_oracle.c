@@ -1341,3 +1341,102 @@ double or_hypervolume(const double *pts, int n, int d, const double *ref)
     free(q);
     return v;
 }
+
+/* ------------------------------------------------------------------------ */
+/* synthetic benchmark inputs, restated so that the CPU baseline never loads */
+/* the engine library: SplitMix64 draws, amino acids uniform over the 20     */
+/* standard letters plus the appended stop (src/main.cu:517 appends 'Z'),    */
+/* codon weights Dirichlet(1) per amino acid scaled to max 1 and ordered     */
+/* ascending inside each group (the reference treats the last synonymous     */
+/* codon as the best one, include/utils.cuh:1090, include/mutation.cuh:105).  */
+/* Both must equal the engine's pe_synthetic_protein / pe_dirichlet_table     */
+/* draw for draw (a CPU test compares them).                                  */
+/* ------------------------------------------------------------------------ */
+
+static uint64_t or_splitmix64(uint64_t *x)
+{
+    uint64_t z = (*x += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+void or_synthetic_protein(int L, uint64_t seed, int8_t *aa_out)
+{
+    uint64_t x = seed;
+    for (int i = 0; i < L; i++) aa_out[i] = (int8_t)(((or_splitmix64(&x) >> 32) * 20ull) >> 32);
+    aa_out[L] = 20;
+}
+
+void or_dirichlet_table(uint64_t seed, or_codon_table *out)
+{
+    /* standard genetic code grouped by amino acid in index order A C D E F G H I K L M N P Q R S T V W Y stop */
+    static const char *groups[21] = {"GCU GCC GCA GCG", "UGU UGC", "GAU GAC", "GAA GAG", "UUU UUC",
+                                     "GGU GGC GGA GGG", "CAU CAC", "AUU AUC AUA", "AAA AAG",
+                                     "UUA UUG CUU CUC CUA CUG", "AUG", "AAU AAC", "CCU CCC CCA CCG", "CAA CAG",
+                                     "CGU CGC CGA CGG AGA AGG", "UCU UCC UCA UCG AGU AGC", "ACU ACC ACA ACG",
+                                     "GUU GUC GUA GUG", "UGG", "UAU UAC", "UAA UAG UGA"};
+    memset(out, 0, sizeof *out);
+    uint64_t x = seed;
+    int id = 0;
+    for (int a = 0; a < 21; a++) {
+        const char *g = groups[a];
+        int k = (int)(strlen(g) + 1) / 4;
+        uint8_t base[6][3];
+        for (int j = 0; j < k; j++)
+            for (int b = 0; b < 3; b++) {
+                char c = g[4 * j + b];
+                base[j][b] = c == 'A' ? 0 : c == 'C' ? 1 : c == 'G' ? 2 : 3;
+            }
+        double gam[6], gmax = 0.0;
+        for (int j = 0; j < k; j++) {
+            double u = (double)((or_splitmix64(&x) >> 11) + 1) * (1.0 / 9007199254740992.0);
+            gam[j] = -log(u);
+            if (gam[j] > gmax) gmax = gam[j];
+        }
+        float w[6];
+        int order[6];
+        for (int j = 0; j < k; j++) {
+            w[j] = (float)(gam[j] / gmax);
+            order[j] = j;
+        }
+        for (int j = 1; j < k; j++) { /* stable insertion sort, ascending weight */
+            int o = order[j], t = j;
+            while (t > 0 && w[order[t - 1]] > w[o]) {
+                order[t] = order[t - 1];
+                t--;
+            }
+            order[t] = o;
+        }
+        out->start[a] = (int8_t)id;
+        out->count[a] = (int8_t)k;
+        for (int j = 0; j < k; j++) {
+            memcpy(out->nt[id + j], base[order[j]], 3);
+            out->weight[id + j] = w[order[j]];
+        }
+        id += k;
+    }
+    for (int i = 0; i < OR_NUM_SENSE * OR_NUM_SENSE; i++) {
+        double u = (double)(or_splitmix64(&x) >> 11) * (1.0 / 9007199254740992.0);
+        out->cps[i] = (float)(0.8 * u - 0.4);
+    }
+    out->ref_gc3 = 0.3810f;
+    out->ref_gc = 0.3977f;
+}
+
+/* Load a 2N state (e.g. the CUDA engine's current population) so that the
+ * next or_generation starts from it. */
+void or_set_state(or_state *st, const uint8_t *pop, const float *obj, const int8_t *objidx, const int32_t *pql,
+                  const int32_t *survivors, const float *extremes, uint32_t gen)
+{
+    const or_problem *pr = &st->pr;
+    size_t N2 = 2 * (size_t)pr->N, sl = (size_t)pr->m * pr->L;
+    int b = st->cur;
+    memcpy(st->pop[b], pop, N2 * sl);
+    memcpy(st->obj[b], obj, N2 * st->M * sizeof(float));
+    memcpy(st->objidx[b], objidx, N2 * 2 * st->M);
+    memcpy(st->pql[b], pql, N2 * 3 * sizeof(int32_t));
+    memcpy(st->surv, survivors, sizeof(int32_t) * (size_t)pr->N);
+    memcpy(st->ext, extremes, sizeof(float) * st->M * st->M);
+    st->gen = gen;
+}

@@ -115,6 +115,14 @@ void or_mutate_eval_batch(const or_problem *pr, uint32_t gen, const int32_t *idx
                           const int32_t *ppql, uint8_t *child, float *cobj, int8_t *cobjidx,
                           int32_t *cpql, int32_t *ops, int threads);
 
+/* synthetic inputs (same draws as the engine's pe_synthetic_protein / pe_dirichlet_table):
+ * aa_out receives L amino indices and the stop (L+1 entries) */
+void or_synthetic_protein(int L, uint64_t seed, int8_t *aa_out);
+void or_dirichlet_table(uint64_t seed, or_codon_table *out);
+/* replace the current 2N set, survivors, extreme points and generation counter */
+void or_set_state(or_state *st, const uint8_t *pop, const float *obj, const int8_t *objidx, const int32_t *pql,
+                  const int32_t *survivors, const float *extremes, uint32_t gen);
+
 /* Exact hypervolume of points in [0,1]^d w.r.t. reference point r (minimisation). */
 double or_hypervolume(const double *pts, int n, int d, const double *ref);
 

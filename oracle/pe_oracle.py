@@ -73,6 +73,9 @@ def lib():
         L.or_sl_sample_batch.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, P]
         L.or_mutate_eval_light_batch.argtypes = [C.POINTER(OrProblem), C.c_uint32, P, C.c_int, P, P, P, P, P, P, P,
                                                  P, C.c_int]
+        L.or_synthetic_protein.argtypes = [C.c_int, C.c_uint64, P]
+        L.or_dirichlet_table.argtypes = [C.c_uint64, C.POINTER(OrTable)]
+        L.or_set_state.argtypes = [P, P, P, P, P, P, P, C.c_uint32]
         L.or_hypervolume.argtypes = [P, C.c_int, C.c_int, P]
         L.or_hypervolume.restype = C.c_double
         _lib = L
@@ -200,6 +203,18 @@ class Run:
         lib().or_get(self.h, _p(ids), _p(obj), _p(objidx), _p(pql), _p(surv), _p(ext), _p(gen))
         return ids, obj, objidx, pql, surv, ext, int(gen[0])
 
+    def set_state(self, ids, obj, objidx, pql, survivors, extremes, generation: int):
+        """Start the next generation from this 2N state (e.g. the CUDA engine's)."""
+        pr = self.prob
+        N2 = 2 * pr.N
+        a = [np.ascontiguousarray(ids, np.uint8).reshape(N2, pr.m, pr.L),
+             np.ascontiguousarray(obj, np.float32).reshape(N2, pr.M),
+             np.ascontiguousarray(objidx, np.int8).reshape(N2, 2 * pr.M),
+             np.ascontiguousarray(pql, np.int32).reshape(N2, 3),
+             np.ascontiguousarray(survivors, np.int32).reshape(pr.N),
+             np.ascontiguousarray(extremes, np.float32).reshape(pr.M, pr.M)]
+        lib().or_set_state(self.h, *[_p(x) for x in a], generation)
+
     def close(self):
         if self.h:
             lib().or_destroy(self.h)
@@ -207,6 +222,26 @@ class Run:
 
     def __del__(self):
         self.close()
+
+
+def synthetic_protein(L: int, seed: int) -> np.ndarray:
+    """L amino indices uniform over the 20 standard letters, then the stop (index 20)."""
+    out = np.zeros(L + 1, np.int8)
+    lib().or_synthetic_protein(L, seed, _p(out))
+    return out
+
+
+def dirichlet_table(seed: int) -> dict:
+    """Standard genetic code with Dirichlet(1) weights per amino acid (max 1, ascending
+    inside each group) and seeded codon-pair scores, as the arrays Problem takes."""
+    t = OrTable()
+    lib().or_dirichlet_table(seed, C.byref(t))
+    return {"nt": np.ctypeslib.as_array(t.nt).reshape(64, 3).astype(np.uint8).copy(),
+            "weight": np.ctypeslib.as_array(t.weight).astype(np.float32).copy(),
+            "cps": np.ctypeslib.as_array(t.cps).astype(np.float32).copy(),
+            "start": np.ctypeslib.as_array(t.start).astype(np.int8).copy(),
+            "count": np.ctypeslib.as_array(t.count).astype(np.int8).copy(),
+            "ref_gc3": float(t.ref_gc3), "ref_gc": float(t.ref_gc)}
 
 
 def das_dennis(M: int, p: int) -> np.ndarray:

@@ -10,11 +10,18 @@
 // per-CDS partial results, per-solution completion counters) lives in one
 // fixed-size file-scope device array instead of being allocated.
 //
-// The array is reserved in every device's memory once this library is loaded
-// and stays until the process exits.  Every call uses the same array and finds
-// it holding the previous call's data, so each call clears the parts that must
-// start at zero itself; calls that overlap on the GPU (different streams, or a
-// call issued while the previous one still runs elsewhere) race on it.
+// When the array's memory is taken: CUDA loads this file's device code, and with
+// it the array, on each device the first time the code is used there (lazy module
+// loading, the default since CUDA 12.2), so the first call on a device reserves
+// the 8 MiB -- a call with n_solutions = 0 does only that set-up.  Make that call
+// while setting up, before the host application's memory manager takes the
+// device's memory and before any stream capture; with CUDA_MODULE_LOADING=EAGER
+// the array is reserved when the CUDA context is created instead.  Afterwards the
+// array stays reserved until the process exits, and no call allocates.  Every call
+// uses the same array and finds it holding the previous call's data, so each call
+// clears the parts that must start at zero itself; calls that overlap on the GPU
+// (different streams, or a call issued while the previous one still runs
+// elsewhere) race on it.
 #include <algorithm>
 #include <cstdint>
 #include <cstdio>
@@ -36,9 +43,9 @@ std::mutex g_mu;
 unsigned char *g_scratch_ptr[kMaxDevices] = {nullptr};
 
 // nucleotide codes (one byte each, 0..3) -> (lo, hi) bit planes; outputs preset to
-// NaN so a solution whose scan did not finish is visible as NaN
+// NaN and -1 so a solution whose scan did not finish shows it in all three outputs
 __global__ void k_pack_nt(const uint8_t *__restrict__ nt, int items, int n, int W, int Wp, uint2 *planes,
-                          int nsol, float *value)
+                          int nsol, float *value, int32_t *pql)
 {
     size_t total = (size_t)items * Wp;
     for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
@@ -56,8 +63,10 @@ __global__ void k_pack_nt(const uint8_t *__restrict__ nt, int items, int n, int 
         }
         planes[e] = make_uint2(lo, hi);
     }
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nsol; i += gridDim.x * blockDim.x)
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nsol; i += gridDim.x * blockDim.x) {
         value[i] = __int_as_float(0x7fc00000);
+        pql[3 * i] = pql[3 * i + 1] = pql[3 * i + 2] = -1;
+    }
 }
 
 __global__ void k_clear_counters(int32_t *counter, int nsol, int32_t *status)
@@ -66,9 +75,11 @@ __global__ void k_clear_counters(int32_t *counter, int nsol, int32_t *status)
     if (blockIdx.x == 0 && threadIdx.x == 0) *status = 0;
 }
 
-__global__ void k_copy_cds(const int8_t *objidx, int nsol, int8_t *cds)
+// the stem's CDS, or -1 where the scan did not finish (value still NaN)
+__global__ void k_copy_cds(const int8_t *objidx, const float *value, int nsol, int8_t *cds)
 {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nsol; i += gridDim.x * blockDim.x) cds[i] = objidx[2 * i];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nsol; i += gridDim.x * blockDim.x)
+        cds[i] = isnan(value[i]) ? (int8_t)-1 : objidx[2 * i];
 }
 
 // device address of the scratch array for the current device (looked up once per device)
@@ -103,15 +114,27 @@ using namespace pe;
 extern "C" int pe_hairpin_noalloc(const uint8_t *d_nt, int32_t n_solutions, int32_t m, int32_t L, float *d_value,
                                   int32_t *d_pql, int8_t *d_cds, void *cuda_stream)
 {
-    if (!d_nt || !d_value || !d_pql || !d_cds || n_solutions < 0) {
-        set_error_text("pe_hairpin_noalloc: null pointer or negative count");
+    if (n_solutions < 0) {
+        set_error_text("pe_hairpin_noalloc: negative count");
+        return PE_ERR_ARG;
+    }
+    if (n_solutions == 0) {
+        // set-up only: load this file's device code on the current device, which
+        // reserves the scratch array, and look its address up
+        unsigned char *base = nullptr;
+        const char *err = nullptr;
+        int rc = scratch_for_current_device(&base, &err);
+        if (rc != PE_OK) set_error_text(err);
+        return rc;
+    }
+    if (!d_nt || !d_value || !d_pql || !d_cds) {
+        set_error_text("pe_hairpin_noalloc: null pointer");
         return PE_ERR_ARG;
     }
     if (m < 1 || m > kMaxCds || L < 3) {
         set_error_text("pe_hairpin_noalloc: need 1 <= m <= 64 CDSs and L >= 3 positions");
         return PE_ERR_ARG;
     }
-    if (n_solutions == 0) return PE_OK;
     Shape s{};
     s.L = L;
     s.Lp = (L + 15) & ~15;
@@ -167,7 +190,7 @@ extern "C" int pe_hairpin_noalloc(const uint8_t *d_nt, int32_t n_solutions, int3
     k_clear_counters<<<(n_solutions + 255) / 256, 256, 0, st>>>(counter, n_solutions, status);
     size_t words = items * s.Wp;
     int blocks = (int)std::min<size_t>((words + 255) / 256, 4096);
-    k_pack_nt<<<blocks, 256, 0, st>>>(d_nt, (int)items, s.n, s.W, s.Wp, planes, n_solutions, d_value);
+    k_pack_nt<<<blocks, 256, 0, st>>>(d_nt, (int)items, s.n, s.W, s.Wp, planes, n_solutions, d_value, d_pql);
     PopBuf buf{};
     buf.planes = planes;
     buf.obj = d_value;
@@ -175,7 +198,7 @@ extern "C" int pe_hairpin_noalloc(const uint8_t *d_nt, int32_t n_solutions, int3
     buf.pql = d_pql;
     cudaError_t e = launch_sl(s, buf, 0, n_solutions, part, counter, status, st);
     if (e == cudaSuccess) {
-        k_copy_cds<<<(n_solutions + 255) / 256, 256, 0, st>>>(objidx, n_solutions, d_cds);
+        k_copy_cds<<<(n_solutions + 255) / 256, 256, 0, st>>>(objidx, d_value, n_solutions, d_cds);
         e = cudaGetLastError();
     }
     if (e != cudaSuccess) {

@@ -1,8 +1,9 @@
 """Extract the reference's codon table (include/info.cuh:6-54) into
 data/ref_codon_table.txt (next to this script), the text format read by pe_load_codon_table.
 
-Run in a tree where the reference sources are available:
-    python protein_encoding_v2_nsga-iii_b200/data/make_ref_table.py /root/reference
+Run where the reference sources are available, giving their directory (or
+PE_REFERENCE_DIR):
+    python protein_encoding_v2_nsga-iii_b200/data/make_ref_table.py <reference dir>
 The table is data (genetic code, relative-adaptiveness weights, codon-pair
 scores); the weights are evaluated as the C float expressions they are written as.
 """
@@ -58,4 +59,8 @@ def main(ref_root: str):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    import os
+    src = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PE_REFERENCE_DIR")
+    if not src:
+        sys.exit("usage: make_ref_table.py <reference source directory> (or set PE_REFERENCE_DIR)")
+    main(src)
