@@ -37,14 +37,17 @@ L_AA, M_CDS, POP, PM, P_REF, G_JOB, SEED = 1000, 8, 1024, 0.02, 8, 500, 2024
 # objective set of the plain workload: 1 = the four objectives (default), 0 = the reference's six
 # (then p follows the reference's rule from N: p = 7, 792 points); set by --objectives
 OBJ_SET, P_USE, M_OBJ = 1, P_REF, 4
+# string objective: 0 = the reference's hairpin stem (default), 1 = longest repeated/common substring
+SL_KIND = 0
 WORKLOAD = (f"plain NSGA-III, one synthetic protein L={L_AA} aa (+stop), m={M_CDS} CDSs, N={POP}, Pm={PM}, "
             f"4 objectives, Das-Dennis M=4 p={P_REF} (165 points), design job = {G_JOB} generations")
 
 
-def set_workload(shape: str | None, six: bool):
+def set_workload(shape: str | None, six: bool, lrcs: bool = False):
     """Plain workload other than the default: --shape L,m,N,p (p = 0: the reference's rule
-    from N) and/or the reference's six objectives."""
-    global L_AA, M_CDS, POP, P_REF, G_JOB, OBJ_SET, P_USE, M_OBJ, WORKLOAD
+    from N), the reference's six objectives, and/or the longest repeated/common substring
+    as the string objective."""
+    global L_AA, M_CDS, POP, P_REF, G_JOB, OBJ_SET, P_USE, M_OBJ, WORKLOAD, SL_KIND
     if shape:
         v = [int(x) for x in shape.split(",")]
         L_AA, M_CDS, POP, P_REF = v[:4]
@@ -59,9 +62,11 @@ def set_workload(shape: str | None, six: bool):
             p += 1
         p -= 1
     R = math.comb(M_OBJ + p - 1, p)
+    SL_KIND = 1 if lrcs else 0
     WORKLOAD = (f"plain NSGA-III, one synthetic protein L={L_AA} aa (+stop), m={M_CDS} CDSs, N={POP}, Pm={PM}, "
-                f"{'the reference' + chr(39) + 's 6' if six else '4'} objectives, Das-Dennis M={M_OBJ} p={p} "
-                f"({R} points), design job = {G_JOB} generations")
+                f"{'the reference' + chr(39) + 's 6' if six else '4'} objectives"
+                f"{' (string objective: longest repeated/common substring)' if lrcs else ''}, Das-Dennis M={M_OBJ} "
+                f"p={p} ({R} points), design job = {G_JOB} generations")
 METRIC = "generations/s"
 L2_FLUSH_BYTES = 256 << 20
 # k_sl at this workload, from ncu captures of one launch (the committed k_sl profile summary):
@@ -134,7 +139,12 @@ def roofline(cells: int, sl_seconds: float, clocks: dict) -> dict:
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 20 ms while timing."""
+    """nvidia-smi clocks / throttle reasons sampled every 20 ms while timing.
+
+    A reader thread timestamps every row.  Entering waits (up to 5 s) for the first
+    row, so sampling is running when the timed region starts; leaving waits for one
+    more row, so the region is covered even when it is shorter than the sampling
+    period.  The summary uses the rows from 25 ms before the region to 25 ms after."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -143,40 +153,59 @@ class ClockSampler:
     def __init__(self, index: int):
         self.index = index
         self.proc = None
+        self.rows = []
+        self.t0 = self.t1 = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            r = next(csv.reader(io.StringIO(line)), [])
+            if len(r) >= 9:
+                self.rows.append((time.perf_counter(), [x.strip() for x in r]))
+
+    def _wait_rows(self, n: int, limit_s: float):
+        end = time.perf_counter() + limit_s
+        while len(self.rows) < n and time.perf_counter() < end and self.proc.poll() is None:
+            time.sleep(0.002)
 
     def __enter__(self):
+        import threading
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
                                           "--format=csv,noheader,nounits", "-lms", "20"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True, bufsize=1)
         except OSError:
             self.proc = None
+        if self.proc is not None:
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+            self._wait_rows(1, 5.0)
+        self.t0 = time.perf_counter()
         return self
 
     def __exit__(self, *a):
-        self.rows = []
+        self.t1 = time.perf_counter()
         if self.proc is None:
             return
+        self._wait_rows(len(self.rows) + 1, 1.0)
         self.proc.terminate()
         try:
-            out, _ = self.proc.communicate(timeout=5)
+            self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
-            out, _ = self.proc.communicate()
-        for r in csv.reader(io.StringIO(out)):
-            if len(r) >= 9:
-                self.rows.append([x.strip() for x in r])
+            self.proc.wait()
+        self.thread.join(timeout=2)
 
     def summary(self):
-        rows = getattr(self, "rows", [])
-        if not rows:
+        if not self.rows or self.t0 is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        lo, hi = self.t0 - 0.025, (self.t1 or self.t0) + 0.025
+        rows = [r for t, r in self.rows if lo <= t <= hi] or [self.rows[-1][1]]
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
         mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for r in rows for i, v in enumerate(r[5:9]) if v.lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(rows), "timed_region_s": round((self.t1 or self.t0) - self.t0, 4)}
 
 
 def dist_setup():
@@ -204,7 +233,7 @@ def oracle_problem(orc):
     (the engine library is not loaded)."""
     aa = orc.synthetic_protein(L_AA, SEED)
     table = orc.dirichlet_table(SEED)
-    return orc.Problem(aa, table, M_CDS, POP, PM, objset=OBJ_SET, p=P_USE, seed=SEED)
+    return orc.Problem(aa, table, M_CDS, POP, PM, objset=OBJ_SET, p=P_USE, seed=SEED, slkind=SL_KIND)
 
 
 def time_oracle_generations(run, steps: int, threads: int) -> list[float]:
@@ -269,56 +298,13 @@ def cpu_baseline_one_generation(pe_state, extremes, generation: int) -> dict:
                       f"{generation}; {threads} threads; {sec:.1f} s"}
 
 
-def reference_cuda_build(pe, seconds_limit: float = 90.0, G: int = 10) -> dict:
-    """The reference's own CUDA build (oracle/_ref/Protein_NSGA3, compiled unmodified from
-    its sources) on this GPU at the plain workload's shape with its own settings (six
-    objectives, its codon table, p by its rule), timed by its own `Generation cycles time`
-    print (src/main.cu:702-731, 862); beside it this engine at the same settings and
-    generation count, timed with CUDA events around the back-to-back generations."""
-    import shutil
-    import tempfile
-
-    import torch
-    exe, hv = ROOT / "oracle" / "_ref" / "Protein_NSGA3", ROOT / "oracle" / "_ref" / "hv"
-    if not exe.exists() or not hv.exists():
-        return {"unavailable": "oracle/_ref/Protein_NSGA3 not built (make -C oracle ref needs the reference sources)"}
-    aa = pe.synthetic_protein(L_AA, SEED)
-    letters = "".join(pe.AMINO[int(x)] for x in aa[:-1])
-    res = {"shape": f"L={L_AA} (+stop), N={POP}, m={M_CDS}, Pm={PM}, {G} generations; the reference's six "
-                    f"objectives, its codon table, p by its rule"}
-    with tempfile.TemporaryDirectory() as d:
-        (Path(d) / "p.fasta.txt").write_text(">synthetic\n" + letters + "\n")
-        shutil.copy(hv, Path(d) / "hv")
-        try:
-            out = subprocess.run([str(exe), "p.fasta.txt", str(POP), str(G), str(M_CDS), str(PM)], cwd=d,
-                                 capture_output=True, text=True, timeout=seconds_limit)
-        except subprocess.TimeoutExpired:
-            res["unavailable"] = f"the reference build did not finish within {seconds_limit:.0f} s"
-            return res
-        import re
-        m = re.search(r"Generation cycles time\s*:\s*([0-9.eE+-]+)", out.stdout)
-        if out.returncode != 0 or not m:
-            res["unavailable"] = f"reference build exit {out.returncode}: {out.stdout[-200:]} {out.stderr[-200:]}"
-            return res
-        gen_s = float(m.group(1))
-        res["reference_generations_per_s"] = G / gen_s
-        res["reference_generation_cycles_s"] = gen_s
-    table = pe.load_codon_table(ROOT / "protein_encoding_v2_nsga-iii_b200" / "data" / "ref_codon_table.txt")
-    stream = torch.cuda.Stream()
-    with pe.Engine(aa, table, M_CDS, POP, PM, objectives=pe.OBJ_REF6, ref_p=0, seed=SEED,
-                   stream=stream.cuda_stream) as eng:
-        eng.init()
-        eng.step(3)
-        eng.synchronize()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        eng.step(G)
-        b.record(stream)
-        eng.synchronize()
-        ours = G / (a.elapsed_time(b) / 1000.0)
-    res["engine_generations_per_s"] = ours
-    res["engine_over_reference"] = ours / res["reference_generations_per_s"]
-    return res
+# The reference's own CUDA build (compiled unmodified from its sources) did not
+# terminate on this workload's protein on a B200: 10 generations under a 90 s limit
+# and 100 generations under a 150 s limit were both killed at the limit.  Code that
+# hung is not run again, so the line records that instead of a rate.
+REFERENCE_CUDA_UNAVAILABLE = ("the reference's CUDA build (src/main.cu compiled unmodified for sm_100a) did not "
+                              "terminate on this workload's protein on a B200 (10 generations: killed at a 90 s "
+                              "limit; 100 generations: killed at 150 s); it is not run again")
 
 
 def run_ours(args, world, rank, local):
@@ -334,13 +320,13 @@ def run_ours(args, world, rank, local):
     aa = pe.synthetic_protein(L_AA, SEED)
     table = pe.dirichlet_table(SEED)
     eng = pe.Engine(aa, table, M_CDS, POP, PM, objectives=OBJ_SET, ref_p=P_USE, seed=SEED + rank,
-                    sl_threads=args.sl_threads, stream=stream.cuda_stream)
+                    sl_threads=args.sl_threads, stream=stream.cuda_stream, sl_kind=SL_KIND)
     eng.init()
     eng.set_profiling(True)
     for _ in range(args.warmup):
         eng.step(1)
     eng.synchronize()
-    scans0 = eng.scan_count()
+    scans0, cells0 = eng.scan_count(), eng.scan_cells()
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     stage = np.zeros((args.steps, 3))
@@ -373,11 +359,9 @@ def run_ours(args, world, rank, local):
     windows = [{"generations": [args.warmup + w, args.warmup + min(w + 5, args.steps) - 1],
                 "variation_eval": float(stage[w:w + 5, 0].mean()), "hairpin_scan": float(stage[w:w + 5, 1].mean()),
                 "selection": float(stage[w:w + 5, 2].mean())} for w in range(0, args.steps, 5)]
-    n_nt = 3 * (L_AA + 1)
-    # a child's CDS that its mutation left unchanged keeps its parent's stem result:
-    # the stem-scan work is the CDSs actually scanned
-    scans_per_gen = (eng.scan_count() - scans0) / args.steps
-    cells = scans_per_gen * hairpin_cells_per_cds(n_nt)
+    # a child's CDS (LRCS: CDS pair) that its mutation left unchanged keeps its parent's
+    # result: the string-objective work is the cells of the scans actually run
+    cells = (eng.scan_cells() - cells0) / args.steps
     sl_s = stage_ms[1] / 1000.0
 
     # end-to-end through the public API with host buffers: every rank runs whole design jobs
@@ -391,7 +375,7 @@ def run_ours(args, world, rank, local):
     for job in range(E2E_JOBS):
         t0 = time.perf_counter()
         e2 = pe.Engine(aa, table, M_CDS, POP, PM, objectives=OBJ_SET, ref_p=P_USE, seed=SEED + 7 + rank + 1000 * job,
-                       sl_threads=args.sl_threads)
+                       sl_threads=args.sl_threads, sl_kind=SL_KIND)
         e2.init()
         for _ in range(G_E2E):
             e2.step(1)
@@ -411,14 +395,14 @@ def run_ours(args, world, rank, local):
     if rank == 0:
         # CPU baseline: the oracle on this host, bounded sample (N=1 only)
         cpu, ref_cuda = None, None
-        if world == 1:
+        if world == 1 and not args.no_cpu_baseline:
             # extreme points only steer the normalisation: the survivors' first M objective
             # vectors give the timed generation the same work
             state = eng.population()
             ext = state[1][state[4][:M_OBJ]]
             cpu = cpu_baseline_one_generation(state, ext, eng.generation)
-            if not args.skip_reference_cuda:
-                ref_cuda = reference_cuda_build(pe)
+        if world == 1:
+            ref_cuda = {"unavailable": REFERENCE_CUDA_UNAVAILABLE}
 
         peaks = {}
         try:
@@ -621,15 +605,18 @@ def main():
     ap.add_argument("--jobs", type=int, default=40, help="design requests in the served workload")
     ap.add_argument("--shape", default=None, help="plain workload L,m,N,p[,G] instead of 1000,8,1024,8,500 "
                     "(p=0: the reference's rule from N; G: generations of a design job)")
+    ap.add_argument("--string", choices=["hairpin", "lrcs"], default="hairpin",
+                    help="string objective of the plain workload: the reference's hairpin stem or the longest "
+                         "repeated/common substring")
     ap.add_argument("--objectives", choices=["base4", "ref6"], default="base4",
                     help="objective set of the plain workload (ref6: the reference's six, p by its rule)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=None,
                     help="timed generations (default 500; 3 for --impl reference, whose CPU generations take ~20 s)")
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--skip-reference-cuda", action="store_true",
-                    help="do not run the reference's own CUDA build beside the bench")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true",
+                    help="skip the CPU baseline (one whole oracle generation: minutes at the long-sequence shapes)")
     ap.add_argument("--sl-threads", type=int, default=0, choices=[0, 64, 128, 256],
                     help="stem-scan CTA size (0: timed per instance at init); a fixed size keeps a run "
                          "under a profiler, which slows every launch, on the kernels a plain run picks")
@@ -638,8 +625,8 @@ def main():
     args = ap.parse_args()
     if args.steps is None:
         args.steps = 3 if args.impl == "reference" else 500
-    if args.objectives == "ref6" or args.shape:
-        set_workload(args.shape, args.objectives == "ref6")
+    if args.objectives == "ref6" or args.shape or args.string == "lrcs":
+        set_workload(args.shape, args.objectives == "ref6", args.string == "lrcs")
     world, rank, local = dist_setup()
     if args.workload == "batched":
         run_batched(args)
@@ -653,14 +640,17 @@ def main():
         # threads), so the launches are the same with and without a profiler: the initial
         # scan, then one scan per generation
         eng = pe.Engine(pe.synthetic_protein(L_AA, SEED), pe.dirichlet_table(SEED), M_CDS, POP, PM,
-                        objectives=pe.OBJ_BASE4, ref_p=P_REF, seed=SEED, sl_threads=128)
+                        objectives=OBJ_SET, ref_p=P_USE, seed=SEED, sl_threads=args.sl_threads or 128,
+                        sl_kind=SL_KIND)
         eng.init()
-        scans = [eng.scan_count()]
+        scans, cells = [eng.scan_count()], [eng.scan_cells()]
         for _ in range(2):
             eng.step(1)
             scans.append(eng.scan_count())
+            cells.append(eng.scan_cells())
         eng.close()
-        print(json.dumps({"cds_scans_per_launch": [scans[0]] + [b - a for a, b in zip(scans, scans[1:])]}))
+        print(json.dumps({"scans_per_launch": [scans[0]] + [b - a for a, b in zip(scans, scans[1:])],
+                          "cells_per_launch": [cells[0]] + [b - a for a, b in zip(cells, cells[1:])]}))
         return
     if args.impl == "reference":
         run_reference(args, world, rank)

@@ -52,6 +52,14 @@ typedef enum {
  * BASE4 keeps 0 -minCAI, 1 -minHD, 2 max GC(3) deviation, 3 max hairpin stem. */
 typedef enum { PE_OBJ_REF6 = 0, PE_OBJ_BASE4 = 1 } pe_objective_set;
 typedef enum { PE_GC3 = 0, PE_GC_ALL = 1 } pe_gc_mode;
+/* String objective in the stem slot.  HAIRPIN is the reference's calMaximumSL
+ * (include/utils.cuh:712-888): longest complementary stem / ((3L-4)/2).  LRCS is
+ * the longest repeated or common substring, which the reference only names
+ * (MLRCS, src/auto_execution_experiments.py:45,215): the longest run of identical
+ * nucleotides shared by two CDSs (any offsets) or repeated inside one CDS (two
+ * different starts), / 3L; objidx holds its two CDSs and pql (p, q, length) its
+ * starts in them. */
+typedef enum { PE_SL_HAIRPIN = 0, PE_SL_LRCS = 1 } pe_string_objective;
 
 /* Genetic code and scores (reference: include/info.cuh:6-54). */
 typedef struct pe_codon_table {
@@ -80,6 +88,7 @@ typedef struct pe_config {
                                pe_init_population time the three on the initial
                                population and keep the fastest (results do not
                                depend on it); no counterpart in the reference */
+    int32_t sl_kind;        /* pe_string_objective (0 = the reference's hairpin stem) */
 } pe_config;
 
 typedef struct pe_info {
@@ -189,10 +198,17 @@ int pe_set_profiling(pe_instance *inst, int32_t enable);
 /* Device milliseconds of those stages in the last completed generation
  * (call after pe_synchronize). */
 int pe_stage_times(pe_instance *inst, float *ms3);
-/* CDS stem scans run since pe_create (no reference counterpart): a child's CDS
- * that its mutation left unchanged keeps its parent's stem result and is not
+/* String-objective scans run since pe_create (no reference counterpart): one per
+ * hairpin CDS or LRCS CDS pair.  A child's CDS that its mutation left unchanged
+ * (for LRCS: a pair of two such CDSs) keeps its parent's result and is not
  * scanned again.  Waits for the instance's stream. */
 int pe_scan_count(pe_instance *inst, uint64_t *count);
+/* Counted cells of those scans (no reference counterpart): (n-5)(n-4)/2 per hairpin
+ * CDS scan (the anti-diagonal cells with a loop of >= 4), n^2 per LRCS scan of two
+ * CDSs and n(n-1)/2 per LRCS scan of one CDS against itself, n = 3L nucleotides.
+ * The unit of work of the string-objective kernel's throughput.  Waits for the
+ * instance's stream. */
+int pe_scan_cells(pe_instance *inst, uint64_t *cells);
 
 /* --- allocation-free hairpin-stem evaluation (no counterpart in the reference).
  *

@@ -271,6 +271,65 @@ static void sl_serial(const uint8_t *nt, int m, int n, int *L_out, int *p_out, i
     *cds_out = cds;
 }
 
+/* Longest repeated or common substring: the LRCS flavour of the string
+ * objective.  The reference has no implementation -- it only names MLRCS among
+ * the objectives of its experiment scripts (src/auto_execution_experiments.py:45,
+ * 215) -- so the definition is this build's own, written as one thread would
+ * run it:
+ *   over CDS pairs a <= b in the order (0,0), (0,1), .., (0,m-1), (1,1), (1,2), ..,
+ *   the longest run of identical nucleotides s_a[r] == s_b[r + delta] along one
+ *   diagonal delta of the CDS-a-against-CDS-b matrix; a < b: every delta in
+ *   (-n, n) (a common substring); a == b: delta >= 1 (a substring occurring at two
+ *   different starts, overlaps allowed).
+ * The record is the first pair reaching the maximum, on it the smallest delta,
+ * on that diagonal the smallest start p: (length, p, q = p + delta, a, b).  The
+ * objective value is length / n (maximised; stored as is, smaller is better). */
+void or_lrcs_pair(const uint8_t *sa, const uint8_t *sb, int n, int self, int32_t *out3)
+{
+    int best = 0, bd = 0, bp = 0;
+    for (int delta = self ? 1 : -(n - 1); delta <= n - 1; delta++) {
+        int r_lo = delta < 0 ? -delta : 0, r_hi = delta > 0 ? n - 1 - delta : n - 1;
+        int run = 0;
+        for (int r = r_lo; r <= r_hi; r++) {
+            if (sa[r] == sb[r + delta]) {
+                run++;
+                if (run > best) {
+                    best = run;
+                    bd = delta;
+                    bp = r - run + 1;
+                }
+            } else {
+                run = 0;
+            }
+        }
+    }
+    out3[0] = best;
+    out3[1] = bd;
+    out3[2] = bp;
+}
+
+void or_lrcs(const uint8_t *nt, int m, int n, int32_t *out5)
+{
+    int best = 0, p = 0, q = 0, ba = 0, bb = 0;
+    for (int a = 0; a < m; a++)
+        for (int b = a; b < m; b++) {
+            int32_t r[3];
+            or_lrcs_pair(nt + (size_t)a * n, nt + (size_t)b * n, n, a == b, r);
+            if (r[0] > best) {
+                best = r[0];
+                p = r[2];
+                q = r[2] + r[1];
+                ba = a;
+                bb = b;
+            }
+        }
+    out5[0] = best;
+    out5[1] = p;
+    out5[2] = q;
+    out5[3] = ba;
+    out5[4] = bb;
+}
+
 int or_sl_serial_one(const uint8_t *nt, int n)
 {
     int l, p, q, c;
@@ -439,6 +498,17 @@ static void eval_impl(const or_problem *pr, const uint8_t *sol, float *obj, int8
             }
         }
     }
+    /* longest repeated/common substring in the string slot (see or_lrcs) */
+    if ((s = or_slot_of(pr->objset, OR_K_SL)) >= 0 && with_sl && pr->slkind == OR_SL_LRCS) {
+        int32_t r[5];
+        or_lrcs(nt, m, n, r);
+        obj[s] = (float)r[0] / (float)n;
+        objidx[2 * s] = (int8_t)r[3];
+        objidx[2 * s + 1] = (int8_t)r[4];
+        pql[0] = r[1];
+        pql[1] = r[2];
+        pql[2] = r[0];
+    } else
     /* calMaximumSL (include/utils.cuh:712-888) */
     if ((s = or_slot_of(pr->objset, OR_K_SL)) >= 0 && with_sl) {
         int l, p, q, c;
@@ -707,6 +777,34 @@ int or_mutate(const or_problem *pr, uint32_t gen, int idx, const uint8_t *parent
                * writes an unset buffer when nothing was mutated; here the attempted
                * codon itself is restored. */
         int sl = or_slot_of(pr->objset, OR_K_SL);
+        if (pr->slkind == OR_SL_LRCS) {
+            /* LRCS flavour (no reference counterpart): walk outward from the middle
+             * codon of the repeat's second occurrence (CDS b, nucleotides q .. q+l-1),
+             * mutating each codon with prob Pm (draws as above), and stop at the
+             * first codon changed */
+            int b = pobjidx[2 * sl + 1], q = ppql[1], l = ppql[2];
+            if (l <= 0 || q < 0 || b < 0 || b >= pr->m) break;
+            int a0 = q / 3, a1 = (q + l - 1) / 3, mid = (a0 + a1) / 2;
+            uint8_t *cds = child + (size_t)b * L;
+            int attempt = 0;
+            for (int u = 0; u <= 2 * (a1 - a0); u++) {
+                int a = (u & 1) ? mid - (u + 1) / 2 : mid + u / 2;
+                if (a < a0 || a > a1 || a >= L) continue;
+                int aa = pr->aa[a];
+                int k = t->count[aa];
+                uint32_t r0 = or_draw(pr->seed, TAG_SLMUT, gen, (uint32_t)idx, (uint32_t)attempt, 0);
+                uint32_t r1 = or_draw(pr->seed, TAG_SLMUT, gen, (uint32_t)idx, (uint32_t)attempt, 1);
+                attempt++;
+                if (rng_u01(r0) <= pm && k > 1) {
+                    int cur = cds[a] - t->start[aa];
+                    int nw = (int)rng_uint(r1, (uint32_t)(k - 1));
+                    if (nw == cur) nw++;
+                    cds[a] = (uint8_t)(t->start[aa] + nw);
+                    break;
+                }
+            }
+            break;
+        }
         int c = pobjidx[2 * sl];
         float v = pobj[sl];
         int n = 3 * L, K = (n - 4) / 2;

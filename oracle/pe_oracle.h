@@ -34,6 +34,9 @@ extern "C" {
 enum { OR_K_CAI = 0, OR_K_CBP = 1, OR_K_HSC = 2, OR_K_HD = 3, OR_K_GC = 4, OR_K_SL = 5 };
 enum { OR_OBJSET_REF6 = 0, OR_OBJSET_BASE4 = 1 };
 enum { OR_GC3 = 0, OR_GCALL = 1 };
+/* flavour of the string objective in the SL slot: the reference's hairpin stem, or
+ * the longest repeated/common substring (no reference implementation: parity unpinned) */
+enum { OR_SL_HAIRPIN = 0, OR_SL_LRCS = 1 };
 
 typedef struct {
     uint8_t nt[OR_NUM_CODON][3];     /* nucleotide codes A=0 C=1 G=2 U=3 */
@@ -56,6 +59,7 @@ typedef struct {
     uint64_t seed;
     const int8_t *aa; /* [L] amino-acid index (0..20, 20 = stop) */
     const or_codon_table *tab;
+    int slkind;       /* OR_SL_HAIRPIN or OR_SL_LRCS */
 } or_problem;
 
 /* --- helpers shared with tests --- */
@@ -75,6 +79,12 @@ void or_eval(const or_problem *pr, const uint8_t *sol, float *obj, int8_t *objid
 int  or_mutate(const or_problem *pr, uint32_t gen, int idx, const uint8_t *parent,
                const float *pobj, const int8_t *pobjidx, const int32_t *ppql, uint8_t *child);
 int  or_sl_serial_one(const uint8_t *nt, int n);   /* calOneCDS_SL max l */
+/* longest repeated/common substring of m CDSs of n nucleotides: length, starts p (in
+ * CDS a) and q (in CDS b), pair (a, b) -- see lrcs_serial */
+void or_lrcs(const uint8_t *nt, int m, int n, int32_t *out5);
+/* one pair: longest run on the diagonals delta >= 1 (self) or all (a != b); out: length,
+ * delta, start p (first pair rule: smallest delta, then smallest p) */
+void or_lrcs_pair(const uint8_t *sa, const uint8_t *sb, int n, int self, int32_t *out3);
 /* timing-sample helpers (bounded slices of the same work) */
 void or_eval_light(const or_problem *pr, const uint8_t *sol, float *obj, int8_t *objidx, int32_t *pql);
 int  or_sl_serial_strided(const uint8_t *nt, int n, int offset, int stride);

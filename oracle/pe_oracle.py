@@ -23,7 +23,7 @@ class OrTable(C.Structure):
 class OrProblem(C.Structure):
     _fields_ = [("L", C.c_int), ("m", C.c_int), ("N", C.c_int), ("objset", C.c_int), ("gcmode", C.c_int),
                 ("p", C.c_int), ("pm", C.c_float), ("seed", C.c_uint64), ("aa", C.c_void_p),
-                ("tab", C.POINTER(OrTable))]
+                ("tab", C.POINTER(OrTable)), ("slkind", C.c_int)]
 
 
 class OrSelectInfo(C.Structure):
@@ -60,6 +60,8 @@ def lib():
         L.or_eval.argtypes = [C.POINTER(OrProblem), P, P, P, P]
         L.or_mutate.argtypes = [C.POINTER(OrProblem), C.c_uint32, C.c_int, P, P, P, P, P]
         L.or_sl_serial_one.argtypes = [P, C.c_int]
+        L.or_lrcs.argtypes = [P, C.c_int, C.c_int, P]
+        L.or_lrcs_pair.argtypes = [P, P, C.c_int, C.c_int, P]
         L.or_select.argtypes = [C.POINTER(OrProblem), C.c_uint32, P, P, P, C.c_int, P, P, C.POINTER(OrSelectInfo)]
         L.or_create.argtypes = [C.POINTER(OrProblem)]
         L.or_create.restype = C.c_void_p
@@ -102,7 +104,7 @@ class Problem:
     """A problem description shared by every oracle call."""
 
     def __init__(self, aa, table_arrays: dict, m: int, N: int, pm: float, objset: int = 1, gcmode: int = 0,
-                 p: int = 0, seed: int = 0):
+                 p: int = 0, seed: int = 0, slkind: int = 0):
         self.aa = np.ascontiguousarray(aa, np.int8)
         self.L = len(self.aa)
         self.m, self.N = m, N
@@ -113,7 +115,7 @@ class Problem:
         self.R = lib().or_num_ref(self.M, p)
         self.tab = make_table(table_arrays)
         self.c = OrProblem(self.L, m, N, objset, gcmode, p, pm, seed, self.aa.ctypes.data_as(C.c_void_p),
-                           C.pointer(self.tab))
+                           C.pointer(self.tab), slkind)
         self.refpts = das_dennis(self.M, p)
 
     def slot(self, kind: int) -> int:
@@ -266,6 +268,23 @@ def det_exp(x: float) -> float:
 def sl_serial_one(nt) -> int:
     nt = np.ascontiguousarray(nt, np.uint8)
     return lib().or_sl_serial_one(_p(nt), len(nt))
+
+
+def lrcs(nt) -> tuple:
+    """Longest repeated/common substring of m CDSs (rows of nt): (length, p, q, a, b)."""
+    nt = np.ascontiguousarray(nt, np.uint8)
+    out = np.zeros(5, np.int32)
+    lib().or_lrcs(_p(nt), nt.shape[0], nt.shape[1], _p(out))
+    return tuple(int(x) for x in out)
+
+
+def lrcs_pair(sa, sb, self_pair: bool) -> tuple:
+    """(length, delta, p) of one pair."""
+    sa = np.ascontiguousarray(sa, np.uint8)
+    sb = np.ascontiguousarray(sb, np.uint8)
+    out = np.zeros(3, np.int32)
+    lib().or_lrcs_pair(_p(sa), _p(sb), len(sa), int(self_pair), _p(out))
+    return tuple(int(x) for x in out)
 
 
 def sl_sample(nt_cds, offset: int, stride: int, threads: int = 0) -> np.ndarray:

@@ -28,6 +28,9 @@ AMINO = "ACDEFGHIKLMNPQRSTVWYZ"
 NT = "ACGU"
 OBJ_REF6, OBJ_BASE4 = 0, 1
 GC3, GC_ALL = 0, 1
+# string objective in the stem slot: the reference's hairpin stem, or the longest
+# repeated/common substring (see pe_string_objective in the header)
+SL_HAIRPIN, SL_LRCS = 0, 1
 # slot layout per objective set (kinds: CAI CBP HSC HD GC SL)
 OBJ_NAMES = {OBJ_REF6: ["mCAI", "mCBP", "mHSC", "mHD", "MGC", "MSL"], OBJ_BASE4: ["mCAI", "mHD", "MGC", "MSL"]}
 
@@ -76,7 +79,7 @@ class CodonTable(C.Structure):
 class Config(C.Structure):
     _fields_ = [("n_cds", C.c_int32), ("pop_size", C.c_int32), ("mutation_prob", C.c_float),
                 ("objectives", C.c_int32), ("gc_mode", C.c_int32), ("ref_p", C.c_int32), ("seed", C.c_uint64),
-                ("stream_priority", C.c_int32), ("sl_threads", C.c_int32)]
+                ("stream_priority", C.c_int32), ("sl_threads", C.c_int32), ("sl_kind", C.c_int32)]
 
 
 class Info(C.Structure):
@@ -117,6 +120,7 @@ def lib() -> C.CDLL:
             "pe_load_codon_table": [C.c_char_p, C.POINTER(CodonTable)],
             "pe_hypervolume": [P, C.c_int32, C.c_int32, P, C.POINTER(C.c_double)],
             "pe_set_profiling": [P, C.c_int32], "pe_stage_times": [P, P], "pe_scan_count": [P, P],
+            "pe_scan_cells": [P, P],
             "pe_hairpin_noalloc": [P, C.c_int32, C.c_int32, C.c_int32, P, P, P, P],
             "pe_batch_create": [P, C.c_int32, C.POINTER(P)], "pe_batch_step": [P, C.c_int32],
             "pe_batch_synchronize": [P], "pe_batch_destroy": [P],
@@ -192,9 +196,10 @@ def hairpin_noalloc(d_nt: int, n_solutions: int, m: int, L: int, d_value: int, d
                                  C.c_void_p(d_cds), C.c_void_p(stream) if stream else None))
 
 
-def instance_bytes(aa_len: int, n_cds: int, pop_size: int, objectives: int = OBJ_BASE4, ref_p: int = 0) -> int:
+def instance_bytes(aa_len: int, n_cds: int, pop_size: int, objectives: int = OBJ_BASE4, ref_p: int = 0,
+                   sl_kind: int = SL_HAIRPIN) -> int:
     """Device bytes an Engine of this shape allocates (admission by memory footprint)."""
-    cfg = Config(n_cds, pop_size, 0.0, objectives, GC3, ref_p, 0)
+    cfg = Config(n_cds, pop_size, 0.0, objectives, GC3, ref_p, 0, 0, 0, sl_kind)
     out = C.c_uint64(0)
     _ck(lib().pe_instance_bytes(C.byref(cfg), aa_len, C.byref(out)))
     return out.value
@@ -215,10 +220,12 @@ class Engine:
 
     def __init__(self, aa, table: CodonTable, n_cds: int, pop_size: int, mutation_prob: float,
                  objectives: int = OBJ_BASE4, gc_mode: int = GC3, ref_p: int = 0, seed: int = 0, stream=None,
-                 stream_priority: int = 0, sl_threads: int = 0):
+                 stream_priority: int = 0, sl_threads: int = 0, sl_kind: int = SL_HAIRPIN):
         self.aa = np.ascontiguousarray(aa, np.int8)
         self.table = table
-        cfg = Config(n_cds, pop_size, mutation_prob, objectives, gc_mode, ref_p, seed, stream_priority, sl_threads)
+        self.sl_kind = sl_kind
+        cfg = Config(n_cds, pop_size, mutation_prob, objectives, gc_mode, ref_p, seed, stream_priority, sl_threads,
+                     sl_kind)
         h = C.c_void_p()
         _ck(lib().pe_create(C.byref(cfg), _ptr(self.aa), len(self.aa), C.byref(table),
                             None if stream is None else C.c_void_p(stream), C.byref(h)))
@@ -277,9 +284,16 @@ class Engine:
         return out
 
     def scan_count(self) -> int:
-        """CDS stem scans run so far (a child's unchanged CDS keeps its parent's result)."""
+        """String-objective scans run so far: CDSs (hairpin) or CDS pairs (LRCS); a child's
+        unchanged CDS (pair) keeps its parent's result."""
         v = C.c_uint64(0)
         _ck(lib().pe_scan_count(self._h, C.byref(v)))
+        return v.value
+
+    def scan_cells(self) -> int:
+        """Counted cells of those scans (the string-objective kernel's unit of work)."""
+        v = C.c_uint64(0)
+        _ck(lib().pe_scan_cells(self._h, C.byref(v)))
         return v.value
 
     def population(self):

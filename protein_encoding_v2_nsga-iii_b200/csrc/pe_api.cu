@@ -162,7 +162,7 @@ struct pe_instance {
     int2 *d_part = nullptr;
     int32_t *d_counter = nullptr;
     int32_t *d_status = nullptr;
-    unsigned long long *d_scanned = nullptr;  // CDS stem scans run
+    unsigned long long *d_scanned = nullptr;  // [0] string-objective scans run, [1] their counted cells
     float *d_ext = nullptr;
     uint32_t *d_gen = nullptr;
     int cur = 0;
@@ -198,13 +198,13 @@ int alloc_pop(pe_instance *in, PopBuf &b, int nsol)
     if ((rc = in->alloc(&b.obj, (size_t)nsol * s.M))) return rc;
     if ((rc = in->alloc(&b.objidx, (size_t)nsol * 2 * s.M))) return rc;
     if ((rc = in->alloc(&b.pql, (size_t)nsol * 3))) return rc;
-    if ((rc = in->alloc(&b.cds, (size_t)nsol * s.m))) return rc;
+    if ((rc = in->alloc(&b.cds, (size_t)nsol * s.nres))) return rc;
     CK(cudaMemsetAsync(b.ids, 0, (size_t)nsol * s.m * s.Lp, in->stream));
     CK(cudaMemsetAsync(b.planes, 0, (size_t)nsol * s.m * s.Wp * sizeof(uint2), in->stream));
     CK(cudaMemsetAsync(b.obj, 0, (size_t)nsol * s.M * sizeof(float), in->stream));
     CK(cudaMemsetAsync(b.objidx, 0, (size_t)nsol * 2 * s.M, in->stream));
     CK(cudaMemsetAsync(b.pql, 0, (size_t)nsol * 3 * sizeof(int32_t), in->stream));
-    CK(cudaMemsetAsync(b.cds, 0xff, (size_t)nsol * s.m * sizeof(int2), in->stream));  // x = -1: to scan
+    CK(cudaMemsetAsync(b.cds, 0xff, (size_t)nsol * s.nres * sizeof(int2), in->stream));  // x = -1: to scan
     return PE_OK;
 }
 
@@ -350,6 +350,8 @@ int pe_create(const pe_config *cfg, const int8_t *aa_idx, int32_t aa_len, const 
     if (cfg->gc_mode != PE_GC3 && cfg->gc_mode != PE_GC_ALL) return fail(PE_ERR_ARG, "bad gc mode");
     if (cfg->sl_threads != 0 && cfg->sl_threads != 64 && cfg->sl_threads != 128 && cfg->sl_threads != 256)
         return fail(PE_ERR_ARG, "sl_threads must be 0, 64, 128 or 256, got %d", cfg->sl_threads);
+    if (cfg->sl_kind != PE_SL_HAIRPIN && cfg->sl_kind != PE_SL_LRCS)
+        return fail(PE_ERR_ARG, "sl_kind must be PE_SL_HAIRPIN or PE_SL_LRCS, got %d", cfg->sl_kind);
     // table validation
     {
         int expect = 0;
@@ -385,6 +387,8 @@ int pe_create(const pe_config *cfg, const int8_t *aa_idx, int32_t aa_len, const 
     s.pm = cfg->mutation_prob;
     s.seed = cfg->seed;
     s.sl_threads = cfg->sl_threads;
+    s.sl_kind = cfg->sl_kind;
+    s.nres = s.sl_kind == PE_SL_LRCS ? m * (m + 1) / 2 : m;
     {
         static const int ref6[6] = {K_CAI, K_CBP, K_HSC, K_HD, K_GC, K_SL};
         static const int base4[4] = {K_CAI, K_HD, K_GC, K_SL};
@@ -498,9 +502,9 @@ int pe_create(const pe_config *cfg, const int8_t *aa_idx, int32_t aa_len, const 
     if ((rc = in->alloc(&in->sc.cand, (size_t)N2))) return cleanup(rc);
     if ((rc = in->alloc(&in->sc.info, 8))) return cleanup(rc);
     if ((rc = in->alloc(&in->sc.finfo, 3 * PE_MAX_OBJ))) return cleanup(rc);
-    if ((rc = in->alloc(&in->d_part, (size_t)N2 * m))) return cleanup(rc);
+    if ((rc = in->alloc(&in->d_part, (size_t)N2 * s.nres))) return cleanup(rc);
     if ((rc = in->alloc(&in->d_counter, (size_t)N2))) return cleanup(rc);
-    if ((rc = in->alloc(&in->d_scanned, 1))) return cleanup(rc);
+    if ((rc = in->alloc(&in->d_scanned, 2))) return cleanup(rc);
     if ((rc = in->alloc(&in->d_status, 1))) return cleanup(rc);
     if ((rc = in->alloc(&in->d_ext, (size_t)s.M * s.M))) return cleanup(rc);
     if ((rc = in->alloc(&in->d_gen, 1))) return cleanup(rc);
@@ -516,7 +520,7 @@ int pe_create(const pe_config *cfg, const int8_t *aa_idx, int32_t aa_len, const 
     CKC(cudaMemcpyAsync(in->d_aa, aa_idx, (size_t)L, cudaMemcpyHostToDevice, st));
     CKC(cudaMemcpyAsync(in->d_ref, ref.data(), ref.size() * sizeof(float), cudaMemcpyHostToDevice, st));
     CKC(cudaMemsetAsync(in->d_counter, 0, (size_t)N2 * sizeof(int32_t), st));
-    CKC(cudaMemsetAsync(in->d_scanned, 0, sizeof(unsigned long long), st));
+    CKC(cudaMemsetAsync(in->d_scanned, 0, 2 * sizeof(unsigned long long), st));
     CKC(cudaMemsetAsync(in->d_status, 0, sizeof(int32_t), st));
     CKC(cudaMemsetAsync(in->d_ext, 0, (size_t)s.M * s.M * sizeof(float), st));
     CKC(cudaMemsetAsync(in->d_gen, 0, sizeof(uint32_t), st));
@@ -694,6 +698,16 @@ int pe_scan_count(pe_instance *in, uint64_t *count)
     return PE_OK;
 }
 
+int pe_scan_cells(pe_instance *in, uint64_t *cells)
+{
+    if (!in || !cells) return fail(PE_ERR_ARG, "null argument");
+    unsigned long long v = 0;
+    CK(cudaMemcpyAsync(&v, in->d_scanned + 1, sizeof v, cudaMemcpyDeviceToHost, in->stream));
+    CK(cudaStreamSynchronize(in->stream));
+    *cells = (uint64_t)v;
+    return PE_OK;
+}
+
 int pe_instance_bytes(const pe_config *cfg, int32_t aa_len, uint64_t *bytes)
 {
     if (!cfg || !bytes || aa_len < 3 || cfg->pop_size < 1 || cfg->n_cds < 2) return fail(PE_ERR_ARG, "bad arguments");
@@ -712,8 +726,9 @@ int pe_instance_bytes(const pe_config *cfg, int32_t aa_len, uint64_t *bytes)
     uint64_t t = r(sizeof(DevTables)) + r(L) + r(R * M * 4);
     t += 2 * (r(N2 * m * Lp) + r(N2 * m * Wp * 8) + r(N2 * M * 4) + r(N2 * 2 * M) + r(N2 * 12));
     t += r(N * 4) + r(N2 * words * 4) + 6 * r(N2 * 4) + 3 * r(R * 4) + r((R + 1) * 4) + r(32) + r(72);
-    t += r(N2 * m * 8) + r(N2 * 4) + r(4) + r(M * M * 4) + r(4);
-    t += 2 * r(N2 * m * 8) + r(8);  // per-CDS stem results of both buffers, scan count
+    const uint64_t nres = cfg->sl_kind == PE_SL_LRCS ? m * (m + 1) / 2 : m;
+    t += r(N2 * nres * 8) + r(N2 * 4) + r(4) + r(M * M * 4) + r(4);
+    t += 2 * r(N2 * nres * 8) + r(16);  // per-CDS (per-pair) string results of both buffers, scan counts
     *bytes = t;
     return PE_OK;
 }
@@ -892,7 +907,7 @@ int pe_eval_objectives(pe_instance *in, const uint8_t *codon_idx, int32_t n, flo
     int32_t *counter;
     int rc;
     if ((rc = t.pop(s, b, n))) return rc;
-    if ((rc = t.get(&part, (size_t)n * s.m))) return rc;
+    if ((rc = t.get(&part, (size_t)n * s.nres))) return rc;
     if ((rc = t.get(&counter, (size_t)n))) return rc;
     CK(cudaMemsetAsync(b.ids, 0, (size_t)n * s.m * s.Lp, in->stream));
     CK(cudaMemsetAsync(b.obj, 0, (size_t)n * s.M * sizeof(float), in->stream));

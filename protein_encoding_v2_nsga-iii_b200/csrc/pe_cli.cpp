@@ -8,6 +8,8 @@
 //   --seed S                  RNG seed (the reference seeds from time())
 //   --objectives ref6|base4   objective set (default ref6, as the reference)
 //   --gc gc3|gc               GC objective flavour (default gc3)
+//   --string hairpin|lrcs     string objective: the reference's hairpin stem (default)
+//                             or the longest repeated/common substring
 //   --ref-p P                 Das-Dennis partitions (default: reference rule)
 //   --codon-table FILE        codon table text file (default: the reference table
 //                             shipped in data/ref_codon_table.txt next to lib/)
@@ -50,7 +52,7 @@ static std::string exe_dir()
 int main(int argc, char **argv)
 {
     if (argc < 6) {
-        fprintf(stderr, "usage: %s <fasta> <N> <G> <m> <Pm> [--seed S] [--objectives ref6|base4] [--gc gc3|gc]\n"
+        fprintf(stderr, "usage: %s <fasta> <N> <G> <m> <Pm> [--seed S] [--objectives ref6|base4] [--gc gc3|gc] [--string hairpin|lrcs]\n"
                         "       [--ref-p P] [--codon-table FILE | --dirichlet SEED] [--synthetic-protein L:SEED]"
                         " [--out DIR]\n",
                 argv[0]);
@@ -87,6 +89,7 @@ int main(int argc, char **argv)
         if (a == "--seed") cfg.seed = strtoull(next(), nullptr, 10);
         else if (a == "--objectives") cfg.objectives = std::string(next()) == "base4" ? PE_OBJ_BASE4 : PE_OBJ_REF6;
         else if (a == "--gc") cfg.gc_mode = std::string(next()) == "gc" ? PE_GC_ALL : PE_GC3;
+        else if (a == "--string") cfg.sl_kind = std::string(next()) == "lrcs" ? PE_SL_LRCS : PE_SL_HAIRPIN;
         else if (a == "--ref-p") cfg.ref_p = atoi(next());
         else if (a == "--codon-table") table_path = next();
         else if (a == "--dirichlet") dirichlet = atol(next());

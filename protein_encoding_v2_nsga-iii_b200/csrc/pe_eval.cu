@@ -109,6 +109,17 @@ __device__ bool cta_full_hairpin(const Shape &s, const SmemTab &st, const uint8_
     return found;
 }
 
+// CDS pair of LRCS result r: (0,0), (0,1), .., (0,m-1), (1,1), (1,2), ..
+__host__ __device__ __forceinline__ void lrcs_pair_of(int m, int r, int &a, int &b)
+{
+    a = 0;
+    while (r >= m - a) {
+        r -= m - a;
+        a++;
+    }
+    b = a + r;
+}
+
 struct VarSmem {
     SmemTab tab;
     int64_t cds_val[kMaxCds];   // per-CDS sums
@@ -120,6 +131,7 @@ struct VarSmem {
     int32_t sl_old;
     int32_t sl_mut;
     int32_t op;
+    unsigned long long changed;  // CDSs whose planes the mutation changed (bit c)
 };
 
 // Every objective except the hairpin stem, for the solution in smem.
@@ -500,6 +512,36 @@ __device__ void mutate_solution(const Shape &s, const DevTables *gt, VarSmem &sm
     }
     case 6: {  // mutationSL (:775-969): attempts at the stem's centre codons
         int ss = s.slot[K_SL];
+        if (s.sl_kind == PE_SL_LRCS) {
+            // LRCS flavour (no reference counterpart): walk outward from the middle codon
+            // of the repeat's second occurrence (CDS b, nucleotides q .. q+l-1), mutating
+            // each codon with prob Pm, and stop at the first codon changed
+            if (tid == 0) {
+                const int b = sm.pobjidx[2 * ss + 1], q = sm.ppql[1], l = sm.ppql[2];
+                if (l > 0 && q >= 0 && b >= 0 && b < s.m) {
+                    const int a0 = q / 3, a1 = (q + l - 1) / 3, mid = (a0 + a1) / 2;
+                    uint8_t *row = ids + b * s.Lp;
+                    int attempt = 0;
+                    for (int u = 0; u <= 2 * (a1 - a0); u++) {
+                        const int a = (u & 1) ? mid - (u + 1) / 2 : mid + u / 2;
+                        if (a < a0 || a > a1 || a >= L) continue;
+                        const int am = aa[a], k = st.count[am];
+                        const uint32_t r0 = draw(s.seed, TAG_SLMUT, gen, ridx, (uint32_t)attempt, 0);
+                        const uint32_t r1 = draw(s.seed, TAG_SLMUT, gen, ridx, (uint32_t)attempt, 1);
+                        attempt++;
+                        if (rng_u01(r0) <= pm && k > 1) {
+                            const int cur = row[a] - st.start[am];
+                            int nw = (int)rng_uint(r1, (uint32_t)(k - 1));
+                            if (nw == cur) nw++;
+                            row[a] = (uint8_t)(st.start[am] + nw);
+                            break;
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+            break;
+        }
         int c = sm.pobjidx[2 * ss];
         float v = sm.pobj[ss];
         int P = sm.ppql[0], Ls = sm.ppql[2];
@@ -592,13 +634,13 @@ __global__ void __launch_bounds__(kVarThreads) k_variation(Shape s, const DevTab
             for (int a = s.L + tid; a < s.Lp; a += nth) ids[c * s.Lp + a] = 0;
         if (tid == 0 && surv) surv[i] = i;
         if (dst.cds)
-            for (int c = tid; c < s.m; c += nth) dst.cds[(size_t)i * s.m + c] = make_int2(-1, 0);
+            for (int c = tid; c < s.nres; c += nth) dst.cds[(size_t)i * s.nres + c] = make_int2(-1, 0);
     } else if (MODE == MODE_EVAL) {
         const uint4 *g = reinterpret_cast<const uint4 *>(dst.ids + (size_t)i * sol_bytes);
         uint4 *d = reinterpret_cast<uint4 *>(ids);
         for (size_t e = tid; e < sol_bytes / 16; e += nth) d[e] = g[e];
         if (dst.cds)
-            for (int c = tid; c < s.m; c += nth) dst.cds[(size_t)i * s.m + c] = make_int2(-1, 0);
+            for (int c = tid; c < s.nres; c += nth) dst.cds[(size_t)i * s.nres + c] = make_int2(-1, 0);
     } else {  // MODE_MUTATE
         gen = *d_gen;
         ridx = rng_idx ? (uint32_t)rng_idx[i] : (uint32_t)i;
@@ -628,8 +670,8 @@ __global__ void __launch_bounds__(kVarThreads) k_variation(Shape s, const DevTab
             if (tid < 2 * s.M) dst.objidx[dslot * 2 * s.M + tid] = src.objidx[(size_t)par * 2 * s.M + tid];
             if (tid < 3) dst.pql[dslot * 3 + tid] = src.pql[(size_t)par * 3 + tid];
             if (dst.cds)
-                for (int c = tid; c < s.m; c += nth)
-                    dst.cds[dslot * s.m + c] = src.cds ? src.cds[(size_t)par * s.m + c] : make_int2(-1, 0);
+                for (int c = tid; c < s.nres; c += nth)
+                    dst.cds[dslot * s.nres + c] = src.cds ? src.cds[(size_t)par * s.nres + c] : make_int2(-1, 0);
         }
         out_slot = child_base + i;
         if (tid == 0) {
@@ -667,8 +709,11 @@ __global__ void __launch_bounds__(kVarThreads) k_variation(Shape s, const DevTab
     __syncthreads();
     pack_planes(s, sm.tab, ids, planes, tid, nth, MODE == MODE_MUTATE ? dirty : nullptr);
     if (MODE == MODE_MUTATE && dst.cds) {
-        // a CDS none of whose plane words changed keeps its parent's hairpin result
+        // a CDS none of whose plane words changed keeps its parent's hairpin result;
+        // an LRCS pair of two such CDSs keeps its parent's pair result
         const int par = parent_of[i];
+        if (tid == 0) sm.changed = 0ull;
+        __syncthreads();
         for (int c = tid; c < s.m; c += nth) {
             bool changed = src.cds == nullptr;
             const int b0 = c * s.Wp, b1 = b0 + s.Wp;  // this CDS's bits [b0, b1)
@@ -677,7 +722,20 @@ __global__ void __launch_bounds__(kVarThreads) k_variation(Shape s, const DevTab
                 const uint32_t mask = hi - lo == 32 ? ~0u : ((1u << (hi - lo)) - 1u) << lo;
                 changed = (dirty[wd] & mask) != 0u;
             }
-            dst.cds[(size_t)out_slot * s.m + c] = changed ? make_int2(-1, 0) : src.cds[(size_t)par * s.m + c];
+            if (changed) atomicOr(&sm.changed, 1ull << c);
+        }
+        __syncthreads();
+        const unsigned long long ch = sm.changed;
+        for (int c = tid; c < s.nres; c += nth) {
+            bool changed;
+            if (s.sl_kind == PE_SL_LRCS) {
+                int a, b;
+                lrcs_pair_of(s.m, c, a, b);
+                changed = ((ch >> a) | (ch >> b)) & 1ull;
+            } else {
+                changed = (ch >> c) & 1ull;
+            }
+            dst.cds[(size_t)out_slot * s.nres + c] = changed ? make_int2(-1, 0) : src.cds[(size_t)par * s.nres + c];
         }
     }
     __syncthreads();
@@ -789,6 +847,48 @@ cudaError_t launch_mutate(const Shape &s, const DevTables *tab, const int8_t *aa
 
 __device__ __forceinline__ uint32_t fshr(uint32_t lo, uint32_t hi, int sh) { return __funnelshift_r(lo, hi, sh); }
 
+// The same scan serves the longest repeated/common substring (LRCS flavour):
+// for CDSs a and b, T is b's own planes (not a reverse complement), so a cell
+// (r, delta) matches iff s_a[r] == s_b[r + delta] and the runs along a fixed
+// delta are common substrings.  Its diagonals are every delta in (-n, n) for
+// a != b and delta >= 1 for a == b (a substring at two different starts), each
+// over all rows r in [max(0, -delta), min(n-1, n-1-delta)].  FL selects the
+// flavour at compile time: 0 hairpin, 1 LRCS.
+struct SlGeo {
+    int n;
+    int dlo, dhi;  // diagonals (shifts delta) scanned
+    int D0;        // first band's shift (a multiple of 32, <= dlo)
+    int ng;        // band groups
+};
+
+template <int FL> __host__ __device__ __forceinline__ SlGeo sl_geo(int n, bool self_pair)
+{
+    SlGeo g;
+    g.n = n;
+    if (FL == 0) {
+        g.dlo = -(n - 6);
+        g.dhi = n - 6;
+    } else {
+        g.dlo = self_pair ? 1 : -(n - 1);
+        g.dhi = n - 1;
+    }
+    g.D0 = g.dlo >= 0 ? (g.dlo & ~31) : -((-g.dlo + 31) & ~31);
+    const int nb = g.dhi >= g.dlo ? (g.dhi - g.D0) / 32 + 1 : 0;
+    g.ng = (nb + 2) / 3;
+    return g;
+}
+
+// counted rows of diagonal delta
+template <int FL> __device__ __forceinline__ void sl_diag_rows(int n, int delta, int &r_lo, int &r_hi)
+{
+    r_lo = max(0, -delta);
+    r_hi = FL == 0 ? ((n - 6 - delta) >> 1) : min(n - 1, n - 1 - delta);
+}
+
+// order key of a diagonal among equally long runs (smaller wins): the hairpin
+// keeps the smallest anti-diagonal d = n-1-delta, LRCS the smallest delta
+template <int FL> __device__ __forceinline__ int sl_key(int n, int delta) { return FL == 0 ? n - 1 - delta : delta + n; }
+
 template <bool MASKED>
 __device__ __forceinline__ void sl_word(uint2 sv, uint2 tv, int k, int r_lo, int r_hi, int &cur, int &dbest)
 {
@@ -816,13 +916,13 @@ __device__ __forceinline__ void sl_word(uint2 sv, uint2 tv, int k, int r_lo, int
     }
 }
 
+template <int FL>
 __device__ void sl_scan(const uint2 *__restrict__ S, const uint32_t *__restrict__ Tlo, const uint32_t *__restrict__ Thi,
-                        int n, int *next_chunk, int lane,
-                        int &best, int &bestd)
+                        const SlGeo &geo, int *next_chunk, int lane, int &best, int &bestd)
 {
-    const int dmax = n - 6;
-    if (dmax < 0) return;
-    const int ndiag = 2 * dmax + 1;
+    const int n = geo.n;
+    if (geo.dhi < geo.dlo) return;
+    const int ndiag = geo.dhi - geo.dlo + 1;
     const int nchunks = (ndiag + 31) >> 5;
     const int c0 = nchunks >> 1;
     for (;;) {
@@ -833,10 +933,10 @@ __device__ void sl_scan(const uint2 *__restrict__ S, const uint32_t *__restrict_
         t = __shfl_sync(0xffffffffu, t, 0);
         if (t >= nchunks) break;
         const int ch = (t & 1) ? c0 - 1 - (t >> 1) : c0 + (t >> 1);
-        const int delta = -dmax + 32 * ch + lane;
-        const bool valid = delta <= dmax;
-        int r_lo = valid ? max(0, -delta) : 1;
-        int r_hi = valid ? ((n - 6 - delta) >> 1) : 0;
+        const int delta = geo.dlo + 32 * ch + lane;
+        const bool valid = delta <= geo.dhi;
+        int r_lo = 1, r_hi = 0;
+        if (valid) sl_diag_rows<FL>(n, delta, r_lo, r_hi);
         const int klo = r_lo >> 5, khi = r_hi >> 5;
         const int kmin = warp_min_i(valid ? klo : 0x7fffffff);
         const int kmax = warp_max_i(valid ? khi : -1);
@@ -863,7 +963,7 @@ __device__ void sl_scan(const uint2 *__restrict__ S, const uint32_t *__restrict_
         for (; k <= kmax; k++) sl_word<true>(S[k], tw(k), k, r_lo, r_hi, cur, dbest);
         dbest = max(dbest, cur);
         if (valid) {
-            int d = n - 1 - delta;
+            int d = sl_key<FL>(n, delta);
             if (dbest > best) {
                 best = dbest;
                 bestd = d;
@@ -934,18 +1034,20 @@ __host__ __device__ __forceinline__ void sl_group_segments(int n, int d0, int &s
 // diagonal j of the mask, the rows where its run reached 8 inside segment s are
 // found again from 64 rows of match bits (same cells as the band scan), and
 // each run is followed to its end and clipped to the diagonal's counted range.
-__device__ void sl_band_entry(uint32_t mask, int d0, int s, int n, const uint2 *__restrict__ S,
+template <int FL>
+__device__ void sl_band_entry(uint32_t mask, int d0, int s, const SlGeo &geo, const uint2 *__restrict__ S,
                               const uint32_t *__restrict__ Tlo, const uint32_t *__restrict__ Thi, int &best, int &bestd)
 {
-    const int dmax = n - 6;
+    const int n = geo.n;
     const int R0 = 32 * (s - 1);
     const uint2 SA = s >= 1 ? S[s - 1] : make_uint2(0u, 0u), SB = S[s];
     while (mask) {
         const int j = __ffs(mask) - 1;
         mask &= mask - 1;
         const int delta = d0 + j;
-        if (delta < -dmax || delta > dmax) continue;
-        const int r_hi = (n - 6 - delta) >> 1;
+        if (delta < geo.dlo || delta > geo.dhi) continue;
+        int r_lo_d, r_hi;
+        sl_diag_rows<FL>(n, delta, r_lo_d, r_hi);
         // match bits of rows R0 .. R0+63 on this diagonal, zero where the row or
         // its T index falls outside [0, n)
         const int i0 = R0 + delta, w0 = (i0 >> 5) + kSlGuardRows, sh = i0 & 31;
@@ -994,7 +1096,7 @@ __device__ void sl_band_entry(uint32_t mask, int d0, int s, int n, const uint2 *
                 break;
             }
             const int L = min(e, r_hi) - a + 1;
-            const int d = n - 1 - delta;
+            const int d = sl_key<FL>(n, delta);
             if (L > best || (L == best && d < bestd)) {
                 best = L;
                 bestd = d;
@@ -1022,13 +1124,26 @@ __device__ __forceinline__ uint32_t word_of(const uint4 &w, int i)
     return i == 0 ? w.x : i == 1 ? w.y : i == 2 ? w.z : w.w;
 }
 
+// segments of the rows a group of bands starting at shift d0 covers
+template <int FL> __device__ __forceinline__ void sl_group_rows(int n, int d0, int &s_lo, int &s_hi)
+{
+    if (FL == 0) {
+        sl_group_segments(n, d0, s_lo, s_hi);
+    } else {
+        s_lo = max(0, -(d0 + 32 * kBandGroup - 1)) >> 5;
+        s_hi = min(n - 1, n - 1 - d0) >> 5;
+    }
+}
+
+template <int FL>
 __device__ void sl_band_scan(const uint4 *__restrict__ E4, const int *__restrict__ poffT,
-                             const int *__restrict__ gstart, int ng, const uint2 *__restrict__ S,
-                             const uint32_t *__restrict__ Tlo, const uint32_t *__restrict__ Thi, int n,
+                             const int *__restrict__ gstart, const SlGeo &geo, const uint2 *__restrict__ S,
+                             const uint32_t *__restrict__ Tlo, const uint32_t *__restrict__ Thi,
                              int2 *__restrict__ queue, int *next_chunk, int lane, int &best, int &bestd)
 {
+    const int ng = geo.ng, n = geo.n;
     if (ng <= 0) return;
-    const int D0 = sl_band_base(n);
+    const int D0 = geo.D0;
     const int nitems = gstart[ng];
     const int nchunks = (nitems + 31) >> 5;
     const unsigned lt = (1u << lane) - 1u;
@@ -1053,7 +1168,7 @@ __device__ void sl_band_scan(const uint4 *__restrict__ E4, const int *__restrict
             grp = lo;
             const int d0 = D0 + 32 * kBandGroup * grp;
             int s_lo, s_hi;
-            sl_group_segments(n, d0, s_lo, s_hi);
+            sl_group_rows<FL>(n, d0, s_lo, s_hi);
             s = s_lo + (item - gstart[grp]);
             // E4 entry x holds T words x-kEqGuard .. x+3-kEqGuard; row 32u + t reads entry
             // u + d0/32 + kEqGuard of the row's plane, words g, g+1 for band g, at bit offset t;
@@ -1101,6 +1216,15 @@ __device__ void sl_band_scan(const uint4 *__restrict__ E4, const int *__restrict
                 }
             }
         }
+        if (FL == 1) {
+            // LRCS: drop the diagonals below the first one scanned (delta <= 0 of a self pair)
+            const int d0 = D0 + 32 * kBandGroup * grp;
+#pragma unroll
+            for (int g = 0; g < kBandGroup; g++) {
+                const int below = geo.dlo - (d0 + 32 * g);
+                if (below > 0) pend[g] &= below >= 32 ? 0u : (0xffffffffu << below);
+            }
+        }
         // queue the (band, segment) pairs with rising edges; measure 32 at a time
 #pragma unroll
         for (int g = 0; g < kBandGroup; g++) {
@@ -1111,7 +1235,8 @@ __device__ void sl_band_scan(const uint4 *__restrict__ E4, const int *__restrict
                 __syncwarp();
                 if (qn >= 32) {
                     const int2 q = queue[lane];
-                    sl_band_entry((uint32_t)q.x, D0 + 32 * (q.y >> 16), q.y & 0xffff, n, S, Tlo, Thi, best, bestd);
+                    sl_band_entry<FL>((uint32_t)q.x, D0 + 32 * (q.y >> 16), q.y & 0xffff, geo, S, Tlo, Thi, best,
+                                      bestd);
                     __syncwarp();
                     if (lane < qn - 32) queue[lane] = queue[32 + lane];
                     qn -= 32;
@@ -1122,7 +1247,7 @@ __device__ void sl_band_scan(const uint4 *__restrict__ E4, const int *__restrict
     }
     if (lane < qn) {
         const int2 q = queue[lane];
-        sl_band_entry((uint32_t)q.x, D0 + 32 * (q.y >> 16), q.y & 0xffff, n, S, Tlo, Thi, best, bestd);
+        sl_band_entry<FL>((uint32_t)q.x, D0 + 32 * (q.y >> 16), q.y & 0xffff, geo, S, Tlo, Thi, best, bestd);
     }
     __syncwarp();
 }
@@ -1162,7 +1287,10 @@ __device__ __forceinline__ int plane_nt(const uint2 *P, int x)
     return (int)(((w.x >> b) & 1u) | (((w.y >> b) & 1u) << 1));
 }
 
-template <int NT>
+template <int FL> __device__ void lrcs_combine(const Shape &s, PopBuf &buf, size_t gsol, const int2 *res,
+                                               unsigned char *tab, int tid, int lane, int warp, int *shared_res);
+
+template <int NT, int FL>
 __global__ void __launch_bounds__(NT) k_sl(Shape s, PopBuf buf, int base, int2 *part, int32_t *counter,
                                                  int32_t *status, unsigned long long *scanned)
 {
@@ -1177,13 +1305,17 @@ __global__ void __launch_bounds__(NT) k_sl(Shape s, PopBuf buf, int base, int2 *
     tab = reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(tab) + 15) & ~uintptr_t(15));
 
     const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarps = nth >> 5;
-    const int sol = blockIdx.x / s.m, c = blockIdx.x - sol * s.m;
+    const int nres = FL == 0 ? s.m : s.nres;
+    const int sol = blockIdx.x / nres, c = blockIdx.x - sol * nres;
     const size_t gsol = (size_t)(base + sol);
-    const uint2 *P = buf.planes + (gsol * s.m + c) * s.Wp;
+    // hairpin: CDS c against its reverse complement; LRCS: pair c = (pa, pb)
+    int pa = c, pb = c;
+    if (FL == 1) lrcs_pair_of(s.m, c, pa, pb);
+    const uint2 *P = buf.planes + (gsol * s.m + pa) * s.Wp;
 
-    // this CDS's result: carried over from the parent when the mutation left the CDS
-    // as it was, else found by the scan below
-    int2 *res = buf.cds ? buf.cds + gsol * s.m : part + (size_t)sol * s.m;
+    // this CDS's (pair's) result: carried over from the parent when the mutation left
+    // the CDS (both CDSs) as it was, else found by the scan below
+    int2 *res = buf.cds ? buf.cds + gsol * nres : part + (size_t)sol * nres;
     const bool reuse = buf.cds != nullptr && res[c].x >= 0;
     if (!reuse) {
         // stage S (the CDS planes) with one bulk async copy (TMA engine)
@@ -1234,11 +1366,18 @@ __global__ void __launch_bounds__(NT) k_sl(Shape s, PopBuf buf, int base, int2 *
             for (int w = s.Wp + tid; w < W + 2; w += nth) S[w] = make_uint2(0u, 0u);
         }
         __syncthreads();
-        // reverse complement planes, zero outside [0, W)
+        // T: reverse complement planes (hairpin) or CDS pb's own planes (LRCS), zero outside [0, W)
+        const uint2 *Pb = buf.planes + (gsol * s.m + pb) * s.Wp;
         for (int e = tid; e < W + 2 * G + 1; e += nth) {
             int w = e - G;
             uint32_t lo = 0, hi = 0;
-            if (w >= 0 && w < W) {
+            if (FL == 1) {
+                if (w >= 0 && w < W) {
+                    const uint2 v = pa == pb ? S[w] : Pb[w];
+                    lo = v.x;
+                    hi = v.y;
+                }
+            } else if (w >= 0 && w < W) {
                 int start = n - 32 - 32 * w;  // source bit of T bit 31 ... bit 0 is source n-1-32w
                 int q = start >> 5, sh = start & 31;
                 uint32_t a0 = (q >= 0 && q < W) ? S[q].x : 0u, a1 = (q + 1 >= 0 && q + 1 < W) ? S[q + 1].x : 0u;
@@ -1257,7 +1396,8 @@ __global__ void __launch_bounds__(NT) k_sl(Shape s, PopBuf buf, int base, int2 *
         //                 shared memory); pitch 17 words
         //   gstart[g]     first item of band group g (items: the group's 32-row segments)
         const int PS = sl_plane_stride(W), NSP = W + 2;
-        const int ng = sl_num_groups(n), D0 = sl_band_base(n);
+        const SlGeo geo = sl_geo<FL>(n, pa == pb);
+        const int ng = geo.ng, D0 = geo.D0;
         uint4 *E4 = reinterpret_cast<uint4 *>(tab);
         int *poffT = reinterpret_cast<int *>(E4 + 5 * PS);
         int *gstart = poffT + kSegPitch * NSP;
@@ -1292,8 +1432,8 @@ __global__ void __launch_bounds__(NT) k_sl(Shape s, PopBuf buf, int base, int2 *
                 int x = 0;
                 if (g < ng) {
                     int s_lo, s_hi;
-                    sl_group_segments(n, D0 + 32 * kBandGroup * g, s_lo, s_hi);
-                    x = s_hi - s_lo + 1;
+                    sl_group_rows<FL>(n, D0 + 32 * kBandGroup * g, s_lo, s_hi);
+                    x = max(0, s_hi - s_lo + 1);
                 }
                 for (int o = 1; o < 32; o <<= 1) {
                     const int y = __shfl_up_sync(0xffffffffu, x, o);
@@ -1308,7 +1448,7 @@ __global__ void __launch_bounds__(NT) k_sl(Shape s, PopBuf buf, int base, int2 *
         __syncthreads();
 
         int best = 0, bestd = 0x7fffffff;
-        sl_band_scan(E4, poffT, gstart, ng, S, Tlo, Thi, n, sm.queue[warp], &sm.next_chunk, lane, best, bestd);
+        sl_band_scan<FL>(E4, poffT, gstart, geo, S, Tlo, Thi, sm.queue[warp], &sm.next_chunk, lane, best, bestd);
         // CTA reduction of (best, smallest anti-diagonal)
         for (int o = 16; o > 0; o >>= 1) {
             int ob = __shfl_xor_sync(0xffffffffu, best, o), od = __shfl_xor_sync(0xffffffffu, bestd, o);
@@ -1331,7 +1471,7 @@ __global__ void __launch_bounds__(NT) k_sl(Shape s, PopBuf buf, int base, int2 *
             // no run reaches 8: exact per-word runs
             best = 0;
             bestd = 0x7fffffff;
-            sl_scan(S, Tlo, Thi, n, &sm.next_chunk, lane, best, bestd);
+            sl_scan<FL>(S, Tlo, Thi, geo, &sm.next_chunk, lane, best, bestd);
             for (int o = 16; o > 0; o >>= 1) {
                 int ob = __shfl_xor_sync(0xffffffffu, best, o), od = __shfl_xor_sync(0xffffffffu, bestd, o);
                 pair_reduce(best, bestd, ob, od);
@@ -1354,15 +1494,27 @@ __global__ void __launch_bounds__(NT) k_sl(Shape s, PopBuf buf, int base, int2 *
     if (tid == 0) {
         if (!reuse) {
             res[c] = make_int2(sm.res[0], sm.res[1]);
-            if (scanned) atomicAdd(scanned, 1ull);
+            if (scanned) {
+                // scans, and the counted cells they covered
+                unsigned long long cells;
+                if (FL == 1) cells = pa == pb ? (unsigned long long)n * (n - 1) / 2 : (unsigned long long)n * n;
+                else cells = n > 5 ? (unsigned long long)(n - 5) * (n - 4) / 2 : 0ull;
+                atomicAdd(&scanned[0], 1ull);
+                atomicAdd(&scanned[1], cells);
+            }
         }
         __threadfence();
         int old = atomicAdd(&counter[sol], 1);
-        sm.last = (old == s.m - 1);
+        sm.last = (old == nres - 1);
     }
     __syncthreads();
     if (!sm.last) return;
     __threadfence();
+    if (FL == 1) {
+        if (tid == 0) counter[sol] = 0;
+        lrcs_combine<FL>(s, buf, gsol, res, tab, tid, lane, warp, sm.res);
+        return;
+    }
     // ---- last CTA of this solution: combine CDSs (largest CDS index on ties)
     if (tid == 0) {
         int Lb = -1, cb = 0, db = 0;
@@ -1497,6 +1649,113 @@ __global__ void __launch_bounds__(NT) k_sl(Shape s, PopBuf buf, int base, int2 *
     }
 }
 
+// LRCS combine (last CTA of a solution): the pair with the longest run (the
+// first pair on ties), its diagonal (the smallest delta reaching that length),
+// and on it the first run of that length.  Every run of the pair is at most Lb
+// long, so a run of Lb starts wherever Lb consecutive rows match; one warp takes
+// 32 rows per lane from the two CDSs' planes staged in shared memory, carries run
+// lengths across lanes with a scan, and the lowest lane holding a run of Lb that
+// ends in its word gives the start.
+template <int FL> __device__ void lrcs_combine(const Shape &s, PopBuf &buf, size_t gsol, const int2 *res,
+                                               unsigned char *tab, int tid, int lane, int warp, int *shared_res)
+{
+    if (tid == 0) {
+        int Lb = 0, rb = 0, kb = s.n;
+        for (int r = 0; r < s.nres; r++) {
+            const int2 v = __ldcg(&res[r]);
+            if (v.x > Lb) {
+                Lb = v.x;
+                rb = r;
+                kb = v.y;
+            }
+        }
+        shared_res[0] = Lb;
+        shared_res[1] = rb;
+        shared_res[2] = kb;
+    }
+    __syncthreads();
+    const int Lb = shared_res[0], n = s.n, delta = shared_res[2] - n;
+    int a, b;
+    lrcs_pair_of(s.m, shared_res[1], a, b);
+    const int slot = s.slot[K_SL];
+    float *obj = buf.obj + gsol * s.M;
+    int8_t *objidx = buf.objidx + gsol * 2 * s.M;
+    int32_t *pql = buf.pql + gsol * 3;
+    if (Lb <= 0) {
+        if (tid == 0) {
+            obj[slot] = 0.0f;
+            objidx[2 * slot] = 0;
+            objidx[2 * slot + 1] = 0;
+            pql[0] = pql[1] = pql[2] = 0;
+        }
+        return;
+    }
+    if (warp != 0) return;
+    uint2 *Qa = reinterpret_cast<uint2 *>(tab), *Qb = Qa + s.Wp;
+    const uint2 *Ga = buf.planes + (gsol * s.m + a) * s.Wp, *Gb = buf.planes + (gsol * s.m + b) * s.Wp;
+    for (int w = lane; w < s.Wp; w += 32) {
+        Qa[w] = Ga[w];
+        Qb[w] = Gb[w];
+    }
+    __syncwarp();
+    const int r_lo = max(0, -delta), r_hi = min(n - 1, n - 1 - delta);
+    const int nwords = (r_hi - r_lo + 1 + 31) >> 5;
+    // rows r .. r+31 of the diagonal: s_a[r + j] against s_b[r + delta + j]
+    auto diag_word = [&](int r) -> uint32_t {
+        const int ws = r >> 5, bs = r & 31, i = r + delta, wt = i >> 5, bt = i & 31;
+        const uint32_t alo = fshr(Qa[ws].x, Qa[ws + 1].x, bs), ahi = fshr(Qa[ws].y, Qa[ws + 1].y, bs);
+        const uint32_t blo = fshr(Qb[wt].x, Qb[wt + 1].x, bt), bhi = fshr(Qb[wt].y, Qb[wt + 1].y, bt);
+        return ~((alo ^ blo) | (ahi ^ bhi));
+    };
+    int first = -1;
+    uint32_t carry = 0;  // run length ending at the last row of the previous pass
+    for (int k0 = 0; k0 < nwords && first < 0; k0 += 32) {
+        const int k = k0 + lane, r0 = r_lo + 32 * k;
+        uint32_t X = 0u, nb = 0u;
+        if (k < nwords) {
+            X = diag_word(r0);
+            const int rows = r_hi - r0 + 1;
+            if (rows < 32) X &= (1u << rows) - 1u;
+            if (lane == 31 && r0 + 32 <= r_hi) nb = diag_word(r0 + 32) & 1u;
+        }
+        const uint32_t nb_lane = __shfl_down_sync(0xffffffffu, X & 1u, 1);
+        if (lane < 31) nb = nb_lane;
+        uint32_t A = X == 0xffffffffu, Bv = A ? 32u : (uint32_t)__clz((int)~X);
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t A2 = __shfl_up_sync(0xffffffffu, A, o), B2 = __shfl_up_sync(0xffffffffu, Bv, o);
+            if (lane >= o) {
+                Bv = A * B2 + Bv;
+                A &= A2;
+            }
+        }
+        const uint32_t E = A * carry + Bv;
+        uint32_t cin = __shfl_up_sync(0xffffffffu, E, 1);
+        if (lane == 0) cin = carry;
+        carry = __shfl_sync(0xffffffffu, E, 31);
+        const uint32_t ends = X & ~((X >> 1) | (nb << 31));
+        const uint32_t starts = X & ~((X << 1) | (cin ? 1u : 0u));
+        int cand = -1;
+        uint32_t e_bits = ends;
+        while (e_bits && cand < 0) {
+            const int e = __ffs((int)e_bits) - 1;
+            e_bits &= e_bits - 1;
+            const uint32_t sm_ = starts & ((2u << e) - 1u);
+            const int len = sm_ ? e - (31 - __clz((int)sm_)) + 1 : e + 1 + (int)cin;
+            if (len >= Lb) cand = r0 + e - len + 1;
+        }
+        const unsigned has = __ballot_sync(0xffffffffu, cand >= 0);
+        if (has) first = __shfl_sync(0xffffffffu, cand, __ffs((int)has) - 1);
+    }
+    if (lane == 0) {
+        obj[slot] = __fdiv_rn((float)Lb, (float)n);
+        objidx[2 * slot] = (int8_t)a;
+        objidx[2 * slot + 1] = (int8_t)b;
+        pql[0] = first;
+        pql[1] = first >= 0 ? first + delta : -1;
+        pql[2] = Lb;
+    }
+}
+
 static size_t sl_smem_bytes_nt(const Shape &s, size_t head)
 {
     const int G = kSlGuardRows, W = s.W;
@@ -1504,8 +1763,9 @@ static size_t sl_smem_bytes_nt(const Shape &s, size_t head)
     b += (size_t)(W + 2) * sizeof(uint2);
     b += 2 * (size_t)(W + 2 * G + 1) * sizeof(uint32_t);
     b += 16;  // alignment of the band-scan tables
+    const int ng = s.sl_kind == PE_SL_LRCS ? sl_geo<1>(s.n, false).ng : sl_num_groups(s.n);
     const size_t band = (size_t)5 * sl_plane_stride(W) * sizeof(uint4) + (size_t)kSegPitch * (W + 2) * sizeof(int) +
-                        (size_t)(sl_num_groups(s.n) + 1) * sizeof(int);
+                        (size_t)(ng + 1) * sizeof(int);
     b += band;
     return b;
 }
@@ -1517,9 +1777,15 @@ static cudaError_t launch_sl_nt(const Shape &s, PopBuf buf, int base, int count,
                                 int32_t *status, cudaStream_t st, unsigned long long *scanned)
 {
     const size_t smem = sl_smem_bytes_nt(s, sizeof(SlSmem<NT>));
-    cudaError_t e = raise_smem_limit((const void *)k_sl<NT>, smem);
+    if (s.sl_kind == PE_SL_LRCS) {
+        cudaError_t e = raise_smem_limit((const void *)k_sl<NT, 1>, smem);
+        if (e != cudaSuccess) return e;
+        k_sl<NT, 1><<<count * s.nres, NT, smem, st>>>(s, buf, base, part, counter, status, scanned);
+        return cudaGetLastError();
+    }
+    cudaError_t e = raise_smem_limit((const void *)k_sl<NT, 0>, smem);
     if (e != cudaSuccess) return e;
-    k_sl<NT><<<count * s.m, NT, smem, st>>>(s, buf, base, part, counter, status, scanned);
+    k_sl<NT, 0><<<count * s.m, NT, smem, st>>>(s, buf, base, part, counter, status, scanned);
     return cudaGetLastError();
 }
 

@@ -38,6 +38,8 @@ struct Shape {
     uint64_t seed;
     int slot[6];  // slot of each Kind or -1
     int sl_threads;  // stem-scan CTA size (64, 128 or 256; 0 = 128), picked per instance by timing
+    int sl_kind;     // string objective: PE_SL_HAIRPIN or PE_SL_LRCS
+    int nres;        // string-objective results per solution: m CDSs (hairpin) or m(m+1)/2 CDS pairs (LRCS)
 };
 
 // Device-resident tables derived from pe_codon_table.
@@ -63,9 +65,11 @@ struct PopBuf {
     float *obj;        // [2N][M]
     int8_t *objidx;    // [2N][2M]
     int32_t *pql;      // [2N][3]
-    // [2N][m] hairpin scan of each CDS: (longest stem, its anti-diagonal); x = -1 marks a
-    // CDS to scan.  A child's unchanged CDSs carry their parent's result, so only the
-    // CDSs its mutation touched are scanned.  nullptr: every CDS is scanned.
+    // [2N][nres] string-objective scan of each CDS (hairpin: (longest stem, its
+    // anti-diagonal)) or CDS pair (LRCS: (longest common run, delta + n)); x = -1 marks
+    // one to scan.  A child's unchanged CDSs (pairs of unchanged CDSs) carry their
+    // parent's result, so only what its mutation touched is scanned.  nullptr: every
+    // one is scanned.
     int2 *cds;
 };
 
