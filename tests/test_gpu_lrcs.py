@@ -133,7 +133,7 @@ def test_scan_cells_count_the_scans(pe, gpu):
         eng.init()
         eng.step(3)
         assert eng.scan_cells() == eng.scan_count() * (n - 5) * (n - 4) // 2
-    with pe.Engine(aa, tabc, 3, 32, 0.05, objectives=1, ref_p=3, seed=2, sl_kind=pe.SL_LRCS) as eng:
+    with pe.Engine(aa, tabc, 3, 32, 0.05, objectives=1, ref_p=3, seed=2, sl_kind=pe.SL_LRCS, sl_threads=128) as eng:
         eng.init()
         # the initial population scans every pair: 3 self pairs and 3 cross pairs per solution
         assert eng.scan_count() == 32 * 6
