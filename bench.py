@@ -69,20 +69,24 @@ def set_workload(shape: str | None, six: bool, lrcs: bool = False):
                 f"p={p} ({R} points), design job = {G_JOB} generations")
 METRIC = "generations/s"
 L2_FLUSH_BYTES = 256 << 20
-# k_sl at this workload, from ncu captures of one launch (the committed k_sl profile summary):
-# ALU-pipe warp instructions (69 % of its peak of 2 per SM per clock, of active cycles),
-# shared-memory data-pipe wavefronts (73 % of 1 per SM per clock), thread instructions and
-# DRAM bytes per launch
-SL_SMEM_WAVEFRONTS_PER_LAUNCH = 27776979
-SL_ALU_WARP_INST_PER_LAUNCH = 46420822
-SL_THREAD_INST_PER_LAUNCH = 2483621141
-SL_DRAM_BYTES_PER_LAUNCH = 2475520
-SL_SMEM_PCT_NCU, SL_ALU_PIPE_PCT_NCU = 73.22, 69.25
+# The string-objective kernel (k_sl) per flavour, from one ncu capture of one launch each
+# (the committed k_sl profile summaries give the commands and these same numbers): ALU-pipe
+# warp instructions, shared-memory data-pipe wavefronts, thread instructions and DRAM bytes
+# of the launch, the counted cells it covered, and the percentages ncu reported.  The
+# roofline scales the counts by the cells a timed generation scanned.  `source` is the
+# sha256 prefix of the kernel's source section (pe_eval.cu from the k_sl banner on) at the
+# capture; a host test fails when the source changes without a new capture.
+SL_NCU = {
+    "hairpin": {"workload": "L=1000 m=8 N=1024, generation 1 (2311 CDSs scanned)",
+                "cells": 10389102811, "smem_wavefronts": 27777383, "alu_warp_inst": 46193071,
+                "thread_inst": 2467353682, "dram_bytes": 2475264, "smem_pct": 73.60, "alu_pct": 68.93,
+                "source": "e0b78e963863413d"},
+    "lrcs": {"workload": "L=3000 m=4 N=4096, generation 1 (18320 CDS pairs scanned)",
+             "cells": 1250515745682, "smem_wavefronts": 2679463383, "alu_warp_inst": 5438849899,
+             "thread_inst": 252175890553, "dram_bytes": 34812416, "smem_pct": 72.53, "alu_pct": 74.60,
+             "source": "e0b78e963863413d"},
+}
 SM_COUNT, SMEM_WAVEFRONTS_PER_SM_CLK, ALU_WARP_INST_PER_SM_CLK = 148, 1, 2
-# CDSs the captured launch scanned (of 1024 x 8: the others kept their parents' results)
-# and its counted cells (4495501 per CDS of 3003 nucleotides)
-SL_CDS_PER_LAUNCH = 2311
-SL_CELLS_PER_LAUNCH = SL_CDS_PER_LAUNCH * 4495501
 # kernels one generation launches (one CUDA graph replay): k_variation, k_sl, k_dominance,
 # k_select, k_assoc, k_niche
 KERNELS_PER_GENERATION = 6
@@ -103,18 +107,19 @@ def hairpin_cells_per_cds(n: int) -> int:
     return k * (k + 1) // 2 if k > 0 else 0
 
 
-def roofline(cells: int, sl_seconds: float, clocks: dict) -> dict:
-    """Roofline of the stem scan (integer bit work on shared-memory tables) on its two
-    busiest units: the ALU pipe (achieved = ALU warp instructions per launch, ncu, / the
-    launch time measured here; peak = 2 per SM per clock x 148 SMs x the SM clock sampled
-    during the timed region) and the shared-memory data pipe (wavefronts per launch
-    against 1 per SM per clock).  The headline figures are those of the unit with the
-    larger fraction; the other is reported beside them."""
-    scale = cells / SL_CELLS_PER_LAUNCH   # the ncu counts are for one launch of the default shape
+def roofline(cells: float, sl_seconds: float, clocks: dict, kind: str = "hairpin") -> dict:
+    """Roofline of the string-objective scan (integer bit work on shared-memory tables) on
+    its two busiest units: the ALU pipe (achieved = ALU warp instructions per launch, ncu,
+    scaled to the cells scanned, / the launch time measured here; peak = 2 per SM per clock
+    x 148 SMs x the SM clock sampled during the timed region) and the shared-memory data
+    pipe (wavefronts per launch against 1 per SM per clock).  The headline figures are those
+    of the unit with the larger fraction; the other is reported beside them."""
+    c = SL_NCU[kind]
+    scale = cells / c["cells"]
     mhz = clocks.get("sm_mhz") or 1965.0
-    smem = SL_SMEM_WAVEFRONTS_PER_LAUNCH * scale / sl_seconds / 1e9
+    smem = c["smem_wavefronts"] * scale / sl_seconds / 1e9
     smem_peak = SM_COUNT * SMEM_WAVEFRONTS_PER_SM_CLK * mhz * 1e6 / 1e9
-    alu = SL_ALU_WARP_INST_PER_LAUNCH * scale / sl_seconds / 1e9
+    alu = c["alu_warp_inst"] * scale / sl_seconds / 1e9
     alu_peak = SM_COUNT * ALU_WARP_INST_PER_SM_CLK * mhz * 1e6 / 1e9
     units = {
         "alu": {"achieved": alu, "peak": alu_peak, "frac": alu / alu_peak, "unit": "G ALU warp-inst/s",
@@ -126,16 +131,17 @@ def roofline(cells: int, sl_seconds: float, clocks: dict) -> dict:
     bound = max(units, key=lambda k: units[k]["frac"])
     other = "smem" if bound == "alu" else "alu"
     head = units[bound]
-    return {"bound": bound, "kernel": "k_sl (hairpin-stem scan)", "unit": head["unit"], "achieved": head["achieved"],
-            "peak": head["peak"], "frac": head["frac"], "traffic": SL_DRAM_BYTES_PER_LAUNCH * scale,
+    name = "k_sl (hairpin-stem scan)" if kind == "hairpin" else "k_sl (longest repeated/common substring scan)"
+    return {"bound": bound, "kernel": name, "unit": head["unit"], "achieved": head["achieved"],
+            "peak": head["peak"], "frac": head["frac"], "traffic": c["dram_bytes"] * scale,
             "peak_source": head["peak_source"] + "; MEASURED_PEAKS.json has no integer or shared-memory peak",
             other: {k: v for k, v in units[other].items() if k != "peak_source"},
-            "algorithmic_bytes_per_launch": SL_DRAM_BYTES_PER_LAUNCH * scale,
+            "algorithmic_bytes_per_launch": c["dram_bytes"] * scale,
             "cells_per_launch": cells, "cells_per_s": cells / sl_seconds,
-            "counted_cells": "cells of the CDSs scanned (unchanged CDSs keep their parents' results)",
-            "lane_ops_per_cell": SL_THREAD_INST_PER_LAUNCH / SL_CELLS_PER_LAUNCH,
-            "ncu_pct_of_peak": {"smem_wavefronts": SL_SMEM_PCT_NCU, "alu_pipe": SL_ALU_PIPE_PCT_NCU},
-            "instruction_count": "ncu, L=1000 m=8 N=1024" + ("" if cells == SL_CELLS_PER_LAUNCH else "; scaled by cells")}
+            "counted_cells": "cells of the scans run (unchanged CDSs keep their parents' results)",
+            "lane_ops_per_cell": c["thread_inst"] / c["cells"],
+            "ncu_pct_of_peak": {"smem_wavefronts": c["smem_pct"], "alu_pipe": c["alu_pct"]},
+            "instruction_count": f"ncu, {c['workload']}; scaled by cells"}
 
 
 class ClockSampler:
@@ -418,7 +424,7 @@ def run_ours(args, world, rank, local):
             "designs_per_s": value / G_JOB,
             "stage_ms": {"variation_eval": stage_ms[0], "hairpin_scan": stage_ms[1], "selection": stage_ms[2]},
             "stage_ms_windows": windows,
-            "roofline": roofline(cells, sl_s, clocks),
+            "roofline": roofline(cells, sl_s, clocks, "lrcs" if SL_KIND else "hairpin"),
             "clocks": clocks,
             "e2e": {"value": world * G_E2E / e2e_s, "unit": "generations/s", "h2d_bytes_per_step": world * h2d / G_E2E,
                     "d2h_bytes_per_step": world * d2h,

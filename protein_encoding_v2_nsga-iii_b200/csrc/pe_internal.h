@@ -74,7 +74,7 @@ struct PopBuf {
 };
 
 struct SelectScratch {
-    uint32_t *dom;       // [2N][2N/32] bit j of row i: j dominates i
+    uint32_t *dom;       // [2N][2N/32] bit j of row i: i dominates j
     int32_t *np;         // [2N]
     int32_t *front;      // [2N]
     int32_t *sorted;     // [2N] fronts 0..last

@@ -62,17 +62,18 @@ __global__ void __launch_bounds__(256) k_dominance(Shape s, const float *__restr
 #pragma unroll 2
     for (int w = warp; w < words; w += 8) {
         int j = 32 * w + lane;
-        bool bit = false;
+        bool by = false, over = false;  // j dominates i; i dominates j
         if (j < N2 && j != i) {
             float oj[kMaxObj];
 #pragma unroll
             for (int k = 0; k < (MM > 0 ? MM : kMaxObj); k++)
                 if (k < M) oj[k] = __ldg(&obj[(size_t)j * M + k]);
-            bit = dominates(oj, oi, M);
+            by = dominates(oj, oi, M);
+            over = dominates(oi, oj, M);
         }
-        uint32_t word = __ballot_sync(0xffffffffu, bit);
+        const uint32_t word = __ballot_sync(0xffffffffu, over);
         if (lane == 0) dom[(size_t)i * words + w] = word;
-        cnt += __popc(word);
+        cnt += __popc(__ballot_sync(0xffffffffu, by));
     }
     if (lane == 0) wsum[warp] = cnt;
     __syncthreads();
@@ -326,6 +327,35 @@ __device__ int hyperplane_nadir(int M, const float *ext, const float *ideal, flo
     return __any_sync(full, exc) ? 1 : 0;
 }
 
+// exclusive block scan of an int over the CTA; returns the prefix and leaves
+// the total in *total (all threads)
+__device__ __forceinline__ int block_scan_value(int v, SelSmem &sm, int *total)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+    int inc = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+    }
+    if (lane == 31) sm.warp_tot[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        const int w = lane < nwarps ? sm.warp_tot[lane] : 0;
+        int x = w;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane < nwarps) sm.warp_tot[lane] = x - w;
+        if (lane == 31) sm.warp_tot[32] = x;
+    }
+    __syncthreads();
+    const int r = sm.warp_tot[warp] + inc - v;
+    *total = sm.warp_tot[32];
+    __syncthreads();
+    return r;
+}
+
 __global__ void __launch_bounds__(kSelThreads, 1) k_select(Shape s, const float *__restrict__ obj, float *ext,
                                                         const float *__restrict__ refpts, SelectScratch sc,
                                                         int32_t *surv, uint32_t *d_gen, int bump_gen)
@@ -334,15 +364,25 @@ __global__ void __launch_bounds__(kSelThreads, 1) k_select(Shape s, const float 
     SelSmem &sm = *reinterpret_cast<SelSmem *>(smem_raw);
     const int N = s.N, N2 = 2 * N, M = s.M, R = s.R;
     const int words = (N2 + 31) >> 5;
-    uint32_t *fmask = reinterpret_cast<uint32_t *>(smem_raw + ((sizeof(SelSmem) + 15) & ~size_t(15)));
-    ExtSmem &xs = *reinterpret_cast<ExtSmem *>(fmask + (((N2 + 31) / 32 + 3) & ~3));
+    // ready[w]: solutions whose last dominator was just assigned (the next front); npl: the
+    // dominators of each solution not yet assigned to a front
+    uint32_t *ready = reinterpret_cast<uint32_t *>(smem_raw + ((sizeof(SelSmem) + 15) & ~size_t(15)));
+    int *npl = reinterpret_cast<int *>(ready + ((words + 3) & ~3));
+    ExtSmem &xs = *reinterpret_cast<ExtSmem *>(npl + ((N2 + 3) & ~3));
     const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5;
     (void)d_gen;
     (void)bump_gen;
 
     // ---------------- front 0 (np == 0), ascending index
-    for (int i = tid; i < N2; i += nth) sc.front[i] = -1;
-    if (tid == 0) sm.rc = 0;
+    for (int i = tid; i < N2; i += nth) {
+        sc.front[i] = -1;
+        npl[i] = sc.np[i];
+    }
+    for (int w = tid; w < words; w += nth) ready[w] = 0u;
+    if (tid == 0) {
+        sm.rc = 0;
+        sm.count = 0;
+    }
     __syncthreads();
     for (int base = 0; base < N2; base += nth) {
         int i = base + tid;
@@ -365,50 +405,58 @@ __global__ void __launch_bounds__(kSelThreads, 1) k_select(Shape s, const float 
         sm.nfront = 1;
     }
     __syncthreads();
-    // ---------------- later fronts (only while fewer than N are assigned)
+    // ---------------- later fronts (only while fewer than N are assigned).  The rows of
+    // the last front's members (whom each dominates) decrement their dominatees' counts;
+    // a solution whose count reaches 0 joins the next front.  Every row is read once over
+    // all fronts.  The next front is listed in ascending index from the ready mask.
     if (f0 < N) {
         for (int it = 0; it < N2 - 1; it++) {
-            for (int w = tid; w < words; w += nth) fmask[w] = 0u;
-            __syncthreads();
-            for (int u = sm.fstart + tid; u < sm.fstart + sm.fsize; u += nth) {
-                int j = sc.sorted[u];
-                atomicOr(&fmask[j >> 5], 1u << (j & 31));
+            const int fs = sm.fstart, fz = sm.fsize, cf = sm.nfront;
+            for (int u = tid; u < fz * words; u += nth) {
+                const int q = u / words, w = u - q * words;
+                uint32_t x = sc.dom[(size_t)sc.sorted[fs + q] * words + w];
+                while (x) {
+                    const int b = __ffs(x) - 1;
+                    x &= x - 1;
+                    if (atomicSub(&npl[32 * w + b], 1) == 1) atomicOr(&ready[w], 1u << b);
+                }
             }
             __syncthreads();
             const int rc0 = sm.rc;
-            const int cf = sm.nfront;
-            for (int base = 0; base < N2; base += nth) {
-                int i = base + tid;
-                int flag = 0;
-                if (i < N2 && sc.front[i] < 0) {
-                    const uint32_t *row = sc.dom + (size_t)i * words;
-                    int dec = 0;
-                    for (int w = 0; w < words; w++) {
-                        uint32_t f = fmask[w];
-                        if (f) dec += __popc(row[w] & f);
-                    }
-                    int v = sc.np[i] - dec;
-                    sc.np[i] = v;
-                    flag = (v == 0);
-                }
+            for (int base = 0; base < words; base += nth) {
+                const int w = base + tid;
+                const uint32_t x = w < words ? ready[w] : 0u;
                 int tot;
-                int pos = block_scan_flag(flag, sm, &tot);
-                if (flag) {
-                    sc.front[i] = cf;
-                    sc.sorted[sm.rc + pos] = i;
+                int pos = rc0 + sm.count + block_scan_value(__popc(x), sm, &tot);
+                if (w < words) {
+                    ready[w] = 0u;
+                    uint32_t y = x;
+                    while (y) {
+                        const int b = __ffs(y) - 1;
+                        y &= y - 1;
+                        const int i = 32 * w + b;
+                        sc.front[i] = cf;
+                        sc.sorted[pos++] = i;
+                    }
                 }
                 __syncthreads();
-                if (tid == 0) sm.rc += tot;
+                if (tid == 0) sm.count += tot;
                 __syncthreads();
             }
             if (tid == 0) {
+                const int tot = sm.count;
+                sm.count = 0;
                 sm.fstart = rc0;
-                sm.fsize = sm.rc - rc0;
+                sm.fsize = tot;
+                sm.rc = rc0 + tot;
                 sm.nfront = cf + 1;
                 if (sm.rc >= N) sm.cut = (sm.rc == N);
+                // no solution became ready: the rest is never assigned (a cycle of the
+                // epsilon-dominance relation); the remaining rounds would add empty fronts
+                if (tot == 0) sm.nfront = N2;
             }
             __syncthreads();
-            if (sm.rc >= N) break;
+            if (sm.rc >= N || sm.fsize == 0) break;
         }
     }
     const int rc = sm.rc;
@@ -679,35 +727,6 @@ __global__ void __launch_bounds__(256) k_assoc(Shape s, const float *__restrict_
     }
 }
 
-// exclusive block scan of an int over the CTA; returns the prefix and leaves
-// the total in *total (all threads)
-__device__ __forceinline__ int block_scan_value(int v, SelSmem &sm, int *total)
-{
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
-    int inc = v;
-    for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, inc, o);
-        if (lane >= o) inc += y;
-    }
-    if (lane == 31) sm.warp_tot[warp] = inc;
-    __syncthreads();
-    if (warp == 0) {
-        const int w = lane < nwarps ? sm.warp_tot[lane] : 0;
-        int x = w;
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
-        }
-        if (lane < nwarps) sm.warp_tot[lane] = x - w;
-        if (lane == 31) sm.warp_tot[32] = x;
-    }
-    __syncthreads();
-    const int r = sm.warp_tot[warp] + inc - v;
-    *total = sm.warp_tot[32];
-    __syncthreads();
-    return r;
-}
-
 // referenceBasedSorting phase 2 (:1182-1279): candidate lists and niche levels.
 //
 // The reference visits levels 0, 1, 2, ... and, within a level, the reference
@@ -935,7 +954,8 @@ size_t niche_smem_bytes(const Shape &s)
 size_t select_smem_bytes(const Shape &s)
 {
     const int N2 = 2 * s.N, words = (N2 + 31) >> 5;
-    return ((sizeof(SelSmem) + 15) & ~size_t(15)) + (size_t)((words + 3) & ~3) * 4 + sizeof(ExtSmem);
+    return ((sizeof(SelSmem) + 15) & ~size_t(15)) + (size_t)((words + 3) & ~3) * 4 + (size_t)((N2 + 3) & ~3) * 4 +
+           sizeof(ExtSmem);
 }
 
 cudaError_t launch_select(const Shape &s, const float *obj, float *ext, const float *refpts, SelectScratch sc,
