@@ -78,13 +78,13 @@ L2_FLUSH_BYTES = 256 << 20
 # capture; a host test fails when the source changes without a new capture.
 SL_NCU = {
     "hairpin": {"workload": "L=1000 m=8 N=1024, generation 1 (2311 CDSs scanned)",
-                "cells": 10389102811, "smem_wavefronts": 27777383, "alu_warp_inst": 46193071,
-                "thread_inst": 2467353682, "dram_bytes": 2475264, "smem_pct": 73.60, "alu_pct": 68.93,
-                "source": "e0b78e963863413d"},
+                "cells": 10389102811, "smem_wavefronts": 27778286, "alu_warp_inst": 46226541,
+                "thread_inst": 2470901893, "dram_bytes": 2475520, "smem_pct": 73.14, "alu_pct": 68.95,
+                "source": "fb06a34e80d29fe3"},
     "lrcs": {"workload": "L=3000 m=4 N=4096, generation 1 (18320 CDS pairs scanned)",
-             "cells": 1250515745682, "smem_wavefronts": 2679463383, "alu_warp_inst": 5438849899,
-             "thread_inst": 252175890553, "dram_bytes": 34812416, "smem_pct": 72.53, "alu_pct": 74.60,
-             "source": "e0b78e963863413d"},
+             "cells": 1250515745682, "smem_wavefronts": 2679467847, "alu_warp_inst": 5439112299,
+             "thread_inst": 252208658699, "dram_bytes": 34456064, "smem_pct": 72.64, "alu_pct": 74.60,
+             "source": "fb06a34e80d29fe3"},
 }
 SM_COUNT, SMEM_WAVEFRONTS_PER_SM_CLK, ALU_WARP_INST_PER_SM_CLK = 148, 1, 2
 # kernels one generation launches (one CUDA graph replay): k_variation, k_sl, k_dominance,
@@ -355,10 +355,8 @@ def run_ours(args, world, rank, local):
         torch.distributed.barrier()
     step_ms = [a.elapsed_time(b) for a, b in ev]
     total_s = sum(step_ms) / 1000.0
-    t = torch.tensor([total_s], dtype=torch.float64, device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    max_s = float(t.item())
+    replicas = load_pkg_module("replicas")
+    max_s = replicas.max_over_ranks(total_s, dev)
     value = world * args.steps / max_s
     stage_ms = stage.mean(axis=0)
     # stage times per window of 5 timed generations (early generations are front-heavy)
@@ -389,11 +387,7 @@ def run_ours(args, world, rank, local):
         final = e2.population()
         e2.close()
         job_s.append(time.perf_counter() - t0)
-    e2e_s = statistics.median(job_s)
-    te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
-    e2e_s = float(te.item())
+    e2e_s = replicas.max_over_ranks(statistics.median(job_s), dev)
     h2d = aa.nbytes + 4 * (64 * 4 + 61 * 61 + 12)
     d2h = obj_host.nbytes + sum(a.nbytes for a in final) / G_E2E
 
@@ -464,14 +458,26 @@ def batched_jobs(master_seed: int, count: int = 64):
     return jobs
 
 
-def run_batched(args):
-    """Config 4: 64 design jobs (N=512, 300 generations) as one batch vs one at a time."""
+def run_batched(args, world: int = 1, rank: int = 0, local: int = 0):
+    """Config 4: 64 design jobs (N=512, 300 generations) as one batch.  On N GPUs the
+    jobs are sharded across the ranks by estimated stem-scan cells (longest first onto
+    the least-loaded rank; no data-path collective), each rank runs its shard as one
+    batch, the time is the slowest rank's and every job's result is gathered on rank 0.
+    At N=1 the same jobs also run one at a time (the plain per-protein form)."""
     import torch
     pe = load_pkg()
-    torch.cuda.set_device(0)
+    rep = load_pkg_module("replicas")
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
     G = args.generations or 300
     jobs = batched_jobs(SEED)
     N, pm = 512, 0.02
+    costs = [N * m * hairpin_cells_per_cds(3 * (L + 1)) for L, m, _ in jobs]
+    mine = rep.shard_jobs(costs, world)[rank]
 
     def make(j):
         L, m, seed = jobs[j]
@@ -480,40 +486,59 @@ def run_batched(args):
         e.init()
         return e
 
-    cells = sum(N * m * hairpin_cells_per_cds(3 * (L + 1)) for L, m, _ in jobs) * G
-    # one at a time (the plain per-protein form)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for j in range(len(jobs)):
-        e = make(j)
-        e.step(G)
-        e.synchronize()
-        e.close()
-    t_plain = time.perf_counter() - t0
-    # all together (same accounting: create + init + generations)
-    with ClockSampler(0) as clk:
+    cells = sum(costs) * G
+    t_plain = None
+    if world == 1:
+        # one at a time (the plain per-protein form)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        engines = [make(j) for j in range(len(jobs))]
-        with pe.Batch(engines) as b:
-            b.step(G)
-            b.synchronize()
-        t_batch = time.perf_counter() - t0
-    scanned_cells = sum(e.scan_count() * hairpin_cells_per_cds(3 * (L + 1)) for e, (L, _, _) in zip(engines, jobs))
-    for e in engines:
+        for j in range(len(jobs)):
+            e = make(j)
+            e.step(G)
+            e.synchronize()
+            e.close()
+        t_plain = time.perf_counter() - t0
+    # this rank's shard together (create + init + generations)
+    if world > 1:
+        torch.distributed.barrier()
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        engines = [make(j) for j in mine]
+        if engines:
+            with pe.Batch(engines) as b:
+                b.step(G)
+                b.synchronize()
+        t_rank = time.perf_counter() - t0
+    results = {}
+    for j, e in zip(mine, engines):
+        surv = e.survivor_objectives()
+        results[j] = {"rank": rank, "scan_cells": e.scan_cells(),
+                      "hv": float(load_pkg_module("server").front_hypervolume(pe, surv, pe.OBJ_BASE4))}
         e.close()
-    line = {"metric": "designs/s", "value": len(jobs) / t_batch, "unit": "designs/s", "n_gpus": 1,
-            "steps": G, "warmup": 0, "ms_per_step": 1000.0 * t_batch / G, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": {"workload": f"batched: {len(jobs)} proteins, L log-uniform [100, 3000], m in {{2,4,8}}, "
-                                   f"N={N}, Pm={pm}, 4 objectives, {G} generations, one graph launch per 2 "
-                                   f"generations for all instances",
-                       "plain_designs_per_s": len(jobs) / t_plain, "batched_over_plain": t_plain / t_batch,
-                       "stem_cells_per_s": scanned_cells / t_batch,
-                       "stem_cells_scanned_of_all": scanned_cells / cells,
-                       "timing": "wall clock per mode, each including create + init + all generations"},
-            "clocks": clk.summary()}
-    print(json.dumps(line), flush=True)
+    t_batch = rep.max_over_ranks(t_rank, dev)
+    results = rep.gather_results(results)
+    if rank == 0:
+        assert sorted(results) == list(range(len(jobs)))
+        scanned_cells = sum(r["scan_cells"] for r in results.values())
+        line = {"metric": "designs/s", "value": len(jobs) / t_batch, "unit": "designs/s", "n_gpus": world,
+                "steps": G, "warmup": 0, "ms_per_step": 1000.0 * t_batch / G, "higher_is_better": True,
+                "scaling": "strong" if world > 1 else "weak", "vs_baseline": None, "dtype": "u32",
+                "data": "synthetic",
+                "config": {"workload": f"batched: {len(jobs)} proteins, L log-uniform [100, 3000], m in {{2,4,8}}, "
+                                       f"N={N}, Pm={pm}, 4 objectives, {G} generations, one graph launch per 2 "
+                                       f"generations for all instances of a rank",
+                           "parallelism": f"job shards over {world} GPU(s) by stem-scan cells"},
+                "stem_cells_per_s": scanned_cells / t_batch, "stem_cells_scanned_of_all": scanned_cells / cells,
+                "mean_final_hv": float(np.mean([r["hv"] for r in results.values()])),
+                "timing": "wall clock per mode, each including create + init + all generations; N>1: slowest rank",
+                "clocks": clk.summary()}
+        if t_plain is not None:
+            line["plain_designs_per_s"] = len(jobs) / t_plain
+            line["batched_over_plain"] = t_plain / t_batch
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
 
 
 def served_jobs(pe, srv_mod, master_seed: int, count: int, rate: float):
@@ -635,7 +660,7 @@ def main():
         set_workload(args.shape, args.objectives == "ref6", args.string == "lrcs")
     world, rank, local = dist_setup()
     if args.workload == "batched":
-        run_batched(args)
+        run_batched(args, world, rank, local)
         return
     if args.workload == "served":
         run_served(args)

@@ -189,6 +189,80 @@ int pe_batch_step(pe_batch *batch, int32_t generations);
 int pe_batch_synchronize(pe_batch *batch);
 int pe_batch_destroy(pe_batch *batch);
 
+/* --- served design jobs (no counterpart in the reference, which designs one
+ *     protein per process, src/main.cu:467-901): continuous batching on one GPU.
+ *
+ * Jobs are submitted at any time and admitted by device footprint
+ * (pe_instance_bytes) against memory_budget and by max_active, in arrival order
+ * or shortest estimated work first (a job waiting longer than max_wait_s goes
+ * first).  Each resident job keeps its population on the device and is driven by
+ * its own host thread, `tick` generations per replay, so the kernels of all
+ * resident jobs overlap.  A job retires at its generation budget, when the
+ * hypervolume of its survivors' normalised objectives (src/main.cu:789-858) has
+ * not improved for `stall` generations (checked every hv_every generations), or
+ * when cancelled (between two replays).  A job's result is the same as the job
+ * run alone.  All calls are thread-safe. */
+typedef enum { PE_ORDER_ARRIVAL = 0, PE_ORDER_SHORTEST = 1 } pe_admission_order;
+typedef enum { PE_JOB_QUEUED = 0, PE_JOB_RUNNING = 1, PE_JOB_DONE = 2, PE_JOB_FAILED = 3,
+               PE_JOB_CANCELLED = 4 } pe_job_state;
+typedef enum { PE_REASON_BUDGET = 0, PE_REASON_STALL = 1, PE_REASON_ERROR = 2,
+               PE_REASON_CANCELLED = 3 } pe_job_reason;
+
+typedef struct pe_server_config {
+    uint64_t memory_budget;  /* device bytes for resident jobs; 0 = 80 % of the free memory */
+    int32_t max_active;      /* resident-job cap (0: nothing is admitted) */
+    int32_t tick;            /* generations per replay (0 = 10) */
+    int32_t hv_every;        /* generations between hypervolume checks (0 = 25) */
+    int32_t order;           /* pe_admission_order */
+    double max_wait_s;       /* a job queued longer goes first (0 = off) */
+    int32_t priorities;      /* 1: stream priority from estimated work (short jobs first) */
+} pe_server_config;
+
+typedef struct pe_job_spec {
+    pe_config cfg;                 /* the instance (stream_priority is set by the server) */
+    const int8_t *aa_idx;          /* protein, copied at submit */
+    int32_t aa_len;
+    const pe_codon_table *table;   /* copied at submit */
+    int32_t generations;           /* generation budget */
+    int32_t stall;                 /* retire after this many generations without a
+                                      hypervolume gain (0 = never) */
+    int32_t keep_codons;           /* 1: keep the survivors' codon ids for pe_job_result */
+} pe_job_spec;
+
+typedef struct pe_job_status {
+    int32_t state;                 /* pe_job_state */
+    int32_t reason;                /* pe_job_reason, -1 while queued or running */
+    int32_t generations_run;
+    int32_t priority;              /* stream priority it runs (or would run) at */
+    double hypervolume;            /* of the final survivors (done jobs), else -1 */
+    double submitted_s, started_s, finished_s;  /* server clock; -1 = not yet */
+    uint64_t device_bytes;         /* footprint it was admitted with */
+    char error[256];               /* failed jobs: the error */
+} pe_job_status;
+
+typedef struct pe_server_stats {
+    int32_t queued, active, peak_active;
+    uint64_t used_bytes, peak_used_bytes, memory_budget;
+} pe_server_stats;
+
+typedef struct pe_server pe_server;
+int pe_server_create(const pe_server_config *cfg, pe_server **out);
+int pe_batch_submit(pe_server *server, const pe_job_spec *spec, int64_t *job_id);
+int pe_poll(pe_server *server, int64_t job_id, pe_job_status *status);
+/* Results of a done job: survivor_obj [N][M] (minimisation form, the survivors in
+ * selection order) and, when submitted with keep_codons, survivor_codons [N][m][L];
+ * either may be NULL. */
+int pe_job_result(pe_server *server, int64_t job_id, float *survivor_obj, uint8_t *survivor_codons);
+/* A queued job is dropped at once; a running one stops after its current replay
+ * (nothing of it left in flight) and frees its memory; a finished one is kept. */
+int pe_cancel(pe_server *server, int64_t job_id);
+int pe_server_clock(pe_server *server, double *seconds);   /* seconds since pe_server_create */
+int pe_server_get_stats(pe_server *server, pe_server_stats *stats);
+/* Wait until no job is queued or running (timeout_s <= 0: no limit; PE_ERR_TIMEOUT). */
+int pe_server_drain(pe_server *server, double timeout_s);
+/* Cancels what is queued or running, waits for the running jobs to stop, frees. */
+int pe_server_destroy(pe_server *server);
+
 /* --- instrumentation (no counterpart in the reference, which only times the
  *     whole loop with cudaEvents, src/main.cu:702-731) --- */
 
@@ -198,6 +272,14 @@ int pe_set_profiling(pe_instance *inst, int32_t enable);
 /* Device milliseconds of those stages in the last completed generation
  * (call after pe_synchronize). */
 int pe_stage_times(pe_instance *inst, float *ms3);
+/* Polls a bounded device wait (the hairpin/LRCS scan's wait for its staged planes)
+ * makes before it gives up, sets a status and lets pe_synchronize return
+ * PE_ERR_TIMEOUT: 0 = the default (4,194,304), > 0 = that many, < 0 = none (it gives
+ * up at once: a test of the timeout path; the kernel still lets its copy land, within
+ * a second bound, before it returns).  pe_init_population clears the status and
+ * restarts the population.  No counterpart in the reference, whose spin-waits are
+ * unbounded (include/utils.cuh:873, include/sorting.cuh:939,949). */
+int pe_set_wait_limit(pe_instance *inst, int32_t polls);
 /* String-objective scans run since pe_create (no reference counterpart): one per
  * hairpin CDS or LRCS CDS pair.  A child's CDS that its mutation left unchanged
  * (for LRCS: a pair of two such CDSs) keeps its parent's result and is not

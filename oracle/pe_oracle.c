@@ -123,6 +123,19 @@ uint32_t or_draw(uint64_t seed, uint32_t tag, uint32_t gen, uint32_t idx, uint32
 #define TAG_MUT 3u
 #define TAG_SLMUT 4u
 #define TAG_NICHE 5u
+#define TAG_MUTP 6u
+
+/* The probability test of codon position pos in a mutation operator: word pos % 4
+ * of the Philox block with counter (TAG_MUTP, gen, idx, pos / 4), so one block
+ * serves four consecutive positions. */
+static uint32_t or_pdraw(uint64_t seed, uint32_t gen, uint32_t idx, uint32_t pos)
+{
+    uint32_t ctr[4] = {TAG_MUTP, gen, idx, pos >> 2};
+    uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    uint32_t out[4];
+    or_philox4x32_10(ctr, key, out);
+    return out[pos & 3];
+}
 
 static inline uint32_t rng_uint(uint32_t r, uint32_t k) { return (uint32_t)(((uint64_t)r * k) >> 32); }
 /* uniform float in (0,1], 24-bit grid */
@@ -541,6 +554,7 @@ void or_eval_light(const or_problem *pr, const uint8_t *sol, float *obj, int8_t 
 /* ------------------------------------------------------------------------ */
 
 #define DRAW(pos, j) or_draw(pr->seed, TAG_MUT, gen, (uint32_t)idx, (uint32_t)(pos), (uint32_t)(j))
+#define PDRAW(pos) or_pdraw(pr->seed, gen, (uint32_t)idx, (uint32_t)(pos))
 
 /* Fisher-Yates as indexArrayShuffling (include/utils.cuh:203-218), draws 1..k-1 */
 static void shuffle_idx(const or_problem *pr, uint32_t gen, int idx, int pos, int k, int *arr)
@@ -606,7 +620,7 @@ int or_mutate(const or_problem *pr, uint32_t gen, int idx, const uint8_t *parent
         for (int pos = 0; pos < m * L; pos++) {
             int aa = pr->aa[pos % L];
             int k = t->count[aa];
-            if (rng_u01(DRAW(pos, 0)) > pm || k == 1) continue;
+            if (rng_u01(PDRAW(pos)) > pm || k == 1) continue;
             int cur = child[pos] - t->start[aa];
             int nw = (int)rng_uint(DRAW(pos, 1), (uint32_t)(k - 1));
             if (nw >= cur) nw++;
@@ -618,7 +632,7 @@ int or_mutate(const or_problem *pr, uint32_t gen, int idx, const uint8_t *parent
         for (int a = 0; a < L; a++) {
             int aa = pr->aa[a];
             int k = t->count[aa];
-            if (rng_u01(DRAW(a, 0)) > pm || k == 1) continue;
+            if (rng_u01(PDRAW(a)) > pm || k == 1) continue;
             int cur = child[c * L + a] - t->start[aa];
             if (cur == k - 1) continue;
             int nw = cur + 1 + (int)rng_uint(DRAW(a, 1), (uint32_t)(k - 1 - cur));
@@ -637,7 +651,7 @@ int or_mutate(const or_problem *pr, uint32_t gen, int idx, const uint8_t *parent
             if ((a % 2) != parity) continue;
             int aa = pr->aa[a];
             int k = t->count[aa];
-            if (rng_u01(DRAW(a, 0)) > pm2 || k == 1) continue;
+            if (rng_u01(PDRAW(a)) > pm2 || k == 1) continue;
             int curg = par[a];
             int cur = curg - t->start[aa];
             int left = a > 0 ? par[a - 1] : -1;
@@ -671,7 +685,7 @@ int or_mutate(const or_problem *pr, uint32_t gen, int idx, const uint8_t *parent
             if ((a % 2) != parity) continue;
             int aa = pr->aa[a];
             int k = t->count[aa];
-            if (rng_u01(DRAW(a, 0)) > pm2 || k == 1) continue;
+            if (rng_u01(PDRAW(a)) > pm2 || k == 1) continue;
             int cur = par[a] - t->start[aa];
             int hasl = a > 0, hasr = a < L - 1;
             int curs = (hasl ? hsc_pair(t, par[a - 1], par[a]) : 0) + (hasr ? hsc_pair(t, par[a], par[a + 1]) : 0);
@@ -695,7 +709,7 @@ int or_mutate(const or_problem *pr, uint32_t gen, int idx, const uint8_t *parent
         for (int a = 0; a < L; a++) {
             int aa = pr->aa[a];
             int k = t->count[aa];
-            if (rng_u01(DRAW(a, 0)) > pm || k == 1) continue;
+            if (rng_u01(PDRAW(a)) > pm || k == 1) continue;
             int arr[6];
             shuffle_idx(pr, gen, idx, a, k, arr);
             const uint8_t *x = t->nt[parent[c1 * L + a]];
@@ -750,7 +764,7 @@ int or_mutate(const or_problem *pr, uint32_t gen, int idx, const uint8_t *parent
         for (int a = 0; a < L; a++) {
             int aa = pr->aa[a];
             int k = t->count[aa];
-            if (rng_u01(DRAW(a, 0)) > prob || k == 1) continue;
+            if (rng_u01(PDRAW(a)) > prob || k == 1) continue;
             int arr[6];
             shuffle_idx(pr, gen, idx, a, k, arr);
             int curg = parent[c * L + a];

@@ -88,6 +88,34 @@ class Info(C.Structure):
                 ("device_bytes", C.c_uint64), ("sl_threads", C.c_int32)]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("memory_budget", C.c_uint64), ("max_active", C.c_int32), ("tick", C.c_int32),
+                ("hv_every", C.c_int32), ("order", C.c_int32), ("max_wait_s", C.c_double),
+                ("priorities", C.c_int32)]
+
+
+class JobSpec(C.Structure):
+    _fields_ = [("cfg", Config), ("aa_idx", C.c_void_p), ("aa_len", C.c_int32), ("table", C.POINTER(CodonTable)),
+                ("generations", C.c_int32), ("stall", C.c_int32), ("keep_codons", C.c_int32)]
+
+
+class JobStatus(C.Structure):
+    _fields_ = [("state", C.c_int32), ("reason", C.c_int32), ("generations_run", C.c_int32),
+                ("priority", C.c_int32), ("hypervolume", C.c_double), ("submitted_s", C.c_double),
+                ("started_s", C.c_double), ("finished_s", C.c_double), ("device_bytes", C.c_uint64),
+                ("error", C.c_char * 256)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("queued", C.c_int32), ("active", C.c_int32), ("peak_active", C.c_int32),
+                ("used_bytes", C.c_uint64), ("peak_used_bytes", C.c_uint64), ("memory_budget", C.c_uint64)]
+
+
+JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_FAILED, JOB_CANCELLED = range(5)
+REASONS = {-1: None, 0: "budget", 1: "stall", 2: "error", 3: "cancelled"}
+ORDER_ARRIVAL, ORDER_SHORTEST = 0, 1
+
+
 class SelectInfo(C.Structure):
     _fields_ = [("rank_count", C.c_int32), ("last_front_size", C.c_int32), ("n_fronts", C.c_int32),
                 ("cut", C.c_int32), ("hyp_exception", C.c_int32), ("ideal", C.c_float * 6),
@@ -120,11 +148,17 @@ def lib() -> C.CDLL:
             "pe_load_codon_table": [C.c_char_p, C.POINTER(CodonTable)],
             "pe_hypervolume": [P, C.c_int32, C.c_int32, P, C.POINTER(C.c_double)],
             "pe_set_profiling": [P, C.c_int32], "pe_stage_times": [P, P], "pe_scan_count": [P, P],
-            "pe_scan_cells": [P, P],
+            "pe_scan_cells": [P, P], "pe_set_wait_limit": [P, C.c_int32],
             "pe_hairpin_noalloc": [P, C.c_int32, C.c_int32, C.c_int32, P, P, P, P],
             "pe_batch_create": [P, C.c_int32, C.POINTER(P)], "pe_batch_step": [P, C.c_int32],
             "pe_batch_synchronize": [P], "pe_batch_destroy": [P],
             "pe_instance_bytes": [C.POINTER(Config), C.c_int32, C.POINTER(C.c_uint64)],
+            "pe_server_create": [C.POINTER(ServerConfig), C.POINTER(P)],
+            "pe_batch_submit": [P, C.POINTER(JobSpec), C.POINTER(C.c_int64)],
+            "pe_poll": [P, C.c_int64, C.POINTER(JobStatus)], "pe_job_result": [P, C.c_int64, P, P],
+            "pe_cancel": [P, C.c_int64], "pe_server_clock": [P, C.POINTER(C.c_double)],
+            "pe_server_get_stats": [P, C.POINTER(ServerStats)], "pe_server_drain": [P, C.c_double],
+            "pe_server_destroy": [P],
         }
         for name, args in sig.items():
             f = getattr(L, name)
@@ -289,6 +323,10 @@ class Engine:
         v = C.c_uint64(0)
         _ck(lib().pe_scan_count(self._h, C.byref(v)))
         return v.value
+
+    def set_wait_limit(self, polls: int):
+        """Polls of the bounded device waits (0 default, < 0: give up at once; tests)."""
+        _ck(lib().pe_set_wait_limit(self._h, polls))
 
     def scan_cells(self) -> int:
         """Counted cells of those scans (the string-objective kernel's unit of work)."""

@@ -680,6 +680,21 @@ int pe_set_profiling(pe_instance *in, int32_t enable)
     return PE_OK;
 }
 
+int pe_set_wait_limit(pe_instance *in, int32_t polls)
+{
+    if (!in) return fail(PE_ERR_ARG, "null instance");
+    CK(cudaStreamSynchronize(in->stream));
+    if (polls != in->s.wait_limit) {
+        in->s.wait_limit = polls;
+        for (int i = 0; i < 2; i++)
+            if (in->graph[i]) {
+                cudaGraphExecDestroy(in->graph[i]);
+                in->graph[i] = nullptr;
+            }
+    }
+    return PE_OK;
+}
+
 int pe_stage_times(pe_instance *in, float *ms3)
 {
     if (!in || !ms3) return fail(PE_ERR_ARG, "null argument");
@@ -768,6 +783,10 @@ int pe_init_population(pe_instance *in)
 {
     if (!in) return fail(PE_ERR_ARG, "null instance");
     Shape &s = in->s;
+    // a fresh start: clears a status left by a device wait that gave up, and the
+    // per-solution counters of scans that did not finish
+    CK(cudaMemsetAsync(in->d_status, 0, sizeof(int32_t), in->stream));
+    CK(cudaMemsetAsync(in->d_counter, 0, (size_t)2 * s.N * sizeof(int32_t), in->stream));
     CK(launch_init(s, in->d_tab, in->d_aa, in->buf[0], in->d_surv, in->stream));
     bool scanned = false;
     if (in->cfg.sl_threads == 0 && s.sl_threads == 0) {

@@ -323,6 +323,19 @@ __device__ void light_eval(const Shape &s, const DevTables *gt, VarSmem &sm, con
 
 #define MDRAW(pos, j) draw(s.seed, TAG_MUT, gen, ridx, (uint32_t)(pos), (uint32_t)(j))
 
+// The probability tests of codon positions 4q .. 4q+3: one Philox4x32-10 block with
+// counter (TAG_MUTP, gen, idx, q), word p % 4 for position p.  Each thread takes four
+// consecutive positions, so a block is computed once for four tests.
+__device__ __forceinline__ uint4 pdraw4(const Shape &s, uint32_t gen, uint32_t ridx, int q)
+{
+    return philox4x32_10(make_uint4(TAG_MUTP, gen, ridx, (uint32_t)q),
+                         make_uint2((uint32_t)s.seed, (uint32_t)(s.seed >> 32)));
+}
+__device__ __forceinline__ uint32_t word4(const uint4 &w, int u)
+{
+    return u == 0 ? w.x : u == 1 ? w.y : u == 2 ? w.z : w.w;
+}
+
 __device__ __forceinline__ void shuffle_k(const Shape &s, uint32_t gen, uint32_t ridx, int pos, int k, int *arr)
 {
     // indexArrayShuffling (include/utils.cuh:203-218): draws 1..k-1
@@ -346,30 +359,42 @@ __device__ void mutate_solution(const Shape &s, const DevTables *gt, VarSmem &sm
     const int op = sm.op;
     switch (op) {
     case 0: {  // mutationRandom (:16-63)
-        for (int pos = tid; pos < m * L; pos += nth) {
-            int c = pos / L, a = pos - c * L;
-            int am = aa[a];
-            int k = st.count[am];
-            if (rng_u01(MDRAW(pos, 0)) > pm || k == 1) continue;
-            uint8_t *cell = ids + c * s.Lp + a;
-            int cur = *cell - st.start[am];
-            int nw = (int)rng_uint(MDRAW(pos, 1), (uint32_t)(k - 1));
-            if (nw >= cur) nw++;
-            *cell = (uint8_t)(st.start[am] + nw);
+        for (int q = tid; 4 * q < m * L; q += nth) {
+            const uint4 w4 = pdraw4(s, gen, ridx, q);
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int pos = 4 * q + u;
+                if (pos >= m * L) break;
+                int c = pos / L, a = pos - c * L;
+                int am = aa[a];
+                int k = st.count[am];
+                if (rng_u01(word4(w4, u)) > pm || k == 1) continue;
+                uint8_t *cell = ids + c * s.Lp + a;
+                int cur = *cell - st.start[am];
+                int nw = (int)rng_uint(MDRAW(pos, 1), (uint32_t)(k - 1));
+                if (nw >= cur) nw++;
+                *cell = (uint8_t)(st.start[am] + nw);
+            }
         }
         break;
     }
     case 1: {  // mutationCAI, SELECT_UPPER_RANDOM (:65-142)
         int c = sm.pobjidx[2 * s.slot[K_CAI]];
-        for (int a = tid; a < L; a += nth) {
-            int am = aa[a];
-            int k = st.count[am];
-            if (rng_u01(MDRAW(a, 0)) > pm || k == 1) continue;
-            uint8_t *cell = ids + c * s.Lp + a;
-            int cur = *cell - st.start[am];
-            if (cur == k - 1) continue;
-            int nw = cur + 1 + (int)rng_uint(MDRAW(a, 1), (uint32_t)(k - 1 - cur));
-            *cell = (uint8_t)(st.start[am] + nw);
+        for (int q = tid; 4 * q < L; q += nth) {
+            const uint4 w4 = pdraw4(s, gen, ridx, q);
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int a = 4 * q + u;
+                if (a >= L) break;
+                int am = aa[a];
+                int k = st.count[am];
+                if (rng_u01(word4(w4, u)) > pm || k == 1) continue;
+                uint8_t *cell = ids + c * s.Lp + a;
+                int cur = *cell - st.start[am];
+                if (cur == k - 1) continue;
+                int nw = cur + 1 + (int)rng_uint(MDRAW(a, 1), (uint32_t)(k - 1 - cur));
+                *cell = (uint8_t)(st.start[am] + nw);
+            }
         }
         break;
     }
@@ -378,11 +403,15 @@ __device__ void mutate_solution(const Shape &s, const DevTables *gt, VarSmem &sm
         float pm2 = __fmul_rn(pm, 2.0f);
         int parity = (int)(gen & 1u);
         uint8_t *row = ids + c * s.Lp;
-        for (int a = tid; a < L - 1; a += nth) {
+        for (int q = tid; 4 * q < L - 1; q += nth) {
+          const uint4 w4 = pdraw4(s, gen, ridx, q);
+          for (int u = 0; u < 4; u++) {
+            const int a = 4 * q + u;
+            if (a >= L - 1) break;
             if ((a & 1) != parity) continue;
             int am = aa[a];
             int k = st.count[am];
-            if (rng_u01(MDRAW(a, 0)) > pm2 || k == 1) continue;
+            if (rng_u01(word4(w4, u)) > pm2 || k == 1) continue;
             int curg = row[a];
             int cur = curg - st.start[am];
             int left = a > 0 ? row[a - 1] : -1;
@@ -400,6 +429,7 @@ __device__ void mutate_solution(const Shape &s, const DevTables *gt, VarSmem &sm
                 if (ns > curs) up[nup++] = j;
             }
             if (nup > 0) row[a] = (uint8_t)(st.start[am] + up[rng_uint(MDRAW(a, 1), (uint32_t)nup)]);
+          }
         }
         break;
     }
@@ -408,11 +438,15 @@ __device__ void mutate_solution(const Shape &s, const DevTables *gt, VarSmem &sm
         float pm2 = __fmul_rn(pm, 2.0f);
         int parity = (int)(gen & 1u);
         uint8_t *row = ids + c * s.Lp;
-        for (int a = tid; a < L; a += nth) {
+        for (int q = tid; 4 * q < L; q += nth) {
+          const uint4 w4 = pdraw4(s, gen, ridx, q);
+          for (int u = 0; u < 4; u++) {
+            const int a = 4 * q + u;
+            if (a >= L) break;
             if ((a & 1) != parity) continue;
             int am = aa[a];
             int k = st.count[am];
-            if (rng_u01(MDRAW(a, 0)) > pm2 || k == 1) continue;
+            if (rng_u01(word4(w4, u)) > pm2 || k == 1) continue;
             int cur = row[a] - st.start[am];
             bool hl = a > 0, hr = a < L - 1;
             int lft = hl ? row[a - 1] : 0, rgt = hr ? row[a + 1] : 0;
@@ -425,16 +459,21 @@ __device__ void mutate_solution(const Shape &s, const DevTables *gt, VarSmem &sm
                 if (ns > curs) up[nup++] = j;
             }
             if (nup > 0) row[a] = (uint8_t)(st.start[am] + up[rng_uint(MDRAW(a, 1), (uint32_t)nup)]);
+          }
         }
         break;
     }
     case 4: {  // mutationHD (:390-534)
         int hs = s.slot[K_HD];
         int c1 = sm.pobjidx[2 * hs], c2 = sm.pobjidx[2 * hs + 1];
-        for (int a = tid; a < L; a += nth) {
+        for (int q = tid; 4 * q < L; q += nth) {
+          const uint4 w4 = pdraw4(s, gen, ridx, q);
+          for (int u = 0; u < 4; u++) {
+            const int a = 4 * q + u;
+            if (a >= L) break;
             int am = aa[a];
             int k = st.count[am];
-            if (rng_u01(MDRAW(a, 0)) > pm || k == 1) continue;
+            if (rng_u01(word4(w4, u)) > pm || k == 1) continue;
             int arr[6];
             shuffle_k(s, gen, ridx, a, k, arr);
             int x = ids[c1 * s.Lp + a];
@@ -472,6 +511,7 @@ __device__ void mutate_solution(const Shape &s, const DevTables *gt, VarSmem &sm
                 }
             }
             if (best_m != -1 || best_pair != -1) ids[c1 * s.Lp + a] = (uint8_t)(st.start[am] + best);
+          }
         }
         break;
     }
@@ -488,10 +528,14 @@ __device__ void mutate_solution(const Shape &s, const DevTables *gt, VarSmem &sm
             prob = __fdiv_rn(__fmul_rn(sm.pobj[gs], refGC), (float)L);
         }
         uint8_t *row = ids + c * s.Lp;
-        for (int a = tid; a < L; a += nth) {
+        for (int q = tid; 4 * q < L; q += nth) {
+          const uint4 w4 = pdraw4(s, gen, ridx, q);
+          for (int u = 0; u < 4; u++) {
+            const int a = 4 * q + u;
+            if (a >= L) break;
             int am = aa[a];
             int k = st.count[am];
-            if (rng_u01(MDRAW(a, 0)) > prob || k == 1) continue;
+            if (rng_u01(word4(w4, u)) > prob || k == 1) continue;
             int arr[6];
             shuffle_k(s, gen, ridx, a, k, arr);
             int curg = row[a];
@@ -507,6 +551,7 @@ __device__ void mutate_solution(const Shape &s, const DevTables *gt, VarSmem &sm
                     break;
                 }
             }
+          }
         }
         break;
     }
@@ -1338,7 +1383,8 @@ __global__ void __launch_bounds__(NT) k_sl(Shape s, PopBuf buf, int base, int2 *
             }
             // bounded wait on phase 0
             int done = 0;
-            for (int it = 0; it < (1 << 22) && !done; it++) {
+            const int polls = wait_polls(s.wait_limit);
+            for (int it = 0; it < polls && !done; it++) {
                 uint32_t ok;
                 asm volatile(
                     "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"

@@ -19,7 +19,7 @@ constexpr int kSelThreads = 1024;    // selection CTA
 constexpr int kSlGuardRows = 8;      // zero guard rows around the shifted T copies
 
 // RNG stream tags (Philox counter word 0)
-constexpr uint32_t TAG_INIT = 1u, TAG_OP = 2u, TAG_MUT = 3u, TAG_SLMUT = 4u, TAG_NICHE = 5u;
+constexpr uint32_t TAG_INIT = 1u, TAG_OP = 2u, TAG_MUT = 3u, TAG_SLMUT = 4u, TAG_NICHE = 5u, TAG_MUTP = 6u;
 
 // Problem shape, passed by value to every kernel.
 struct Shape {
@@ -40,7 +40,14 @@ struct Shape {
     int sl_threads;  // stem-scan CTA size (64, 128 or 256; 0 = 128), picked per instance by timing
     int sl_kind;     // string objective: PE_SL_HAIRPIN or PE_SL_LRCS
     int nres;        // string-objective results per solution: m CDSs (hairpin) or m(m+1)/2 CDS pairs (LRCS)
+    int wait_limit;  // polls of a bounded device wait: 0 = the default, < 0 = give up at once (tests)
 };
+
+// polls of a bounded device wait before it gives up and reports PE_ERR_TIMEOUT
+__host__ __device__ __forceinline__ int wait_polls(int wait_limit)
+{
+    return wait_limit > 0 ? wait_limit : (wait_limit < 0 ? 0 : (1 << 22));
+}
 
 // Device-resident tables derived from pe_codon_table.
 struct DevTables {
@@ -74,7 +81,7 @@ struct PopBuf {
 };
 
 struct SelectScratch {
-    uint32_t *dom;       // [2N][2N/32] bit j of row i: i dominates j
+    uint32_t *dom;       // [2N][2N/32] bit j of row i: j dominates i
     int32_t *np;         // [2N]
     int32_t *front;      // [2N]
     int32_t *sorted;     // [2N] fronts 0..last

@@ -22,6 +22,8 @@
 #include <cuda_runtime.h>
 
 #include "pe_device.cuh"
+#include <cooperative_groups.h>
+
 #include "pe_internal.h"
 
 namespace pe {
@@ -62,18 +64,17 @@ __global__ void __launch_bounds__(256) k_dominance(Shape s, const float *__restr
 #pragma unroll 2
     for (int w = warp; w < words; w += 8) {
         int j = 32 * w + lane;
-        bool by = false, over = false;  // j dominates i; i dominates j
+        bool bit = false;
         if (j < N2 && j != i) {
             float oj[kMaxObj];
 #pragma unroll
             for (int k = 0; k < (MM > 0 ? MM : kMaxObj); k++)
                 if (k < M) oj[k] = __ldg(&obj[(size_t)j * M + k]);
-            by = dominates(oj, oi, M);
-            over = dominates(oi, oj, M);
+            bit = dominates(oj, oi, M);
         }
-        const uint32_t word = __ballot_sync(0xffffffffu, over);
+        const uint32_t word = __ballot_sync(0xffffffffu, bit);
         if (lane == 0) dom[(size_t)i * words + w] = word;
-        cnt += __popc(__ballot_sync(0xffffffffu, by));
+        cnt += __popc(word);
     }
     if (lane == 0) wsum[warp] = cnt;
     __syncthreads();
@@ -356,6 +357,172 @@ __device__ __forceinline__ int block_scan_value(int v, SelSmem &sm, int *total)
     return r;
 }
 
+// nonDominatedSorting (include/sorting.cuh:974-1089): fronts peeled on the
+// dominance bit matrix by a cluster of kFrontCtas CTAs.  CTA c owns the rows
+// [c*RR, c*RR + RR) (RR a multiple of 32, so each CTA's rows are whole mask
+// words).  Per front: every CTA puts its rows that joined the front into its
+// slice of the front mask (in its shared memory); after one cluster barrier each
+// CTA assembles the whole mask from the slices (distributed shared memory),
+// lists its own members in ascending index (prefix popcounts over the mask), and
+// tests each of its unassigned rows against the mask -- one warp per row,
+// coalesced loads of the row, dominators in the front subtracted from the row's
+// count -- to fill its slice of the next front.  Slices are double-buffered, so
+// one barrier per front suffices.  Every CTA sees the same masks and counts, so
+// they stop together: when fronts 0..f hold N or more solutions, or when a front
+// comes out empty (a cycle of the epsilon-dominance relation leaves the rest
+// unassigned; the reference's loop would then run out its 2N-1 rounds on empty
+// fronts, which the recorded front count reproduces).
+constexpr int kFrontCtas = 8;
+constexpr int kFrontThreads = 1024;
+
+__host__ __device__ __forceinline__ int front_rows_per_cta(int N2)
+{
+    return ((N2 + kFrontCtas - 1) / kFrontCtas + 31) & ~31;
+}
+
+__global__ void __cluster_dims__(kFrontCtas, 1, 1) __launch_bounds__(kFrontThreads, 1)
+    k_fronts(Shape s, SelectScratch sc)
+{
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    extern __shared__ __align__(16) unsigned char fsm_raw[];
+    __shared__ int s_warp[32];
+    const int c = (int)cluster.block_rank();
+    const int N = s.N, N2 = 2 * N, words = (N2 + 31) >> 5;
+    const int RR = front_rows_per_cta(N2), sw = RR >> 5;
+    const int r0 = c * RR, nrow = max(0, min(N2, r0 + RR) - r0);
+    uint32_t *fmask = reinterpret_cast<uint32_t *>(fsm_raw);          // words: the current front
+    uint32_t *slice = fmask + ((words + 3) & ~3);                      // [2][sw]: own rows joining a front
+    int *npr = reinterpret_cast<int *>(slice + 2 * ((sw + 3) & ~3));   // [RR]: unassigned dominators
+    int *wpre = npr + RR;                                              // [words]: members before each word
+    const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarps = nth >> 5;
+    const int swp = (sw + 3) & ~3;
+
+    for (int q = tid; q < RR; q += nth) {
+        const int v = q < nrow ? sc.np[r0 + q] : -1;
+        npr[q] = v;
+        if (q < nrow) sc.front[r0 + q] = -1;
+    }
+    for (int w = tid; w < 2 * swp; w += nth) slice[w] = 0u;
+    __syncthreads();
+    for (int q = tid; q < nrow; q += nth)
+        if (npr[q] == 0) atomicOr(&slice[q >> 5], 1u << (q & 31));
+    int rc = 0, fstart = 0, fsize = 0, nfront = 0, cut = 0, f0 = 0, par = 0;
+    for (int it = 0; it < N2; it++) {
+        cluster.sync();  // every slice of this front is complete
+        for (int w = tid; w < words; w += nth) {
+            const int owner = w / sw, off = w - owner * sw;
+            const uint32_t *rs = cluster.map_shared_rank(slice + par * swp, owner);
+            fmask[w] = rs[off];
+        }
+        __syncthreads();
+        // exclusive prefix of the mask words' popcounts (words <= 32 * nth)
+        int carry = 0;
+        for (int base = 0; base < words; base += nth) {
+            const int w = base + tid;
+            const int v = w < words ? __popc(fmask[w]) : 0;
+            int inc = v;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, inc, o);
+                if (lane >= o) inc += y;
+            }
+            if (lane == 31) s_warp[warp] = inc;
+            __syncthreads();
+            if (warp == 0) {
+                int x = lane < nwarps ? s_warp[lane] : 0;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, x, o);
+                    if (lane >= o) x += y;
+                }
+                s_warp[lane] = x;  // inclusive over warps
+            }
+            __syncthreads();
+            if (w < words) wpre[w] = carry + (warp ? s_warp[warp - 1] : 0) + inc - v;
+            const int tot_here = s_warp[31];
+            __syncthreads();
+            carry += tot_here;
+        }
+        const int tot = carry;
+        // own members of front `it`, in ascending index
+        for (int w = (r0 >> 5) + tid; w < min(words, (r0 >> 5) + sw); w += nth) {
+            uint32_t x = fmask[w];
+            int pos = rc + wpre[w];
+            while (x) {
+                const int b = __ffs(x) - 1;
+                x &= x - 1;
+                const int i = 32 * w + b;
+                sc.front[i] = it;
+                sc.sorted[pos++] = i;
+            }
+        }
+        fstart = rc;
+        fsize = tot;
+        rc += tot;
+        nfront = it + 1;
+        if (it == 0) f0 = tot;
+        if (rc >= N) {
+            cut = rc == N;
+            break;
+        }
+        if (tot == 0) {
+            nfront = N2;
+            break;
+        }
+        // the next front: own unassigned rows whose remaining dominators are all in this one
+        const int nx = par ^ 1;
+        for (int w = tid; w < sw; w += nth) slice[nx * swp + w] = 0u;
+        __syncthreads();
+        // four rows per warp at a time, so their loads are in flight together
+        for (int q0 = warp; q0 < nrow; q0 += 4 * nwarps) {
+            const uint32_t *row[4];
+            bool act[4];
+            int dec[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int q = q0 + u * nwarps;
+                act[u] = q < nrow && npr[q] > 0;  // rows assigned already are skipped
+                row[u] = sc.dom + (size_t)(r0 + (act[u] ? q : 0)) * words;
+                dec[u] = 0;
+            }
+            for (int w = lane; w < words; w += 32) {
+                const uint32_t f = fmask[w];
+                if (!f) continue;
+#pragma unroll
+                for (int u = 0; u < 4; u++)
+                    if (act[u]) dec[u] += __popc(__ldg(&row[u][w]) & f);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                int d = dec[u];
+                for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+                const int q = q0 + u * nwarps;
+                if (lane == 0 && act[u] && d) {
+                    const int v = npr[q] - d;
+                    npr[q] = v;
+                    if (v == 0) atomicOr(&slice[nx * swp + (q >> 5)], 1u << (q & 31));
+                }
+            }
+        }
+        par = nx;
+        __syncthreads();
+    }
+    if (c == 0 && tid == 0) {
+        sc.info[0] = rc;
+        sc.info[1] = fsize;
+        sc.info[2] = nfront;
+        sc.info[3] = cut;
+        sc.info[6] = fstart;
+        sc.info[7] = f0;
+    }
+    cluster.sync();  // no CTA leaves while another may still read its slices
+}
+
+size_t fronts_smem_bytes(const Shape &s)
+{
+    const int N2 = 2 * s.N, words = (N2 + 31) >> 5, RR = front_rows_per_cta(N2), sw = RR >> 5;
+    return (size_t)((words + 3) & ~3) * 4 + (size_t)2 * ((sw + 3) & ~3) * 4 + (size_t)RR * 4 + (size_t)words * 4;
+}
+
 __global__ void __launch_bounds__(kSelThreads, 1) k_select(Shape s, const float *__restrict__ obj, float *ext,
                                                         const float *__restrict__ refpts, SelectScratch sc,
                                                         int32_t *surv, uint32_t *d_gen, int bump_gen)
@@ -364,103 +531,24 @@ __global__ void __launch_bounds__(kSelThreads, 1) k_select(Shape s, const float 
     SelSmem &sm = *reinterpret_cast<SelSmem *>(smem_raw);
     const int N = s.N, N2 = 2 * N, M = s.M, R = s.R;
     const int words = (N2 + 31) >> 5;
-    // ready[w]: solutions whose last dominator was just assigned (the next front); npl: the
-    // dominators of each solution not yet assigned to a front
-    uint32_t *ready = reinterpret_cast<uint32_t *>(smem_raw + ((sizeof(SelSmem) + 15) & ~size_t(15)));
-    int *npl = reinterpret_cast<int *>(ready + ((words + 3) & ~3));
-    ExtSmem &xs = *reinterpret_cast<ExtSmem *>(npl + ((N2 + 3) & ~3));
+    ExtSmem &xs = *reinterpret_cast<ExtSmem *>(smem_raw + ((sizeof(SelSmem) + 15) & ~size_t(15)));
     const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5;
     (void)d_gen;
     (void)bump_gen;
+    (void)words;
 
-    // ---------------- front 0 (np == 0), ascending index
-    for (int i = tid; i < N2; i += nth) {
-        sc.front[i] = -1;
-        npl[i] = sc.np[i];
-    }
-    for (int w = tid; w < words; w += nth) ready[w] = 0u;
+    // fronts 0..last: peeled by k_fronts (front[], sorted[] and the counts in info)
+    const int rc = sc.info[0];
+    const int last_size = sc.info[1];
+    const int f0 = sc.info[7];
     if (tid == 0) {
-        sm.rc = 0;
-        sm.count = 0;
+        sm.rc = rc;
+        sm.fsize = last_size;
+        sm.fstart = sc.info[6];
+        sm.nfront = sc.info[2];
+        sm.cut = sc.info[3];
     }
     __syncthreads();
-    for (int base = 0; base < N2; base += nth) {
-        int i = base + tid;
-        int flag = (i < N2) && sc.np[i] == 0;
-        int tot;
-        int pos = block_scan_flag(flag, sm, &tot);
-        if (flag) {
-            sc.front[i] = 0;
-            sc.sorted[sm.rc + pos] = i;
-        }
-        __syncthreads();
-        if (tid == 0) sm.rc += tot;
-        __syncthreads();
-    }
-    const int f0 = sm.rc;
-    if (tid == 0) {
-        sm.fstart = 0;
-        sm.fsize = f0;
-        sm.cut = (f0 == N);
-        sm.nfront = 1;
-    }
-    __syncthreads();
-    // ---------------- later fronts (only while fewer than N are assigned).  The rows of
-    // the last front's members (whom each dominates) decrement their dominatees' counts;
-    // a solution whose count reaches 0 joins the next front.  Every row is read once over
-    // all fronts.  The next front is listed in ascending index from the ready mask.
-    if (f0 < N) {
-        for (int it = 0; it < N2 - 1; it++) {
-            const int fs = sm.fstart, fz = sm.fsize, cf = sm.nfront;
-            for (int u = tid; u < fz * words; u += nth) {
-                const int q = u / words, w = u - q * words;
-                uint32_t x = sc.dom[(size_t)sc.sorted[fs + q] * words + w];
-                while (x) {
-                    const int b = __ffs(x) - 1;
-                    x &= x - 1;
-                    if (atomicSub(&npl[32 * w + b], 1) == 1) atomicOr(&ready[w], 1u << b);
-                }
-            }
-            __syncthreads();
-            const int rc0 = sm.rc;
-            for (int base = 0; base < words; base += nth) {
-                const int w = base + tid;
-                const uint32_t x = w < words ? ready[w] : 0u;
-                int tot;
-                int pos = rc0 + sm.count + block_scan_value(__popc(x), sm, &tot);
-                if (w < words) {
-                    ready[w] = 0u;
-                    uint32_t y = x;
-                    while (y) {
-                        const int b = __ffs(y) - 1;
-                        y &= y - 1;
-                        const int i = 32 * w + b;
-                        sc.front[i] = cf;
-                        sc.sorted[pos++] = i;
-                    }
-                }
-                __syncthreads();
-                if (tid == 0) sm.count += tot;
-                __syncthreads();
-            }
-            if (tid == 0) {
-                const int tot = sm.count;
-                sm.count = 0;
-                sm.fstart = rc0;
-                sm.fsize = tot;
-                sm.rc = rc0 + tot;
-                sm.nfront = cf + 1;
-                if (sm.rc >= N) sm.cut = (sm.rc == N);
-                // no solution became ready: the rest is never assigned (a cycle of the
-                // epsilon-dominance relation); the remaining rounds would add empty fronts
-                if (tot == 0) sm.nfront = N2;
-            }
-            __syncthreads();
-            if (sm.rc >= N || sm.fsize == 0) break;
-        }
-    }
-    const int rc = sm.rc;
-    const int last_size = sm.fsize;
 
     // ---------------- ideal / worst (exact min / max), objective by objective
     for (int k = 0; k < M; k++) {
@@ -792,49 +880,57 @@ __global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc
         __syncthreads();
     }
     if (tid == 0) coff[R] = sm.i0;
-    // candidate lists in ascending position: each member takes a slot in its point's
-    // range (kq counts the fill), then finds its place by counting the members of
-    // that range before it.  On the way, the nearest member of each point (the first
-    // in list order among equal distances) is found -- the pick at level 0, which is a
-    // point's first pick whenever it has one, so it is made here for every point with
-    // niche count 0 (a point that ends up picking nothing never reads its list).
-    // pofs and kq serve as scratch: the least distance bits, then the least rank.
+    // candidate lists in ascending position, one warp per reference point: the warp
+    // scans the last front's members 32 at a time, and a ballot of "associated with
+    // this point" gives each member its place after the ones before it.  On the way,
+    // the nearest member of a point with niche count 0 (the first in list order among
+    // equal distances) -- its pick at level 0, which is the point's first pick
+    // whenever it has one -- is found and moved to the list's end right there (a
+    // point that ends up picking nothing never reads its list).
     const int nm = rc - count0;
-    for (int t = tid; t < nm; t += nth) {
-        const int j = las[t];
-        cand[coff[j] + atomicAdd(&kq[j], 1)] = t;
-    }
-    __syncthreads();
-    for (int j = tid; j < R; j += nth) {
-        pofs[j] = 0x7fffffff;
-        kq[j] = 0x7fffffff;
-    }
-    for (int t = tid; t < nm; t += nth) {
-        const int j = las[t], b = coff[j], e = b + nj[j];
-        int r = 0;
-        for (int u = b; u < e; u++) r += cand[u] < t;
-        las[t] = b + r;  // only this thread reads las[t]
-    }
-    __syncthreads();
-    for (int t = tid; t < nm; t += nth) {
-        cand[las[t]] = lsol[t];
-        const int j = sc.assoc[count0 + t];
-        // distances are >= +0 (or FLT_MAX), so their bits order as the values do
-        if (cj[j] == 0) atomicMin(&pofs[j], __float_as_int(sc.dist[lsol[t]]));
-    }
-    __syncthreads();
-    for (int t = tid; t < nm; t += nth) {
-        const int j = sc.assoc[count0 + t];
-        if (cj[j] == 0 && __float_as_int(sc.dist[lsol[t]]) == pofs[j]) atomicMin(&kq[j], las[t] - coff[j]);
-    }
-    __syncthreads();
-    for (int j = tid; j < R; j += nth)
-        if (cj[j] == 0 && nj[j] > 0) {
-            int *cl = cand + coff[j];
-            const int slot = kq[j], last = nj[j] - 1, pick = cl[slot];
-            cl[slot] = cl[last];
-            cl[last] = pick;
+    for (int j = warp; j < R; j += nwarps) {
+        if (nj[j] == 0) continue;
+        int *cl = cand + coff[j];
+        const bool lvl0 = cj[j] == 0;
+        int run = 0;
+        uint32_t bd = 0xffffffffu;  // distance bits (>= +0, so they order as the values do)
+        int br = 0x7fffffff;        // list position of that member
+        for (int t0 = 0; t0 < nm; t0 += 32) {
+            const int t = t0 + lane;
+            const bool mine = t < nm && las[t] == j;
+            const uint32_t bal = __ballot_sync(0xffffffffu, mine);
+            if (mine) {
+                const int r = run + __popc(bal & ((1u << lane) - 1u));
+                const int sol = lsol[t];
+                cl[r] = sol;
+                if (lvl0) {
+                    const uint32_t d = __float_as_uint(sc.dist[sol]);
+                    if (d < bd) {
+                        bd = d;
+                        br = r;
+                    }
+                }
+            }
+            run += __popc(bal);
         }
+        if (lvl0) {
+            for (int o = 16; o > 0; o >>= 1) {
+                const uint32_t od = __shfl_xor_sync(0xffffffffu, bd, o);
+                const int orr = __shfl_xor_sync(0xffffffffu, br, o);
+                if (od < bd || (od == bd && orr < br)) {
+                    bd = od;
+                    br = orr;
+                }
+            }
+            __syncwarp();
+            if (lane == 0) {
+                const int last = nj[j] - 1, pick = cl[br];
+                cl[br] = cl[last];
+                cl[last] = pick;
+            }
+        }
+    }
+    __syncthreads();
     // active points per level, then picks before each level: lv[l] = picks at levels < l
     if (tid == 0) {
         sm.i0 = 0;
@@ -953,9 +1049,8 @@ size_t niche_smem_bytes(const Shape &s)
 
 size_t select_smem_bytes(const Shape &s)
 {
-    const int N2 = 2 * s.N, words = (N2 + 31) >> 5;
-    return ((sizeof(SelSmem) + 15) & ~size_t(15)) + (size_t)((words + 3) & ~3) * 4 + (size_t)((N2 + 3) & ~3) * 4 +
-           sizeof(ExtSmem);
+    (void)s;
+    return ((sizeof(SelSmem) + 15) & ~size_t(15)) + sizeof(ExtSmem);
 }
 
 cudaError_t launch_select(const Shape &s, const float *obj, float *ext, const float *refpts, SelectScratch sc,
@@ -966,6 +1061,10 @@ cudaError_t launch_select(const Shape &s, const float *obj, float *ext, const fl
     else k_dominance<0><<<2 * s.N, 256, 0, st>>>(s, obj, sc.dom, sc.np);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
+    const size_t fsm = fronts_smem_bytes(s);
+    if ((e = raise_smem_limit((const void *)k_fronts, fsm)) != cudaSuccess) return e;
+    k_fronts<<<kFrontCtas, kFrontThreads, fsm, st>>>(s, sc);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
     size_t smem = select_smem_bytes(s);
     e = raise_smem_limit((const void *)k_select, smem);
     if (e != cudaSuccess) return e;

@@ -38,6 +38,23 @@ def max_over_ranks(seconds: float, device=None) -> float:
     return float(t.item())
 
 
+def gather_results(local: dict) -> dict:
+    """Every rank's {job index: result} merged (all ranks call this in the same order;
+    a job index appears on exactly one rank)."""
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return dict(local)
+    parts = [None] * dist.get_world_size()
+    dist.all_gather_object(parts, local)
+    merged = {}
+    for part in parts:
+        for k, v in part.items():
+            if k in merged:
+                raise ValueError(f"job {k} reported by two ranks")
+            merged[k] = v
+    return merged
+
+
 def whole_job_rate(units_per_rank: float, world: int, max_seconds: float) -> float:
     """Aggregate throughput: units processed by all ranks / slowest rank's time."""
     return units_per_rank * world / max_seconds

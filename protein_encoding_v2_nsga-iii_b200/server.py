@@ -86,6 +86,7 @@ class Job:
     mutation_prob: float = 0.02
     stall: int = 50                 # 0 disables the stall rule
     arrival: float = 0.0            # seconds from the start of the run
+    sl_kind: int = 0                # string objective: 0 hairpin stem, 1 longest repeated/common substring
     job_id: int = -1
     # filled by the server
     submitted: float | None = None
@@ -262,3 +263,130 @@ def latency_stats(done: list[Job]) -> dict:
 "host_hv_s": float(sum(j.hv_s for j in done)), "host_read_s": float(sum(j.read_s for j in done)),
             "gpu_wait_s": float(sum(j.gpu_s for j in done))}
 
+
+
+class NativeServer:
+    """The same served mode run by the library's own serving core (pe_server_create,
+    pe_batch_submit, pe_poll, pe_job_result, pe_cancel in include/pe_nsga3.h): this
+    class only submits jobs at their arrival times and reads their status and
+    results; admission, the per-job host threads, stall checks and retirement run in
+    C++.  Same constructor arguments and run() contract as Server; `priority` is a
+    switch here (the core derives each job's stream priority from its estimated work)."""
+
+    def __init__(self, pe, memory_budget: int, max_active: int = 64, tick: int = 10, hv_every: int = 25,
+                 keep_population: bool = False, priority=True, order: str = "arrival",
+                 max_wait: float | None = None, poll_s: float = 0.001):
+        if order not in ("arrival", "shortest"):
+            raise ValueError("order must be 'arrival' or 'shortest'")
+        self.pe = pe
+        self.keep_population = keep_population
+        self.poll_s = poll_s
+        cfg = pe.ServerConfig(int(memory_budget), max_active, tick, hv_every,
+                              pe.ORDER_SHORTEST if order == "shortest" else pe.ORDER_ARRIVAL,
+                              float(max_wait or 0.0), 1 if priority else 0)
+        h = pe.C.c_void_p()
+        pe._ck(pe.lib().pe_server_create(pe.C.byref(cfg), pe.C.byref(h)))
+        self._h = h
+        self._jobs: dict[int, Job] = {}
+        self._keep = []   # host buffers the core copies at submit (kept until then)
+        self.peak_active = 0
+        self.peak_used = 0
+        self.used = 0
+
+    def clock(self) -> float:
+        v = self.pe.C.c_double(0.0)
+        self.pe._ck(self.pe.lib().pe_server_clock(self._h, self.pe.C.byref(v)))
+        return v.value
+
+    def stats(self):
+        st = self.pe.ServerStats()
+        self.pe._ck(self.pe.lib().pe_server_get_stats(self._h, self.pe.C.byref(st)))
+        return st
+
+    def submit(self, job: Job) -> int:
+        pe = self.pe
+        aa = np.ascontiguousarray(job.aa, np.int8)
+        cfg = pe.Config(job.n_cds, job.pop_size, job.mutation_prob, job.objectives, pe.GC3, 0, job.seed, 0, 0,
+                        getattr(job, "sl_kind", 0))
+        spec = pe.JobSpec(cfg, aa.ctypes.data_as(pe.C.c_void_p), len(aa), pe.C.pointer(job.table), job.generations,
+                          job.stall, 1 if self.keep_population else 0)
+        jid = pe.C.c_int64(0)
+        pe._ck(pe.lib().pe_batch_submit(self._h, pe.C.byref(spec), pe.C.byref(jid)))
+        job.job_id = int(jid.value)
+        self._jobs[job.job_id] = job
+        return job.job_id
+
+    def cancel(self, job: Job):
+        self.pe._ck(self.pe.lib().pe_cancel(self._h, job.job_id))
+
+    def status(self, job: Job):
+        st = self.pe.JobStatus()
+        self.pe._ck(self.pe.lib().pe_poll(self._h, job.job_id, self.pe.C.byref(st)))
+        return st
+
+    def _collect(self, job: Job, st, t0: float):
+        pe = self.pe
+        job.generations_run = st.generations_run
+        job.reason = pe.REASONS.get(st.reason)
+        job.priority = st.priority
+        job.submitted = st.submitted_s - t0
+        job.start = st.started_s - t0 if st.started_s >= 0 else None
+        job.end = st.finished_s - t0
+        if st.state == pe.JOB_FAILED:
+            job.error = st.error.decode()
+        if st.state == pe.JOB_DONE:
+            M = 4 if job.objectives == pe.OBJ_BASE4 else 6
+            obj = np.zeros((job.pop_size, M), np.float32)
+            codons = np.zeros((job.pop_size, job.n_cds, len(job.aa)), np.uint8) if self.keep_population else None
+            pe._ck(pe.lib().pe_job_result(self._h, job.job_id, obj.ctypes.data_as(pe.C.c_void_p),
+                                          None if codons is None else codons.ctypes.data_as(pe.C.c_void_p)))
+            job.survivors = obj
+            job.hv = st.hypervolume
+            if codons is not None:
+                job.population = (codons, obj)
+
+    def run(self, jobs: list[Job]) -> list[Job]:
+        """Serve `jobs` with real-time arrivals (job.arrival seconds after the start);
+        returns the finished jobs in completion order."""
+        pe = self.pe
+        pending = deque(sorted(jobs, key=lambda j: j.arrival))
+        t0 = self.clock()
+        live: list[Job] = []
+        done: list[Job] = []
+        while pending or live:
+            now = self.clock() - t0
+            while pending and pending[0].arrival <= now:
+                job = pending.popleft()
+                self.submit(job)
+                live.append(job)
+            st_all = self.stats()
+            self.peak_active = max(self.peak_active, st_all.peak_active)
+            self.peak_used = max(self.peak_used, st_all.peak_used_bytes)
+            still = []
+            for job in live:
+                st = self.status(job)
+                if st.state in (pe.JOB_DONE, pe.JOB_FAILED, pe.JOB_CANCELLED):
+                    self._collect(job, st, t0)
+                    done.append(job)
+                else:
+                    still.append(job)
+            live = still
+            if pending or live:
+                wait = self.poll_s
+                if pending and not live:
+                    wait = max(0.0, pending[0].arrival - (self.clock() - t0))
+                time.sleep(min(wait, 0.05) if live else wait)
+        st_all = self.stats()
+        self.used = st_all.used_bytes
+        return done
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.pe.lib().pe_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -35,7 +35,11 @@ def _worker(rank, world, port, q):
     t = rep.max_over_ranks(1.5 + rank)
     shards = rep.shard_jobs([5, 1, 9, 3, 3, 7], world)
     seed = rep.replica_seed(2024, rank)
-    q.put((rank, t, shards, seed))
+    # end to end: each rank "runs" its shard of jobs and the results are gathered
+    costs = [5, 1, 9, 3, 3, 7]
+    mine = shards[rank]
+    gathered = rep.gather_results({j: {"rank": rank, "cost": costs[j]} for j in mine})
+    q.put((rank, t, shards, seed, gathered))
     dist.barrier()
     dist.destroy_process_group()
 
@@ -51,7 +55,10 @@ def test_two_rank_timing_and_sharding():
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    assert all(t == 2.5 for _, t, _, _ in res)                 # max over ranks
+    assert all(t == 2.5 for _, t, _, _, _ in res)              # max over ranks
+    for _, _, shards_r, _, gathered in res:                    # every rank holds every job's result once
+        assert sorted(gathered) == list(range(6))
+        assert all(gathered[j]["rank"] == r for r, s in enumerate(shards_r) for j in s)
     assert res[0][2] == res[1][2]                              # same assignment on every rank
     shards = res[0][2]
     assert sorted(i for s in shards for i in s) == list(range(6))
