@@ -560,8 +560,11 @@ def served_jobs(pe, srv_mod, master_seed: int, count: int, rate: float):
 
 
 def run_served(args):
-    """Config 5: Poisson arrivals of design jobs, served with continuous batching,
-    against the plain form (one job at a time, in arrival order) on the same jobs."""
+    """Config 5: Poisson arrivals of design jobs served by the library's serving core
+    (pe_server_*: continuous batching, footprint admission, stall retirement), against
+    the plain form (the same core with one resident job at a time, in arrival order) on
+    the first --plain-jobs jobs of the same stream, whose results must equal the served
+    ones."""
     import copy
 
     import torch
@@ -573,48 +576,46 @@ def run_served(args):
     free, _ = torch.cuda.mem_get_info()
     budget = int(free * 0.8)
     lines = {}
-    modes = (("served", 16, srv_mod.work_priority, "shortest"), ("served_all_resident", 64, None, "arrival"),
-             ("plain", 1, None, "arrival"))
-    for mode, max_active, prio, order in modes:
-        jobs = [copy.copy(j) for j in base]
-        srv = srv_mod.Server(pe, memory_budget=budget, max_active=max_active, tick=10, hv_every=25, priority=prio,
-                             order=order, max_wait=60.0)
+    n_plain = min(count, args.plain_jobs)
+    modes = (("served", base, 16, True, "shortest"), ("plain", base[:n_plain], 1, False, "arrival"))
+    for mode, jobset, max_active, prio, order in modes:
+        jobs = [copy.copy(j) for j in jobset]
+        srv = srv_mod.NativeServer(pe, memory_budget=budget, max_active=max_active, tick=10, hv_every=25,
+                                   priority=prio, order=order, max_wait=60.0)
         with ClockSampler(0) as clk:
             done = srv.run(jobs)
+        stats = srv.stats()
+        srv.close()
         st = srv_mod.latency_stats(done)
-        st["peak_active"], st["peak_gb"] = srv.peak_active, srv.peak_used / 1e9
+        st["peak_active"], st["peak_gb"] = stats.peak_active, stats.peak_used_bytes / 1e9
         st["generations"] = sum(j.generations_run for j in done)
         st["mean_hv"] = float(np.mean([j.hv for j in done if j.hv is not None]))
         st["clocks"] = clk.summary()
-        st["hv"] = {j.job_id: j.hv for j in done}
+        st["hv"] = {int(round(j.arrival * 1e9)): j.hv for j in done}
         lines[mode] = st
         if st["failed"]:
             raise RuntimeError(f"{st['failed']} jobs failed: " + "; ".join(j.error for j in done if j.error))
-    s, q, p = lines["served"], lines["served_all_resident"], lines["plain"]
-    same_hv = all(s["hv"][k] == p["hv"][k] == q["hv"][k] for k in s["hv"])
+    s, p = lines["served"], lines["plain"]
+    same_hv = all(s["hv"][k] == v for k, v in p["hv"].items())
     line = {"metric": "designs/s", "value": s["designs_per_s"], "unit": "designs/s", "n_gpus": 1,
             "steps": count, "warmup": 0, "ms_per_step": 1000.0 * s["span_s"] / count, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": {"workload": f"served: {count} Poisson arrivals at 20 jobs/s (the first {count} of the "
-                                   "2000-job stream), L log-uniform [50, 5000], m U[2,10], N in "
-                                   "{256,512,1024,2048}, G U[200,1000], stop on hypervolume stall over 50 "
-                                   "generations (checked every 25), 4 objectives, Pm=0.02",
-                       "p50_s": s["p50_s"], "p99_s": s["p99_s"], "mean_s": s["mean_s"],
-                       "plain_p50_s": p["p50_s"], "plain_p99_s": p["p99_s"],
-                       "plain_designs_per_s": p["designs_per_s"],
-                       "all_resident_p50_s": q["p50_s"], "all_resident_p99_s": q["p99_s"],
-                       "all_resident_designs_per_s": q["designs_per_s"],
-                       "host_hv_s": s["host_hv_s"], "plain_host_hv_s": p["host_hv_s"],
-                       "served_over_plain": s["designs_per_s"] / p["designs_per_s"],
-                       "stalled_jobs": s["stalled"], "generations": s["generations"],
-                       "mean_final_hv": s["mean_hv"], "same_results_as_plain": same_hv,
-                       "peak_resident_jobs": s["peak_active"], "peak_device_gb": s["peak_gb"],
-                       "memory_budget_gb": budget / 1e9,
-                       "policy": "up to 16 resident jobs, shortest estimated work admitted first (a job "
-                                 "waiting over 60 s goes first), stream priority by estimated work; "
-                                 "all_resident = up to 64 resident in arrival order, equal priorities; "
-                                 "plain = one resident job at a time in arrival order",
-                       "timing": "wall clock from each arrival to its result on the host"},
+            "config": {"workload": f"served: {count} Poisson arrivals at 20 jobs/s"
+                                   f"{'' if count == 2000 else f' (the first {count} of the 2000-job stream)'}, "
+                                   "L log-uniform [50, 5000], m U[2,10], N in {256,512,1024,2048}, G U[200,1000], "
+                                   "stop on hypervolume stall over 50 generations (checked every 25), "
+                                   "4 objectives, Pm=0.02"},
+            "p50_s": s["p50_s"], "p99_s": s["p99_s"], "mean_s": s["mean_s"],
+            "plain_jobs": n_plain, "plain_p50_s": p["p50_s"], "plain_p99_s": p["p99_s"],
+            "plain_designs_per_s": p["designs_per_s"],
+            "served_over_plain_designs_per_s": s["designs_per_s"] / p["designs_per_s"],
+            "stalled_jobs": s["stalled"], "generations": s["generations"], "mean_final_hv": s["mean_hv"],
+            "same_results_as_plain": same_hv, "peak_resident_jobs": s["peak_active"],
+            "peak_device_gb": s["peak_gb"], "memory_budget_gb": budget / 1e9,
+            "policy": "C++ serving core: up to 16 resident jobs, shortest estimated work admitted first (a job "
+                      "waiting over 60 s goes first), stream priority by estimated work; plain = the same core "
+                      "with one resident job at a time in arrival order",
+            "timing": "wall clock from each arrival to its result on the host",
             "clocks": s["clocks"], "plain_clocks": p["clocks"]}
     print(json.dumps(line), flush=True)
 
@@ -633,7 +634,9 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--workload", choices=["plain", "batched", "served"], default="plain")
     ap.add_argument("--generations", type=int, default=0, help="generations per job (batched)")
-    ap.add_argument("--jobs", type=int, default=40, help="design requests in the served workload")
+    ap.add_argument("--jobs", type=int, default=2000, help="design requests in the served workload")
+    ap.add_argument("--plain-jobs", type=int, default=200,
+                    help="served workload: jobs of the stream also run one at a time (the plain form)")
     ap.add_argument("--shape", default=None, help="plain workload L,m,N,p[,G] instead of 1000,8,1024,8,500 "
                     "(p=0: the reference's rule from N; G: generations of a design job)")
     ap.add_argument("--string", choices=["hairpin", "lrcs"], default="hairpin",

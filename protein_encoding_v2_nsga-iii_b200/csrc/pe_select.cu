@@ -410,39 +410,30 @@ __global__ void __cluster_dims__(kFrontCtas, 1, 1) __launch_bounds__(kFrontThrea
     int rc = 0, fstart = 0, fsize = 0, nfront = 0, cut = 0, f0 = 0, par = 0;
     for (int it = 0; it < N2; it++) {
         cluster.sync();  // every slice of this front is complete
-        for (int w = tid; w < words; w += nth) {
-            const int owner = w / sw, off = w - owner * sw;
-            const uint32_t *rs = cluster.map_shared_rank(slice + par * swp, owner);
-            fmask[w] = rs[off];
-        }
-        __syncthreads();
-        // exclusive prefix of the mask words' popcounts (words <= 32 * nth)
-        int carry = 0;
-        for (int base = 0; base < words; base += nth) {
-            const int w = base + tid;
-            const int v = w < words ? __popc(fmask[w]) : 0;
-            int inc = v;
+        // warp 0 assembles the whole mask from the slices and the exclusive prefix of its
+        // words' popcounts (lane l: words [l*per, l*per + per))
+        if (warp == 0) {
+            const int per = (words + 31) >> 5, w0 = lane * per;
+            int sum = 0;
+            for (int w = w0; w < min(words, w0 + per); w++) {
+                const int owner = w / sw, off = w - owner * sw;
+                const uint32_t *rs = cluster.map_shared_rank(slice + par * swp, owner);
+                const uint32_t x = rs[off];
+                fmask[w] = x;
+                wpre[w] = sum;
+                sum += __popc(x);
+            }
+            int inc = sum;
             for (int o = 1; o < 32; o <<= 1) {
                 const int y = __shfl_up_sync(0xffffffffu, inc, o);
                 if (lane >= o) inc += y;
             }
-            if (lane == 31) s_warp[warp] = inc;
-            __syncthreads();
-            if (warp == 0) {
-                int x = lane < nwarps ? s_warp[lane] : 0;
-                for (int o = 1; o < 32; o <<= 1) {
-                    const int y = __shfl_up_sync(0xffffffffu, x, o);
-                    if (lane >= o) x += y;
-                }
-                s_warp[lane] = x;  // inclusive over warps
-            }
-            __syncthreads();
-            if (w < words) wpre[w] = carry + (warp ? s_warp[warp - 1] : 0) + inc - v;
-            const int tot_here = s_warp[31];
-            __syncthreads();
-            carry += tot_here;
+            const int before = inc - sum;
+            for (int w = w0; w < min(words, w0 + per); w++) wpre[w] += before;
+            if (lane == 31) s_warp[0] = inc;
         }
-        const int tot = carry;
+        __syncthreads();
+        const int tot = s_warp[0];
         // own members of front `it`, in ascending index
         for (int w = (r0 >> 5) + tid; w < min(words, (r0 >> 5) + sw); w += nth) {
             uint32_t x = fmask[w];
@@ -472,31 +463,32 @@ __global__ void __cluster_dims__(kFrontCtas, 1, 1) __launch_bounds__(kFrontThrea
         const int nx = par ^ 1;
         for (int w = tid; w < sw; w += nth) slice[nx * swp + w] = 0u;
         __syncthreads();
-        // four rows per warp at a time, so their loads are in flight together
-        for (int q0 = warp; q0 < nrow; q0 += 4 * nwarps) {
-            const uint32_t *row[4];
-            bool act[4];
-            int dec[4];
+        // eight rows per warp at a time, so their loads are in flight together
+        for (int q0 = warp; q0 < nrow; q0 += 8 * nwarps) {
+            const uint32_t *base = sc.dom + (size_t)(r0 + q0) * words;
+            const size_t step = (size_t)nwarps * words;  // between the warp's rows u and u+1
+            unsigned act = 0u;
+            int dec[8];
 #pragma unroll
-            for (int u = 0; u < 4; u++) {
+            for (int u = 0; u < 8; u++) {
                 const int q = q0 + u * nwarps;
-                act[u] = q < nrow && npr[q] > 0;  // rows assigned already are skipped
-                row[u] = sc.dom + (size_t)(r0 + (act[u] ? q : 0)) * words;
+                if (q < nrow && npr[q] > 0) act |= 1u << u;  // rows assigned already are skipped
                 dec[u] = 0;
             }
+            if (!act) continue;
             for (int w = lane; w < words; w += 32) {
                 const uint32_t f = fmask[w];
                 if (!f) continue;
 #pragma unroll
-                for (int u = 0; u < 4; u++)
-                    if (act[u]) dec[u] += __popc(__ldg(&row[u][w]) & f);
+                for (int u = 0; u < 8; u++)
+                    if (act & (1u << u)) dec[u] += __popc(__ldg(base + u * step + w) & f);
             }
 #pragma unroll
-            for (int u = 0; u < 4; u++) {
+            for (int u = 0; u < 8; u++) {
                 int d = dec[u];
                 for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
                 const int q = q0 + u * nwarps;
-                if (lane == 0 && act[u] && d) {
+                if (lane == 0 && (act & (1u << u)) && d) {
                     const int v = npr[q] - d;
                     npr[q] = v;
                     if (v == 0) atomicOr(&slice[nx * swp + (q >> 5)], 1u << (q & 31));
