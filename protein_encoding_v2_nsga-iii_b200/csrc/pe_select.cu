@@ -85,6 +85,50 @@ __global__ void __launch_bounds__(256) k_dominance(Shape s, const float *__restr
     }
 }
 
+// The same rows, kDomRows per CTA (one warp per row), with every objective vector
+// staged once per CTA in shared memory, objective-major so the lanes of a warp read
+// 32 consecutive words: the matrix crosses L2 once per CTA instead of once per row.
+constexpr int kDomRows = 16;
+constexpr size_t kDomTiledSmemMax = 200 * 1024;  // the staged matrix must fit beside nothing else
+
+template <int MM>
+__global__ void __launch_bounds__(32 * kDomRows) k_dominance_tiled(Shape s, const float *__restrict__ obj,
+                                                                   uint32_t *__restrict__ dom,
+                                                                   int32_t *__restrict__ np)
+{
+    extern __shared__ float ot[];  // [M][N2]
+    const int M = MM > 0 ? MM : s.M;
+    const int N2 = 2 * s.N, words = (N2 + 31) >> 5;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int e = tid; e < N2 * M; e += blockDim.x) {
+        const int j = e / M, k = e - j * M;
+        ot[k * N2 + j] = obj[e];
+    }
+    __syncthreads();
+    const int i = blockIdx.x * kDomRows + warp;
+    if (i >= N2) return;
+    float oi[kMaxObj];
+#pragma unroll
+    for (int k = 0; k < (MM > 0 ? MM : kMaxObj); k++)
+        if (k < M) oi[k] = ot[k * N2 + i];
+    int cnt = 0;
+    for (int w = 0; w < words; w++) {
+        const int j = 32 * w + lane;
+        bool bit = false;
+        if (j < N2 && j != i) {
+            float oj[kMaxObj];
+#pragma unroll
+            for (int k = 0; k < (MM > 0 ? MM : kMaxObj); k++)
+                if (k < M) oj[k] = ot[k * N2 + j];
+            bit = dominates(oj, oi, M);
+        }
+        const uint32_t word = __ballot_sync(0xffffffffu, bit);
+        if (lane == 0) dom[(size_t)i * words + w] = word;
+        cnt += __popc(word);
+    }
+    if (lane == 0) np[i] = cnt;
+}
+
 // Across the lanes of a warp, lane w holding v: the smallest (largest) value, the
 // lowest lane among equal ones -- what a loop over w = 0, 1, ... keeping the first
 // strictly better value returns (including which of -0 / +0).
@@ -410,18 +454,21 @@ __global__ void __cluster_dims__(kFrontCtas, 1, 1) __launch_bounds__(kFrontThrea
     int rc = 0, fstart = 0, fsize = 0, nfront = 0, cut = 0, f0 = 0, par = 0;
     for (int it = 0; it < N2; it++) {
         cluster.sync();  // every slice of this front is complete
-        // warp 0 assembles the whole mask from the slices and the exclusive prefix of its
-        // words' popcounts (lane l: words [l*per, l*per + per))
+        // the whole mask from the slices (one remote load per thread and word), then
+        // warp 0 takes the exclusive prefix of the words' popcounts (lane l: words
+        // [l*per, l*per + per))
+        for (int w = tid; w < words; w += nth) {
+            const int owner = w / sw, off = w - owner * sw;
+            const uint32_t *rs = cluster.map_shared_rank(slice + par * swp, owner);
+            fmask[w] = rs[off];
+        }
+        __syncthreads();
         if (warp == 0) {
             const int per = (words + 31) >> 5, w0 = lane * per;
             int sum = 0;
             for (int w = w0; w < min(words, w0 + per); w++) {
-                const int owner = w / sw, off = w - owner * sw;
-                const uint32_t *rs = cluster.map_shared_rank(slice + par * swp, owner);
-                const uint32_t x = rs[off];
-                fmask[w] = x;
                 wpre[w] = sum;
-                sum += __popc(x);
+                sum += __popc(fmask[w]);
             }
             int inc = sum;
             for (int o = 1; o < 32; o <<= 1) {
@@ -874,52 +921,49 @@ __global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc
     if (tid == 0) coff[R] = sm.i0;
     // candidate lists in ascending position, one warp per reference point: the warp
     // scans the last front's members 32 at a time, and a ballot of "associated with
-    // this point" gives each member its place after the ones before it.  On the way,
-    // the nearest member of a point with niche count 0 (the first in list order among
-    // equal distances) -- its pick at level 0, which is the point's first pick
-    // whenever it has one -- is found and moved to the list's end right there (a
-    // point that ends up picking nothing never reads its list).
+    // this point" gives each member its place after the ones before it.
     const int nm = rc - count0;
     for (int j = warp; j < R; j += nwarps) {
         if (nj[j] == 0) continue;
         int *cl = cand + coff[j];
-        const bool lvl0 = cj[j] == 0;
         int run = 0;
-        uint32_t bd = 0xffffffffu;  // distance bits (>= +0, so they order as the values do)
-        int br = 0x7fffffff;        // list position of that member
-        for (int t0 = 0; t0 < nm; t0 += 32) {
+        for (int t0 = 0; t0 < nm && run < nj[j]; t0 += 32) {
             const int t = t0 + lane;
             const bool mine = t < nm && las[t] == j;
             const uint32_t bal = __ballot_sync(0xffffffffu, mine);
-            if (mine) {
-                const int r = run + __popc(bal & ((1u << lane) - 1u));
-                const int sol = lsol[t];
-                cl[r] = sol;
-                if (lvl0) {
-                    const uint32_t d = __float_as_uint(sc.dist[sol]);
-                    if (d < bd) {
-                        bd = d;
-                        br = r;
-                    }
-                }
-            }
+            if (mine) cl[run + __popc(bal & ((1u << lane) - 1u))] = lsol[t];
             run += __popc(bal);
         }
-        if (lvl0) {
-            for (int o = 16; o > 0; o >>= 1) {
-                const uint32_t od = __shfl_xor_sync(0xffffffffu, bd, o);
-                const int orr = __shfl_xor_sync(0xffffffffu, br, o);
-                if (od < bd || (od == bd && orr < br)) {
-                    bd = od;
-                    br = orr;
-                }
+    }
+    __syncthreads();
+    // the nearest member of a point with niche count 0 (the first in list order among
+    // equal distances) is its pick at level 0, which is the point's first pick whenever
+    // it has one: it is moved to the list's end here (a point that ends up picking
+    // nothing never reads its list).  One warp per point, the list read 32 at a time.
+    for (int j = warp; j < R; j += nwarps) {
+        if (nj[j] == 0 || cj[j] != 0) continue;
+        int *cl = cand + coff[j];
+        uint32_t bd = 0xffffffffu;  // distance bits (>= +0, so they order as the values do)
+        int br = 0x7fffffff;
+        for (int r = lane; r < nj[j]; r += 32) {
+            const uint32_t d = __float_as_uint(sc.dist[cl[r]]);
+            if (d < bd) {
+                bd = d;
+                br = r;
             }
-            __syncwarp();
-            if (lane == 0) {
-                const int last = nj[j] - 1, pick = cl[br];
-                cl[br] = cl[last];
-                cl[last] = pick;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const uint32_t od = __shfl_xor_sync(0xffffffffu, bd, o);
+            const int orr = __shfl_xor_sync(0xffffffffu, br, o);
+            if (od < bd || (od == bd && orr < br)) {
+                bd = od;
+                br = orr;
             }
+        }
+        if (lane == 0) {
+            const int last = nj[j] - 1, pick = cl[br];
+            cl[br] = cl[last];
+            cl[last] = pick;
         }
     }
     __syncthreads();
@@ -1048,10 +1092,28 @@ size_t select_smem_bytes(const Shape &s)
 cudaError_t launch_select(const Shape &s, const float *obj, float *ext, const float *refpts, SelectScratch sc,
                           int32_t *surv, uint32_t *d_gen, int bump_gen, cudaStream_t st)
 {
-    if (s.M == 4) k_dominance<4><<<2 * s.N, 256, 0, st>>>(s, obj, sc.dom, sc.np);
-    else if (s.M == 6) k_dominance<6><<<2 * s.N, 256, 0, st>>>(s, obj, sc.dom, sc.np);
-    else k_dominance<0><<<2 * s.N, 256, 0, st>>>(s, obj, sc.dom, sc.np);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e;
+    const size_t dsm = (size_t)2 * s.N * s.M * sizeof(float);
+    if (dsm <= kDomTiledSmemMax) {
+        const int g = (2 * s.N + kDomRows - 1) / kDomRows;
+        if (s.M == 4) {
+            if ((e = raise_smem_limit((const void *)k_dominance_tiled<4>, dsm)) != cudaSuccess) return e;
+            k_dominance_tiled<4><<<g, 32 * kDomRows, dsm, st>>>(s, obj, sc.dom, sc.np);
+        } else if (s.M == 6) {
+            if ((e = raise_smem_limit((const void *)k_dominance_tiled<6>, dsm)) != cudaSuccess) return e;
+            k_dominance_tiled<6><<<g, 32 * kDomRows, dsm, st>>>(s, obj, sc.dom, sc.np);
+        } else {
+            if ((e = raise_smem_limit((const void *)k_dominance_tiled<0>, dsm)) != cudaSuccess) return e;
+            k_dominance_tiled<0><<<g, 32 * kDomRows, dsm, st>>>(s, obj, sc.dom, sc.np);
+        }
+    } else if (s.M == 4) {
+        k_dominance<4><<<2 * s.N, 256, 0, st>>>(s, obj, sc.dom, sc.np);
+    } else if (s.M == 6) {
+        k_dominance<6><<<2 * s.N, 256, 0, st>>>(s, obj, sc.dom, sc.np);
+    } else {
+        k_dominance<0><<<2 * s.N, 256, 0, st>>>(s, obj, sc.dom, sc.np);
+    }
+    e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     const size_t fsm = fronts_smem_bytes(s);
     if ((e = raise_smem_limit((const void *)k_fronts, fsm)) != cudaSuccess) return e;
