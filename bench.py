@@ -88,8 +88,8 @@ SL_NCU = {
 }
 SM_COUNT, SMEM_WAVEFRONTS_PER_SM_CLK, ALU_WARP_INST_PER_SM_CLK = 148, 1, 2
 # kernels one generation launches (one CUDA graph replay): k_variation, k_sl, k_dominance,
-# k_select, k_assoc, k_niche
-KERNELS_PER_GENERATION = 6
+# k_fronts, k_select, k_assoc, k_niche
+KERNELS_PER_GENERATION = 7
 
 
 def load_pkg():

@@ -122,9 +122,10 @@ __host__ __device__ __forceinline__ void lrcs_pair_of(int m, int r, int &a, int 
 
 struct VarSmem {
     SmemTab tab;
-    int64_t cds_val[kMaxCds];   // per-CDS sums
-    int32_t cds_cnt[kMaxCds];
-    int32_t pair_cnt[kMaxCds * (kMaxCds - 1) / 2 > 2016 ? 2016 : kMaxCds * (kMaxCds - 1) / 2];
+    int64_t cds_val[kMaxCds];   // per-CDS sums: CAI (float bits)
+    int64_t cds_val2[kMaxCds];  // CBP sums
+    int32_t cds_cnt[kMaxCds];   // GC counts
+    int32_t cds_cnt2[kMaxCds];  // HSC counts
     float pobj[kMaxObj];
     int8_t pobjidx[2 * kMaxObj];
     int32_t ppql[3];
@@ -137,18 +138,27 @@ struct VarSmem {
 // Every objective except the hairpin stem, for the solution in smem.
 // Reference evaluators: include/utils.cuh:271-710.  Per-CDS sums are exact
 // integers (fixed-point log weights for CAI, fixed-point CPS), so the result
-// does not depend on the reduction order.
+// does not depend on the reduction order.  One pass: the warps take the per-CDS
+// and per-pair sums of every objective as one list of tasks (CAI, CBP, HSC, GC per
+// CDS; HD per CDS pair); after one barrier, one thread per objective (each in its
+// own warp) reduces over the CDSs in CDS order, as the reference's loops do.
 __device__ void light_eval(const Shape &s, const DevTables *gt, VarSmem &sm, const uint8_t *ids, const uint2 *planes,
-                           float *obj, int8_t *objidx, int tid, int nth)
+                           int32_t *pair_cnt, float *obj, int8_t *objidx, int tid, int nth)
 {
     const int warp = tid >> 5, lane = tid & 31, nwarps = nth >> 5;
     const int L = s.L, m = s.m;
     const SmemTab &st = sm.tab;
-    int slot;
-    // ---- CAI: exp(mean log w) per CDS
-    if ((slot = s.slot[K_CAI]) >= 0) {
-        for (int c = warp; c < m; c += nwarps) {
-            const uint8_t *row = ids + c * s.Lp;
+    const int sCAI = s.slot[K_CAI], sCBP = s.slot[K_CBP], sHSC = s.slot[K_HSC], sHD = s.slot[K_HD],
+              sGC = s.slot[K_GC];
+    const int npairs = m * (m - 1) / 2;
+    // task list: [0, m) CAI, [m, 2m) CBP, [2m, 3m) HSC, [3m, 4m) GC, then the HD pairs
+    const int ntask = 4 * m + (sHD >= 0 ? npairs : 0);
+    for (int task = warp; task < ntask; task += nwarps) {
+        const int kind = task < 4 * m ? task / m : 4;
+        const int c = task < 4 * m ? task - kind * m : 0;
+        const uint8_t *row = ids + c * s.Lp;
+        if (kind == 0) {  // CAI: exp(mean log w)
+            if (sCAI < 0) continue;
             long long S = 0;
             int z = 0;
             for (int a = lane; a < L; a += 32) {
@@ -163,124 +173,25 @@ __device__ void light_eval(const Shape &s, const DevTables *gt, VarSmem &sm, con
                 float cai = z ? 0.0f : (float)det_exp(x);
                 sm.cds_val[c] = (int64_t)__float_as_int(cai);
             }
-        }
-        __syncthreads();
-        if (tid == 0) {
-            float best = 0.0f;
-            int bi = 0;
-            for (int c = 0; c < m; c++) {
-                float v = -__int_as_float((int)sm.cds_val[c]);
-                if (c == 0 || v >= best) {
-                    best = v;
-                    bi = c;
-                }
-            }
-            obj[slot] = best;
-            objidx[2 * slot] = (int8_t)bi;
-            objidx[2 * slot + 1] = 0;
-        }
-        __syncthreads();
-    }
-    // ---- CBP: mean codon-pair score over pairs a in [0, L-3]
-    if ((slot = s.slot[K_CBP]) >= 0) {
-        for (int c = warp; c < m; c += nwarps) {
-            const uint8_t *row = ids + c * s.Lp;
+        } else if (kind == 1) {  // CBP: codon-pair score sum over pairs a in [0, L-3]
+            if (sCBP < 0) continue;
             long long S = 0;
             for (int a = lane; a < L - 2; a += 32) {
                 int c1 = row[a], c2 = row[a + 1];
                 if (c1 < 61 && c2 < 61) S += __ldg(&gt->cpsf[c1 * 61 + c2]);
             }
             S = warp_sum(S);
-            if (lane == 0) sm.cds_val[c] = S;
-        }
-        __syncthreads();
-        if (tid == 0) {
-            float best = 0.0f;
-            int bi = 0;
-            for (int c = 0; c < m; c++) {
-                double x = __ddiv_rn(__dmul_rn((double)sm.cds_val[c], 1.0 / 4294967296.0), (double)(L - 2));
-                float v = -(float)x;
-                if (c == 0 || v >= best) {
-                    best = v;
-                    bi = c;
-                }
-            }
-            obj[slot] = best;
-            objidx[2 * slot] = (int8_t)bi;
-            objidx[2 * slot + 1] = 0;
-        }
-        __syncthreads();
-    }
-    // ---- HSC: hidden stop codons in the +1/+2 frames per boundary
-    if ((slot = s.slot[K_HSC]) >= 0) {
-        for (int c = warp; c < m; c += nwarps) {
-            const uint8_t *row = ids + c * s.Lp;
+            if (lane == 0) sm.cds_val2[c] = S;
+        } else if (kind == 2) {  // HSC: hidden stop codons in the +1/+2 frames per boundary
+            if (sHSC < 0) continue;
             int cnt = 0;
             for (int a = lane; a < L - 1; a += 32) cnt += __ldg(&gt->hsc[row[a] * 64 + row[a + 1]]);
             cnt = warp_sum(cnt);
-            if (lane == 0) sm.cds_cnt[c] = cnt;
-        }
-        __syncthreads();
-        if (tid == 0) {
-            float best = 0.0f;
-            int bi = 0;
-            for (int c = 0; c < m; c++) {
-                float v = -__fdiv_rn((float)sm.cds_cnt[c], (float)(L - 1));
-                if (c == 0 || v >= best) {
-                    best = v;
-                    bi = c;
-                }
-            }
-            obj[slot] = best;
-            objidx[2 * slot] = (int8_t)bi;
-            objidx[2 * slot + 1] = 0;
-        }
-        __syncthreads();
-    }
-    // ---- HD: nucleotide mismatches over CDS pairs (i<j), XOR/popcount of planes
-    if ((slot = s.slot[K_HD]) >= 0) {
-        const int npairs = m * (m - 1) / 2;
-        for (int pi = warp; pi < npairs; pi += nwarps) {
-            int i = 0, rem = pi;
-            while (rem >= m - 1 - i) {
-                rem -= m - 1 - i;
-                i++;
-            }
-            int j = i + 1 + rem;
-            const uint2 *A = planes + i * s.Wp, *B = planes + j * s.Wp;
-            int cnt = 0;
-            for (int w = lane; w < s.W; w += 32) {
-                uint2 x = A[w], y = B[w];
-                cnt += __popc((x.x ^ y.x) | (x.y ^ y.y));
-            }
-            cnt = warp_sum(cnt);
-            if (lane == 0) sm.pair_cnt[pi] = cnt;
-        }
-        __syncthreads();
-        if (tid == 0) {
-            float best = 0.0f;
-            int bi = 0, bj = 1, pi = 0;
-            for (int i = 0; i < m - 1; i++)
-                for (int j = i + 1; j < m; j++, pi++) {
-                    float v = -__fdiv_rn((float)sm.pair_cnt[pi], (float)s.n);
-                    if (pi == 0 || v >= best) {
-                        best = v;
-                        bi = i;
-                        bj = j;
-                    }
-                }
-            obj[slot] = best;
-            objidx[2 * slot] = (int8_t)bi;
-            objidx[2 * slot + 1] = (int8_t)bj;
-        }
-        __syncthreads();
-    }
-    // ---- GC3 (or whole-CDS GC) deviation from the reference fraction
-    if ((slot = s.slot[K_GC]) >= 0) {
-        for (int c = warp; c < m; c += nwarps) {
+            if (lane == 0) sm.cds_cnt2[c] = cnt;
+        } else if (kind == 3) {  // GC3 (or whole-CDS GC) count
+            if (sGC < 0) continue;
             int cnt = 0;
             if (s.gcmode == PE_GC3) {
-                const uint8_t *row = ids + c * s.Lp;
                 for (int a = lane; a < L; a += 32) cnt += st.gc3[row[a]];
             } else {
                 const uint2 *A = planes + c * s.Wp;
@@ -288,32 +199,109 @@ __device__ void light_eval(const Shape &s, const DevTables *gt, VarSmem &sm, con
             }
             cnt = warp_sum(cnt);
             if (lane == 0) sm.cds_cnt[c] = cnt;
+        } else {  // HD: nucleotide mismatches of CDS pair pi (i<j), XOR/popcount of planes
+            const int pi = task - 4 * m;
+            int i = 0, rem = pi;
+            while (rem >= m - 1 - i) {
+                rem -= m - 1 - i;
+                i++;
+            }
+            const int j = i + 1 + rem;
+            const uint2 *A = planes + i * s.Wp, *B = planes + j * s.Wp;
+            int cnt = 0;
+            for (int w = lane; w < s.W; w += 32) {
+                uint2 x = A[w], y = B[w];
+                cnt += __popc((x.x ^ y.x) | (x.y ^ y.y));
+            }
+            cnt = warp_sum(cnt);
+            if (lane == 0) pair_cnt[pi] = cnt;
         }
-        __syncthreads();
-        if (tid == 0) {
-            float best = 0.0f;
-            int bi = 0, dir = 1;
-            for (int c = 0; c < m; c++) {
-                float dev, diff;
-                if (s.gcmode == PE_GC3) {
-                    diff = __fsub_rn(__fdiv_rn((float)sm.cds_cnt[c], (float)L), gt->ref_gc3);
-                    dev = fabsf(diff);
-                } else {
-                    float refGC = __fmul_rn((float)s.n, gt->ref_gc);
-                    diff = __fsub_rn((float)sm.cds_cnt[c], refGC);
-                    dev = __fdiv_rn(fabsf(diff), refGC);
-                }
-                if (c == 0 || dev >= best) {
-                    best = dev;
-                    bi = c;
-                    dir = diff < 0.0f ? 1 : -1;
+    }
+    __syncthreads();
+    // the reductions over CDSs, one objective per warp (lane 0), in CDS order; the
+    // last CDS reaching the extreme wins (the reference's `>=`)
+    if (lane != 0) return;
+    if (warp == 0 && sCAI >= 0) {
+        float best = 0.0f;
+        int bi = 0;
+        for (int c = 0; c < m; c++) {
+            float v = -__int_as_float((int)sm.cds_val[c]);
+            if (c == 0 || v >= best) {
+                best = v;
+                bi = c;
+            }
+        }
+        obj[sCAI] = best;
+        objidx[2 * sCAI] = (int8_t)bi;
+        objidx[2 * sCAI + 1] = 0;
+    }
+    if (warp == 1 % nwarps && sCBP >= 0) {
+        float best = 0.0f;
+        int bi = 0;
+        for (int c = 0; c < m; c++) {
+            double x = __ddiv_rn(__dmul_rn((double)sm.cds_val2[c], 1.0 / 4294967296.0), (double)(L - 2));
+            float v = -(float)x;
+            if (c == 0 || v >= best) {
+                best = v;
+                bi = c;
+            }
+        }
+        obj[sCBP] = best;
+        objidx[2 * sCBP] = (int8_t)bi;
+        objidx[2 * sCBP + 1] = 0;
+    }
+    if (warp == 2 % nwarps && sHSC >= 0) {
+        float best = 0.0f;
+        int bi = 0;
+        for (int c = 0; c < m; c++) {
+            float v = -__fdiv_rn((float)sm.cds_cnt2[c], (float)(L - 1));
+            if (c == 0 || v >= best) {
+                best = v;
+                bi = c;
+            }
+        }
+        obj[sHSC] = best;
+        objidx[2 * sHSC] = (int8_t)bi;
+        objidx[2 * sHSC + 1] = 0;
+    }
+    if (warp == 3 % nwarps && sHD >= 0) {
+        float best = 0.0f;
+        int bi = 0, bj = 1, pi = 0;
+        for (int i = 0; i < m - 1; i++)
+            for (int j = i + 1; j < m; j++, pi++) {
+                float v = -__fdiv_rn((float)pair_cnt[pi], (float)s.n);
+                if (pi == 0 || v >= best) {
+                    best = v;
+                    bi = i;
+                    bj = j;
                 }
             }
-            obj[slot] = best;
-            objidx[2 * slot] = (int8_t)bi;
-            objidx[2 * slot + 1] = (int8_t)dir;
+        obj[sHD] = best;
+        objidx[2 * sHD] = (int8_t)bi;
+        objidx[2 * sHD + 1] = (int8_t)bj;
+    }
+    if (warp == 4 % nwarps && sGC >= 0) {
+        float best = 0.0f;
+        int bi = 0, dir = 1;
+        for (int c = 0; c < m; c++) {
+            float dev, diff;
+            if (s.gcmode == PE_GC3) {
+                diff = __fsub_rn(__fdiv_rn((float)sm.cds_cnt[c], (float)L), gt->ref_gc3);
+                dev = fabsf(diff);
+            } else {
+                float refGC = __fmul_rn((float)s.n, gt->ref_gc);
+                diff = __fsub_rn((float)sm.cds_cnt[c], refGC);
+                dev = __fdiv_rn(fabsf(diff), refGC);
+            }
+            if (c == 0 || dev >= best) {
+                best = dev;
+                bi = c;
+                dir = diff < 0.0f ? 1 : -1;
+            }
         }
-        __syncthreads();
+        obj[sGC] = best;
+        objidx[2 * sGC] = (int8_t)bi;
+        objidx[2 * sGC + 1] = (int8_t)dir;
     }
 }
 
@@ -655,6 +643,8 @@ __global__ void __launch_bounds__(kVarThreads) k_variation(Shape s, const DevTab
     int8_t *aa = reinterpret_cast<int8_t *>(planes + (size_t)s.m * s.Wp);
     // MODE_MUTATE: plane words the mutation touched (bit c * Wp + w)
     uint32_t *dirty = reinterpret_cast<uint32_t *>(aa + ((s.L + 15) & ~15));
+    // HD mismatch counts of the m(m-1)/2 CDS pairs
+    int32_t *pair_cnt = reinterpret_cast<int32_t *>(dirty + (s.m * s.Wp + 31) / 32);
 
     const int tid = threadIdx.x, nth = blockDim.x;
     const int i = blockIdx.x;
@@ -795,14 +785,15 @@ __global__ void __launch_bounds__(kVarThreads) k_variation(Shape s, const DevTab
         const uint4 *ps = reinterpret_cast<const uint4 *>(planes);
         for (size_t e = tid; e < sol_words / 2; e += nth) pd[e] = ps[e];
     }
-    light_eval(s, gt, sm, ids, planes, dst.obj + (size_t)out_slot * s.M, dst.objidx + (size_t)out_slot * 2 * s.M, tid,
-               nth);
+    light_eval(s, gt, sm, ids, planes, pair_cnt, dst.obj + (size_t)out_slot * s.M,
+               dst.objidx + (size_t)out_slot * 2 * s.M, tid, nth);
 }
 
 size_t var_smem_bytes(const Shape &s)
 {
     return ((sizeof(VarSmem) + 15) & ~size_t(15)) + (size_t)s.m * s.Lp + (size_t)s.m * s.Wp * sizeof(uint2) +
-           (size_t)((s.L + 15) & ~15) + (size_t)((s.m * s.Wp + 31) / 32) * sizeof(uint32_t);
+           (size_t)((s.L + 15) & ~15) + (size_t)((s.m * s.Wp + 31) / 32) * sizeof(uint32_t) +
+           (size_t)(s.m * (s.m - 1) / 2) * sizeof(int32_t);
 }
 
 cudaError_t raise_smem_limit(const void *func, size_t bytes)

@@ -919,53 +919,58 @@ __global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc
         __syncthreads();
     }
     if (tid == 0) coff[R] = sm.i0;
-    // candidate lists in ascending position, one warp per reference point: the warp
-    // scans the last front's members 32 at a time, and a ballot of "associated with
-    // this point" gives each member its place after the ones before it.
+    // candidate lists in ascending position: one warp walks the last front's members
+    // in order, 32 at a time; __match_any_sync groups the lanes of the same point,
+    // each lane's place is its point's fill so far plus the lanes of its group below
+    // it, and the group's lowest lane advances the fill (kq counts it).  las[t] then
+    // holds the member's place in the lists.
     const int nm = rc - count0;
-    for (int j = warp; j < R; j += nwarps) {
-        if (nj[j] == 0) continue;
-        int *cl = cand + coff[j];
-        int run = 0;
-        for (int t0 = 0; t0 < nm && run < nj[j]; t0 += 32) {
+    if (warp == 0) {
+        for (int t0 = 0; t0 < nm; t0 += 32) {
             const int t = t0 + lane;
-            const bool mine = t < nm && las[t] == j;
-            const uint32_t bal = __ballot_sync(0xffffffffu, mine);
-            if (mine) cl[run + __popc(bal & ((1u << lane) - 1u))] = lsol[t];
-            run += __popc(bal);
+            const int j = t < nm ? las[t] : -1 - lane;  // lanes past the end match nobody
+            const unsigned peers = __match_any_sync(0xffffffffu, j);
+            if (t < nm) {
+                const int leader = __ffs(peers) - 1;
+                const int below = __popc(peers & ((1u << lane) - 1u));
+                const int pos = coff[j] + kq[j] + below;
+                cand[pos] = lsol[t];
+                las[t] = pos;
+                __syncwarp(peers);
+                if (lane == leader) kq[j] += __popc(peers);
+            }
+            __syncwarp();
         }
     }
     __syncthreads();
     // the nearest member of a point with niche count 0 (the first in list order among
     // equal distances) is its pick at level 0, which is the point's first pick whenever
-    // it has one: it is moved to the list's end here (a point that ends up picking
-    // nothing never reads its list).  One warp per point, the list read 32 at a time.
-    for (int j = warp; j < R; j += nwarps) {
-        if (nj[j] == 0 || cj[j] != 0) continue;
-        int *cl = cand + coff[j];
-        uint32_t bd = 0xffffffffu;  // distance bits (>= +0, so they order as the values do)
-        int br = 0x7fffffff;
-        for (int r = lane; r < nj[j]; r += 32) {
-            const uint32_t d = __float_as_uint(sc.dist[cl[r]]);
-            if (d < bd) {
-                bd = d;
-                br = r;
-            }
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            const uint32_t od = __shfl_xor_sync(0xffffffffu, bd, o);
-            const int orr = __shfl_xor_sync(0xffffffffu, br, o);
-            if (od < bd || (od == bd && orr < br)) {
-                bd = od;
-                br = orr;
-            }
-        }
-        if (lane == 0) {
-            const int last = nj[j] - 1, pick = cl[br];
-            cl[br] = cl[last];
+    // it has one: found with two atomicMin passes over the members (distance bits,
+    // then place) and moved to the list's end (a point that ends up picking nothing
+    // never reads its list).  pofs and kq serve as scratch.
+    for (int j = tid; j < R; j += nth) {
+        pofs[j] = 0x7fffffff;
+        kq[j] = 0x7fffffff;
+    }
+    __syncthreads();
+    for (int t = tid; t < nm; t += nth) {
+        const int j = sc.assoc[count0 + t];
+        // distances are >= +0 (or FLT_MAX), so their bits order as the values do
+        if (cj[j] == 0) atomicMin(&pofs[j], __float_as_int(sc.dist[lsol[t]]));
+    }
+    __syncthreads();
+    for (int t = tid; t < nm; t += nth) {
+        const int j = sc.assoc[count0 + t];
+        if (cj[j] == 0 && __float_as_int(sc.dist[lsol[t]]) == pofs[j]) atomicMin(&kq[j], las[t] - coff[j]);
+    }
+    __syncthreads();
+    for (int j = tid; j < R; j += nth)
+        if (cj[j] == 0 && nj[j] > 0) {
+            int *cl = cand + coff[j];
+            const int slot = kq[j], last = nj[j] - 1, pick = cl[slot];
+            cl[slot] = cl[last];
             cl[last] = pick;
         }
-    }
     __syncthreads();
     // active points per level, then picks before each level: lv[l] = picks at levels < l
     if (tid == 0) {
