@@ -158,6 +158,7 @@ struct pe_instance {
     float *d_ref = nullptr;
     PopBuf buf[2]{};
     int32_t *d_surv = nullptr;
+    int32_t *d_order = nullptr;  // [2][N] CTA order of the variation kernel, by generation parity
     SelectScratch sc{};
     int2 *d_part = nullptr;
     int32_t *d_counter = nullptr;
@@ -199,12 +200,14 @@ int alloc_pop(pe_instance *in, PopBuf &b, int nsol)
     if ((rc = in->alloc(&b.objidx, (size_t)nsol * 2 * s.M))) return rc;
     if ((rc = in->alloc(&b.pql, (size_t)nsol * 3))) return rc;
     if ((rc = in->alloc(&b.cds, (size_t)nsol * s.nres))) return rc;
+    if ((rc = in->alloc(&b.aux, (size_t)nsol * s.naux))) return rc;
     CK(cudaMemsetAsync(b.ids, 0, (size_t)nsol * s.m * s.Lp, in->stream));
     CK(cudaMemsetAsync(b.planes, 0, (size_t)nsol * s.m * s.Wp * sizeof(uint2), in->stream));
     CK(cudaMemsetAsync(b.obj, 0, (size_t)nsol * s.M * sizeof(float), in->stream));
     CK(cudaMemsetAsync(b.objidx, 0, (size_t)nsol * 2 * s.M, in->stream));
     CK(cudaMemsetAsync(b.pql, 0, (size_t)nsol * 3 * sizeof(int32_t), in->stream));
     CK(cudaMemsetAsync(b.cds, 0xff, (size_t)nsol * s.nres * sizeof(int2), in->stream));  // x = -1: to scan
+    CK(cudaMemsetAsync(b.aux, 0, (size_t)nsol * s.naux * sizeof(int32_t), in->stream));
     return PE_OK;
 }
 
@@ -261,7 +264,7 @@ cudaError_t enqueue_generation(pe_instance *in, int src)
     cudaError_t e = mark(in, 0);
     if (e != cudaSuccess) return e;
     e = launch_mutate(s, in->d_tab, in->d_aa, in->buf[src], in->buf[dst], in->d_surv, nullptr, s.N, 0, s.N, in->d_gen,
-                      nullptr, in->stream);
+                      nullptr, in->d_order, in->stream);
     if (e != cudaSuccess) return e;
     if ((e = mark(in, 1)) != cudaSuccess) return e;
     e = launch_sl(s, in->buf[dst], s.N, s.N, in->d_part, in->d_counter, in->d_status, in->stream, in->d_scanned);
@@ -389,6 +392,7 @@ int pe_create(const pe_config *cfg, const int8_t *aa_idx, int32_t aa_len, const 
     s.sl_threads = cfg->sl_threads;
     s.sl_kind = cfg->sl_kind;
     s.nres = s.sl_kind == PE_SL_LRCS ? m * (m + 1) / 2 : m;
+    s.naux = AUX_HD(m) + m * (m - 1) / 2;
     {
         static const int ref6[6] = {K_CAI, K_CBP, K_HSC, K_HD, K_GC, K_SL};
         static const int base4[4] = {K_CAI, K_HD, K_GC, K_SL};
@@ -489,6 +493,7 @@ int pe_create(const pe_config *cfg, const int8_t *aa_idx, int32_t aa_len, const 
         if ((rc = alloc_pop(in, in->buf[b], 2 * N))) return cleanup(rc);
     const int N2 = 2 * N, words = (N2 + 31) / 32;
     if ((rc = in->alloc(&in->d_surv, (size_t)N))) return cleanup(rc);
+    if ((rc = in->alloc(&in->d_order, (size_t)2 * N))) return cleanup(rc);
     if ((rc = in->alloc(&in->sc.dom, (size_t)N2 * words))) return cleanup(rc);
     if ((rc = in->alloc(&in->sc.np, (size_t)N2))) return cleanup(rc);
     if ((rc = in->alloc(&in->sc.front, (size_t)N2))) return cleanup(rc);
@@ -496,10 +501,8 @@ int pe_create(const pe_config *cfg, const int8_t *aa_idx, int32_t aa_len, const 
     if ((rc = in->alloc(&in->sc.assoc, (size_t)N2))) return cleanup(rc);
     if ((rc = in->alloc(&in->sc.dist, (size_t)N2))) return cleanup(rc);
     if ((rc = in->alloc(&in->sc.rho, (size_t)s.R))) return cleanup(rc);
-    if ((rc = in->alloc(&in->sc.fill, (size_t)s.R))) return cleanup(rc);
     if ((rc = in->alloc(&in->sc.ncand, (size_t)s.R))) return cleanup(rc);
-    if ((rc = in->alloc(&in->sc.coff, (size_t)s.R + 1))) return cleanup(rc);
-    if ((rc = in->alloc(&in->sc.cand, (size_t)N2))) return cleanup(rc);
+    if ((rc = in->alloc(&in->sc.trank, (size_t)N2 + s.M))) return cleanup(rc);
     if ((rc = in->alloc(&in->sc.info, 8))) return cleanup(rc);
     if ((rc = in->alloc(&in->sc.finfo, 3 * PE_MAX_OBJ))) return cleanup(rc);
     if ((rc = in->alloc(&in->d_part, (size_t)N2 * s.nres))) return cleanup(rc);
@@ -510,6 +513,10 @@ int pe_create(const pe_config *cfg, const int8_t *aa_idx, int32_t aa_len, const 
     if ((rc = in->alloc(&in->d_gen, 1))) return cleanup(rc);
     std::vector<float> ref((size_t)s.R * s.M);
     das_dennis(s.M, p, ref.data());
+    std::vector<uint32_t> trank((size_t)N2 + s.M);
+    tree_order_ranks(N2 + s.M, trank.data());
+    std::vector<int32_t> ident((size_t)N2);  // both halves of d_order: children in index order
+    for (int k = 0; k < N2; k++) ident[(size_t)k] = k % N;
     cudaStream_t st = in->stream;
 #define CKC(call)                                                                                   \
     do {                                                                                            \
@@ -519,6 +526,8 @@ int pe_create(const pe_config *cfg, const int8_t *aa_idx, int32_t aa_len, const 
     CKC(cudaMemcpyAsync(in->d_tab, &ht, sizeof ht, cudaMemcpyHostToDevice, st));
     CKC(cudaMemcpyAsync(in->d_aa, aa_idx, (size_t)L, cudaMemcpyHostToDevice, st));
     CKC(cudaMemcpyAsync(in->d_ref, ref.data(), ref.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+    CKC(cudaMemcpyAsync(in->sc.trank, trank.data(), trank.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    CKC(cudaMemcpyAsync(in->d_order, ident.data(), ident.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
     CKC(cudaMemsetAsync(in->d_counter, 0, (size_t)N2 * sizeof(int32_t), st));
     CKC(cudaMemsetAsync(in->d_scanned, 0, 2 * sizeof(unsigned long long), st));
     CKC(cudaMemsetAsync(in->d_status, 0, sizeof(int32_t), st));
@@ -740,10 +749,11 @@ int pe_instance_bytes(const pe_config *cfg, int32_t aa_len, uint64_t *bytes)
     auto r = [](uint64_t b) { return (b + 511) & ~uint64_t(511); };  // allocation granularity
     uint64_t t = r(sizeof(DevTables)) + r(L) + r(R * M * 4);
     t += 2 * (r(N2 * m * Lp) + r(N2 * m * Wp * 8) + r(N2 * M * 4) + r(N2 * 2 * M) + r(N2 * 12));
-    t += r(N * 4) + r(N2 * words * 4) + 6 * r(N2 * 4) + 3 * r(R * 4) + r((R + 1) * 4) + r(32) + r(72);
+    t += r(N * 4) + r(N2 * 4) + r(N2 * words * 4) + 5 * r(N2 * 4) + 2 * r(R * 4) + r((N2 + M) * 4) + r(32) + r(72);
     const uint64_t nres = cfg->sl_kind == PE_SL_LRCS ? m * (m + 1) / 2 : m;
     t += r(N2 * nres * 8) + r(N2 * 4) + r(4) + r(M * M * 4) + r(4);
     t += 2 * r(N2 * nres * 8) + r(16);  // per-CDS (per-pair) string results of both buffers, scan counts
+    t += 2 * r(N2 * (5 * m + m * (m - 1) / 2) * 4);  // per-CDS sums of the light objectives, both buffers
     *bytes = t;
     return PE_OK;
 }
@@ -973,7 +983,7 @@ int pe_mutate(pe_instance *in, uint32_t generation, const int32_t *idx, int32_t 
     CK(cudaMemcpyAsync(d_par, ident.data(), (size_t)n * sizeof(int32_t), cudaMemcpyHostToDevice, in->stream));
     CK(cudaMemcpyAsync(d_idx, idx, (size_t)n * sizeof(int32_t), cudaMemcpyHostToDevice, in->stream));
     CK(cudaMemcpyAsync(d_g, &generation, sizeof(uint32_t), cudaMemcpyHostToDevice, in->stream));
-    CK(launch_mutate(s, in->d_tab, in->d_aa, src, dst, d_par, d_idx, n, -1, 0, d_g, d_ops, in->stream));
+    CK(launch_mutate(s, in->d_tab, in->d_aa, src, dst, d_par, d_idx, n, -1, 0, d_g, d_ops, nullptr, in->stream));
     if (children)
         CK(cudaMemcpy2DAsync(children, (size_t)s.L, dst.ids, (size_t)s.Lp, (size_t)s.L, (size_t)n * s.m,
                              cudaMemcpyDeviceToHost, in->stream));

@@ -122,10 +122,6 @@ __host__ __device__ __forceinline__ void lrcs_pair_of(int m, int r, int &a, int 
 
 struct VarSmem {
     SmemTab tab;
-    int64_t cds_val[kMaxCds];   // per-CDS sums: CAI (float bits)
-    int64_t cds_val2[kMaxCds];  // CBP sums
-    int32_t cds_cnt[kMaxCds];   // GC counts
-    int32_t cds_cnt2[kMaxCds];  // HSC counts
     float pobj[kMaxObj];
     int8_t pobjidx[2 * kMaxObj];
     int32_t ppql[3];
@@ -135,78 +131,145 @@ struct VarSmem {
     unsigned long long changed;  // CDSs whose planes the mutation changed (bit c)
 };
 
-// Every objective except the hairpin stem, for the solution in smem.
+// Across a warp whose lanes hold (value, index) with index -1 for none: the largest
+// value, the highest index among equal ones, left in every lane; returns the lane
+// that held it.  Values are never NaN.
+__device__ __forceinline__ int warp_last_max(float &v, int &idx)
+{
+    int src = threadIdx.x & 31;
+    for (int o = 16; o > 0; o >>= 1) {
+        const float ov = __shfl_xor_sync(0xffffffffu, v, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, idx, o), os = __shfl_xor_sync(0xffffffffu, src, o);
+        if (oi >= 0 && (idx < 0 || ov > v || (ov == v && oi > idx))) {
+            v = ov;
+            idx = oi;
+            src = os;
+        }
+    }
+    return src;
+}
+
+// the same for the smallest count, the highest index among equal ones
+__device__ __forceinline__ void warp_last_min(int &v, int &idx)
+{
+    for (int o = 16; o > 0; o >>= 1) {
+        const int ov = __shfl_xor_sync(0xffffffffu, v, o), oi = __shfl_xor_sync(0xffffffffu, idx, o);
+        if (oi >= 0 && (idx < 0 || ov < v || (ov == v && oi > idx))) {
+            v = ov;
+            idx = oi;
+        }
+    }
+}
+
+// index of the k-th set bit (k from 0) of a nonzero mask
+__device__ __forceinline__ int nth_set_bit(unsigned long long mask, int k)
+{
+    for (int i = 0; i < k; i++) mask &= mask - 1ull;
+    return __ffsll((long long)mask) - 1;
+}
+
+// Every objective except the string objective, for the solution in smem.
 // Reference evaluators: include/utils.cuh:271-710.  Per-CDS sums are exact
 // integers (fixed-point log weights for CAI, fixed-point CPS), so the result
-// does not depend on the reduction order.  One pass: the warps take the per-CDS
-// and per-pair sums of every objective as one list of tasks (CAI, CBP, HSC, GC per
-// CDS; HD per CDS pair); after one barrier, one thread per objective (each in its
-// own warp) reduces over the CDSs in CDS order, as the reference's loops do.
-__device__ void light_eval(const Shape &s, const DevTables *gt, VarSmem &sm, const uint8_t *ids, const uint2 *planes,
-                           int32_t *pair_cnt, float *obj, int8_t *objidx, int tid, int nth)
+// does not depend on the reduction order.
+//
+// The per-CDS (per-pair) sums sit in `ax` in the aux layout (AUX_* offsets): CAI
+// value bits, CBP sum halves, HSC count, GC count per CDS, then the HD count of
+// every CDS pair.  Only the CDSs in `changed` (and the pairs touching one) are
+// summed; the others are taken from the parent's aux `pax`, bit for bit what the
+// sums give for an unchanged CDS (pax == nullptr: `changed` holds every CDS).  The
+// warps share one list of tasks: for each changed CDS, one per enabled per-CDS
+// objective, then its HD pairs.  After one barrier the sums go to `cax` (the
+// child's aux) and one thread per objective (each in its own warp) reduces over the
+// CDSs in CDS order, as the reference's loops do.
+__device__ void light_eval(const Shape &s, const DevTables *gt, const SmemTab &st, const uint8_t *ids,
+                           const uint2 *planes, int32_t *ax, unsigned long long changed, const int32_t *pax,
+                           int32_t *cax, float *obj, int8_t *objidx, int tid, int nth)
 {
     const int warp = tid >> 5, lane = tid & 31, nwarps = nth >> 5;
     const int L = s.L, m = s.m;
-    const SmemTab &st = sm.tab;
     const int sCAI = s.slot[K_CAI], sCBP = s.slot[K_CBP], sHSC = s.slot[K_HSC], sHD = s.slot[K_HD],
               sGC = s.slot[K_GC];
     const int npairs = m * (m - 1) / 2;
-    // task list: [0, m) CAI, [m, 2m) CBP, [2m, 3m) HSC, [3m, 4m) GC, then the HD pairs
-    const int ntask = 4 * m + (sHD >= 0 ? npairs : 0);
-    for (int task = warp; task < ntask; task += nwarps) {
-        const int kind = task < 4 * m ? task / m : 4;
-        const int c = task < 4 * m ? task - kind * m : 0;
-        const uint8_t *row = ids + c * s.Lp;
-        if (kind == 0) {  // CAI: exp(mean log w)
-            if (sCAI < 0) continue;
-            long long S = 0;
-            int z = 0;
-            for (int a = lane; a < L; a += 32) {
-                int id = row[a];
-                S += st.lw[id];
-                z |= st.wzero[id];
-            }
-            S = warp_sum(S);
-            z = __any_sync(0xffffffffu, z);
-            if (lane == 0) {
-                double x = __ddiv_rn(__dmul_rn((double)S, 1.0 / 4294967296.0), (double)L);
-                float cai = z ? 0.0f : (float)det_exp(x);
-                sm.cds_val[c] = (int64_t)__float_as_int(cai);
-            }
-        } else if (kind == 1) {  // CBP: codon-pair score sum over pairs a in [0, L-3]
-            if (sCBP < 0) continue;
-            long long S = 0;
-            for (int a = lane; a < L - 2; a += 32) {
-                int c1 = row[a], c2 = row[a + 1];
-                if (c1 < 61 && c2 < 61) S += __ldg(&gt->cpsf[c1 * 61 + c2]);
-            }
-            S = warp_sum(S);
-            if (lane == 0) sm.cds_val2[c] = S;
-        } else if (kind == 2) {  // HSC: hidden stop codons in the +1/+2 frames per boundary
-            if (sHSC < 0) continue;
-            int cnt = 0;
-            for (int a = lane; a < L - 1; a += 32) cnt += __ldg(&gt->hsc[row[a] * 64 + row[a + 1]]);
-            cnt = warp_sum(cnt);
-            if (lane == 0) sm.cds_cnt2[c] = cnt;
-        } else if (kind == 3) {  // GC3 (or whole-CDS GC) count
-            if (sGC < 0) continue;
-            int cnt = 0;
-            if (s.gcmode == PE_GC3) {
-                for (int a = lane; a < L; a += 32) cnt += st.gc3[row[a]];
+    // the enabled per-CDS objectives, 2 bits each
+    int kp = 0, K = 0;
+    if (sCAI >= 0) kp |= 0 << (2 * K++);
+    if (sCBP >= 0) kp |= 1 << (2 * K++);
+    if (sHSC >= 0) kp |= 2 << (2 * K++);
+    if (sGC >= 0) kp |= 3 << (2 * K++);
+    const int nch = __popcll(changed);
+    const int ncds_tasks = K * nch;
+    const int ntask = ncds_tasks + (sHD >= 0 ? nch * (m - 1) : 0);
+    if (pax) {
+        const int nax = AUX_HD(m) + (sHD >= 0 ? npairs : 0);
+        for (int e = tid; e < nax; e += nth) {
+            bool keep;
+            if (e < AUX_HD(m)) {
+                keep = !((changed >> (e % m)) & 1ull);
             } else {
-                const uint2 *A = planes + c * s.Wp;
-                for (int w = lane; w < s.W; w += 32) cnt += __popc(A[w].x ^ A[w].y);
+                int i = 0, rem = e - AUX_HD(m);
+                while (rem >= m - 1 - i) {
+                    rem -= m - 1 - i;
+                    i++;
+                }
+                keep = !(((changed >> i) | (changed >> (i + 1 + rem))) & 1ull);
             }
-            cnt = warp_sum(cnt);
-            if (lane == 0) sm.cds_cnt[c] = cnt;
-        } else {  // HD: nucleotide mismatches of CDS pair pi (i<j), XOR/popcount of planes
-            const int pi = task - 4 * m;
-            int i = 0, rem = pi;
-            while (rem >= m - 1 - i) {
-                rem -= m - 1 - i;
-                i++;
+            if (keep) ax[e] = pax[e];
+        }
+    }
+    for (int task = warp; task < ntask; task += nwarps) {
+        if (task < ncds_tasks) {
+            const int kind = (kp >> (2 * (task % K))) & 3;
+            const int c = nth_set_bit(changed, task / K);
+            const uint8_t *row = ids + c * s.Lp;
+            if (kind == 0) {  // CAI: exp(mean log w)
+                long long S = 0;
+                int z = 0;
+                for (int a = lane; a < L; a += 32) {
+                    int id = row[a];
+                    S += st.lw[id];
+                    z |= st.wzero[id];
+                }
+                S = warp_sum(S);
+                z = __any_sync(0xffffffffu, z);
+                if (lane == 0) {
+                    double x = __ddiv_rn(__dmul_rn((double)S, 1.0 / 4294967296.0), (double)L);
+                    float cai = z ? 0.0f : (float)det_exp(x);
+                    ax[AUX_CAI(m) + c] = __float_as_int(cai);
+                }
+            } else if (kind == 1) {  // CBP: codon-pair score sum over pairs a in [0, L-3]
+                long long S = 0;
+                for (int a = lane; a < L - 2; a += 32) {
+                    int c1 = row[a], c2 = row[a + 1];
+                    if (c1 < 61 && c2 < 61) S += __ldg(&gt->cpsf[c1 * 61 + c2]);
+                }
+                S = warp_sum(S);
+                if (lane == 0) {
+                    ax[AUX_CBP_LO(m) + c] = (int32_t)(uint32_t)(unsigned long long)S;
+                    ax[AUX_CBP_HI(m) + c] = (int32_t)(uint32_t)((unsigned long long)S >> 32);
+                }
+            } else if (kind == 2) {  // HSC: hidden stop codons in the +1/+2 frames per boundary
+                int cnt = 0;
+                for (int a = lane; a < L - 1; a += 32) cnt += __ldg(&gt->hsc[row[a] * 64 + row[a + 1]]);
+                cnt = warp_sum(cnt);
+                if (lane == 0) ax[AUX_HSC(m) + c] = cnt;
+            } else {  // GC3 (or whole-CDS GC) count
+                int cnt = 0;
+                if (s.gcmode == PE_GC3) {
+                    for (int a = lane; a < L; a += 32) cnt += st.gc3[row[a]];
+                } else {
+                    const uint2 *A = planes + c * s.Wp;
+                    for (int w = lane; w < s.W; w += 32) cnt += __popc(A[w].x ^ A[w].y);
+                }
+                cnt = warp_sum(cnt);
+                if (lane == 0) ax[AUX_GC(m) + c] = cnt;
             }
-            const int j = i + 1 + rem;
+        } else {  // HD: nucleotide mismatches of a pair with a changed CDS, XOR/popcount of planes
+            const int u = task - ncds_tasks, r = u / (m - 1), k = u - r * (m - 1);
+            const int c = nth_set_bit(changed, r), d = k < c ? k : k + 1;
+            if (((changed >> d) & 1ull) && d < c) continue;  // summed for d's task
+            const int i = min(c, d), j = max(c, d);
+            const int pi = i * (2 * m - i - 1) / 2 + (j - i - 1);
             const uint2 *A = planes + i * s.Wp, *B = planes + j * s.Wp;
             int cnt = 0;
             for (int w = lane; w < s.W; w += 32) {
@@ -214,94 +277,120 @@ __device__ void light_eval(const Shape &s, const DevTables *gt, VarSmem &sm, con
                 cnt += __popc((x.x ^ y.x) | (x.y ^ y.y));
             }
             cnt = warp_sum(cnt);
-            if (lane == 0) pair_cnt[pi] = cnt;
+            if (lane == 0) ax[AUX_HD(m) + pi] = cnt;
         }
     }
     __syncthreads();
-    // the reductions over CDSs, one objective per warp (lane 0), in CDS order; the
-    // last CDS reaching the extreme wins (the reference's `>=`)
-    if (lane != 0) return;
+    if (cax)
+        for (int e = tid; e < AUX_HD(m) + npairs; e += nth) cax[e] = ax[e];
+    if (warp >= 5) return;
+    // The reductions over CDSs, one objective per warp.  The reference's loops keep the
+    // last CDS whose value reaches the extreme (`>=`); no value is NaN, so that is the
+    // highest index holding the extreme, found here with the lanes over CDSs (pairs).
+    // HD and HSC divide counts by a constant: a correctly rounded quotient of counts
+    // below 2^23 by the same divisor is strictly increasing in the count, so their
+    // extremes are found on the counts and divided once.
     if (warp == 0 && sCAI >= 0) {
         float best = 0.0f;
-        int bi = 0;
-        for (int c = 0; c < m; c++) {
-            float v = -__int_as_float((int)sm.cds_val[c]);
-            if (c == 0 || v >= best) {
+        int bi = -1;
+        for (int c = lane; c < m; c += 32) {
+            const float v = -__int_as_float(ax[AUX_CAI(m) + c]);
+            if (bi < 0 || v >= best) {
                 best = v;
                 bi = c;
             }
         }
-        obj[sCAI] = best;
-        objidx[2 * sCAI] = (int8_t)bi;
-        objidx[2 * sCAI + 1] = 0;
+        warp_last_max(best, bi);
+        if (lane == 0) {
+            obj[sCAI] = best;
+            objidx[2 * sCAI] = (int8_t)bi;
+            objidx[2 * sCAI + 1] = 0;
+        }
     }
     if (warp == 1 % nwarps && sCBP >= 0) {
         float best = 0.0f;
-        int bi = 0;
-        for (int c = 0; c < m; c++) {
-            double x = __ddiv_rn(__dmul_rn((double)sm.cds_val2[c], 1.0 / 4294967296.0), (double)(L - 2));
-            float v = -(float)x;
-            if (c == 0 || v >= best) {
+        int bi = -1;
+        for (int c = lane; c < m; c += 32) {
+            const long long S = (long long)(((unsigned long long)(uint32_t)ax[AUX_CBP_HI(m) + c] << 32) |
+                                            (uint32_t)ax[AUX_CBP_LO(m) + c]);
+            const double x = __ddiv_rn(__dmul_rn((double)S, 1.0 / 4294967296.0), (double)(L - 2));
+            const float v = -(float)x;
+            if (bi < 0 || v >= best) {
                 best = v;
                 bi = c;
             }
         }
-        obj[sCBP] = best;
-        objidx[2 * sCBP] = (int8_t)bi;
-        objidx[2 * sCBP + 1] = 0;
+        warp_last_max(best, bi);
+        if (lane == 0) {
+            obj[sCBP] = best;
+            objidx[2 * sCBP] = (int8_t)bi;
+            objidx[2 * sCBP + 1] = 0;
+        }
     }
-    if (warp == 2 % nwarps && sHSC >= 0) {
-        float best = 0.0f;
-        int bi = 0;
-        for (int c = 0; c < m; c++) {
-            float v = -__fdiv_rn((float)sm.cds_cnt2[c], (float)(L - 1));
-            if (c == 0 || v >= best) {
-                best = v;
+    if (warp == 2 % nwarps && sHSC >= 0) {  // the largest -count/(L-1): the last smallest count
+        int bc = 0, bi = -1;
+        for (int c = lane; c < m; c += 32) {
+            const int cnt = ax[AUX_HSC(m) + c];
+            if (bi < 0 || cnt <= bc) {
+                bc = cnt;
                 bi = c;
             }
         }
-        obj[sHSC] = best;
-        objidx[2 * sHSC] = (int8_t)bi;
-        objidx[2 * sHSC + 1] = 0;
+        warp_last_min(bc, bi);
+        if (lane == 0) {
+            obj[sHSC] = -__fdiv_rn((float)bc, (float)(L - 1));
+            objidx[2 * sHSC] = (int8_t)bi;
+            objidx[2 * sHSC + 1] = 0;
+        }
     }
-    if (warp == 3 % nwarps && sHD >= 0) {
-        float best = 0.0f;
-        int bi = 0, bj = 1, pi = 0;
-        for (int i = 0; i < m - 1; i++)
-            for (int j = i + 1; j < m; j++, pi++) {
-                float v = -__fdiv_rn((float)pair_cnt[pi], (float)s.n);
-                if (pi == 0 || v >= best) {
-                    best = v;
-                    bi = i;
-                    bj = j;
-                }
+    if (warp == 3 % nwarps && sHD >= 0) {  // the largest -count/n: the last pair with the smallest count
+        int bc = 0, bp = -1;
+        for (int pi = lane; pi < npairs; pi += 32) {
+            const int cnt = ax[AUX_HD(m) + pi];
+            if (bp < 0 || cnt <= bc) {
+                bc = cnt;
+                bp = pi;
             }
-        obj[sHD] = best;
-        objidx[2 * sHD] = (int8_t)bi;
-        objidx[2 * sHD + 1] = (int8_t)bj;
+        }
+        warp_last_min(bc, bp);
+        if (lane == 0) {
+            int i = 0, rem = bp;
+            while (rem >= m - 1 - i) {
+                rem -= m - 1 - i;
+                i++;
+            }
+            obj[sHD] = -__fdiv_rn((float)bc, (float)s.n);
+            objidx[2 * sHD] = (int8_t)i;
+            objidx[2 * sHD + 1] = (int8_t)(i + 1 + rem);
+        }
     }
     if (warp == 4 % nwarps && sGC >= 0) {
         float best = 0.0f;
-        int bi = 0, dir = 1;
-        for (int c = 0; c < m; c++) {
+        int bi = -1, dir = 1;
+        for (int c = lane; c < m; c += 32) {
             float dev, diff;
+            const int cnt = ax[AUX_GC(m) + c];
             if (s.gcmode == PE_GC3) {
-                diff = __fsub_rn(__fdiv_rn((float)sm.cds_cnt[c], (float)L), gt->ref_gc3);
+                diff = __fsub_rn(__fdiv_rn((float)cnt, (float)L), gt->ref_gc3);
                 dev = fabsf(diff);
             } else {
-                float refGC = __fmul_rn((float)s.n, gt->ref_gc);
-                diff = __fsub_rn((float)sm.cds_cnt[c], refGC);
+                const float refGC = __fmul_rn((float)s.n, gt->ref_gc);
+                diff = __fsub_rn((float)cnt, refGC);
                 dev = __fdiv_rn(fabsf(diff), refGC);
             }
-            if (c == 0 || dev >= best) {
+            if (bi < 0 || dev >= best) {
                 best = dev;
                 bi = c;
                 dir = diff < 0.0f ? 1 : -1;
             }
         }
-        obj[sGC] = best;
-        objidx[2 * sGC] = (int8_t)bi;
-        objidx[2 * sGC + 1] = (int8_t)dir;
+        const int w = warp_last_max(best, bi);
+        dir = __shfl_sync(0xffffffffu, dir, w);
+        if (lane == 0) {
+            obj[sGC] = best;
+            objidx[2 * sGC] = (int8_t)bi;
+            objidx[2 * sGC + 1] = (int8_t)dir;
+        }
     }
 }
 
@@ -338,8 +427,21 @@ __device__ __forceinline__ void shuffle_k(const Shape &s, uint32_t gen, uint32_t
     }
 }
 
+// Marks the plane words codon a of CDS c covers (nucleotides 3a .. 3a+2: one or two
+// words) as changed: bit c * Wp + w of `dirty`.  Every operator marks each codon it
+// leaves different from the parent's, so the marked words are exactly the words
+// whose packed nucleotides differ (distinct codon ids are distinct triplets).
+__device__ __forceinline__ void mark_codon(const Shape &s, uint32_t *dirty, int c, int a)
+{
+    const int w0 = (3 * a) >> 5, w1 = min((3 * a + 2) >> 5, s.W - 1);
+    for (int w = w0; w <= w1; w++) {
+        const int bit = c * s.Wp + w;
+        atomicOr(&dirty[bit >> 5], 1u << (bit & 31));
+    }
+}
+
 __device__ void mutate_solution(const Shape &s, const DevTables *gt, VarSmem &sm, const int8_t *aa, uint8_t *ids,
-                                uint32_t gen, uint32_t ridx, int tid, int nth)
+                                uint32_t *dirty, uint32_t gen, uint32_t ridx, int tid, int nth)
 {
     const SmemTab &st = sm.tab;
     const int L = s.L, m = s.m;
@@ -362,6 +464,7 @@ __device__ void mutate_solution(const Shape &s, const DevTables *gt, VarSmem &sm
                 int nw = (int)rng_uint(MDRAW(pos, 1), (uint32_t)(k - 1));
                 if (nw >= cur) nw++;
                 *cell = (uint8_t)(st.start[am] + nw);
+                mark_codon(s, dirty, c, a);
             }
         }
         break;
@@ -382,6 +485,7 @@ __device__ void mutate_solution(const Shape &s, const DevTables *gt, VarSmem &sm
                 if (cur == k - 1) continue;
                 int nw = cur + 1 + (int)rng_uint(MDRAW(a, 1), (uint32_t)(k - 1 - cur));
                 *cell = (uint8_t)(st.start[am] + nw);
+                mark_codon(s, dirty, c, a);
             }
         }
         break;
@@ -416,7 +520,10 @@ __device__ void mutate_solution(const Shape &s, const DevTables *gt, VarSmem &sm
                 if (right < 61 && g < 61) ns = __fadd_rn(ns, __ldg(&gt->cps[g * 61 + right]));
                 if (ns > curs) up[nup++] = j;
             }
-            if (nup > 0) row[a] = (uint8_t)(st.start[am] + up[rng_uint(MDRAW(a, 1), (uint32_t)nup)]);
+            if (nup > 0) {
+                row[a] = (uint8_t)(st.start[am] + up[rng_uint(MDRAW(a, 1), (uint32_t)nup)]);
+                mark_codon(s, dirty, c, a);
+            }
           }
         }
         break;
@@ -446,7 +553,10 @@ __device__ void mutate_solution(const Shape &s, const DevTables *gt, VarSmem &sm
                 int ns = (hl ? __ldg(&gt->hsc[lft * 64 + g]) : 0) + (hr ? __ldg(&gt->hsc[g * 64 + rgt]) : 0);
                 if (ns > curs) up[nup++] = j;
             }
-            if (nup > 0) row[a] = (uint8_t)(st.start[am] + up[rng_uint(MDRAW(a, 1), (uint32_t)nup)]);
+            if (nup > 0) {
+                row[a] = (uint8_t)(st.start[am] + up[rng_uint(MDRAW(a, 1), (uint32_t)nup)]);
+                mark_codon(s, dirty, c, a);
+            }
           }
         }
         break;
@@ -498,7 +608,10 @@ __device__ void mutate_solution(const Shape &s, const DevTables *gt, VarSmem &sm
                     best = sh;
                 }
             }
-            if (best_m != -1 || best_pair != -1) ids[c1 * s.Lp + a] = (uint8_t)(st.start[am] + best);
+            if (best_m != -1 || best_pair != -1) {
+                ids[c1 * s.Lp + a] = (uint8_t)(st.start[am] + best);
+                mark_codon(s, dirty, c1, a);
+            }
           }
         }
         break;
@@ -536,6 +649,7 @@ __device__ void mutate_solution(const Shape &s, const DevTables *gt, VarSmem &sm
                 int ngc = s.gcmode == PE_GC3 ? st.gc3[g] : st.gcn[g];
                 if ((dir == 1 && ngc > cgc) || (dir == -1 && ngc < cgc)) {
                     row[a] = (uint8_t)g;
+                    mark_codon(s, dirty, c, a);
                     break;
                 }
             }
@@ -567,6 +681,7 @@ __device__ void mutate_solution(const Shape &s, const DevTables *gt, VarSmem &sm
                             int nw = (int)rng_uint(r1, (uint32_t)(k - 1));
                             if (nw == cur) nw++;
                             row[a] = (uint8_t)(st.start[am] + nw);
+                            mark_codon(s, dirty, b, a);
                             break;
                         }
                     }
@@ -614,7 +729,10 @@ __device__ void mutate_solution(const Shape &s, const DevTables *gt, VarSmem &sm
             __syncthreads();
             bool full = cta_full_hairpin(s, st, row, tid, nth);
             float thr = full ? 1.0f : 0.0f;
-            if (s.K > 0 && v > thr) break;  // keep the change
+            if (s.K > 0 && v > thr) {  // keep the change
+                if (tid == 0 && sm.sl_mut) mark_codon(s, dirty, c, a);
+                break;
+            }
             if (tid == 0 && sm.sl_mut) row[a] = (uint8_t)sm.sl_old;
             __syncthreads();
         }
@@ -625,16 +743,68 @@ __device__ void mutate_solution(const Shape &s, const DevTables *gt, VarSmem &sm
     }
 }
 
+// The operator of a child (src/main.cu:172-211): uniform over the seven, or over the
+// five kept with four objectives.
+__device__ __forceinline__ int operator_of(const Shape &s, uint32_t gen, uint32_t ridx)
+{
+    const uint32_t r = draw(s.seed, TAG_OP, gen, ridx, 0, 0);
+    if (s.objset == PE_OBJ_REF6) return (int)rng_uint(r, 7);
+    const int k = (int)rng_uint(r, 5);  // 0, 1, 4, 5, 6
+    return k < 2 ? k : k + 2;
+}
+
+// The children 0 .. n-1 of generation gen in the order their CTAs should start:
+// by operator, the ones that take longest first (random, HD, GC, CBP, HSC, CAI, stem).
+// Any order gives the same results (each CTA writes only its own child); this one
+// leaves the short CTAs for the last wave.  One CTA; the order within an operator
+// is arbitrary.
+__device__ void order_children(const Shape &s, uint32_t gen, int n, int32_t *out, int tid, int nth)
+{
+    __shared__ int cnt[8], cur[8];
+    const int lane = tid & 31;
+    const int cls_of_op[7] = {0, 5, 3, 4, 1, 2, 6};
+    if (tid < 8) cnt[tid] = 0;
+    __syncthreads();
+    for (int base = 0; base < n; base += nth) {
+        const int c = base + tid;
+        const int cls = c < n ? cls_of_op[operator_of(s, gen, (uint32_t)c)] : -1;
+        for (int k = 0; k < 7; k++) {
+            const unsigned b = __ballot_sync(0xffffffffu, cls == k);
+            if (lane == 0 && b) atomicAdd(&cnt[k], __popc(b));
+        }
+    }
+    __syncthreads();
+    if (tid == 0) {
+        int run = 0;
+        for (int k = 0; k < 7; k++) {
+            cur[k] = run;
+            run += cnt[k];
+        }
+    }
+    __syncthreads();
+    for (int base = 0; base < n; base += nth) {
+        const int c = base + tid;
+        const int cls = c < n ? cls_of_op[operator_of(s, gen, (uint32_t)c)] : -1;
+        for (int k = 0; k < 7; k++) {
+            const unsigned b = __ballot_sync(0xffffffffu, cls == k);
+            int pos = 0;
+            if (lane == 0 && b) pos = atomicAdd(&cur[k], __popc(b));
+            pos = __shfl_sync(0xffffffffu, pos, 0);
+            if (cls == k) out[pos + __popc(b & ((1u << lane) - 1u))] = c;
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // k_variation: one CTA (kVarThreads) per solution
 // ---------------------------------------------------------------------------
 template <int MODE>
-__global__ void __launch_bounds__(kVarThreads) k_variation(Shape s, const DevTables *__restrict__ gt,
+__global__ void __launch_bounds__(kVarThreads, 4) k_variation(Shape s, const DevTables *__restrict__ gt,
                                                            const int8_t *__restrict__ aa_g, PopBuf src, PopBuf dst,
                                                            const int32_t *__restrict__ parent_of,
                                                            const int32_t *__restrict__ rng_idx, int copy_base,
                                                            int child_base, const uint32_t *__restrict__ d_gen,
-                                                           int32_t *ops, int32_t *surv)
+                                                           int32_t *ops, int32_t *surv, int32_t *order)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     VarSmem &sm = *reinterpret_cast<VarSmem *>(smem_raw);
@@ -643,11 +813,16 @@ __global__ void __launch_bounds__(kVarThreads) k_variation(Shape s, const DevTab
     int8_t *aa = reinterpret_cast<int8_t *>(planes + (size_t)s.m * s.Wp);
     // MODE_MUTATE: plane words the mutation touched (bit c * Wp + w)
     uint32_t *dirty = reinterpret_cast<uint32_t *>(aa + ((s.L + 15) & ~15));
-    // HD mismatch counts of the m(m-1)/2 CDS pairs
-    int32_t *pair_cnt = reinterpret_cast<int32_t *>(dirty + (s.m * s.Wp + 31) / 32);
+    // the per-CDS (per-pair) sums of the light objectives, aux layout
+    int32_t *ax = reinterpret_cast<int32_t *>(dirty + (s.m * s.Wp + 31) / 32);
 
     const int tid = threadIdx.x, nth = blockDim.x;
-    const int i = blockIdx.x;
+    // MODE_MUTATE with an order: CTA b makes child order[gen parity][b] (heaviest
+    // operators first, so the CTAs of the last wave are the short ones)
+    const uint32_t gen0 = MODE == MODE_MUTATE ? *d_gen : 0u;
+    const int i = MODE == MODE_MUTATE && order ? order[(gen0 & 1u) * gridDim.x + blockIdx.x] : (int)blockIdx.x;
+    if (MODE == MODE_MUTATE && order && blockIdx.x == gridDim.x - 1)
+        order_children(s, gen0 + 1u, (int)gridDim.x, order + ((gen0 + 1u) & 1u) * gridDim.x, tid, nth);
     const size_t sol_bytes = (size_t)s.m * s.Lp;
     const size_t sol_words = (size_t)s.m * s.Wp;
 
@@ -677,80 +852,76 @@ __global__ void __launch_bounds__(kVarThreads) k_variation(Shape s, const DevTab
         if (dst.cds)
             for (int c = tid; c < s.nres; c += nth) dst.cds[(size_t)i * s.nres + c] = make_int2(-1, 0);
     } else {  // MODE_MUTATE
-        gen = *d_gen;
+        gen = gen0;
         ridx = rng_idx ? (uint32_t)rng_idx[i] : (uint32_t)i;
         int par = parent_of[i];
-        const uint4 *g = reinterpret_cast<const uint4 *>(src.ids + (size_t)par * sol_bytes);
-        uint4 *d = reinterpret_cast<uint4 *>(ids);
-        for (size_t e = tid; e < sol_bytes / 16; e += nth) d[e] = g[e];
-        // the parent's planes: the child's differ only in the words its mutation touches
+        // the parent's codon ids and planes into shared memory (the child's planes differ
+        // only in the words its mutation touches) and, when the parent survives, into
+        // its slot of the next population.  Each thread issues up to four 16-byte loads
+        // before their stores, so the loads of a pass are in flight together.
         {
+            const uint4 *g = reinterpret_cast<const uint4 *>(src.ids + (size_t)par * sol_bytes);
             const uint4 *ps = reinterpret_cast<const uint4 *>(src.planes + (size_t)par * sol_words);
+            uint4 *d = reinterpret_cast<uint4 *>(ids);
             uint4 *pd = reinterpret_cast<uint4 *>(planes);
-            for (size_t e = tid; e < sol_words / 2; e += nth) pd[e] = ps[e];
+            const size_t dslot = (size_t)(copy_base + i);
+            uint4 *gd = copy_base >= 0 ? reinterpret_cast<uint4 *>(dst.ids + dslot * sol_bytes) : nullptr;
+            uint4 *pdd = copy_base >= 0 ? reinterpret_cast<uint4 *>(dst.planes + dslot * sol_words) : nullptr;
+            const int nid = (int)(sol_bytes / 16), ntot = nid + (int)(sol_words / 2);
+            for (int e0 = tid; e0 < ntot; e0 += 4 * nth) {
+                uint4 v[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int e = e0 + u * nth;
+                    if (e < ntot) v[u] = e < nid ? g[e] : ps[e - nid];
+                }
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    const int e = e0 + u * nth;
+                    if (e < nid) {
+                        d[e] = v[u];
+                        if (gd) gd[e] = v[u];
+                    } else if (e < ntot) {
+                        pd[e - nid] = v[u];
+                        if (pdd) pdd[e - nid] = v[u];
+                    }
+                }
+            }
             for (int e = tid; e < (int)((sol_words + 31) / 32); e += nth) dirty[e] = 0u;
         }
         if (tid < s.M) sm.pobj[tid] = src.obj[(size_t)par * s.M + tid];
         if (tid < 2 * s.M) sm.pobjidx[tid] = src.objidx[(size_t)par * 2 * s.M + tid];
         if (tid < 3) sm.ppql[tid] = src.pql[(size_t)par * 3 + tid];
         if (copy_base >= 0) {
-            // the surviving parent keeps its slot: copy ids, planes and objectives
-            size_t dslot = (size_t)(copy_base + i);
-            uint4 *gd = reinterpret_cast<uint4 *>(dst.ids + dslot * sol_bytes);
-            for (size_t e = tid; e < sol_bytes / 16; e += nth) gd[e] = g[e];
-            const uint4 *ps = reinterpret_cast<const uint4 *>(src.planes + (size_t)par * sol_words);
-            uint4 *pd = reinterpret_cast<uint4 *>(dst.planes + dslot * sol_words);
-            for (size_t e = tid; e < sol_words / 2; e += nth) pd[e] = ps[e];
+            // the surviving parent keeps its slot: its objectives and per-CDS results too
+            const size_t dslot = (size_t)(copy_base + i);
             if (tid < s.M) dst.obj[dslot * s.M + tid] = src.obj[(size_t)par * s.M + tid];
             if (tid < 2 * s.M) dst.objidx[dslot * 2 * s.M + tid] = src.objidx[(size_t)par * 2 * s.M + tid];
             if (tid < 3) dst.pql[dslot * 3 + tid] = src.pql[(size_t)par * 3 + tid];
+            if (dst.aux)
+                for (int e = tid; e < s.naux; e += nth) dst.aux[dslot * s.naux + e] = src.aux[(size_t)par * s.naux + e];
             if (dst.cds)
                 for (int c = tid; c < s.nres; c += nth)
                     dst.cds[dslot * s.nres + c] = src.cds ? src.cds[(size_t)par * s.nres + c] : make_int2(-1, 0);
         }
         out_slot = child_base + i;
         if (tid == 0) {
-            uint32_t r = draw(s.seed, TAG_OP, gen, ridx, 0, 0);
-            int op;
-            if (s.objset == PE_OBJ_REF6) {
-                op = (int)rng_uint(r, 7);
-            } else {
-                const int map5[5] = {0, 1, 4, 5, 6};
-                op = map5[rng_uint(r, 5)];
-            }
+            const int op = operator_of(s, gen, ridx);
             sm.op = op;
             if (ops) ops[i] = op;
         }
         __syncthreads();
-        mutate_solution(s, gt, sm, aa, ids, gen, ridx, tid, nth);
-        __syncthreads();
-        // mark the plane words of every 4-codon group that differs from the parent
-        // (codons a .. a+3 are nucleotides 3a .. 3a+11: one or two words)
-        for (size_t e = tid; e < sol_bytes / 16; e += nth) {
-            const uint4 pv = g[e], cv = reinterpret_cast<const uint4 *>(ids)[e];
-            const uint32_t pw[4] = {pv.x, pv.y, pv.z, pv.w}, cw[4] = {cv.x, cv.y, cv.z, cv.w};
-#pragma unroll
-            for (int k = 0; k < 4; k++) {
-                if (pw[k] == cw[k]) continue;
-                const int q = 16 * (int)e + 4 * k, c = q / s.Lp, a = q - c * s.Lp;
-                const int w0 = (3 * a) >> 5, w1 = min((3 * a + 11) >> 5, s.W - 1);
-                for (int w = w0; w <= w1; w++) {
-                    const int bit = c * s.Wp + w;
-                    atomicOr(&dirty[bit >> 5], 1u << (bit & 31));
-                }
-            }
-        }
+        mutate_solution(s, gt, sm, aa, ids, dirty, gen, ridx, tid, nth);
     }
     __syncthreads();
     pack_planes(s, sm.tab, ids, planes, tid, nth, MODE == MODE_MUTATE ? dirty : nullptr);
-    if (MODE == MODE_MUTATE && dst.cds) {
-        // a CDS none of whose plane words changed keeps its parent's hairpin result;
-        // an LRCS pair of two such CDSs keeps its parent's pair result
-        const int par = parent_of[i];
+    // CDSs the mutation changed (bit c); every CDS outside MODE_MUTATE
+    unsigned long long chmask = s.m == 64 ? ~0ull : (1ull << s.m) - 1ull;
+    if (MODE == MODE_MUTATE && (dst.cds || src.aux)) {
         if (tid == 0) sm.changed = 0ull;
         __syncthreads();
         for (int c = tid; c < s.m; c += nth) {
-            bool changed = src.cds == nullptr;
+            bool changed = false;
             const int b0 = c * s.Wp, b1 = b0 + s.Wp;  // this CDS's bits [b0, b1)
             for (int wd = b0 >> 5; wd <= (b1 - 1) >> 5 && !changed; wd++) {
                 const int lo = max(b0, 32 * wd) - 32 * wd, hi = min(b1, 32 * wd + 32) - 32 * wd;
@@ -761,16 +932,24 @@ __global__ void __launch_bounds__(kVarThreads) k_variation(Shape s, const DevTab
         }
         __syncthreads();
         const unsigned long long ch = sm.changed;
-        for (int c = tid; c < s.nres; c += nth) {
-            bool changed;
-            if (s.sl_kind == PE_SL_LRCS) {
-                int a, b;
-                lrcs_pair_of(s.m, c, a, b);
-                changed = ((ch >> a) | (ch >> b)) & 1ull;
-            } else {
-                changed = (ch >> c) & 1ull;
+        if (src.aux) chmask = ch;
+        if (dst.cds) {
+            // a CDS none of whose plane words changed keeps its parent's hairpin result;
+            // an LRCS pair of two such CDSs keeps its parent's pair result
+            const int par = parent_of[i];
+            for (int c = tid; c < s.nres; c += nth) {
+                bool changed;
+                if (src.cds == nullptr) {
+                    changed = true;
+                } else if (s.sl_kind == PE_SL_LRCS) {
+                    int a, b;
+                    lrcs_pair_of(s.m, c, a, b);
+                    changed = ((ch >> a) | (ch >> b)) & 1ull;
+                } else {
+                    changed = (ch >> c) & 1ull;
+                }
+                dst.cds[(size_t)out_slot * s.nres + c] = changed ? make_int2(-1, 0) : src.cds[(size_t)par * s.nres + c];
             }
-            dst.cds[(size_t)out_slot * s.nres + c] = changed ? make_int2(-1, 0) : src.cds[(size_t)par * s.nres + c];
         }
     }
     __syncthreads();
@@ -785,7 +964,9 @@ __global__ void __launch_bounds__(kVarThreads) k_variation(Shape s, const DevTab
         const uint4 *ps = reinterpret_cast<const uint4 *>(planes);
         for (size_t e = tid; e < sol_words / 2; e += nth) pd[e] = ps[e];
     }
-    light_eval(s, gt, sm, ids, planes, pair_cnt, dst.obj + (size_t)out_slot * s.M,
+    const int32_t *pax = MODE == MODE_MUTATE && src.aux ? src.aux + (size_t)parent_of[i] * s.naux : nullptr;
+    int32_t *cax = dst.aux ? dst.aux + (size_t)out_slot * s.naux : nullptr;
+    light_eval(s, gt, sm.tab, ids, planes, ax, chmask, pax, cax, dst.obj + (size_t)out_slot * s.M,
                dst.objidx + (size_t)out_slot * 2 * s.M, tid, nth);
 }
 
@@ -793,7 +974,7 @@ size_t var_smem_bytes(const Shape &s)
 {
     return ((sizeof(VarSmem) + 15) & ~size_t(15)) + (size_t)s.m * s.Lp + (size_t)s.m * s.Wp * sizeof(uint2) +
            (size_t)((s.L + 15) & ~15) + (size_t)((s.m * s.Wp + 31) / 32) * sizeof(uint32_t) +
-           (size_t)(s.m * (s.m - 1) / 2) * sizeof(int32_t);
+           (size_t)s.naux * sizeof(int32_t);
 }
 
 cudaError_t raise_smem_limit(const void *func, size_t bytes)
@@ -823,7 +1004,7 @@ cudaError_t launch_init(const Shape &s, const DevTables *tab, const int8_t *aa, 
     cudaError_t e = set_var_attr<MODE_INIT>(smem);
     if (e != cudaSuccess) return e;
     k_variation<MODE_INIT><<<s.N, kVarThreads, smem, st>>>(s, tab, aa, dst, dst, nullptr, nullptr, -1, 0, nullptr,
-                                                            nullptr, surv);
+                                                            nullptr, surv, nullptr);
     return cudaGetLastError();
 }
 
@@ -842,20 +1023,22 @@ cudaError_t launch_light_eval(const Shape &s, const DevTables *tab, const int8_t
     b.objidx += (size_t)base * 2 * s.M;
     b.pql += (size_t)base * 3;
     k_variation<MODE_EVAL><<<count, kVarThreads, smem, st>>>(s, tab, aa, b, b, nullptr, nullptr, -1, 0, nullptr,
-                                                              nullptr, nullptr);
+                                                              nullptr, nullptr, nullptr);
     return cudaGetLastError();
 }
 
 cudaError_t launch_mutate(const Shape &s, const DevTables *tab, const int8_t *aa, PopBuf src, PopBuf dst,
                           const int32_t *parent_of, const int32_t *rng_idx, int count, int copy_base, int child_base,
-                          const uint32_t *d_gen, int32_t *ops, cudaStream_t st)
+                          const uint32_t *d_gen, int32_t *ops, int32_t *order, cudaStream_t st)
 {
     if (count <= 0) return cudaSuccess;
+    // a child reuses its parent's per-CDS sums only when both buffers carry them
+    if ((src.aux == nullptr) != (dst.aux == nullptr)) return cudaErrorInvalidValue;
     size_t smem = var_smem_bytes(s);
     cudaError_t e = set_var_attr<MODE_MUTATE>(smem);
     if (e != cudaSuccess) return e;
     k_variation<MODE_MUTATE><<<count, kVarThreads, smem, st>>>(s, tab, aa, src, dst, parent_of, rng_idx, copy_base,
-                                                                child_base, d_gen, ops, nullptr);
+                                                                child_base, d_gen, ops, nullptr, order);
     return cudaGetLastError();
 }
 

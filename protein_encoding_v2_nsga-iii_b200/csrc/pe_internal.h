@@ -41,7 +41,18 @@ struct Shape {
     int sl_kind;     // string objective: PE_SL_HAIRPIN or PE_SL_LRCS
     int nres;        // string-objective results per solution: m CDSs (hairpin) or m(m+1)/2 CDS pairs (LRCS)
     int wait_limit;  // polls of a bounded device wait: 0 = the default, < 0 = give up at once (tests)
+    int naux;        // int32 words of per-CDS sums per solution: AUX_HD(m) + m(m-1)/2
 };
+
+// Per-solution sums of the light objectives (PopBuf.aux), int32 words: per CDS c the
+// CAI value bits, the CBP fixed-point sum (low and high halves), the HSC count and
+// the GC count; then the HD mismatch count of every CDS pair (i < j, row-major).
+#define AUX_CAI(m) 0
+#define AUX_CBP_LO(m) (m)
+#define AUX_CBP_HI(m) (2 * (m))
+#define AUX_HSC(m) (3 * (m))
+#define AUX_GC(m) (4 * (m))
+#define AUX_HD(m) (5 * (m))
 
 // polls of a bounded device wait before it gives up and reports PE_ERR_TIMEOUT
 __host__ __device__ __forceinline__ int wait_polls(int wait_limit)
@@ -78,6 +89,9 @@ struct PopBuf {
     // parent's result, so only what its mutation touched is scanned.  nullptr: every
     // one is scanned.
     int2 *cds;
+    // [2N][naux] per-CDS (per-pair) sums of the light objectives: a child's unchanged
+    // CDSs take their parent's.  nullptr: every CDS is summed.
+    int32_t *aux;
 };
 
 struct SelectScratch {
@@ -88,10 +102,8 @@ struct SelectScratch {
     int32_t *assoc;      // [2N]
     float *dist;         // [2N]
     int32_t *rho;        // [R]
-    int32_t *fill;       // [R]
     int32_t *ncand;      // [R]
-    int32_t *coff;       // [R+1]
-    int32_t *cand;       // [2N]
+    uint32_t *trank;     // [2N + M] place of each extreme-point search position in the reduction-tree order
     int32_t *info;       // [8] rank_count, last_size, n_fronts, cut, hyp_exc, status
     float *finfo;        // [3*M] ideal, worst, nadir
 };
@@ -103,7 +115,7 @@ cudaError_t launch_light_eval(const Shape &s, const DevTables *tab, const int8_t
                               cudaStream_t st);
 cudaError_t launch_mutate(const Shape &s, const DevTables *tab, const int8_t *aa, PopBuf src, PopBuf dst,
                           const int32_t *parent_of, const int32_t *rng_idx, int count, int copy_base, int child_base,
-                          const uint32_t *d_gen, int32_t *ops, cudaStream_t st);
+                          const uint32_t *d_gen, int32_t *ops, int32_t *order, cudaStream_t st);
 cudaError_t launch_sl(const Shape &s, PopBuf buf, int base, int count, int2 *part, int32_t *counter,
                       int32_t *status, cudaStream_t st, unsigned long long *scanned = nullptr);
 size_t sl_smem_bytes(const Shape &s);
@@ -121,5 +133,8 @@ cudaError_t launch_select(const Shape &s, const float *obj, float *ext, const fl
                           int32_t *surv, uint32_t *d_gen, int bump_gen, cudaStream_t st);
 size_t select_smem_bytes(const Shape &s);
 size_t niche_smem_bytes(const Shape &s);
+// place of every position 0 .. B-1 of the extreme-point search in the reference's
+// reduction-tree order (0xffffffff: a position the tree leaves out)
+void tree_order_ranks(int B, uint32_t *rank);
 
 }  // namespace pe

@@ -20,6 +20,7 @@
 #include <cfloat>
 #include <cstdint>
 #include <cuda_runtime.h>
+#include <vector>
 
 #include "pe_device.cuh"
 #include <cooperative_groups.h>
@@ -85,50 +86,6 @@ __global__ void __launch_bounds__(256) k_dominance(Shape s, const float *__restr
     }
 }
 
-// The same rows, kDomRows per CTA (one warp per row), with every objective vector
-// staged once per CTA in shared memory, objective-major so the lanes of a warp read
-// 32 consecutive words: the matrix crosses L2 once per CTA instead of once per row.
-constexpr int kDomRows = 16;
-constexpr size_t kDomTiledSmemMax = 200 * 1024;  // the staged matrix must fit beside nothing else
-
-template <int MM>
-__global__ void __launch_bounds__(32 * kDomRows) k_dominance_tiled(Shape s, const float *__restrict__ obj,
-                                                                   uint32_t *__restrict__ dom,
-                                                                   int32_t *__restrict__ np)
-{
-    extern __shared__ float ot[];  // [M][N2]
-    const int M = MM > 0 ? MM : s.M;
-    const int N2 = 2 * s.N, words = (N2 + 31) >> 5;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int e = tid; e < N2 * M; e += blockDim.x) {
-        const int j = e / M, k = e - j * M;
-        ot[k * N2 + j] = obj[e];
-    }
-    __syncthreads();
-    const int i = blockIdx.x * kDomRows + warp;
-    if (i >= N2) return;
-    float oi[kMaxObj];
-#pragma unroll
-    for (int k = 0; k < (MM > 0 ? MM : kMaxObj); k++)
-        if (k < M) oi[k] = ot[k * N2 + i];
-    int cnt = 0;
-    for (int w = 0; w < words; w++) {
-        const int j = 32 * w + lane;
-        bool bit = false;
-        if (j < N2 && j != i) {
-            float oj[kMaxObj];
-#pragma unroll
-            for (int k = 0; k < (MM > 0 ? MM : kMaxObj); k++)
-                if (k < M) oj[k] = ot[k * N2 + j];
-            bit = dominates(oj, oi, M);
-        }
-        const uint32_t word = __ballot_sync(0xffffffffu, bit);
-        if (lane == 0) dom[(size_t)i * words + w] = word;
-        cnt += __popc(word);
-    }
-    if (lane == 0) np[i] = cnt;
-}
-
 // Across the lanes of a warp, lane w holding v: the smallest (largest) value, the
 // lowest lane among equal ones -- what a loop over w = 0, 1, ... keeping the first
 // strictly better value returns (including which of -0 / +0).
@@ -169,8 +126,10 @@ __device__ __forceinline__ float warp_first_max(float v, int lane)
 // merged lists, each merge listing its first slot, then (odd h) slot h-1, then the
 // other.  tree_key gives a position's place in that order, the choice made at
 // every level (0 first, 1 the odd slot, 2 the other), root level in the highest
-// bits; positions that level 1 leaves out (odd B) never win and get ~0.
-__device__ __forceinline__ uint64_t tree_key(int p, int B)
+// bits; positions that level 1 leaves out (odd B) never win and get ~0.  The
+// kernels read a position's place in that order from a table made once per shape
+// (tree_order_ranks), so a tie costs one load.
+__host__ __device__ inline uint64_t tree_key(int p, int B)
 {
     int h = B >> 1;
     if (p >= 2 * h) return ~0ull;
@@ -196,6 +155,21 @@ __device__ __forceinline__ uint64_t tree_key(int p, int B)
     return key;
 }
 
+void tree_order_ranks(int B, uint32_t *rank)
+{
+    std::vector<std::pair<uint64_t, int>> k((size_t)B);
+    for (int p = 0; p < B; p++) k[(size_t)p] = {tree_key(p, B), p};
+    std::sort(k.begin(), k.end());
+    for (int r = 0; r < B; r++) rank[k[(size_t)r].second] = k[(size_t)r].first == ~0ull ? 0xffffffffu : (uint32_t)r;
+}
+
+// place of position p in tree order, as a key (~0: never wins)
+__device__ __forceinline__ uint64_t tree_rank(const uint32_t *trank, int p)
+{
+    const uint32_t r = __ldg(&trank[p]);
+    return r == 0xffffffffu ? ~0ull : (uint64_t)r;
+}
+
 // candidate of the extreme-point search: ASF value bits (values are >= +0, so their
 // bits order as the values do) and position (kNoPos: none yet).  Tree keys are only
 // needed between equal values, so they are computed then.
@@ -205,13 +179,6 @@ struct ExtCand {
     uint32_t v;
     uint32_t pos;
 };
-
-__device__ __forceinline__ bool ext_before(uint32_t v, uint32_t pos, const ExtCand &c, int B)
-{
-    if (v != c.v) return v < c.v;
-    if (c.pos == kNoPos) return true;
-    return tree_key((int)pos, B) < tree_key((int)c.pos, B);
-}
 
 struct SelSmem {
     int warp_tot[33];
@@ -259,6 +226,36 @@ __device__ __forceinline__ int block_scan_flag(int flag, SelSmem &sm, int *total
     return res;
 }
 
+// asf_all for a row held in registers (fixed-size arrays, M <= kMaxObj live entries)
+__device__ __forceinline__ void asf_rows(const float (&x)[kMaxObj], const float (&ideal)[kMaxObj], int M,
+                                         float (&out)[kMaxObj])
+{
+    float tmp[kMaxObj] = {};
+    float m1 = -1.0f, m2 = -1.0f;  // largest and second largest tmp_k
+    int a1 = -1;
+#pragma unroll
+    for (int k = 0; k < kMaxObj; k++) {
+        if (k >= M) break;
+        float t = __fsub_rn(x[k], ideal[k]);
+        if ((double)t < 0.001) t = 0.0f;
+        tmp[k] = t;
+        if (t > m1) {
+            m2 = m1;
+            m1 = t;
+            a1 = k;
+        } else if (t > m2) {
+            m2 = t;
+        }
+    }
+    const float q1 = m1 >= 0.0f ? __fdiv_rn(m1, 1e-6f) : -FLT_MAX;
+    const float q2 = m2 >= 0.0f ? __fdiv_rn(m2, 1e-6f) : -FLT_MAX;
+#pragma unroll
+    for (int i = 0; i < kMaxObj; i++) {
+        const float q = i == a1 ? q2 : q1;  // largest over k != i
+        out[i] = i < M && tmp[i] > q ? tmp[i] : q;
+    }
+}
+
 // ASF (include/sorting.cuh:428-449) of point x for every axis i: the largest of
 // tmp_k / w_k with tmp_k = x_k - ideal_k (0 below 0.001), w_i = 1 and the other
 // weights 1e-6.  Every tmp_k is >= 0 and a correctly rounded division is monotone in
@@ -290,86 +287,66 @@ __device__ __forceinline__ void asf_all(const float *x, const float *ideal, int 
     }
 }
 
-// the same for one axis i: one division
-__device__ __forceinline__ float asf_axis(const float *x, const float *ideal, int i, int M)
+// Hyperplane intercepts (GaussianElimination, include/sorting.cuh:555-599, and the
+// check of :929-956) by one thread, MM known at compile time so the augmented matrix
+// stays in registers.  Row r of [E | 1] is extreme point r; every element
+// goes through the reference's operations in its order: a near-zero pivot takes the
+// first later row with a usable entry added to its row, each later row subtracts
+// (its entry / pivot) times the pivot row, back substitution sums in ascending
+// column order.  Returns 1 when the intercepts are unusable (residual off by more
+// than 1e-6, or an intercept not above 1e-6, NaN or infinite), else writes
+// nadir = ideal + intercepts and returns 0.
+template <int MM>
+__device__ int hyperplane_nadir(const float *ext, const float *ideal, float *nadir)
 {
-    float ti = 0.0f, m = -1.0f;  // tmp_i and the largest tmp_k over k != i
-    for (int k = 0; k < M; k++) {
-        float t = __fsub_rn(x[k], ideal[k]);
-        if ((double)t < 0.001) t = 0.0f;
-        if (k == i) ti = t;
-        else if (t > m) m = t;
+    float a[MM][MM + 1];
+#pragma unroll
+    for (int r = 0; r < MM; r++) {
+#pragma unroll
+        for (int j = 0; j < MM; j++) a[r][j] = ext[r * MM + j];
+        a[r][MM] = 1.0f;
     }
-    const float q = m >= 0.0f ? __fdiv_rn(m, 1e-6f) : -FLT_MAX;
-    return ti > q ? ti : q;
-}
-
-// element j of a row held in registers (j known only at run time)
-__device__ __forceinline__ float row_at(const float (&row)[kMaxObj + 1], int j)
-{
-    float v = row[0];
 #pragma unroll
-    for (int q = 1; q <= kMaxObj; q++)
-        if (j == q) v = row[q];
-    return v;
-}
-
-// Hyperplane through the extreme points by Gaussian elimination
-// (GaussianElimination, include/sorting.cuh:555-599) and its check (:929-956), by
-// one warp: lane r < M holds row r of [ext | 1] and does that row's share of every
-// step, with the same operations in the same order as the serial loops.  Writes
-// nadir = ideal + intercepts; returns 1 (all lanes) when the hyperplane is unusable.
-__device__ int hyperplane_nadir(int M, const float *ext, const float *ideal, float *nadir, int lane)
-{
-    const unsigned full = 0xffffffffu;
-    const bool mine = lane < M;
-    float row[kMaxObj + 1];
+    for (int c = 0; c < MM; c++) {
+        if ((double)fabsf(a[c][c]) <= 1e-6) {
+            bool added = false;
 #pragma unroll
-    for (int j = 0; j <= kMaxObj; j++) row[j] = (mine && j < M) ? ext[lane * M + j] : (j == M ? 1.0f : 0.0f);
-    for (int c = 0; c < M; c++) {
-        const float pcc = __shfl_sync(full, row_at(row, c), c);
-        if ((double)fabsf(pcc) <= 1e-6) {
-            // add the first later row with a usable entry in column c
-            const unsigned cand = __ballot_sync(full, mine && lane > c && (double)fabsf(row_at(row, c)) > 1e-6);
-            if (cand) {
-                const int r = __ffs(cand) - 1;
+            for (int r = c + 1; r < MM; r++) {
+                if (!added && (double)fabsf(a[r][c]) > 1e-6) {
 #pragma unroll
-                for (int j = 0; j <= kMaxObj; j++) {
-                    const float vr = __shfl_sync(full, row[j], r);
-                    if (lane == c && j >= c && j <= M) row[j] = __fadd_rn(row[j], vr);
+                    for (int j = c; j <= MM; j++) a[c][j] = __fadd_rn(a[c][j], a[r][j]);
+                    added = true;
                 }
             }
         }
-        const float pc = __shfl_sync(full, row_at(row, c), c);
-        const float f = __fdiv_rn(row_at(row, c), pc);
-        const bool elim = mine && lane > c;
+        const float pc = a[c][c];
 #pragma unroll
-        for (int j = 0; j <= kMaxObj; j++) {
-            const float vc = __shfl_sync(full, row[j], c);
-            if (elim && j >= c && j <= M) row[j] = __fsub_rn(row[j], __fmul_rn(f, vc));
+        for (int r = c + 1; r < MM; r++) {
+            const float f = __fdiv_rn(a[r][c], pc);
+#pragma unroll
+            for (int j = c; j <= MM; j++) a[r][j] = __fsub_rn(a[r][j], __fmul_rn(f, a[c][j]));
         }
     }
-    // back substitution: lane r finds x[r] once x[r+1 .. M-1] are known
-    float xr = 0.0f;
-    for (int r = M - 1; r >= 0; r--) {
+    float x[MM];
+#pragma unroll
+    for (int r = MM - 1; r >= 0; r--) {
         float sacc = 0.0f;
-        for (int j = r + 1; j < M; j++) sacc = __fadd_rn(sacc, __fmul_rn(row_at(row, j), __shfl_sync(full, xr, j)));
-        const float xv = __fdiv_rn(__fsub_rn(row_at(row, M), sacc), row_at(row, r));
-        if (lane == r) xr = xv;
+#pragma unroll
+        for (int j = r + 1; j < MM; j++) sacc = __fadd_rn(sacc, __fmul_rn(a[r][j], x[j]));
+        x[r] = __fdiv_rn(__fsub_rn(a[r][MM], sacc), a[r][r]);
     }
     int exc = 0;
-    float res = 0.0f;
-    for (int i = 0; i < M; i++) {
-        const float xi = __shfl_sync(full, xr, i);
-        if (mine) res = __fadd_rn(res, __fmul_rn(xi, __fsub_rn(ext[lane * M + i], ideal[i])));
-    }
-    if (mine) {
+#pragma unroll
+    for (int r = 0; r < MM; r++) {
+        float res = 0.0f;
+#pragma unroll
+        for (int i = 0; i < MM; i++) res = __fadd_rn(res, __fmul_rn(x[i], __fsub_rn(ext[r * MM + i], ideal[i])));
         if (fabsf(__fsub_rn(res, 1.0f)) > 1e-6f || isnan(res) || isinf(res)) exc = 1;
-        const float icp = __fdiv_rn(1.0f, xr);
+        const float icp = __fdiv_rn(1.0f, x[r]);
         if (icp <= 1e-6f || isnan(icp) || isinf(icp)) exc = 1;
-        nadir[lane] = __fadd_rn(ideal[lane], icp);
+        nadir[r] = __fadd_rn(ideal[r], icp);
     }
-    return __any_sync(full, exc) ? 1 : 0;
+    return exc;
 }
 
 // exclusive block scan of an int over the CTA; returns the prefix and leaves
@@ -399,6 +376,82 @@ __device__ __forceinline__ int block_scan_value(int v, SelSmem &sm, int *total)
     *total = sm.warp_tot[32];
     __syncthreads();
     return r;
+}
+
+// Compare-exchange of bitonic stage (k, jj) on a 64-key block held in registers: lane
+// l holds the keys at base + l (e0) and base + l + 32 (e1).  jj <= 32.
+__device__ __forceinline__ void bitonic_reg_stage(uint32_t &e0, uint32_t &e1, int base, int lane, int k, int jj)
+{
+    if (jj == 32) {  // both keys of the pair in this lane
+        const bool asc = ((base + lane) & k) == 0;
+        const uint32_t lo = min(e0, e1), hi = max(e0, e1);
+        e0 = asc ? lo : hi;
+        e1 = asc ? hi : lo;
+    } else {
+        const uint32_t o0 = __shfl_xor_sync(0xffffffffu, e0, jj), o1 = __shfl_xor_sync(0xffffffffu, e1, jj);
+        const bool lower = (lane & jj) == 0;
+        const bool asc0 = ((base + lane) & k) == 0, asc1 = ((base + lane + 32) & k) == 0;
+        e0 = lower == asc0 ? min(e0, o0) : max(e0, o0);
+        e1 = lower == asc1 ? min(e1, o1) : max(e1, o1);
+    }
+}
+
+// Ascending bitonic sort of keys[0, P) (P a power of two) by the whole CTA, called by
+// every thread after the keys are written.  Stages that compare keys 32 or fewer
+// apart run in registers, each warp on its own 64-key blocks; the wider stages go
+// through shared memory with a barrier each.  Returns after a barrier.
+__device__ void block_bitonic_sort(uint32_t *keys, int P, int tid, int nth)
+{
+    const int lane = tid & 31, warp = tid >> 5, nwarps = nth >> 5;
+    __syncthreads();
+    if (P < 64) {  // one warp, through shared memory
+        if (warp == 0)
+            for (int k = 2; k <= P; k <<= 1)
+                for (int jj = k >> 1; jj > 0; jj >>= 1) {
+                    for (int q = lane; q < (P >> 1); q += 32) {
+                        const int i = ((q & ~(jj - 1)) << 1) | (q & (jj - 1)), ixj = i + jj;
+                        const uint32_t a = keys[i], b = keys[ixj];
+                        if ((a > b) == ((i & k) == 0)) {
+                            keys[i] = b;
+                            keys[ixj] = a;
+                        }
+                    }
+                    __syncwarp();
+                }
+        __syncthreads();
+        return;
+    }
+    const int nblk = P >> 6;
+    for (int b = warp; b < nblk; b += nwarps) {  // phases k <= 64: inside each block
+        const int base = b << 6;
+        uint32_t e0 = keys[base + lane], e1 = keys[base + lane + 32];
+        for (int k = 2; k <= 64; k <<= 1)
+            for (int jj = k >> 1; jj > 0; jj >>= 1) bitonic_reg_stage(e0, e1, base, lane, k, jj);
+        keys[base + lane] = e0;
+        keys[base + lane + 32] = e1;
+    }
+    for (int k = 128; k <= P; k <<= 1) {
+        for (int jj = k >> 1; jj >= 64; jj >>= 1) {
+            __syncthreads();
+            for (int q = tid; q < (P >> 1); q += nth) {
+                const int i = ((q & ~(jj - 1)) << 1) | (q & (jj - 1)), ixj = i + jj;
+                const uint32_t a = keys[i], b = keys[ixj];
+                if ((a > b) == ((i & k) == 0)) {
+                    keys[i] = b;
+                    keys[ixj] = a;
+                }
+            }
+        }
+        __syncthreads();
+        for (int b = warp; b < nblk; b += nwarps) {
+            const int base = b << 6;
+            uint32_t e0 = keys[base + lane], e1 = keys[base + lane + 32];
+            for (int jj = 32; jj > 0; jj >>= 1) bitonic_reg_stage(e0, e1, base, lane, k, jj);
+            keys[base + lane] = e0;
+            keys[base + lane + 32] = e1;
+        }
+    }
+    __syncthreads();
 }
 
 // nonDominatedSorting (include/sorting.cuh:974-1089): fronts peeled on the
@@ -562,13 +615,16 @@ size_t fronts_smem_bytes(const Shape &s)
     return (size_t)((words + 3) & ~3) * 4 + (size_t)2 * ((sw + 3) & ~3) * 4 + (size_t)RR * 4 + (size_t)words * 4;
 }
 
+// MM: the objective count (4 or 6)
+template <int MM>
 __global__ void __launch_bounds__(kSelThreads, 1) k_select(Shape s, const float *__restrict__ obj, float *ext,
                                                         const float *__restrict__ refpts, SelectScratch sc,
                                                         int32_t *surv, uint32_t *d_gen, int bump_gen)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SelSmem &sm = *reinterpret_cast<SelSmem *>(smem_raw);
-    const int N = s.N, N2 = 2 * N, M = s.M, R = s.R;
+    const int N = s.N, N2 = 2 * N, R = s.R;
+    constexpr int M = MM;
     const int words = (N2 + 31) >> 5;
     ExtSmem &xs = *reinterpret_cast<ExtSmem *>(smem_raw + ((sizeof(SelSmem) + 15) & ~size_t(15)));
     const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5;
@@ -589,22 +645,37 @@ __global__ void __launch_bounds__(kSelThreads, 1) k_select(Shape s, const float 
     }
     __syncthreads();
 
-    // ---------------- ideal / worst (exact min / max), objective by objective
-    for (int k = 0; k < M; k++) {
-        float mn = FLT_MAX, mx = -FLT_MAX;
+    // ---------------- ideal / worst (exact min / max): each thread reads its rows once
+    {
+        float mn[kMaxObj], mx[kMaxObj];
+#pragma unroll
+        for (int k = 0; k < kMaxObj; k++) {
+            mn[k] = FLT_MAX;
+            mx[k] = -FLT_MAX;
+        }
         for (int i = tid; i < N2; i += nth) {
-            const float v = obj[(size_t)i * M + k];
-            if (v < mn) mn = v;
-            if (v > mx) mx = v;
+            const float *x = obj + (size_t)i * M;
+#pragma unroll
+            for (int k = 0; k < kMaxObj; k++) {
+                if (k < M) {
+                    const float v = x[k];
+                    if (v < mn[k]) mn[k] = v;
+                    if (v > mx[k]) mx[k] = v;
+                }
+            }
         }
-        for (int o = 16; o > 0; o >>= 1) {
-            const float a = __shfl_xor_sync(0xffffffffu, mn, o), b = __shfl_xor_sync(0xffffffffu, mx, o);
-            if (a < mn) mn = a;
-            if (b > mx) mx = b;
-        }
-        if (lane == 0) {
-            sm.red[warp * kMaxObj + k] = mn;
-            sm.red[32 * kMaxObj + warp * kMaxObj + k] = mx;
+#pragma unroll
+        for (int k = 0; k < kMaxObj; k++) {
+            if (k >= M) break;
+            for (int o = 16; o > 0; o >>= 1) {
+                const float a = __shfl_xor_sync(0xffffffffu, mn[k], o), b = __shfl_xor_sync(0xffffffffu, mx[k], o);
+                if (a < mn[k]) mn[k] = a;
+                if (b > mx[k]) mx[k] = b;
+            }
+            if (lane == 0) {
+                sm.red[warp * kMaxObj + k] = mn[k];
+                sm.red[32 * kMaxObj + warp * kMaxObj + k] = mx[k];
+            }
         }
     }
     __syncthreads();
@@ -626,17 +697,51 @@ __global__ void __launch_bounds__(kSelThreads, 1) k_select(Shape s, const float 
     {
         const int B = N2 + M;
         for (int e = tid; e < M * M; e += nth) sm.ext[e] = ext[e];
-        for (int i = 0; i < M; i++) {
-            ExtCand best{0xffffffffu, kNoPos};
-            float fmx = -FLT_MAX;
-            for (int t = tid; t < f0; t += nth) {
-                const float *x = obj + (size_t)sc.sorted[t] * M;
-                const uint32_t v = __float_as_uint(asf_axis(x, sm.ideal, i, M));
-                if (ext_before(v, (uint32_t)t, best, B)) best = ExtCand{v, (uint32_t)t};
-                const float xi = x[i];
-                if (xi > fmx) fmx = xi;
+        // one pass over front 0 for every axis: each member's row is read once.  The
+        // objectives take few distinct values, so ASF ties are common: tree places are
+        // looked up only for ties, at most once per member and once per running best.
+        constexpr uint64_t kUnset = ~0ull;
+        ExtCand bests[kMaxObj];
+        uint64_t bks[kMaxObj];  // tree key of each running best (kUnset: not computed yet)
+        float fmxs[kMaxObj], id[kMaxObj];
+#pragma unroll
+        for (int i = 0; i < kMaxObj; i++) {
+            bests[i] = ExtCand{0xffffffffu, kNoPos};
+            bks[i] = kUnset;
+            fmxs[i] = -FLT_MAX;
+            id[i] = i < M ? sm.ideal[i] : 0.0f;
+        }
+        for (int t = tid; t < f0; t += nth) {
+            const float *x = obj + (size_t)sc.sorted[t] * M;
+            float xv[kMaxObj], a[kMaxObj];
+#pragma unroll
+            for (int k = 0; k < kMaxObj; k++) xv[k] = k < M ? x[k] : 0.0f;
+            asf_rows(xv, id, M, a);
+            uint64_t tk = kUnset;  // this member's tree key, once needed
+#pragma unroll
+            for (int i = 0; i < kMaxObj; i++) {
+                if (i < M) {
+                    const uint32_t v = __float_as_uint(a[i]);
+                    bool take = v < bests[i].v || bests[i].pos == kNoPos;
+                    if (!take && v == bests[i].v) {  // tie: the earlier position in tree order
+                        if (tk == kUnset) tk = tree_rank(sc.trank, t);
+                        if (bks[i] == kUnset) bks[i] = tree_rank(sc.trank, (int)bests[i].pos);
+                        take = tk < bks[i];
+                    }
+                    if (take) {
+                        bests[i] = ExtCand{v, (uint32_t)t};
+                        bks[i] = tk;
+                    }
+                    if (xv[i] > fmxs[i]) fmxs[i] = xv[i];
+                }
             }
-            uint64_t bkey = best.pos != kNoPos ? tree_key((int)best.pos, B) : ~0ull;
+        }
+#pragma unroll
+        for (int i = 0; i < kMaxObj; i++) {
+            if (i >= M) break;
+            ExtCand best = bests[i];
+            float fmx = fmxs[i];
+            uint64_t bkey = best.pos == kNoPos ? ~0ull : (bks[i] != kUnset ? bks[i] : tree_rank(sc.trank, (int)best.pos));
             for (int o = 16; o > 0; o >>= 1) {
                 const uint32_t v2 = __shfl_xor_sync(0xffffffffu, best.v, o), p2 = __shfl_xor_sync(0xffffffffu, best.pos, o);
                 const uint64_t k2 = __shfl_xor_sync(0xffffffffu, bkey, o);
@@ -673,7 +778,7 @@ __global__ void __launch_bounds__(kSelThreads, 1) k_select(Shape s, const float 
                 xs.xfkey[warp] = key;
                 sm.red[32 * kMaxObj + warp] = b;  // max of front 0 (MNDF)
             }
-            if (lane == 1) xs.xkey[warp] = tree_key(f0 + warp, B);
+            if (lane == 1) xs.xkey[warp] = tree_rank(sc.trank, f0 + warp);
         }
         __syncthreads();
         // The current extreme point r, as the axes are done in turn, is a copy of an
@@ -698,7 +803,7 @@ __global__ void __launch_bounds__(kSelThreads, 1) k_select(Shape s, const float 
             // not below FLT_MAX: the first filler in tree order, only then
             uint64_t fkey = ~0ull;
             if (__any_sync(0xffffffffu, lane < M && xs.xc[0][lane].v >= vmax)) {
-                for (int t = f0 + M + lane; t < B; t += 32) fkey = min(fkey, tree_key(t, B));
+                for (int t = f0 + M + lane; t < B; t += 32) fkey = min(fkey, tree_rank(sc.trank, t));
                 for (int o = 16; o > 0; o >>= 1) fkey = min(fkey, __shfl_xor_sync(0xffffffffu, fkey, o));
             }
             int src = lane;
@@ -749,13 +854,16 @@ __global__ void __launch_bounds__(kSelThreads, 1) k_select(Shape s, const float 
     }
 
     // ---------------- hyperplane intercepts (GaussianElimination :555-599, check :929-956)
-    if (warp == 0) {
-        const int exc = hyperplane_nadir(M, sm.ext, sm.ideal, sm.nadir, lane);
-        if (lane == 0) sm.hyp = exc;
-        if (exc && lane < M) {
+    if (tid == 0) {
+        const int exc = hyperplane_nadir<MM>(sm.ext, sm.ideal, sm.nadir);
+        sm.hyp = exc;
+        if (exc) {
             // updateNadirValue_MNDF (:685-884): max over front 0, worst when too close to ideal
-            const float b = sm.red[32 * kMaxObj + lane];
-            sm.nadir[lane] = __fsub_rn(b, sm.ideal[lane]) > 1e-6f ? b : sm.worst[lane];
+#pragma unroll
+            for (int k = 0; k < MM; k++) {
+                const float b = sm.red[32 * kMaxObj + k];
+                sm.nadir[k] = __fsub_rn(b, sm.ideal[k]) > 1e-6f ? b : sm.worst[k];
+            }
         }
     }
     __syncthreads();
@@ -876,12 +984,14 @@ __global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc
     int *nj = cj + R;
     int *coff = nj + R;    // R + 1
     int *kq = coff + R + 1;
-    int *lv = kq + R;      // Lsz: level histogram, then picks before each level
-    int *las = lv + Lsz;   // 2N: reference point of each last-front member (position count0 + t)
-    int *lsol = las + N2;  // 2N: the member itself
-    int *cand = lsol + N2; // 2N: candidate lists (CSR by reference point)
-    int *pofs = cand + N2; // R + 1: first pick of each point
-    uint32_t *rnd = reinterpret_cast<uint32_t *>(pofs + R + 1);  // N: the raw draw of every pick
+    int *lv = kq + R;      // Lsz: member distances (bits) for the lists, level histogram, picks before each level
+    // 4N: sort keys (point, member) of the last front's members, then in place the
+    // candidate lists (CSR by reference point)
+    uint32_t *keys = reinterpret_cast<uint32_t *>(lv + Lsz);
+    int *cand = reinterpret_cast<int *>(keys);
+    int *lsol = cand + 2 * N2;  // 2N: the solution of each last-front member (position count0 + t)
+    int *pofs = lsol + N2;      // R + 1: first pick of each point
+    uint32_t *rnd = reinterpret_cast<uint32_t *>(pofs + R + 1);  // N: the list slot of every pick
     const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarps = nth >> 5;
     const uint32_t gen = *d_gen;
     if (sc.info[3]) {  // fronts filled N exactly; k_select wrote the survivors
@@ -889,103 +999,131 @@ __global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc
         return;
     }
     const int rc = sc.info[0], count0 = sc.info[5], need = N - count0;
+    const int nm = rc - count0;  // members of the last front
     for (int j = tid; j < R; j += nth) {
         cj[j] = sc.rho[j];
         nj[j] = sc.ncand[j];
         kq[j] = 0;
     }
-    for (int l = tid; l < Lsz; l += nth) lv[l] = 0;
-    for (int t = count0 + tid; t < rc; t += nth) {
-        las[t - count0] = sc.assoc[t];
-        lsol[t - count0] = sc.sorted[t];
+    // member t of the last front: its sort key (point, then t), the solution, and (in
+    // lv, free until the level histogram) its perpendicular distance as bits.  Keys
+    // past the members pad the sort to a power of two.
+    const int tb = 32 - __clz(max(nm - 1, 1));  // bits of a member index
+    int P = 1;
+    while (P < nm) P <<= 1;
+    for (int t = tid; t < P; t += nth) {
+        if (t < nm) {
+            const int sol = sc.sorted[count0 + t];
+            keys[t] = ((uint32_t)sc.assoc[count0 + t] << tb) | (uint32_t)t;
+            lsol[t] = sol;
+            lv[t] = __float_as_int(sc.dist[sol]);
+        } else {
+            keys[t] = 0xffffffffu;
+        }
     }
     if (tid == 0) sm.i0 = 0;
     __syncthreads();
-    // CSR offsets of the candidate lists; level histogram (+1 at c_j, -1 at c_j + n_j)
+    // CSR offsets of the candidate lists
     for (int base = 0; base < R; base += nth) {
         const int j = base + tid;
         const int v = j < R ? nj[j] : 0;
         int tot;
         const int pos = block_scan_value(v, sm, &tot);
-        if (j < R) {
-            coff[j] = sm.i0 + pos;
-            if (v > 0) {
-                atomicAdd(&lv[min(cj[j], Lsz - 1)], 1);
-                atomicAdd(&lv[min(cj[j] + v, Lsz - 1)], -1);
-            }
-        }
+        if (j < R) coff[j] = sm.i0 + pos;
         __syncthreads();
         if (tid == 0) sm.i0 += tot;
         __syncthreads();
     }
     if (tid == 0) coff[R] = sm.i0;
-    // candidate lists in ascending position: one warp walks the last front's members
-    // in order, 32 at a time; __match_any_sync groups the lanes of the same point,
-    // each lane's place is its point's fill so far plus the lanes of its group below
-    // it, and the group's lowest lane advances the fill (kq counts it).  las[t] then
-    // holds the member's place in the lists.
-    const int nm = rc - count0;
-    if (warp == 0) {
-        for (int t0 = 0; t0 < nm; t0 += 32) {
-            const int t = t0 + lane;
-            const int j = t < nm ? las[t] : -1 - lane;  // lanes past the end match nobody
-            const unsigned peers = __match_any_sync(0xffffffffu, j);
-            if (t < nm) {
-                const int leader = __ffs(peers) - 1;
-                const int below = __popc(peers & ((1u << lane) - 1u));
-                const int pos = coff[j] + kq[j] + below;
-                cand[pos] = lsol[t];
-                las[t] = pos;
-                __syncwarp(peers);
-                if (lane == leader) kq[j] += __popc(peers);
-            }
-            __syncwarp();
-        }
-    }
+    // candidate lists in ascending member order: sorting the keys orders the members
+    // by point, then by member, so point j's list is positions coff[j] .. coff[j] + n_j - 1
+    block_bitonic_sort(keys, P, tid, nth);
+    for (int q = tid; q < nm; q += nth) cand[q] = (int)(keys[q] & ((1u << tb) - 1u));  // member indices t
     __syncthreads();
     // the nearest member of a point with niche count 0 (the first in list order among
     // equal distances) is its pick at level 0, which is the point's first pick whenever
-    // it has one: found with two atomicMin passes over the members (distance bits,
-    // then place) and moved to the list's end (a point that ends up picking nothing
-    // never reads its list).  pofs and kq serve as scratch.
+    // it has one: it is moved to the list's end (a point that ends up picking nothing
+    // never reads its list).  Distances are >= +0 (or FLT_MAX), so their bits order as
+    // the values do.  Lists of up to kShortList members are scanned by one thread;
+    // longer ones are queued (in pofs, free until the picks) for one warp each.
+    constexpr int kShortList = 64;
+    if (tid == 0) sm.i1 = 0;
+    __syncthreads();
     for (int j = tid; j < R; j += nth) {
-        pofs[j] = 0x7fffffff;
-        kq[j] = 0x7fffffff;
-    }
-    __syncthreads();
-    for (int t = tid; t < nm; t += nth) {
-        const int j = sc.assoc[count0 + t];
-        // distances are >= +0 (or FLT_MAX), so their bits order as the values do
-        if (cj[j] == 0) atomicMin(&pofs[j], __float_as_int(sc.dist[lsol[t]]));
-    }
-    __syncthreads();
-    for (int t = tid; t < nm; t += nth) {
-        const int j = sc.assoc[count0 + t];
-        if (cj[j] == 0 && __float_as_int(sc.dist[lsol[t]]) == pofs[j]) atomicMin(&kq[j], las[t] - coff[j]);
-    }
-    __syncthreads();
-    for (int j = tid; j < R; j += nth)
-        if (cj[j] == 0 && nj[j] > 0) {
-            int *cl = cand + coff[j];
-            const int slot = kq[j], last = nj[j] - 1, pick = cl[slot];
-            cl[slot] = cl[last];
-            cl[last] = pick;
+        const int n = nj[j];
+        if (cj[j] != 0 || n == 0) continue;
+        if (n > kShortList) {
+            pofs[atomicAdd(&sm.i1, 1)] = j;
+            continue;
         }
+        int *cl = cand + coff[j];
+        uint32_t bd = 0xffffffffu;
+        int slot = 0;
+        for (int q = 0; q < n; q++) {
+            const uint32_t d = (uint32_t)lv[cl[q]];
+            if (d < bd) {
+                bd = d;
+                slot = q;
+            }
+        }
+        const int pick = cl[slot];
+        cl[slot] = cl[n - 1];
+        cl[n - 1] = pick;
+    }
     __syncthreads();
+    for (int u = warp; u < sm.i1; u += nwarps) {
+        const int j = pofs[u], n = nj[j];
+        int *cl = cand + coff[j];
+        uint64_t best = ~0ull;
+        for (int q = lane; q < n; q += 32) {
+            const uint64_t key = ((uint64_t)(uint32_t)lv[cl[q]] << 32) | (uint32_t)q;
+            best = key < best ? key : best;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const uint64_t other = __shfl_xor_sync(0xffffffffu, best, o);
+            best = other < best ? other : best;
+        }
+        if (lane == 0) {
+            const int slot = (int)(uint32_t)best, pick = cl[slot];
+            cl[slot] = cl[n - 1];
+            cl[n - 1] = pick;
+        }
+    }
+    __syncthreads();
+    // member indices to solutions; then the level histogram (+1 at c_j, -1 at c_j + n_j)
+    for (int q = tid; q < nm; q += nth) cand[q] = lsol[cand[q]];
+    for (int l = tid; l < Lsz; l += nth) lv[l] = 0;
+    if (tid == 0) sm.i4 = 0;
+    __syncthreads();
+    for (int base = 0; base < R; base += nth) {
+        const int j = base + tid;
+        const int v = j < R ? nj[j] : 0;
+        const int l0 = min(j < R ? cj[j] : 0, Lsz - 1), l1 = min((j < R ? cj[j] : 0) + v, Lsz - 1);
+        // most points start at level 0: one add per warp there
+        const unsigned z = __ballot_sync(0xffffffffu, v > 0 && l0 == 0);
+        if (lane == 0 && z) atomicAdd(&lv[0], __popc(z));
+        if (v > 0 && l0 != 0) atomicAdd(&lv[l0], 1);
+        if (v > 0) atomicAdd(&lv[l1], -1);
+        const int top = __reduce_max_sync(0xffffffffu, v > 0 ? l1 : 0);
+        if (lane == 0) atomicMax(&sm.i4, top);
+    }
+    __syncthreads();
+    // every pick falls below level max_j(c_j + n_j): the scans stop there
+    const int Lscan = min(Lsz, sm.i4 + 1);
     // active points per level, then picks before each level: lv[l] = picks at levels < l
     if (tid == 0) {
         sm.i0 = 0;
         sm.i1 = 0;
     }
     __syncthreads();
-    for (int base = 0; base < Lsz; base += nth) {
+    for (int base = 0; base < Lscan; base += nth) {
         const int l = base + tid;
-        const int d = l < Lsz ? lv[l] : 0;
+        const int d = l < Lscan ? lv[l] : 0;
         int tot;
         const int act = sm.i0 + block_scan_value(d, sm, &tot) + d;  // active points at level l
         int tot2;
-        const int before = sm.i1 + block_scan_value(l < Lsz ? act : 0, sm, &tot2);
-        if (l < Lsz) lv[l] = before;
+        const int before = sm.i1 + block_scan_value(l < Lscan ? act : 0, sm, &tot2);
+        if (l < Lscan) lv[l] = before;
         __syncthreads();
         if (tid == 0) {
             sm.i0 += tot;
@@ -999,7 +1137,7 @@ __global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc
         sm.i3 = 0;
     }
     __syncthreads();
-    for (int l = tid; l + 1 < Lsz; l += nth)
+    for (int l = tid; l + 1 < Lscan; l += nth)
         if (lv[l] < need && lv[l + 1] >= need) {
             sm.i2 = l;
             sm.i3 = need - lv[l];
@@ -1019,7 +1157,7 @@ __global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc
         if (tid == 0) sm.i0 += tot;
         __syncthreads();
     }
-    // the raw draws of all picks, computed in parallel (each is keyed by its point and level)
+    // the slot of every pick, computed in parallel (each draw is keyed by its point and level)
     if (tid == 0) sm.i0 = 0;
     __syncthreads();
     for (int base = 0; base < R; base += nth) {
@@ -1033,50 +1171,55 @@ __global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc
     }
     if (tid == 0) pofs[R] = sm.i0;
     __syncthreads();
-    for (int pk = tid; pk < pofs[R]; pk += nth) {
+    // Each pick also gets the key (level, point) of its place among the survivors: the
+    // picks of a level follow those of earlier levels, in ascending point index.  The
+    // keys sit in the second half of the keys region (the lists use the first).
+    const int npick = pofs[R];  // = need
+    uint32_t *pkeys = keys + N2;
+    const int pb = 32 - __clz(max(R - 1, 1));  // bits of a point index
+    int P2 = 1;
+    while (P2 < npick) P2 <<= 1;
+    for (int pk = tid; pk < P2; pk += nth) {
+        if (pk >= npick) {
+            pkeys[pk] = 0xffffffffu;
+            continue;
+        }
         int lo = 0, hi = R - 1;  // point: pofs[lo] <= pk < pofs[lo + 1]
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
             if (pofs[mid] <= pk) lo = mid;
             else hi = mid - 1;
         }
-        const int level = cj[lo] + (pk - pofs[lo]);
-        rnd[pk] = level == 0 ? 0u : draw(s.seed, TAG_NICHE, gen, (uint32_t)lo, (uint32_t)level, 0);
+        const int q = pk - pofs[lo], level = cj[lo] + q, nc = nj[lo] - q;  // nc: candidates left
+        // level 0: the nearest member, already at the list's end
+        rnd[pk] = level == 0 ? (uint32_t)(nc - 1)
+                             : rng_uint(draw(s.seed, TAG_NICHE, gen, (uint32_t)lo, (uint32_t)level, 0), (uint32_t)nc);
+        pkeys[pk] = ((uint32_t)level << pb) | (uint32_t)lo;
     }
     __syncthreads();
-    // each point takes its picks; the q-th pick ends at list position n_j - 1 - q
+    // each point takes its picks (rnd now holds each pick's slot); the q-th pick ends
+    // at list position n_j - 1 - q.  The chain is serial per point: the next slot is
+    // read before this pick's swap is stored.
     for (int j = tid; j < R; j += nth) {
+        const int npk = kq[j];
+        if (npk == 0) continue;
         int *cl = cand + coff[j];
-        int nc = nj[j];
-        for (int q = 0; q < kq[j]; q++) {
-            const int level = cj[j] + q;
-            int slot = 0;
-            if (level == 0) {
-                slot = nc - 1;  // made while the lists were built: already at the end
-            } else {
-                slot = (int)rng_uint(rnd[pofs[j] + q], (uint32_t)nc);
-            }
+        const uint32_t *sl = rnd + pofs[j];
+        int last = nj[j] - 1, slot = (int)sl[0];
+        for (int q = 0; q < npk; q++, last--) {
+            const int nxt = q + 1 < npk ? (int)sl[q + 1] : 0;
             const int pick = cl[slot];
-            cl[slot] = cl[nc - 1];
-            cl[nc - 1] = pick;
-            nc--;
+            cl[slot] = cl[last];
+            cl[last] = pick;
+            slot = nxt;
         }
     }
     for (int t = tid; t < count0; t += nth) surv[t] = sc.sorted[t];
-    __syncthreads();
-    // positions: level l's picks follow the picks of earlier levels, in ascending point index
-    const int lmax = min(Ls, Lsz - 1);
-    for (int l = warp; l <= lmax; l += nwarps) {
-        int run = 0;
-        for (int jb = 0; jb < R; jb += 32) {
-            const int j = jb + lane;
-            const bool act = j < R && nj[j] > 0 && cj[j] <= l && l < cj[j] + nj[j];
-            const uint32_t bal = __ballot_sync(0xffffffffu, act);
-            const int rank = run + __popc(bal & ((1u << lane) - 1u));
-            if (act && (l < Ls || rank < K))
-                surv[count0 + lv[l] + rank] = cand[coff[j] + nj[j] - 1 - (l - cj[j])];
-            run += __popc(bal);
-        }
+    block_bitonic_sort(pkeys, P2, tid, nth);
+    for (int p = tid; p < npick; p += nth) {
+        const uint32_t key = pkeys[p];
+        const int j = (int)(key & ((1u << pb) - 1u)), level = (int)(key >> pb);
+        surv[count0 + p] = cand[coff[j] + nj[j] - 1 - (level - cj[j])];
     }
     __syncthreads();
     if (tid == 0 && bump_gen) *d_gen = gen + 1;
@@ -1084,8 +1227,9 @@ __global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc
 
 size_t niche_smem_bytes(const Shape &s)
 {
+    // cj, nj, coff, kq | lv | keys (4N) | lsol (2N) | pofs | rnd
     return ((sizeof(SelSmem) + 15) & ~size_t(15)) +
-           (size_t)(4 * s.R + 1 + 2 * s.N + 4 + 3 * 2 * s.N + s.R + 1 + s.N) * sizeof(int);
+           (size_t)(4 * s.R + 1 + 2 * s.N + 4 + 4 * s.N + 2 * s.N + s.R + 1 + s.N) * sizeof(int);
 }
 
 size_t select_smem_bytes(const Shape &s)
@@ -1098,20 +1242,7 @@ cudaError_t launch_select(const Shape &s, const float *obj, float *ext, const fl
                           int32_t *surv, uint32_t *d_gen, int bump_gen, cudaStream_t st)
 {
     cudaError_t e;
-    const size_t dsm = (size_t)2 * s.N * s.M * sizeof(float);
-    if (dsm <= kDomTiledSmemMax) {
-        const int g = (2 * s.N + kDomRows - 1) / kDomRows;
-        if (s.M == 4) {
-            if ((e = raise_smem_limit((const void *)k_dominance_tiled<4>, dsm)) != cudaSuccess) return e;
-            k_dominance_tiled<4><<<g, 32 * kDomRows, dsm, st>>>(s, obj, sc.dom, sc.np);
-        } else if (s.M == 6) {
-            if ((e = raise_smem_limit((const void *)k_dominance_tiled<6>, dsm)) != cudaSuccess) return e;
-            k_dominance_tiled<6><<<g, 32 * kDomRows, dsm, st>>>(s, obj, sc.dom, sc.np);
-        } else {
-            if ((e = raise_smem_limit((const void *)k_dominance_tiled<0>, dsm)) != cudaSuccess) return e;
-            k_dominance_tiled<0><<<g, 32 * kDomRows, dsm, st>>>(s, obj, sc.dom, sc.np);
-        }
-    } else if (s.M == 4) {
+    if (s.M == 4) {
         k_dominance<4><<<2 * s.N, 256, 0, st>>>(s, obj, sc.dom, sc.np);
     } else if (s.M == 6) {
         k_dominance<6><<<2 * s.N, 256, 0, st>>>(s, obj, sc.dom, sc.np);
@@ -1125,9 +1256,13 @@ cudaError_t launch_select(const Shape &s, const float *obj, float *ext, const fl
     k_fronts<<<kFrontCtas, kFrontThreads, fsm, st>>>(s, sc);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     size_t smem = select_smem_bytes(s);
-    e = raise_smem_limit((const void *)k_select, smem);
-    if (e != cudaSuccess) return e;
-    k_select<<<1, kSelThreads, smem, st>>>(s, obj, ext, refpts, sc, surv, d_gen, bump_gen);
+    if (s.M == 4) {
+        if ((e = raise_smem_limit((const void *)k_select<4>, smem)) != cudaSuccess) return e;
+        k_select<4><<<1, kSelThreads, smem, st>>>(s, obj, ext, refpts, sc, surv, d_gen, bump_gen);
+    } else {
+        if ((e = raise_smem_limit((const void *)k_select<6>, smem)) != cudaSuccess) return e;
+        k_select<6><<<1, kSelThreads, smem, st>>>(s, obj, ext, refpts, sc, surv, d_gen, bump_gen);
+    }
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     const int warps_needed = 2 * s.N;
     const int ag = std::min((warps_needed + 7) / 8, 148 * 8);
