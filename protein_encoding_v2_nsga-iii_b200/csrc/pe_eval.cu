@@ -225,6 +225,7 @@ __device__ void light_eval(const Shape &s, const DevTables *gt, const SmemTab &s
             if (kind == 0) {  // CAI: exp(mean log w)
                 long long S = 0;
                 int z = 0;
+#pragma unroll 4
                 for (int a = lane; a < L; a += 32) {
                     int id = row[a];
                     S += st.lw[id];
@@ -256,6 +257,7 @@ __device__ void light_eval(const Shape &s, const DevTables *gt, const SmemTab &s
             } else {  // GC3 (or whole-CDS GC) count
                 int cnt = 0;
                 if (s.gcmode == PE_GC3) {
+#pragma unroll 4
                     for (int a = lane; a < L; a += 32) cnt += st.gc3[row[a]];
                 } else {
                     const uint2 *A = planes + c * s.Wp;
@@ -413,18 +415,37 @@ __device__ __forceinline__ uint32_t word4(const uint4 &w, int u)
     return u == 0 ? w.x : u == 1 ? w.y : u == 2 ? w.z : w.w;
 }
 
-__device__ __forceinline__ void shuffle_k(const Shape &s, uint32_t gen, uint32_t ridx, int pos, int k, int *arr)
+// indexArrayShuffling (include/utils.cuh:203-218) of 0 .. k-1 with the draws
+// MDRAW(pos, 1 .. k-1), as a packed array (entry u in bits 3u .. 3u+2).  Draws 1..3
+// are words 1..3 of one Philox block and draws 4, 5 words 0, 1 of the next, so at
+// most two blocks are computed.
+__device__ __forceinline__ uint32_t shuffle_k(const Shape &s, uint32_t gen, uint32_t ridx, int pos, int k)
 {
-    // indexArrayShuffling (include/utils.cuh:203-218): draws 1..k-1
-    for (int i = 0; i < 6; i++) arr[i] = i;
-    int d = 1;
-    for (int i = k - 1; i > 0; i--) {
-        int j = (int)rng_uint(MDRAW(pos, d), (uint32_t)(i + 1));
-        d++;
-        int t = arr[i];
-        arr[i] = arr[j];
-        arr[j] = t;
+    uint32_t arr = 0;
+#pragma unroll
+    for (int u = 0; u < 6; u++) arr |= (uint32_t)u << (3 * u);
+    if (k < 2) return arr;
+    const uint2 key = make_uint2((uint32_t)s.seed, (uint32_t)(s.seed >> 32));
+    const uint4 b0 = philox4x32_10(make_uint4(TAG_MUT, gen, ridx, (uint32_t)pos * 8u), key);
+    uint4 b1 = make_uint4(0u, 0u, 0u, 0u);
+    if (k > 4) b1 = philox4x32_10(make_uint4(TAG_MUT, gen, ridx, (uint32_t)pos * 8u + 1u), key);
+    const uint32_t w[5] = {b0.y, b0.z, b0.w, b1.x, b1.y};  // draws 1 .. 5
+#pragma unroll
+    for (int d = 1; d <= 5; d++) {
+        const int i = k - d;  // i = k-1 down to 1
+        if (i < 1) break;
+        const int j = (int)rng_uint(w[d - 1], (uint32_t)(i + 1));
+        const uint32_t ai = (arr >> (3 * i)) & 7u, aj = (arr >> (3 * j)) & 7u;
+        arr = (arr & ~(7u << (3 * i)) & ~(7u << (3 * j))) | (aj << (3 * i)) | (ai << (3 * j));
     }
+    return arr;
+}
+
+// mismatching nucleotides of two codons from their plane patterns
+__device__ __forceinline__ int codon_mismatch(uint32_t pa, uint32_t pb)
+{
+    const uint32_t x = pa ^ pb;
+    return __popc((x | (x >> 4)) & 7u);
 }
 
 // Marks the plane words codon a of CDS c covers (nucleotides 3a .. 3a+2: one or two
@@ -451,11 +472,13 @@ __device__ void mutate_solution(const Shape &s, const DevTables *gt, VarSmem &sm
     case 0: {  // mutationRandom (:16-63)
         for (int q = tid; 4 * q < m * L; q += nth) {
             const uint4 w4 = pdraw4(s, gen, ridx, q);
+            const int c0 = (4 * q) / L, a0 = 4 * q - c0 * L;  // CDS and codon of position 4q
 #pragma unroll
             for (int u = 0; u < 4; u++) {
                 const int pos = 4 * q + u;
                 if (pos >= m * L) break;
-                int c = pos / L, a = pos - c * L;
+                const bool wrap = a0 + u >= L;  // L >= 3, so a quad crosses at most one CDS boundary
+                const int c = c0 + (wrap ? 1 : 0), a = a0 + u - (wrap ? L : 0);
                 int am = aa[a];
                 int k = st.count[am];
                 if (rng_u01(word4(w4, u)) > pm || k == 1) continue;
@@ -511,17 +534,19 @@ __device__ void mutate_solution(const Shape &s, const DevTables *gt, VarSmem &sm
             float curs = 0.0f;
             if (left >= 0 && left < 61 && curg < 61) curs = __ldg(&gt->cps[left * 61 + curg]);
             if (right < 61 && curg < 61) curs = __fadd_rn(curs, __ldg(&gt->cps[curg * 61 + right]));
-            int up[6], nup = 0;
+            uint32_t up = 0;  // the better synonyms, packed 3 bits each
+            int nup = 0;
             for (int j = 0; j < k; j++) {
                 if (j == cur) continue;
                 int g = st.start[am] + j;
                 float ns = 0.0f;
                 if (left >= 0 && left < 61 && g < 61) ns = __fadd_rn(ns, __ldg(&gt->cps[left * 61 + g]));
                 if (right < 61 && g < 61) ns = __fadd_rn(ns, __ldg(&gt->cps[g * 61 + right]));
-                if (ns > curs) up[nup++] = j;
+                if (ns > curs) up |= (uint32_t)j << (3 * nup++);
             }
             if (nup > 0) {
-                row[a] = (uint8_t)(st.start[am] + up[rng_uint(MDRAW(a, 1), (uint32_t)nup)]);
+                const int pick = (int)rng_uint(MDRAW(a, 1), (uint32_t)nup);
+                row[a] = (uint8_t)(st.start[am] + ((up >> (3 * pick)) & 7u));
                 mark_codon(s, dirty, c, a);
             }
           }
@@ -546,15 +571,17 @@ __device__ void mutate_solution(const Shape &s, const DevTables *gt, VarSmem &sm
             bool hl = a > 0, hr = a < L - 1;
             int lft = hl ? row[a - 1] : 0, rgt = hr ? row[a + 1] : 0;
             int curs = (hl ? __ldg(&gt->hsc[lft * 64 + row[a]]) : 0) + (hr ? __ldg(&gt->hsc[row[a] * 64 + rgt]) : 0);
-            int up[6], nup = 0;
+            uint32_t up = 0;  // the better synonyms, packed 3 bits each
+            int nup = 0;
             for (int j = 0; j < k; j++) {
                 if (j == cur) continue;
                 int g = st.start[am] + j;
                 int ns = (hl ? __ldg(&gt->hsc[lft * 64 + g]) : 0) + (hr ? __ldg(&gt->hsc[g * 64 + rgt]) : 0);
-                if (ns > curs) up[nup++] = j;
+                if (ns > curs) up |= (uint32_t)j << (3 * nup++);
             }
             if (nup > 0) {
-                row[a] = (uint8_t)(st.start[am] + up[rng_uint(MDRAW(a, 1), (uint32_t)nup)]);
+                const int pick = (int)rng_uint(MDRAW(a, 1), (uint32_t)nup);
+                row[a] = (uint8_t)(st.start[am] + ((up >> (3 * pick)) & 7u));
                 mark_codon(s, dirty, c, a);
             }
           }
@@ -572,34 +599,42 @@ __device__ void mutate_solution(const Shape &s, const DevTables *gt, VarSmem &sm
             int am = aa[a];
             int k = st.count[am];
             if (rng_u01(word4(w4, u)) > pm || k == 1) continue;
-            int arr[6];
-            shuffle_k(s, gen, ridx, a, k, arr);
-            int x = ids[c1 * s.Lp + a];
-            int cur = x - st.start[am];
-            int y2 = ids[c2 * s.Lp + a];
-            int cur_pair = 0;
-            for (int b = 0; b < 3; b++) cur_pair += st.nt[x][b] != st.nt[y2][b];
+            const uint32_t arr = shuffle_k(s, gen, ridx, a, k);
+            const int x = ids[c1 * s.Lp + a];
+            const int cur = x - st.start[am];
+            // mismatches of every synonym sh against CDS c2 (np) and its fewest against the
+            // other CDSs (nm), the current codon's too, one pass over the CDSs
+            const uint32_t px = st.pat[x], p2 = st.pat[ids[c2 * s.Lp + a]];
+            uint32_t pg[6];
+            int nmv[6];
+#pragma unroll
+            for (int sh = 0; sh < 6; sh++) {
+                pg[sh] = sh < k ? st.pat[st.start[am] + sh] : 0u;
+                nmv[sh] = 127;
+            }
             int cur_m = 127;
             for (int j = 0; j < m; j++) {
                 if (j == c1) continue;
-                int yj = ids[j * s.Lp + a], d = 0;
-                for (int b = 0; b < 3; b++) d += st.nt[x][b] != st.nt[yj][b];
-                cur_m = min(cur_m, d);
+                const uint32_t py = st.pat[ids[j * s.Lp + a]];
+                cur_m = min(cur_m, codon_mismatch(px, py));
+#pragma unroll
+                for (int sh = 0; sh < 6; sh++)
+                    if (sh < k) nmv[sh] = min(nmv[sh], codon_mismatch(pg[sh], py));
             }
+            const int cur_pair = codon_mismatch(px, p2);
             int best_pair = -1, best_m = -1, best = -1;
-            for (int u = 0; u < k; u++) {
-                int sh = arr[u];
+#pragma unroll
+            for (int u = 0; u < 6; u++) {
+                if (u >= k) break;
+                const int sh = (arr >> (3 * u)) & 7u;
                 if (sh == cur) continue;
-                int g = st.start[am] + sh;
-                int np = 0;
-                for (int b = 0; b < 3; b++) np += st.nt[g][b] != st.nt[y2][b];
-                int nm = 127;
-                for (int j = 0; j < m; j++) {
-                    if (j == c1) continue;
-                    int yj = ids[j * s.Lp + a], d = 0;
-                    for (int b = 0; b < 3; b++) d += st.nt[g][b] != st.nt[yj][b];
-                    nm = min(nm, d);
-                }
+                int np = 0, nm = 0;
+#pragma unroll
+                for (int q = 0; q < 6; q++)
+                    if (q == sh) {
+                        np = codon_mismatch(pg[q], p2);
+                        nm = nmv[q];
+                    }
                 if (nm > cur_m && nm > best_m) {
                     best_m = nm;
                     best = sh;
@@ -637,13 +672,12 @@ __device__ void mutate_solution(const Shape &s, const DevTables *gt, VarSmem &sm
             int am = aa[a];
             int k = st.count[am];
             if (rng_u01(word4(w4, u)) > prob || k == 1) continue;
-            int arr[6];
-            shuffle_k(s, gen, ridx, a, k, arr);
+            const uint32_t arr = shuffle_k(s, gen, ridx, a, k);
             int curg = row[a];
             int cur = curg - st.start[am];
             int cgc = s.gcmode == PE_GC3 ? st.gc3[curg] : st.gcn[curg];
             for (int u = 0; u < k; u++) {
-                int sh = arr[u];
+                int sh = (arr >> (3 * u)) & 7u;
                 if (sh == cur) continue;
                 int g = st.start[am] + sh;
                 int ngc = s.gcmode == PE_GC3 ? st.gc3[g] : st.gcn[g];

@@ -974,7 +974,22 @@ __global__ void __launch_bounds__(256) k_assoc(Shape s, const float *__restrict_
 // only on j, its levels and its list), and writes each level's picks to their
 // positions with one warp per level: the same survivors, in the same order,
 // as the level-by-level loop, in a fixed number of steps.
-__global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc, int32_t *surv, uint32_t *d_gen,
+// k_niche's shared memory without and with the counting sort's [32][R] table; the
+// candidate lists are counted when R <= kCountSortMaxR and the table still fits in
+// the 227 KB a CTA may use
+constexpr int kCountSortMaxR = 512;
+__host__ __device__ inline size_t niche_base_bytes(const Shape &s)
+{
+    // cj, nj, coff, kq | lv | keys (4N) | lsol (2N) | pofs | rnd
+    return ((sizeof(SelSmem) + 15) & ~size_t(15)) +
+           (size_t)(4 * s.R + 1 + 2 * s.N + 4 + 4 * s.N + 2 * s.N + s.R + 1 + s.N) * sizeof(int);
+}
+__host__ __device__ inline bool niche_counting(const Shape &s)
+{
+    return s.R <= kCountSortMaxR && niche_base_bytes(s) + (size_t)32 * s.R * sizeof(int) <= 232448;
+}
+
+__global__ void __launch_bounds__(kSelThreads, 1) k_niche(Shape s, SelectScratch sc, int32_t *surv, uint32_t *d_gen,
                                                        int bump_gen)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1005,22 +1020,29 @@ __global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc
         nj[j] = sc.ncand[j];
         kq[j] = 0;
     }
-    // member t of the last front: its sort key (point, then t), the solution, and (in
-    // lv, free until the level histogram) its perpendicular distance as bits.  Keys
-    // past the members pad the sort to a power of two.
+    // member t of the last front: its point (a sort key (point, then t) for the sort;
+    // the point itself, in the second half of the keys region, for the count), the
+    // solution, and (in lv, free until the level histogram) its perpendicular distance
+    // as bits.  Keys past the members pad the sort to a power of two.
+    const bool counting = niche_counting(s);
+    int *pj = cand + N2;
+    int *hist = reinterpret_cast<int *>(rnd + N);  // [32][R] when counting
     const int tb = 32 - __clz(max(nm - 1, 1));  // bits of a member index
     int P = 1;
     while (P < nm) P <<= 1;
-    for (int t = tid; t < P; t += nth) {
+    for (int t = tid; t < (counting ? nm : P); t += nth) {
         if (t < nm) {
-            const int sol = sc.sorted[count0 + t];
-            keys[t] = ((uint32_t)sc.assoc[count0 + t] << tb) | (uint32_t)t;
+            const int sol = sc.sorted[count0 + t], j = sc.assoc[count0 + t];
+            if (counting) pj[t] = j;
+            else keys[t] = ((uint32_t)j << tb) | (uint32_t)t;
             lsol[t] = sol;
             lv[t] = __float_as_int(sc.dist[sol]);
         } else {
             keys[t] = 0xffffffffu;
         }
     }
+    if (counting)
+        for (int e = tid; e < 32 * R; e += nth) hist[e] = 0;
     if (tid == 0) sm.i0 = 0;
     __syncthreads();
     // CSR offsets of the candidate lists
@@ -1035,10 +1057,30 @@ __global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc
         __syncthreads();
     }
     if (tid == 0) coff[R] = sm.i0;
-    // candidate lists in ascending member order: sorting the keys orders the members
-    // by point, then by member, so point j's list is positions coff[j] .. coff[j] + n_j - 1
-    block_bitonic_sort(keys, P, tid, nth);
-    for (int q = tid; q < nm; q += nth) cand[q] = (int)(keys[q] & ((1u << tb) - 1u));  // member indices t
+    // candidate lists in ascending member order: point j's list is positions coff[j] ..
+    // coff[j] + n_j - 1.  With few points, a counting sort: warp w counts the points of
+    // its chunk of members, each chunk's place in a list follows the earlier chunks',
+    // and one lane per warp places its chunk in order.  Otherwise a sort of the keys
+    // (point, member).
+    if (counting) {
+        const int C = (nm + 31) >> 5, t0 = warp * C, t1 = min(nm, t0 + C);
+        for (int t = t0 + lane; t < t1; t += 32) atomicAdd(&hist[warp * R + pj[t]], 1);
+        __syncthreads();
+        for (int j = tid; j < R; j += nth) {
+            int run = coff[j];
+            for (int w = 0; w < 32; w++) {
+                const int c = hist[w * R + j];
+                hist[w * R + j] = run;
+                run += c;
+            }
+        }
+        __syncthreads();
+        if (lane == 0)
+            for (int t = t0; t < t1; t++) cand[hist[warp * R + pj[t]]++] = t;
+    } else {
+        block_bitonic_sort(keys, P, tid, nth);
+        for (int q = tid; q < nm; q += nth) cand[q] = (int)(keys[q] & ((1u << tb) - 1u));  // member indices t
+    }
     __syncthreads();
     // the nearest member of a point with niche count 0 (the first in list order among
     // equal distances) is its pick at level 0, which is the point's first pick whenever
@@ -1175,13 +1217,17 @@ __global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc
     // picks of a level follow those of earlier levels, in ascending point index.  The
     // keys sit in the second half of the keys region (the lists use the first).
     const int npick = pofs[R];  // = need
+    // survivor order: a warp per level over the points' activity when levels x point
+    // words are few, else a sort of the picks' keys
+    const int lmax = min(Ls, Lsz - 1);
+    const bool by_levels = (lmax + 1) * ((R + 31) >> 5) <= 32 * 24;
     uint32_t *pkeys = keys + N2;
     const int pb = 32 - __clz(max(R - 1, 1));  // bits of a point index
     int P2 = 1;
     while (P2 < npick) P2 <<= 1;
     for (int pk = tid; pk < P2; pk += nth) {
         if (pk >= npick) {
-            pkeys[pk] = 0xffffffffu;
+            if (!by_levels) pkeys[pk] = 0xffffffffu;
             continue;
         }
         int lo = 0, hi = R - 1;  // point: pofs[lo] <= pk < pofs[lo + 1]
@@ -1194,7 +1240,7 @@ __global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc
         // level 0: the nearest member, already at the list's end
         rnd[pk] = level == 0 ? (uint32_t)(nc - 1)
                              : rng_uint(draw(s.seed, TAG_NICHE, gen, (uint32_t)lo, (uint32_t)level, 0), (uint32_t)nc);
-        pkeys[pk] = ((uint32_t)level << pb) | (uint32_t)lo;
+        if (!by_levels) pkeys[pk] = ((uint32_t)level << pb) | (uint32_t)lo;
     }
     __syncthreads();
     // each point takes its picks (rnd now holds each pick's slot); the q-th pick ends
@@ -1215,11 +1261,26 @@ __global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc
         }
     }
     for (int t = tid; t < count0; t += nth) surv[t] = sc.sorted[t];
-    block_bitonic_sort(pkeys, P2, tid, nth);
-    for (int p = tid; p < npick; p += nth) {
-        const uint32_t key = pkeys[p];
-        const int j = (int)(key & ((1u << pb) - 1u)), level = (int)(key >> pb);
-        surv[count0 + p] = cand[coff[j] + nj[j] - 1 - (level - cj[j])];
+    if (by_levels) {
+        __syncthreads();
+        for (int l = warp; l <= lmax; l += nwarps) {
+            int run = 0;
+            for (int jb = 0; jb < R; jb += 32) {
+                const int j = jb + lane;
+                const bool act = j < R && nj[j] > 0 && cj[j] <= l && l < cj[j] + nj[j];
+                const uint32_t bal = __ballot_sync(0xffffffffu, act);
+                const int rank = run + __popc(bal & ((1u << lane) - 1u));
+                if (act && (l < Ls || rank < K)) surv[count0 + lv[l] + rank] = cand[coff[j] + nj[j] - 1 - (l - cj[j])];
+                run += __popc(bal);
+            }
+        }
+    } else {
+        block_bitonic_sort(pkeys, P2, tid, nth);
+        for (int p = tid; p < npick; p += nth) {
+            const uint32_t key = pkeys[p];
+            const int j = (int)(key & ((1u << pb) - 1u)), level = (int)(key >> pb);
+            surv[count0 + p] = cand[coff[j] + nj[j] - 1 - (level - cj[j])];
+        }
     }
     __syncthreads();
     if (tid == 0 && bump_gen) *d_gen = gen + 1;
@@ -1227,9 +1288,7 @@ __global__ void __launch_bounds__(kSelThreads) k_niche(Shape s, SelectScratch sc
 
 size_t niche_smem_bytes(const Shape &s)
 {
-    // cj, nj, coff, kq | lv | keys (4N) | lsol (2N) | pofs | rnd
-    return ((sizeof(SelSmem) + 15) & ~size_t(15)) +
-           (size_t)(4 * s.R + 1 + 2 * s.N + 4 + 4 * s.N + 2 * s.N + s.R + 1 + s.N) * sizeof(int);
+    return niche_base_bytes(s) + (niche_counting(s) ? (size_t)32 * s.R * sizeof(int) : 0);
 }
 
 size_t select_smem_bytes(const Shape &s)
