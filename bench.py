@@ -655,7 +655,9 @@ def main():
                     help="stem-scan CTA size (0: timed per instance at init); a fixed size keeps a run "
                          "under a profiler, which slows every launch, on the kernels a plain run picks")
     ap.add_argument("--profile-case", action="store_true",
-                    help="only build the bench instance, init and run 2 generations (for ncu captures)")
+                    help="only build the bench instance, init and run --profile-gens generations (for ncu captures)")
+    ap.add_argument("--profile-gens", type=int, default=2,
+                    help="generations of --profile-case (e.g. 60 to capture a steady-state selection)")
     args = ap.parse_args()
     if args.steps is None:
         args.steps = 3 if args.impl == "reference" else 500
@@ -678,7 +680,7 @@ def main():
                         sl_kind=SL_KIND)
         eng.init()
         scans, cells = [eng.scan_count()], [eng.scan_cells()]
-        for _ in range(2):
+        for _ in range(args.profile_gens):
             eng.step(1)
             scans.append(eng.scan_count())
             cells.append(eng.scan_cells())

@@ -495,7 +495,7 @@ int pe_create(const pe_config *cfg, const int8_t *aa_idx, int32_t aa_len, const 
     if ((rc = in->alloc(&in->d_surv, (size_t)N))) return cleanup(rc);
     if ((rc = in->alloc(&in->d_order, (size_t)2 * N))) return cleanup(rc);
     if ((rc = in->alloc(&in->sc.dom, (size_t)N2 * words))) return cleanup(rc);
-    if ((rc = in->alloc(&in->sc.np, (size_t)N2))) return cleanup(rc);
+    if ((rc = in->alloc(&in->sc.np, (size_t)N2 * dom_tile_count(N2)))) return cleanup(rc);
     if ((rc = in->alloc(&in->sc.front, (size_t)N2))) return cleanup(rc);
     if ((rc = in->alloc(&in->sc.sorted, (size_t)N2))) return cleanup(rc);
     if ((rc = in->alloc(&in->sc.assoc, (size_t)N2))) return cleanup(rc);
@@ -749,7 +749,8 @@ int pe_instance_bytes(const pe_config *cfg, int32_t aa_len, uint64_t *bytes)
     auto r = [](uint64_t b) { return (b + 511) & ~uint64_t(511); };  // allocation granularity
     uint64_t t = r(sizeof(DevTables)) + r(L) + r(R * M * 4);
     t += 2 * (r(N2 * m * Lp) + r(N2 * m * Wp * 8) + r(N2 * M * 4) + r(N2 * 2 * M) + r(N2 * 12));
-    t += r(N * 4) + r(N2 * 4) + r(N2 * words * 4) + 5 * r(N2 * 4) + 2 * r(R * 4) + r((N2 + M) * 4) + r(32) + r(72);
+    t += r(N * 4) + r(N2 * 4) + r(N2 * words * 4) + r(N2 * (uint64_t)dom_tile_count((int)N2) * 4) + 4 * r(N2 * 4) +
+         2 * r(R * 4) + r((N2 + M) * 4) + r(32) + r(72);
     const uint64_t nres = cfg->sl_kind == PE_SL_LRCS ? m * (m + 1) / 2 : m;
     t += r(N2 * nres * 8) + r(N2 * 4) + r(4) + r(M * M * 4) + r(4);
     t += 2 * r(N2 * nres * 8) + r(16);  // per-CDS (per-pair) string results of both buffers, scan counts

@@ -96,7 +96,7 @@ struct PopBuf {
 
 struct SelectScratch {
     uint32_t *dom;       // [2N][2N/32] bit j of row i: j dominates i
-    int32_t *np;         // [2N]
+    int32_t *np;         // [column tiles][2N] dominators of each row per tile of the matrix
     int32_t *front;      // [2N]
     int32_t *sorted;     // [2N] fronts 0..last
     int32_t *assoc;      // [2N]
@@ -132,6 +132,8 @@ void set_error_text(const char *msg);
 cudaError_t launch_select(const Shape &s, const float *obj, float *ext, const float *refpts, SelectScratch sc,
                           int32_t *surv, uint32_t *d_gen, int bump_gen, cudaStream_t st);
 size_t select_smem_bytes(const Shape &s);
+// column tiles of the dominance matrix: SelectScratch.np holds 2N x this many counts
+int dom_tile_count(int N2);
 size_t niche_smem_bytes(const Shape &s);
 // place of every position 0 .. B-1 of the extreme-point search in the reference's
 // reduction-tree order (0xffffffff: a position the tree leaves out)

@@ -1,9 +1,9 @@
 // pe_select.cu -- environmental selection (sortingKernel, src/main.cu:409-454).
 //
-//  k_dominance  one CTA per solution i: row i of the 2N x 2N dominance bit
-//               matrix (bit j set when j dominates i) built with __ballot_sync,
-//               and np[i] = popc(row) -- replaces the reference's two (2N)^2
-//               bool matrices (include/sorting.cuh:974-1089).
+//  k_dominance  32 x 256 tiles of the 2N x 2N dominance bit matrix (bit j of row
+//               i set when j dominates i) and each row's dominator count per tile
+//               -- replaces the reference's two (2N)^2 bool matrices
+//               (include/sorting.cuh:974-1089).
 //  k_select     one CTA: front peeling on the bit matrix, ideal / worst,
 //               extreme points, hyperplane (Gaussian elimination) or MNDF nadir
 //               (include/sorting.cuh:94-972).
@@ -29,62 +29,89 @@
 
 namespace pe {
 
+// dominate (include/sorting.cuh:94-130): |a-b| <= 1e-6 counts as equal, and a
+// dominates b when it is not worse on any objective and not equal on all of them --
+// that is, some a_k - b_k < -1e-6 and no a_k - b_k > 1e-6.  The rounded difference is
+// 0 only when a_k == b_k (subnormals are kept), so its sign is that of a_k - b_k, and
+// a NaN difference (inf - inf) is neither, as the reference's equal branch takes it.
 __device__ __forceinline__ bool dominates(const float *a, const float *b, int M)
 {
-    // dominate (include/sorting.cuh:94-130): |a-b| <= 1e-6 counts as equal
-    int eq = 0;
-    bool worse = false;
+    bool better = false, worse = false;
 #pragma unroll
     for (int k = 0; k < kMaxObj; k++) {
         if (k >= M) break;
-        float d = fabsf(__fsub_rn(a[k], b[k]));
-        if (d > 1e-6f) {
-            if (a[k] > b[k]) worse = true;
-        } else {
-            eq++;
-        }
+        const float d = __fsub_rn(a[k], b[k]);
+        better |= d < -1e-6f;
+        worse |= d > 1e-6f;
     }
-    return eq != M && !worse;
+    return better && !worse;
 }
 
-// MM: the objective count when known at compile time (4 or 6; 0: s.M at run time),
-// so the two objective vectors stay in registers
+// The dominance matrix in 32 x 256 tiles: CTA (x, y) takes rows 32x .. 32x+31 (one
+// per lane) and columns 256y .. 256y+255 (32 per warp, one matrix word), with the
+// tile's column objectives staged in shared memory (every lane reads the same
+// column: a broadcast) and each lane's row in registers.  A warp builds its 32
+// rows' words bit by bit; the tile is written row by row in 32-byte runs, and each
+// row's dominator count over the tile goes to np[y][row] (k_fronts adds the y's).
+// MM: the objective count when known at compile time (4 or 6; 0: s.M at run time).
+constexpr int kDomTileWords = 8;
 template <int MM>
-__global__ void __launch_bounds__(256) k_dominance(Shape s, const float *__restrict__ obj, uint32_t *__restrict__ dom,
-                                                   int32_t *__restrict__ np)
+__global__ void __launch_bounds__(32 * kDomTileWords) k_dominance(Shape s, const float *__restrict__ obj,
+                                                                  uint32_t *__restrict__ dom, int32_t *__restrict__ np)
 {
-    __shared__ int wsum[8];
+    __shared__ __align__(16) float oc[32 * kDomTileWords * kMaxObj];  // tile columns, objective vectors in column order
+    __shared__ uint32_t tw[32][kDomTileWords + 1];       // the tile's words by row
+    constexpr int KU = MM > 0 ? MM : kMaxObj;
     const int M = MM > 0 ? MM : s.M;
     const int N2 = 2 * s.N, words = (N2 + 31) >> 5;
-    const int i = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int i = blockIdx.x * 32 + lane, j0 = blockIdx.y * 32 * kDomTileWords;
+    const int ncol = min(32 * kDomTileWords, N2 - j0);
+    for (int e = tid; e < ncol * M; e += blockDim.x) oc[e] = obj[(size_t)j0 * M + e];
     float oi[kMaxObj];
 #pragma unroll
-    for (int k = 0; k < (MM > 0 ? MM : kMaxObj); k++)
-        if (k < M) oi[k] = obj[(size_t)i * M + k];
-    int cnt = 0;
-#pragma unroll 2
-    for (int w = warp; w < words; w += 8) {
-        int j = 32 * w + lane;
-        bool bit = false;
-        if (j < N2 && j != i) {
-            float oj[kMaxObj];
-#pragma unroll
-            for (int k = 0; k < (MM > 0 ? MM : kMaxObj); k++)
-                if (k < M) oj[k] = __ldg(&obj[(size_t)j * M + k]);
-            bit = dominates(oj, oi, M);
-        }
-        const uint32_t word = __ballot_sync(0xffffffffu, bit);
-        if (lane == 0) dom[(size_t)i * words + w] = word;
-        cnt += __popc(word);
-    }
-    if (lane == 0) wsum[warp] = cnt;
+    for (int k = 0; k < KU; k++)
+        if (k < M) oi[k] = i < N2 ? obj[(size_t)i * M + k] : 0.0f;
     __syncthreads();
-    if (tid == 0) {
-        int t = 0;
-        for (int w = 0; w < 8; w++) t += wsum[w];
-        np[i] = t;
+    const int wd = blockIdx.y * kDomTileWords + warp;
+    uint32_t word = 0;
+    if (wd < words) {
+        const int b1 = min(32, N2 - 32 * wd);
+        for (int b = 0; b < b1; b++) {
+            const int jl = 32 * warp + b, j = j0 + jl;
+            float oj[kMaxObj];
+            if (MM == 4) {  // one 16-byte broadcast load
+                const float4 v = reinterpret_cast<const float4 *>(oc)[jl];
+                oj[0] = v.x;
+                oj[1] = v.y;
+                oj[2] = v.z;
+                oj[3] = v.w;
+            } else {
+#pragma unroll
+                for (int k = 0; k < KU; k++)
+                    if (k < M) oj[k] = oc[jl * M + k];
+            }
+            if (j != i && dominates(oj, oi, M)) word |= 1u << b;
+        }
+    }
+    tw[lane][warp] = word;
+    __syncthreads();
+    {
+        const int r = tid / kDomTileWords, w = tid % kDomTileWords;
+        const int row = blockIdx.x * 32 + r, wd2 = blockIdx.y * kDomTileWords + w;
+        if (row < N2 && wd2 < words) dom[(size_t)row * words + wd2] = tw[r][w];
+    }
+    if (tid < 32) {
+        int cnt = 0;
+#pragma unroll
+        for (int w = 0; w < kDomTileWords; w++) cnt += __popc(tw[tid][w]);
+        const int row = blockIdx.x * 32 + tid;
+        if (row < N2) np[(size_t)blockIdx.y * N2 + row] = cnt;
     }
 }
+
+// column tiles of the dominance matrix (np holds this many counts per row)
+__host__ __device__ inline int dom_tiles(int N2) { return (((N2 + 31) >> 5) + kDomTileWords - 1) / kDomTileWords; }
 
 // Across the lanes of a warp, lane w holding v: the smallest (largest) value, the
 // lowest lane among equal ones -- what a loop over w = 0, 1, ... keeping the first
@@ -495,8 +522,13 @@ __global__ void __cluster_dims__(kFrontCtas, 1, 1) __launch_bounds__(kFrontThrea
     const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarps = nth >> 5;
     const int swp = (sw + 3) & ~3;
 
+    const int gy = dom_tiles(N2);
     for (int q = tid; q < RR; q += nth) {
-        const int v = q < nrow ? sc.np[r0 + q] : -1;
+        int v = -1;
+        if (q < nrow) {
+            v = 0;
+            for (int y = 0; y < gy; y++) v += sc.np[(size_t)y * N2 + r0 + q];
+        }
         npr[q] = v;
         if (q < nrow) sc.front[r0 + q] = -1;
     }
@@ -892,6 +924,10 @@ __global__ void __launch_bounds__(kSelThreads, 1) k_select(Shape s, const float 
     if (tid == 0) sc.info[5] = rc - last_size;
 }
 
+// reference points staged in k_assoc's shared memory up to this size (larger sets are
+// read from global memory, so the CTAs stay small)
+constexpr size_t kAssocSmemMax = 16 * 1024;
+
 // referenceBasedSorting phase 1 (:1105-1180) on the whole grid: one warp per
 // solution of fronts 0..last, lanes over reference points; perpendicular
 // distance (include/utils.cuh:1149-1171), argmin with the lowest index on ties.
@@ -900,7 +936,7 @@ template <int MM>
 __global__ void __launch_bounds__(256) k_assoc(Shape s, const float *__restrict__ obj,
                                                const float *__restrict__ refpts, SelectScratch sc)
 {
-    if (sc.info[3]) return;  // fronts filled N exactly: no niching
+    if (sc.info[3]) return;  // fronts filled N exactly: no niching (uniform over the grid)
     const int M = MM > 0 ? MM : s.M, R = s.R;
     constexpr int KU = MM > 0 ? MM : kMaxObj;  // unrolled loop bound (k < M guards the rest)
     const int rc = sc.info[0], count0 = sc.info[5];
@@ -913,6 +949,13 @@ __global__ void __launch_bounds__(256) k_assoc(Shape s, const float *__restrict_
         ideal[k] = sc.finfo[k];
         span[k] = __fsub_rn(sc.finfo[2 * M + k], ideal[k]);
     }
+    // the reference points in shared memory when they fit (every warp of the CTA reads them)
+    extern __shared__ __align__(16) float rsm[];
+    const bool staged = (size_t)R * M * sizeof(float) <= kAssocSmemMax;
+    if (staged)
+        for (int e = threadIdx.x; e < R * M; e += blockDim.x) rsm[e] = refpts[e];
+    __syncthreads();
+    const float *rp = staged ? rsm : refpts;
     for (int t = gw; t < rc; t += nw) {
         const int sol = sc.sorted[t];
         float f[kMaxObj];
@@ -923,8 +966,9 @@ __global__ void __launch_bounds__(256) k_assoc(Shape s, const float *__restrict_
         }
         float best = FLT_MAX;
         int bj = 0;
+#pragma unroll 2
         for (int j = lane; j < R; j += 32) {
-            const float *w = refpts + (size_t)j * M;
+            const float *w = rp + (size_t)j * M;
             float num = 0.0f, den = 0.0f;
 #pragma unroll
             for (int k = 0; k < KU; k++) {
@@ -1291,6 +1335,8 @@ size_t niche_smem_bytes(const Shape &s)
     return niche_base_bytes(s) + (niche_counting(s) ? (size_t)32 * s.R * sizeof(int) : 0);
 }
 
+int dom_tile_count(int N2) { return dom_tiles(N2); }
+
 size_t select_smem_bytes(const Shape &s)
 {
     (void)s;
@@ -1301,12 +1347,13 @@ cudaError_t launch_select(const Shape &s, const float *obj, float *ext, const fl
                           int32_t *surv, uint32_t *d_gen, int bump_gen, cudaStream_t st)
 {
     cudaError_t e;
+    const dim3 dgrid((2 * s.N + 31) / 32, dom_tiles(2 * s.N));
     if (s.M == 4) {
-        k_dominance<4><<<2 * s.N, 256, 0, st>>>(s, obj, sc.dom, sc.np);
+        k_dominance<4><<<dgrid, 32 * kDomTileWords, 0, st>>>(s, obj, sc.dom, sc.np);
     } else if (s.M == 6) {
-        k_dominance<6><<<2 * s.N, 256, 0, st>>>(s, obj, sc.dom, sc.np);
+        k_dominance<6><<<dgrid, 32 * kDomTileWords, 0, st>>>(s, obj, sc.dom, sc.np);
     } else {
-        k_dominance<0><<<2 * s.N, 256, 0, st>>>(s, obj, sc.dom, sc.np);
+        k_dominance<0><<<dgrid, 32 * kDomTileWords, 0, st>>>(s, obj, sc.dom, sc.np);
     }
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -1325,9 +1372,10 @@ cudaError_t launch_select(const Shape &s, const float *obj, float *ext, const fl
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     const int warps_needed = 2 * s.N;
     const int ag = std::min((warps_needed + 7) / 8, 148 * 8);
-    if (s.M == 4) k_assoc<4><<<ag, 256, 0, st>>>(s, obj, refpts, sc);
-    else if (s.M == 6) k_assoc<6><<<ag, 256, 0, st>>>(s, obj, refpts, sc);
-    else k_assoc<0><<<ag, 256, 0, st>>>(s, obj, refpts, sc);
+    const size_t rb = (size_t)s.R * s.M * sizeof(float), asm_ = rb <= kAssocSmemMax ? rb : 0;
+    if (s.M == 4) k_assoc<4><<<ag, 256, asm_, st>>>(s, obj, refpts, sc);
+    else if (s.M == 6) k_assoc<6><<<ag, 256, asm_, st>>>(s, obj, refpts, sc);
+    else k_assoc<0><<<ag, 256, asm_, st>>>(s, obj, refpts, sc);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     const size_t nsm = niche_smem_bytes(s);
     if ((e = raise_smem_limit((const void *)k_niche, nsm)) != cudaSuccess) return e;
