@@ -485,6 +485,11 @@ int pe_create(const pe_config *cfg, const int8_t *aa_idx, int32_t aa_len, const 
     }
     ht.ref_gc3 = table->ref_gc3;
     ht.ref_gc = table->ref_gc;
+    for (int i = 0, pi = 0; i < m - 1; i++)
+        for (int j = i + 1; j < m; j++, pi++) {
+            ht.pair_i[pi] = (uint8_t)i;
+            ht.pair_j[pi] = (uint8_t)j;
+        }
 
     if ((rc = in->alloc(&in->d_tab, 1))) return cleanup(rc);
     if ((rc = in->alloc(&in->d_aa, (size_t)L))) return cleanup(rc);

@@ -129,6 +129,7 @@ struct VarSmem {
     int32_t sl_mut;
     int32_t op;
     unsigned long long changed;  // CDSs whose planes the mutation changed (bit c)
+    int32_t ntask;               // entries of the evaluation's task list
 };
 
 // Across a warp whose lanes hold (value, index) with index -1 for none: the largest
@@ -161,13 +162,6 @@ __device__ __forceinline__ void warp_last_min(int &v, int &idx)
     }
 }
 
-// index of the k-th set bit (k from 0) of a nonzero mask
-__device__ __forceinline__ int nth_set_bit(unsigned long long mask, int k)
-{
-    for (int i = 0; i < k; i++) mask &= mask - 1ull;
-    return __ffsll((long long)mask) - 1;
-}
-
 // Every objective except the string objective, for the solution in smem.
 // Reference evaluators: include/utils.cuh:271-710.  Per-CDS sums are exact
 // integers (fixed-point log weights for CAI, fixed-point CPS), so the result
@@ -183,44 +177,59 @@ __device__ __forceinline__ int nth_set_bit(unsigned long long mask, int k)
 // child's aux) and one thread per objective (each in its own warp) reduces over the
 // CDSs in CDS order, as the reference's loops do.
 __device__ void light_eval(const Shape &s, const DevTables *gt, const SmemTab &st, const uint8_t *ids,
-                           const uint2 *planes, int32_t *ax, unsigned long long changed, const int32_t *pax,
-                           int32_t *cax, float *obj, int8_t *objidx, int tid, int nth)
+                           const uint2 *planes, int32_t *ax, int32_t *tl, int *ntl, unsigned long long changed,
+                           const int32_t *pax, int32_t *cax, float *obj, int8_t *objidx, int tid, int nth)
 {
     const int warp = tid >> 5, lane = tid & 31, nwarps = nth >> 5;
     const int L = s.L, m = s.m;
     const int sCAI = s.slot[K_CAI], sCBP = s.slot[K_CBP], sHSC = s.slot[K_HSC], sHD = s.slot[K_HD],
               sGC = s.slot[K_GC];
     const int npairs = m * (m - 1) / 2;
-    // the enabled per-CDS objectives, 2 bits each
-    int kp = 0, K = 0;
-    if (sCAI >= 0) kp |= 0 << (2 * K++);
-    if (sCBP >= 0) kp |= 1 << (2 * K++);
-    if (sHSC >= 0) kp |= 2 << (2 * K++);
-    if (sGC >= 0) kp |= 3 << (2 * K++);
-    const int nch = __popcll(changed);
-    const int ncds_tasks = K * nch;
-    const int ntask = ncds_tasks + (sHD >= 0 ? nch * (m - 1) : 0);
-    if (pax) {
-        const int nax = AUX_HD(m) + (sHD >= 0 ? npairs : 0);
-        for (int e = tid; e < nax; e += nth) {
-            bool keep;
-            if (e < AUX_HD(m)) {
-                keep = !((changed >> (e % m)) & 1ull);
-            } else {
-                int i = 0, rem = e - AUX_HD(m);
-                while (rem >= m - 1 - i) {
-                    rem -= m - 1 - i;
-                    i++;
-                }
-                keep = !(((changed >> i) | (changed >> (i + 1 + rem))) & 1ull);
+    const int kinds[4] = {sCAI >= 0 ? 0 : -1, sCBP >= 0 ? 1 : -1, sHSC >= 0 ? 2 : -1, sGC >= 0 ? 3 : -1};
+    // the task list (warp 0): one entry (kind << 16 | CDS) per changed CDS and enabled
+    // per-CDS objective, then (4 << 16 | pair) per CDS pair with a changed member
+    if (warp == 0) {
+        int n = 0;
+        for (int cb = 0; cb < m; cb += 32) {
+            const int c = cb + lane;
+            const bool on = c < m && ((changed >> c) & 1ull);
+            const unsigned bal = __ballot_sync(0xffffffffu, on);
+            const int r = __popc(bal & ((1u << lane) - 1u));
+            int kk = 0;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                if (kinds[q] < 0) continue;
+                if (on) tl[n + r + kk * __popc(bal)] = (kinds[q] << 16) | c;
+                kk++;
             }
-            if (keep) ax[e] = pax[e];
+            n += kk * __popc(bal);
         }
+        if (sHD >= 0) {
+            for (int pb = 0; pb < npairs; pb += 32) {
+                const int pi = pb + lane;
+                const bool on = pi < npairs && (((changed >> gt->pair_i[pi]) | (changed >> gt->pair_j[pi])) & 1ull);
+                const unsigned bal = __ballot_sync(0xffffffffu, on);
+                if (on) tl[n + __popc(bal & ((1u << lane) - 1u))] = (4 << 16) | pi;
+                n += __popc(bal);
+            }
+        }
+        if (lane == 0) *ntl = n;
     }
+    if (pax) {  // the unchanged CDSs' sums, and the pairs of two unchanged CDSs, from the parent
+        for (int q = 0; q < 5; q++)
+            for (int c = tid; c < m; c += nth)
+                if (!((changed >> c) & 1ull)) ax[q * m + c] = pax[q * m + c];
+        if (sHD >= 0)
+            for (int pi = tid; pi < npairs; pi += nth)
+                if (!(((changed >> gt->pair_i[pi]) | (changed >> gt->pair_j[pi])) & 1ull))
+                    ax[AUX_HD(m) + pi] = pax[AUX_HD(m) + pi];
+    }
+    __syncthreads();
+    const int ntask = *ntl;
     for (int task = warp; task < ntask; task += nwarps) {
-        if (task < ncds_tasks) {
-            const int kind = (kp >> (2 * (task % K))) & 3;
-            const int c = nth_set_bit(changed, task / K);
+        const int ent = tl[task], kind = ent >> 16;
+        if (kind < 4) {
+            const int c = ent & 0xffff;
             const uint8_t *row = ids + c * s.Lp;
             if (kind == 0) {  // CAI: exp(mean log w)
                 long long S = 0;
@@ -267,12 +276,8 @@ __device__ void light_eval(const Shape &s, const DevTables *gt, const SmemTab &s
                 if (lane == 0) ax[AUX_GC(m) + c] = cnt;
             }
         } else {  // HD: nucleotide mismatches of a pair with a changed CDS, XOR/popcount of planes
-            const int u = task - ncds_tasks, r = u / (m - 1), k = u - r * (m - 1);
-            const int c = nth_set_bit(changed, r), d = k < c ? k : k + 1;
-            if (((changed >> d) & 1ull) && d < c) continue;  // summed for d's task
-            const int i = min(c, d), j = max(c, d);
-            const int pi = i * (2 * m - i - 1) / 2 + (j - i - 1);
-            const uint2 *A = planes + i * s.Wp, *B = planes + j * s.Wp;
+            const int pi = ent & 0xffff;
+            const uint2 *A = planes + gt->pair_i[pi] * s.Wp, *B = planes + gt->pair_j[pi] * s.Wp;
             int cnt = 0;
             for (int w = lane; w < s.W; w += 32) {
                 uint2 x = A[w], y = B[w];
@@ -356,14 +361,9 @@ __device__ void light_eval(const Shape &s, const DevTables *gt, const SmemTab &s
         }
         warp_last_min(bc, bp);
         if (lane == 0) {
-            int i = 0, rem = bp;
-            while (rem >= m - 1 - i) {
-                rem -= m - 1 - i;
-                i++;
-            }
             obj[sHD] = -__fdiv_rn((float)bc, (float)s.n);
-            objidx[2 * sHD] = (int8_t)i;
-            objidx[2 * sHD + 1] = (int8_t)(i + 1 + rem);
+            objidx[2 * sHD] = (int8_t)gt->pair_i[bp];
+            objidx[2 * sHD + 1] = (int8_t)gt->pair_j[bp];
         }
     }
     if (warp == 4 % nwarps && sGC >= 0) {
@@ -847,15 +847,18 @@ __global__ void __launch_bounds__(kVarThreads, 4) k_variation(Shape s, const Dev
     int8_t *aa = reinterpret_cast<int8_t *>(planes + (size_t)s.m * s.Wp);
     // MODE_MUTATE: plane words the mutation touched (bit c * Wp + w)
     uint32_t *dirty = reinterpret_cast<uint32_t *>(aa + ((s.L + 15) & ~15));
-    // the per-CDS (per-pair) sums of the light objectives, aux layout
+    // the per-CDS (per-pair) sums of the light objectives, aux layout; then the
+    // evaluation's task list (4m + m(m-1)/2 entries)
     int32_t *ax = reinterpret_cast<int32_t *>(dirty + (s.m * s.Wp + 31) / 32);
+    int32_t *tl = ax + s.naux;
 
     const int tid = threadIdx.x, nth = blockDim.x;
     // MODE_MUTATE with an order: CTA b makes child order[gen parity][b] (heaviest
-    // operators first, so the CTAs of the last wave are the short ones)
+    // operators first, so the CTAs of the last wave are the short ones); CTA 0, which
+    // starts first, writes the next generation's order
     const uint32_t gen0 = MODE == MODE_MUTATE ? *d_gen : 0u;
     const int i = MODE == MODE_MUTATE && order ? order[(gen0 & 1u) * gridDim.x + blockIdx.x] : (int)blockIdx.x;
-    if (MODE == MODE_MUTATE && order && blockIdx.x == gridDim.x - 1)
+    if (MODE == MODE_MUTATE && order && blockIdx.x == 0)
         order_children(s, gen0 + 1u, (int)gridDim.x, order + ((gen0 + 1u) & 1u) * gridDim.x, tid, nth);
     const size_t sol_bytes = (size_t)s.m * s.Lp;
     const size_t sol_words = (size_t)s.m * s.Wp;
@@ -1000,7 +1003,7 @@ __global__ void __launch_bounds__(kVarThreads, 4) k_variation(Shape s, const Dev
     }
     const int32_t *pax = MODE == MODE_MUTATE && src.aux ? src.aux + (size_t)parent_of[i] * s.naux : nullptr;
     int32_t *cax = dst.aux ? dst.aux + (size_t)out_slot * s.naux : nullptr;
-    light_eval(s, gt, sm.tab, ids, planes, ax, chmask, pax, cax, dst.obj + (size_t)out_slot * s.M,
+    light_eval(s, gt, sm.tab, ids, planes, ax, tl, &sm.ntask, chmask, pax, cax, dst.obj + (size_t)out_slot * s.M,
                dst.objidx + (size_t)out_slot * 2 * s.M, tid, nth);
 }
 
@@ -1008,7 +1011,7 @@ size_t var_smem_bytes(const Shape &s)
 {
     return ((sizeof(VarSmem) + 15) & ~size_t(15)) + (size_t)s.m * s.Lp + (size_t)s.m * s.Wp * sizeof(uint2) +
            (size_t)((s.L + 15) & ~15) + (size_t)((s.m * s.Wp + 31) / 32) * sizeof(uint32_t) +
-           (size_t)s.naux * sizeof(int32_t);
+           (size_t)(s.naux + 4 * s.m + s.m * (s.m - 1) / 2) * sizeof(int32_t);
 }
 
 cudaError_t raise_smem_limit(const void *func, size_t bytes)

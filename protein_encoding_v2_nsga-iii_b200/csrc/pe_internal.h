@@ -74,6 +74,8 @@ struct DevTables {
     int64_t cpsf[61 * 61];   // CPS in 2^-32 fixed point
     float cps[61 * 61];
     float ref_gc3, ref_gc;
+    uint8_t pair_i[kMaxCds * (kMaxCds - 1) / 2];  // CDS pair pi (i < j, row-major) of the instance's m
+    uint8_t pair_j[kMaxCds * (kMaxCds - 1) / 2];
 };
 
 // One population buffer (2N solutions).
