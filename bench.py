@@ -78,13 +78,13 @@ L2_FLUSH_BYTES = 256 << 20
 # capture; a host test fails when the source changes without a new capture.
 SL_NCU = {
     "hairpin": {"workload": "L=1000 m=8 N=1024, generation 1 (2311 CDSs scanned)",
-                "cells": 10389102811, "smem_wavefronts": 27778286, "alu_warp_inst": 46226541,
-                "thread_inst": 2470901893, "dram_bytes": 2475520, "smem_pct": 73.14, "alu_pct": 68.95,
-                "source": "fb06a34e80d29fe3"},
+                "cells": 10389102811, "smem_wavefronts": 27777210, "alu_warp_inst": 46313626,
+                "thread_inst": 2487732762, "dram_bytes": 2481920, "smem_pct": 73.05, "alu_pct": 68.92,
+                "source": "d65b815633479dcb"},
     "lrcs": {"workload": "L=3000 m=4 N=4096, generation 1 (18320 CDS pairs scanned)",
-             "cells": 1250515745682, "smem_wavefronts": 2679467847, "alu_warp_inst": 5439112299,
-             "thread_inst": 252208658699, "dram_bytes": 34456064, "smem_pct": 72.64, "alu_pct": 74.60,
-             "source": "fb06a34e80d29fe3"},
+             "cells": 1250515745682, "smem_wavefronts": 2679486081, "alu_warp_inst": 5439675210,
+             "thread_inst": 252279307777, "dram_bytes": 34455552, "smem_pct": 72.65, "alu_pct": 74.60,
+             "source": "d65b815633479dcb"},
 }
 SM_COUNT, SMEM_WAVEFRONTS_PER_SM_CLK, ALU_WARP_INST_PER_SM_CLK = 148, 1, 2
 # kernels one generation launches (one CUDA graph replay): k_variation, k_sl, k_dominance,
@@ -498,7 +498,18 @@ def run_batched(args, world: int = 1, rank: int = 0, local: int = 0):
             e.synchronize()
             e.close()
         t_plain = time.perf_counter() - t0
-    # this rank's shard together (create + init + generations)
+        # the same batch with the batch's stem scans queued (one wave per length class)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        engines = [make(j) for j in mine]
+        with pe.Batch(engines) as b:
+            b.set_scan_queue(True)
+            b.step(G)
+            b.synchronize()
+        for e in engines:
+            e.close()
+        t_queued = time.perf_counter() - t0
+    # this rank's shard together (create + init + generations), a graph branch per member
     if world > 1:
         torch.distributed.barrier()
     with ClockSampler(local) as clk:
@@ -527,7 +538,7 @@ def run_batched(args, world: int = 1, rank: int = 0, local: int = 0):
                 "data": "synthetic",
                 "config": {"workload": f"batched: {len(jobs)} proteins, L log-uniform [100, 3000], m in {{2,4,8}}, "
                                        f"N={N}, Pm={pm}, 4 objectives, {G} generations, one graph launch per 2 "
-                                       f"generations for all instances of a rank",
+                                       f"generations for all instances of a rank, a branch per instance",
                            "parallelism": f"job shards over {world} GPU(s) by stem-scan cells"},
                 "stem_cells_per_s": scanned_cells / t_batch, "stem_cells_scanned_of_all": scanned_cells / cells,
                 "mean_final_hv": float(np.mean([r["hv"] for r in results.values()])),
@@ -536,6 +547,8 @@ def run_batched(args, world: int = 1, rank: int = 0, local: int = 0):
         if t_plain is not None:
             line["plain_designs_per_s"] = len(jobs) / t_plain
             line["batched_over_plain"] = t_plain / t_batch
+            line["queued_scans_designs_per_s"] = len(jobs) / t_queued
+            line["queued_over_branches"] = t_batch / t_queued
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()

@@ -188,6 +188,15 @@ int pe_batch_create(pe_instance *const *instances, int32_t count, pe_batch **out
 int pe_batch_step(pe_batch *batch, int32_t generations);
 int pe_batch_synchronize(pe_batch *batch);
 int pe_batch_destroy(pe_batch *batch);
+/* The string-objective scans of a batch generation queued (1) or not (0, the
+ * default): queued, every member's variation kernel appends the CDS (pair) results
+ * its children's mutations invalidated, and one wave of CTAs per length class (CTA
+ * size = the one the class's members tuned at init, longest CDSs first) takes the
+ * whole batch's queue by ticket, between a variation phase and a selection phase of
+ * all members; not queued, each member's generation is its own branch of the graph
+ * with its own scan launch, so one member's selection overlaps another's scan.
+ * Results are the same. */
+int pe_batch_set_scan_queue(pe_batch *batch, int32_t enable);
 
 /* --- served design jobs (no counterpart in the reference, which designs one
  *     protein per process, src/main.cu:467-901): continuous batching on one GPU.

@@ -151,7 +151,7 @@ def lib() -> C.CDLL:
             "pe_scan_cells": [P, P], "pe_set_wait_limit": [P, C.c_int32],
             "pe_hairpin_noalloc": [P, C.c_int32, C.c_int32, C.c_int32, P, P, P, P],
             "pe_batch_create": [P, C.c_int32, C.POINTER(P)], "pe_batch_step": [P, C.c_int32],
-            "pe_batch_synchronize": [P], "pe_batch_destroy": [P],
+            "pe_batch_synchronize": [P], "pe_batch_destroy": [P], "pe_batch_set_scan_queue": [P, C.c_int32],
             "pe_instance_bytes": [C.POINTER(Config), C.c_int32, C.POINTER(C.c_uint64)],
             "pe_server_create": [C.POINTER(ServerConfig), C.POINTER(P)],
             "pe_batch_submit": [P, C.POINTER(JobSpec), C.POINTER(C.c_int64)],
@@ -401,6 +401,10 @@ class Batch:
 
     def step(self, generations: int = 1):
         _ck(lib().pe_batch_step(self._h, generations))
+
+    def set_scan_queue(self, enable: bool = True):
+        """Queued string scans for the whole batch, or (the default) one scan launch per member."""
+        _ck(lib().pe_batch_set_scan_queue(self._h, int(enable)))
 
     def synchronize(self):
         _ck(lib().pe_batch_synchronize(self._h))

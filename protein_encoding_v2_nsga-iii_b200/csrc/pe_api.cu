@@ -257,6 +257,13 @@ cudaError_t mark(pe_instance *in, int k)
     return cudaEventRecordWithFlags(in->ev[k], in->stream, cudaEventRecordExternal);
 }
 
+// the selection of a generation whose children sit in buf[dst]
+cudaError_t enqueue_selection(pe_instance *in, int dst, bool pdl_first)
+{
+    (void)pdl_first;
+    return launch_select(in->s, in->buf[dst].obj, in->d_ext, in->d_ref, in->sc, in->d_surv, in->d_gen, 1, in->stream);
+}
+
 cudaError_t enqueue_generation(pe_instance *in, int src)
 {
     const Shape &s = in->s;
@@ -546,6 +553,18 @@ int pe_create(const pe_config *cfg, const int8_t *aa_idx, int32_t aa_len, const 
 
 // ---------------------------------------------------------------- batches
 
+// a length class of the batch's queued scan: members with the same string objective
+// and tuned scan CTA size, longest CDSs first
+struct ScanClass {
+    int fl = 0, nt = 128, ctas = 0;
+    size_t smem = 0;
+    std::vector<int> members;
+    int32_t *ticket = nullptr;    // [2] device: next item, CTAs done
+    SlJob *jobs[3][2] = {};       // device job tables per graph (generations 1, 2) and step
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+};
+
 struct pe_batch {
     std::vector<pe_instance *> inst;
     cudaStream_t master = nullptr;
@@ -553,24 +572,180 @@ struct pe_batch {
     std::vector<cudaEvent_t> join;
     cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};  // [generations] for 1 and 2
     std::vector<int> parity[3];                                // instance parities the graph was built for
+    bool queue = false;                                        // queued stem scans (pe_batch_set_scan_queue)
+    std::vector<int32_t *> q_items, q_count;                   // per member: its queue
+    std::vector<ScanClass> classes;
 };
 
-static int batch_capture(pe_batch *b, int gens, cudaGraphExec_t *out)
+static void free_scan_classes(pe_batch *b)
 {
-    cudaGraph_t g = nullptr;
-    CudaLock lock(g_cuda_mu);
-    CK(cudaStreamBeginCapture(b->master, cudaStreamCaptureModeThreadLocal));
+    for (ScanClass &c : b->classes) {
+        for (auto &g : c.jobs)
+            for (SlJob *&j : g)
+                if (j) cudaFree(j), j = nullptr;
+        if (c.ticket) cudaFree(c.ticket);
+        if (c.done) cudaEventDestroy(c.done);
+        if (c.stream) cudaStreamDestroy(c.stream);
+    }
+    b->classes.clear();
+    for (int32_t *p : b->q_items)
+        if (p) cudaFree(p);
+    for (int32_t *p : b->q_count)
+        if (p) cudaFree(p);
+    b->q_items.clear();
+    b->q_count.clear();
+}
+
+// Queues and length classes of the batch's queued scan.  A class is the members with
+// the same string objective and the scan CTA size their init tuning chose; its wave
+// of CTAs is its share of the device, by the members' scan cells per generation.
+static cudaError_t setup_scan_queue(pe_batch *b)
+{
+    const int n = (int)b->inst.size();
+    b->q_items.assign(n, nullptr);
+    b->q_count.assign(n, nullptr);
+    std::map<std::pair<int, int>, int> cls;
+    std::vector<double> work;
+    for (int i = 0; i < n; i++) {
+        const Shape &s = b->inst[i]->s;
+        cudaError_t e = cudaMalloc(&b->q_items[i], (size_t)s.N * s.nres * sizeof(int32_t));
+        if (e == cudaSuccess) e = cudaMalloc(&b->q_count[i], sizeof(int32_t));
+        if (e == cudaSuccess) e = cudaMemset(b->q_count[i], 0, sizeof(int32_t));
+        if (e != cudaSuccess) return e;
+        const int fl = s.sl_kind == PE_SL_LRCS ? 1 : 0, nt = s.sl_threads ? s.sl_threads : 128;
+        auto key = std::make_pair(fl, nt);
+        if (!cls.count(key)) {
+            cls[key] = (int)b->classes.size();
+            b->classes.emplace_back();
+            b->classes.back().fl = fl;
+            b->classes.back().nt = nt;
+            work.push_back(0.0);
+        }
+        const int c = cls[key];
+        b->classes[c].members.push_back(i);
+        b->classes[c].smem = std::max(b->classes[c].smem, sl_queue_smem_bytes(s, nt));
+        work[c] += (double)s.N * s.nres * (double)s.n * s.n;
+    }
+    int dev = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    double total = 0.0;
+    for (double w : work) total += w;
+    for (size_t c = 0; c < b->classes.size(); c++) {
+        ScanClass &k = b->classes[c];
+        if ((int)k.members.size() > kMaxBatchJobs) return cudaErrorInvalidValue;
+        std::sort(k.members.begin(), k.members.end(),
+                  [&](int x, int y) { return b->inst[x]->s.n > b->inst[y]->s.n; });
+        const int per_sm = sl_queue_ctas_per_sm(k.nt, k.fl, k.smem);
+        if (per_sm <= 0) return cudaErrorInvalidConfiguration;
+        const double share = total > 0.0 ? work[c] / total : 1.0;
+        k.ctas = std::max(1, (int)(share * sms * per_sm + 0.5));
+        if ((e = cudaMalloc(&k.ticket, 2 * sizeof(int32_t))) != cudaSuccess) return e;
+        if ((e = cudaMemset(k.ticket, 0, 2 * sizeof(int32_t))) != cudaSuccess) return e;
+        if ((e = cudaStreamCreateWithFlags(&k.stream, cudaStreamNonBlocking)) != cudaSuccess) return e;
+        if ((e = cudaEventCreateWithFlags(&k.done, cudaEventDisableTiming)) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+// the job table of class k for a step whose children go to each member's buffer dst
+static cudaError_t scan_jobs(pe_batch *b, ScanClass &k, const std::vector<int> &dst, SlJob **out)
+{
+    std::vector<SlJob> h(k.members.size());
+    for (size_t q = 0; q < k.members.size(); q++) {
+        const int i = k.members[q];
+        pe_instance *in = b->inst[i];
+        SlJob &j = h[q];
+        j.s = in->s;
+        j.buf = in->buf[dst[i]];
+        j.base = in->s.N;
+        j.part = in->d_part;
+        j.counter = in->d_counter;
+        j.status = in->d_status;
+        j.scanned = in->d_scanned;
+        j.items = b->q_items[i];
+        j.count = b->q_count[i];
+    }
+    if (!*out) {
+        cudaError_t e = cudaMalloc(out, h.size() * sizeof(SlJob));
+        if (e != cudaSuccess) return e;
+    }
+    return cudaMemcpy(*out, h.data(), h.size() * sizeof(SlJob), cudaMemcpyHostToDevice);
+}
+
+// fork every member's stream from the master, run f(member) on it, join them back
+extern "C++" template <class F> cudaError_t batch_branches(pe_batch *b, F f)
+{
     cudaError_t e = cudaEventRecord(b->fork, b->master);
     for (size_t i = 0; i < b->inst.size() && e == cudaSuccess; i++) {
         pe_instance *in = b->inst[i];
         e = cudaStreamWaitEvent(in->stream, b->fork, 0);
-        int src = in->cur;
-        for (int k = 0; k < gens && e == cudaSuccess; k++) {
-            e = enqueue_generation(in, src);
-            src = 1 - src;
-        }
+        if (e == cudaSuccess) e = f((int)i, in);
         if (e == cudaSuccess) e = cudaEventRecord(b->join[i], in->stream);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(b->master, b->join[i], 0);
+    }
+    return e;
+}
+
+static int batch_capture(pe_batch *b, int gens, cudaGraphExec_t *out)
+{
+    const int n = (int)b->inst.size();
+    std::vector<int> src(n);
+    for (int i = 0; i < n; i++) src[i] = b->inst[i]->cur;
+    if (b->queue && b->classes.empty()) {  // queues and classes on first use
+        cudaError_t e0 = setup_scan_queue(b);
+        if (e0 != cudaSuccess) {
+            free_scan_classes(b);
+            return fail(PE_ERR_CUDA, "batch scan queue setup: %s", cudaGetErrorString(e0));
+        }
+    }
+    if (b->queue) {  // the job tables of each step, before the capture
+        std::vector<int> s2 = src;
+        for (int k = 0; k < gens; k++) {
+            std::vector<int> dst(n);
+            for (int i = 0; i < n; i++) dst[i] = 1 - s2[i];
+            for (ScanClass &c : b->classes) CK(scan_jobs(b, c, dst, &c.jobs[gens][k]));
+            s2 = dst;
+        }
+    }
+    cudaGraph_t g = nullptr;
+    CudaLock lock(g_cuda_mu);
+    CK(cudaStreamBeginCapture(b->master, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = cudaSuccess;
+    if (!b->queue) {
+        e = batch_branches(b, [&](int i, pe_instance *in) {
+            cudaError_t e1 = cudaSuccess;
+            int sr = src[i];
+            for (int k = 0; k < gens && e1 == cudaSuccess; k++) {
+                e1 = enqueue_generation(in, sr);
+                sr = 1 - sr;
+            }
+            return e1;
+        });
+    }
+    for (int k = 0; b->queue && k < gens && e == cudaSuccess; k++) {
+        // variation of every member (queueing its scans), the batch's scans by class,
+        // then every member's selection
+        e = batch_branches(b, [&](int i, pe_instance *in) {
+            const Shape &s = in->s;
+            const int sr = src[i], ds = 1 - sr;
+            return launch_mutate(s, in->d_tab, in->d_aa, in->buf[sr], in->buf[ds], in->d_surv, nullptr, s.N, 0, s.N,
+                                 in->d_gen, nullptr, in->d_order, in->stream, b->q_items[i], b->q_count[i],
+                                 in->d_counter);
+        });
+        if (e == cudaSuccess) e = cudaEventRecord(b->fork, b->master);
+        for (ScanClass &c : b->classes) {
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(c.stream, b->fork, 0);
+            if (e == cudaSuccess)
+                e = launch_sl_queue(c.jobs[gens][k], (int)c.members.size(), c.ticket, c.nt, c.fl, c.smem, c.ctas,
+                                    c.stream);
+            if (e == cudaSuccess) e = cudaEventRecord(c.done, c.stream);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(b->master, c.done, 0);
+        }
+        if (e == cudaSuccess)
+            e = batch_branches(b, [&](int i, pe_instance *in) { return enqueue_selection(in, 1 - src[i], false); });
+        for (int i = 0; i < n; i++) src[i] = 1 - src[i];
     }
     cudaError_t e2 = cudaStreamEndCapture(b->master, &g);
     if (e != cudaSuccess || e2 != cudaSuccess) {
@@ -663,12 +838,26 @@ int pe_batch_synchronize(pe_batch *b)
     return PE_OK;
 }
 
+int pe_batch_set_scan_queue(pe_batch *b, int32_t enable)
+{
+    if (!b) return fail(PE_ERR_ARG, "null batch");
+    if ((enable != 0) != b->queue) {
+        CK(cudaStreamSynchronize(b->master));
+        for (auto &g : b->graph)
+            if (g) cudaGraphExecDestroy(g), g = nullptr;
+        for (auto &p : b->parity) p.clear();
+        b->queue = enable != 0;
+    }
+    return PE_OK;
+}
+
 int pe_batch_destroy(pe_batch *b)
 {
     if (!b) return PE_OK;
     if (b->master) cudaStreamSynchronize(b->master);
     for (auto &g : b->graph)
         if (g) cudaGraphExecDestroy(g);
+    free_scan_classes(b);
     for (cudaEvent_t ev : b->join)
         if (ev) cudaEventDestroy(ev);
     if (b->fork) cudaEventDestroy(b->fork);

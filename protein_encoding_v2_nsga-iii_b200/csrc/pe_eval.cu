@@ -838,7 +838,8 @@ __global__ void __launch_bounds__(kVarThreads, 4) k_variation(Shape s, const Dev
                                                            const int32_t *__restrict__ parent_of,
                                                            const int32_t *__restrict__ rng_idx, int copy_base,
                                                            int child_base, const uint32_t *__restrict__ d_gen,
-                                                           int32_t *ops, int32_t *surv, int32_t *order)
+                                                           int32_t *ops, int32_t *surv, int32_t *order,
+                                                           int32_t *q_items, int32_t *q_count, int32_t *q_counter)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     VarSmem &sm = *reinterpret_cast<VarSmem *>(smem_raw);
@@ -988,6 +989,61 @@ __global__ void __launch_bounds__(kVarThreads, 4) k_variation(Shape s, const Dev
                 dst.cds[(size_t)out_slot * s.nres + c] = changed ? make_int2(-1, 0) : src.cds[(size_t)par * s.nres + c];
             }
         }
+        if (q_count) {
+            // queued scan (batches): the results this child's mutation invalidated go to the
+            // queue, in result order; the solution's counter starts at the results kept, so
+            // the combine runs after the last queued one.  A child with none keeps its
+            // parent's string objective, as the combine of the parent's results gives.
+            const int par = parent_of[i], nres = s.nres, lane = tid & 31;
+            if (tid < 32) {
+                int nq = 0;
+                for (int rb = 0; rb < nres; rb += 32) {
+                    const int r = rb + lane;
+                    bool on = false;
+                    if (r < nres) {
+                        if (s.sl_kind == PE_SL_LRCS) {
+                            int a, b;
+                            lrcs_pair_of(s.m, r, a, b);
+                            on = ((ch >> a) | (ch >> b)) & 1ull;
+                        } else {
+                            on = (ch >> r) & 1ull;
+                        }
+                    }
+                    nq += __popc(__ballot_sync(0xffffffffu, on));
+                }
+                int qb = 0;
+                if (lane == 0 && nq > 0) qb = atomicAdd(q_count, nq);
+                qb = __shfl_sync(0xffffffffu, qb, 0);
+                int run = 0;
+                for (int rb = 0; rb < nres; rb += 32) {
+                    const int r = rb + lane;
+                    bool on = false;
+                    if (r < nres) {
+                        if (s.sl_kind == PE_SL_LRCS) {
+                            int a, b;
+                            lrcs_pair_of(s.m, r, a, b);
+                            on = ((ch >> a) | (ch >> b)) & 1ull;
+                        } else {
+                            on = (ch >> r) & 1ull;
+                        }
+                    }
+                    const unsigned bal = __ballot_sync(0xffffffffu, on);
+                    if (on) q_items[qb + run + __popc(bal & ((1u << lane) - 1u))] = i * nres + r;
+                    run += __popc(bal);
+                }
+                if (lane == 0) {
+                    // (with nothing queued the counter stays 0, ready for a plain scan later)
+                    if (nq > 0) q_counter[i] = nres - nq;
+                    if (nq == 0) {
+                        const int sl = s.slot[K_SL];
+                        dst.obj[(size_t)out_slot * s.M + sl] = src.obj[(size_t)par * s.M + sl];
+                        dst.objidx[(size_t)out_slot * 2 * s.M + 2 * sl] = src.objidx[(size_t)par * 2 * s.M + 2 * sl];
+                        dst.objidx[(size_t)out_slot * 2 * s.M + 2 * sl + 1] = src.objidx[(size_t)par * 2 * s.M + 2 * sl + 1];
+                        for (int k = 0; k < 3; k++) dst.pql[(size_t)out_slot * 3 + k] = src.pql[(size_t)par * 3 + k];
+                    }
+                }
+            }
+        }
     }
     __syncthreads();
     // write the (new) solution
@@ -1041,7 +1097,7 @@ cudaError_t launch_init(const Shape &s, const DevTables *tab, const int8_t *aa, 
     cudaError_t e = set_var_attr<MODE_INIT>(smem);
     if (e != cudaSuccess) return e;
     k_variation<MODE_INIT><<<s.N, kVarThreads, smem, st>>>(s, tab, aa, dst, dst, nullptr, nullptr, -1, 0, nullptr,
-                                                            nullptr, surv, nullptr);
+                                                            nullptr, surv, nullptr, nullptr, nullptr, nullptr);
     return cudaGetLastError();
 }
 
@@ -1060,22 +1116,26 @@ cudaError_t launch_light_eval(const Shape &s, const DevTables *tab, const int8_t
     b.objidx += (size_t)base * 2 * s.M;
     b.pql += (size_t)base * 3;
     k_variation<MODE_EVAL><<<count, kVarThreads, smem, st>>>(s, tab, aa, b, b, nullptr, nullptr, -1, 0, nullptr,
-                                                              nullptr, nullptr, nullptr);
+                                                              nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
     return cudaGetLastError();
 }
 
 cudaError_t launch_mutate(const Shape &s, const DevTables *tab, const int8_t *aa, PopBuf src, PopBuf dst,
                           const int32_t *parent_of, const int32_t *rng_idx, int count, int copy_base, int child_base,
-                          const uint32_t *d_gen, int32_t *ops, int32_t *order, cudaStream_t st)
+                          const uint32_t *d_gen, int32_t *ops, int32_t *order, cudaStream_t st, int32_t *q_items,
+                          int32_t *q_count, int32_t *q_counter)
 {
     if (count <= 0) return cudaSuccess;
+    // a queued scan needs the parents' results to carry the unchanged ones
+    if (q_count && (src.cds == nullptr || dst.cds == nullptr)) return cudaErrorInvalidValue;
     // a child reuses its parent's per-CDS sums only when both buffers carry them
     if ((src.aux == nullptr) != (dst.aux == nullptr)) return cudaErrorInvalidValue;
     size_t smem = var_smem_bytes(s);
     cudaError_t e = set_var_attr<MODE_MUTATE>(smem);
     if (e != cudaSuccess) return e;
     k_variation<MODE_MUTATE><<<count, kVarThreads, smem, st>>>(s, tab, aa, src, dst, parent_of, rng_idx, copy_base,
-                                                                child_base, d_gen, ops, nullptr, order);
+                                                                child_base, d_gen, ops, nullptr, order, q_items,
+                                                                q_count, q_counter);
     return cudaGetLastError();
 }
 
@@ -1546,11 +1606,13 @@ __device__ __forceinline__ int plane_nt(const uint2 *P, int x)
 template <int FL> __device__ void lrcs_combine(const Shape &s, PopBuf &buf, size_t gsol, const int2 *res,
                                                unsigned char *tab, int tid, int lane, int warp, int *shared_res);
 
+// One scan item: result `item` = sol * nres + c of solution base + sol (CDS c, or CDS
+// pair c for LRCS), then, in the last of the solution's items to finish, the combine.
+// Called by the whole CTA with the CTA's dynamic shared memory.
 template <int NT, int FL>
-__global__ void __launch_bounds__(NT) k_sl(Shape s, PopBuf buf, int base, int2 *part, int32_t *counter,
-                                                 int32_t *status, unsigned long long *scanned)
+__device__ void sl_item(const Shape &s, PopBuf buf, int base, int2 *part, int32_t *counter, int32_t *status,
+                        unsigned long long *scanned, int item, unsigned char *smem_raw)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     SlSmem<NT> &sm = *reinterpret_cast<SlSmem<NT> *>(smem_raw);
     const int G = kSlGuardRows;
     const int W = s.W, n = s.n;
@@ -1562,7 +1624,7 @@ __global__ void __launch_bounds__(NT) k_sl(Shape s, PopBuf buf, int base, int2 *
 
     const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarps = nth >> 5;
     const int nres = FL == 0 ? s.m : s.nres;
-    const int sol = blockIdx.x / nres, c = blockIdx.x - sol * nres;
+    const int sol = item / nres, c = item - sol * nres;
     const size_t gsol = (size_t)(base + sol);
     // hairpin: CDS c against its reverse complement; LRCS: pair c = (pa, pb)
     int pa = c, pb = c;
@@ -1906,6 +1968,66 @@ __global__ void __launch_bounds__(NT) k_sl(Shape s, PopBuf buf, int base, int2 *
     }
 }
 
+// one CTA per result of solutions base .. base + count - 1
+template <int NT, int FL>
+__global__ void __launch_bounds__(NT) k_sl(Shape s, PopBuf buf, int base, int2 *part, int32_t *counter,
+                                                 int32_t *status, unsigned long long *scanned)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    sl_item<NT, FL>(s, buf, base, part, counter, status, scanned, (int)blockIdx.x, smem_raw);
+}
+
+// The scan items of a whole batch: the variation kernels of the batch's instances
+// queue the results their children's mutations invalidated (SlJob.items, .count), and
+// one wave of CTAs takes them by ticket, the jobs in the order given (longest CDSs
+// first), until all are done.  The last CTA to leave clears the tickets and the
+// counts for the next generation.
+template <int NT, int FL>
+__global__ void __launch_bounds__(NT) k_sl_queue(const SlJob *__restrict__ jobs, int njobs, int32_t *ticket)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int qpre[kMaxBatchJobs + 1];
+    __shared__ int cur_job, cur_item;
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        int run = 0;
+        for (int k = 0; k < njobs; k++) {
+            qpre[k] = run;
+            run += *jobs[k].count;
+        }
+        qpre[njobs] = run;
+    }
+    __syncthreads();
+    const int total = qpre[njobs];
+    for (;;) {
+        if (tid == 0) {
+            const int t = atomicAdd(&ticket[0], 1);
+            int k = -1, it = 0;
+            if (t < total) {
+                k = 0;
+                while (qpre[k + 1] <= t) k++;
+                it = jobs[k].items[t - qpre[k]];
+            }
+            cur_job = k;
+            cur_item = it;
+        }
+        __syncthreads();
+        const int k = cur_job, it = cur_item;
+        if (k < 0) break;
+        const SlJob &J = jobs[k];
+        sl_item<NT, FL>(J.s, J.buf, J.base, J.part, J.counter, J.status, J.scanned, it, smem_raw);
+        __syncthreads();  // the next item reuses the shared memory
+    }
+    if (tid == 0) {
+        __threadfence();
+        if (atomicAdd(&ticket[1], 1) == (int)gridDim.x - 1) {
+            for (int q = 0; q < njobs; q++) *jobs[q].count = 0;
+            ticket[0] = 0;
+            ticket[1] = 0;
+        }
+    }
+}
+
 // LRCS combine (last CTA of a solution): the pair with the longest run (the
 // first pair on ties), its diagonal (the smallest delta reaching that length),
 // and on it the first run of that length.  Every run of the pair is at most Lb
@@ -2028,6 +2150,51 @@ static size_t sl_smem_bytes_nt(const Shape &s, size_t head)
 }
 
 size_t sl_smem_bytes(const Shape &s) { return sl_smem_bytes_nt(s, sizeof(SlSmem<kSlThreadsMax>)); }
+
+// the queued scan's shared memory for a job at CTA size nt
+size_t sl_queue_smem_bytes(const Shape &s, int nt)
+{
+    switch (nt) {
+    case 64: return sl_smem_bytes_nt(s, sizeof(SlSmem<64>));
+    case 256: return sl_smem_bytes_nt(s, sizeof(SlSmem<256>));
+    default: return sl_smem_bytes_nt(s, sizeof(SlSmem<128>));
+    }
+}
+
+template <int NT, int FL> static const void *sl_queue_fn() { return (const void *)k_sl_queue<NT, FL>; }
+static const void *sl_queue_kernel(int nt, int fl)
+{
+    if (fl == 1) return nt == 64 ? sl_queue_fn<64, 1>() : nt == 256 ? sl_queue_fn<256, 1>() : sl_queue_fn<128, 1>();
+    return nt == 64 ? sl_queue_fn<64, 0>() : nt == 256 ? sl_queue_fn<256, 0>() : sl_queue_fn<128, 0>();
+}
+
+int sl_queue_ctas_per_sm(int nt, int fl, size_t smem)
+{
+    const void *fn = sl_queue_kernel(nt, fl);
+    if (raise_smem_limit(fn, smem) != cudaSuccess) return 0;
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, nt == 64 || nt == 256 ? nt : 128, smem) != cudaSuccess) return 0;
+    return n;
+}
+
+cudaError_t launch_sl_queue(const SlJob *jobs, int njobs, int32_t *ticket, int nt, int fl, size_t smem, int ctas,
+                            cudaStream_t st)
+{
+    if (njobs <= 0 || njobs > kMaxBatchJobs || ctas <= 0) return cudaErrorInvalidValue;
+    const void *fn = sl_queue_kernel(nt, fl);
+    cudaError_t e = raise_smem_limit(fn, smem);
+    if (e != cudaSuccess) return e;
+    if (fl == 1) {
+        if (nt == 64) k_sl_queue<64, 1><<<ctas, 64, smem, st>>>(jobs, njobs, ticket);
+        else if (nt == 256) k_sl_queue<256, 1><<<ctas, 256, smem, st>>>(jobs, njobs, ticket);
+        else k_sl_queue<128, 1><<<ctas, 128, smem, st>>>(jobs, njobs, ticket);
+    } else {
+        if (nt == 64) k_sl_queue<64, 0><<<ctas, 64, smem, st>>>(jobs, njobs, ticket);
+        else if (nt == 256) k_sl_queue<256, 0><<<ctas, 256, smem, st>>>(jobs, njobs, ticket);
+        else k_sl_queue<128, 0><<<ctas, 128, smem, st>>>(jobs, njobs, ticket);
+    }
+    return cudaGetLastError();
+}
 
 template <int NT>
 static cudaError_t launch_sl_nt(const Shape &s, PopBuf buf, int base, int count, int2 *part, int32_t *counter,

@@ -110,6 +110,22 @@ struct SelectScratch {
     float *finfo;        // [3*M] ideal, worst, nadir
 };
 
+// One batch member's share of a queued stem scan (k_sl_queue): its shape and the
+// buffers of the generation's children, and the queue of results its variation kernel
+// invalidated (items: sol * nres + c, sol in 0 .. N-1 counted from `base`).
+constexpr int kMaxBatchJobs = 1024;
+struct SlJob {
+    Shape s;
+    PopBuf buf;
+    int base;
+    int2 *part;
+    int32_t *counter;
+    int32_t *status;
+    unsigned long long *scanned;
+    int32_t *items;  // [N * nres]
+    int32_t *count;  // items queued
+};
+
 // launchers (pe_eval.cu)
 cudaError_t launch_init(const Shape &s, const DevTables *tab, const int8_t *aa, PopBuf dst, int32_t *surv,
                         cudaStream_t st);
@@ -117,10 +133,17 @@ cudaError_t launch_light_eval(const Shape &s, const DevTables *tab, const int8_t
                               cudaStream_t st);
 cudaError_t launch_mutate(const Shape &s, const DevTables *tab, const int8_t *aa, PopBuf src, PopBuf dst,
                           const int32_t *parent_of, const int32_t *rng_idx, int count, int copy_base, int child_base,
-                          const uint32_t *d_gen, int32_t *ops, int32_t *order, cudaStream_t st);
+                          const uint32_t *d_gen, int32_t *ops, int32_t *order, cudaStream_t st,
+                          int32_t *q_items = nullptr, int32_t *q_count = nullptr, int32_t *q_counter = nullptr);
 cudaError_t launch_sl(const Shape &s, PopBuf buf, int base, int count, int2 *part, int32_t *counter,
                       int32_t *status, cudaStream_t st, unsigned long long *scanned = nullptr);
 size_t sl_smem_bytes(const Shape &s);
+// the batch's queued stem scan (k_sl_queue): shared memory of a job at CTA size nt,
+// resident CTAs per SM, and the launch of one wave over jobs[0 .. njobs)
+size_t sl_queue_smem_bytes(const Shape &s, int nt);
+int sl_queue_ctas_per_sm(int nt, int fl, size_t smem);
+cudaError_t launch_sl_queue(const SlJob *jobs, int njobs, int32_t *ticket, int nt, int fl, size_t smem, int ctas,
+                            cudaStream_t st);
 // Raise a kernel's dynamic shared-memory limit to at least `bytes` on the current
 // device.  The limit only grows, so launches from different host threads never
 // see it lowered between their own setting and their launch.
