@@ -140,6 +140,12 @@ int pe_get_population(pe_instance *inst, uint8_t *codon_idx, float *obj, int8_t 
                       int32_t *survivors);
 /* Objectives only (2N*M floats): the per-generation progress read. */
 int pe_get_objectives(pe_instance *inst, float *obj);
+/* The same read queued on the instance's stream behind the generations already
+ * queued, without waiting: obj holds the objectives once pe_synchronize returns (or
+ * any later wait on the stream), and must stay valid until then.  With page-locked
+ * host memory the copy overlaps the next generations; with pageable memory the call
+ * returns only after the copy. */
+int pe_read_objectives_async(pe_instance *inst, float *obj);
 
 /* --- operator-level entry points (one device function family each) --- */
 

@@ -138,6 +138,7 @@ def lib() -> C.CDLL:
             "pe_destroy": [P], "pe_get_info": [P, C.POINTER(Info)], "pe_init_population": [P],
             "pe_step": [P, C.c_int32], "pe_synchronize": [P],
             "pe_get_population": [P, P, P, P, P, P], "pe_get_objectives": [P, P],
+            "pe_read_objectives_async": [P, P],
             "pe_eval_objectives": [P, P, C.c_int32, P, P, P],
             "pe_mutate": [P, C.c_uint32, P, C.c_int32, P, P, P, P, P, P],
             "pe_select": [P, C.c_uint32, P, P, P, P, C.POINTER(SelectInfo)],
@@ -348,6 +349,12 @@ class Engine:
         out = np.zeros((2 * self.N, self.M), np.float32) if out is None else out
         _ck(lib().pe_get_objectives(self._h, _ptr(out)))
         return out
+
+    def read_objectives_async(self, out_ptr: int):
+        """Queue the objective read (2N x M float32) into the host memory at out_ptr
+        without waiting; it holds them after synchronize().  Page-locked memory (e.g.
+        a pinned torch tensor's data_ptr()) lets the copy overlap the next generations."""
+        _ck(lib().pe_read_objectives_async(self._h, C.c_void_p(out_ptr)))
 
     def survivor_objectives(self):
         """Objectives of the N solutions the last selection kept (the next parents)."""

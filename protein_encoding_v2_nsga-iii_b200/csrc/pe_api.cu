@@ -1118,6 +1118,16 @@ int pe_get_objectives(pe_instance *in, float *obj)
     return pe_get_population(in, nullptr, obj, nullptr, nullptr, nullptr);
 }
 
+int pe_read_objectives_async(pe_instance *in, float *obj)
+{
+    if (!in || !obj) return fail(PE_ERR_ARG, "bad arguments");
+    if (!in->initialized) return fail(PE_ERR_STATE, "population not initialised");
+    const Shape &s = in->s;
+    CK(cudaMemcpyAsync(obj, in->buf[in->cur].obj, (size_t)2 * s.N * s.M * sizeof(float), cudaMemcpyDeviceToHost,
+                       in->stream));
+    return PE_OK;
+}
+
 int pe_eval_objectives(pe_instance *in, const uint8_t *codon_idx, int32_t n, float *obj, int8_t *objidx, int32_t *pql)
 {
     if (!in || !codon_idx || n < 0) return fail(PE_ERR_ARG, "bad arguments");
