@@ -306,6 +306,17 @@ int pe_scan_count(pe_instance *inst, uint64_t *count);
  * The unit of work of the string-objective kernel's throughput.  Waits for the
  * instance's stream. */
 int pe_scan_cells(pe_instance *inst, uint64_t *cells);
+/* Scans whose seeded first pass gave up (no reference counterpart).  The string
+ * scan first looks up T's 8-nucleotide words in a table (linear in n for
+ * random-like CDSs); on a repetitive CDS, whose table chains grow long, it hands
+ * the CDS to the band scan, which visits every counted cell.  Both give the same
+ * result.  Waits for the instance's stream. */
+int pe_scan_fallbacks(pe_instance *inst, uint64_t *count);
+/* First pass of the string scan (no reference counterpart): 0 = seeded, the
+ * default (CDSs of up to 12,288 nucleotides; longer ones take the band scan),
+ * 1 = the band scan for every CDS.  The result does not depend on it; a test of
+ * the band scan, and a way to compare the two.  Rebuilds the instance's graphs. */
+int pe_set_scan_method(pe_instance *inst, int32_t method);
 
 /* --- allocation-free hairpin-stem evaluation (no counterpart in the reference).
  *

@@ -150,6 +150,7 @@ def lib() -> C.CDLL:
             "pe_hypervolume": [P, C.c_int32, C.c_int32, P, C.POINTER(C.c_double)],
             "pe_set_profiling": [P, C.c_int32], "pe_stage_times": [P, P], "pe_scan_count": [P, P],
             "pe_scan_cells": [P, P], "pe_set_wait_limit": [P, C.c_int32],
+            "pe_scan_fallbacks": [P, P], "pe_set_scan_method": [P, C.c_int32],
             "pe_hairpin_noalloc": [P, C.c_int32, C.c_int32, C.c_int32, P, P, P, P],
             "pe_batch_create": [P, C.c_int32, C.POINTER(P)], "pe_batch_step": [P, C.c_int32],
             "pe_batch_synchronize": [P], "pe_batch_destroy": [P], "pe_batch_set_scan_queue": [P, C.c_int32],
@@ -334,6 +335,16 @@ class Engine:
         v = C.c_uint64(0)
         _ck(lib().pe_scan_cells(self._h, C.byref(v)))
         return v.value
+
+    def scan_fallbacks(self) -> int:
+        """Scans whose seeded first pass gave up on a repetitive CDS (the band scan ran)."""
+        v = C.c_uint64(0)
+        _ck(lib().pe_scan_fallbacks(self._h, C.byref(v)))
+        return v.value
+
+    def set_scan_method(self, method: int):
+        """First pass of the string scan: 0 seeded (default), 1 band scan for every CDS."""
+        _ck(lib().pe_set_scan_method(self._h, method))
 
     def population(self):
         N2 = 2 * self.N

@@ -163,7 +163,8 @@ struct pe_instance {
     int2 *d_part = nullptr;
     int32_t *d_counter = nullptr;
     int32_t *d_status = nullptr;
-    unsigned long long *d_scanned = nullptr;  // [0] string-objective scans run, [1] their counted cells
+    unsigned long long *d_scanned = nullptr;  // [0] string-objective scans run, [1] their counted cells,
+                                              // [2] seeded scans handed to the band scan
     float *d_ext = nullptr;
     uint32_t *d_gen = nullptr;
     int cur = 0;
@@ -306,10 +307,10 @@ int build_graphs(pe_instance *in)
 // Hairpin-scan CTA sizes chosen at init, per (device, L, m, N): instances of a shape
 // already tuned in this process skip the timing.
 struct SlTuneKey {
-    int dev, L, m, N;
+    int dev, L, m, N, kind, method;
     bool operator<(const SlTuneKey &o) const
     {
-        return std::tie(dev, L, m, N) < std::tie(o.dev, o.L, o.m, o.N);
+        return std::tie(dev, L, m, N, kind, method) < std::tie(o.dev, o.L, o.m, o.N, o.kind, o.method);
     }
 };
 std::mutex g_tune_mu;
@@ -519,7 +520,7 @@ int pe_create(const pe_config *cfg, const int8_t *aa_idx, int32_t aa_len, const 
     if ((rc = in->alloc(&in->sc.finfo, 3 * PE_MAX_OBJ))) return cleanup(rc);
     if ((rc = in->alloc(&in->d_part, (size_t)N2 * s.nres))) return cleanup(rc);
     if ((rc = in->alloc(&in->d_counter, (size_t)N2))) return cleanup(rc);
-    if ((rc = in->alloc(&in->d_scanned, 2))) return cleanup(rc);
+    if ((rc = in->alloc(&in->d_scanned, 3))) return cleanup(rc);
     if ((rc = in->alloc(&in->d_status, 1))) return cleanup(rc);
     if ((rc = in->alloc(&in->d_ext, (size_t)s.M * s.M))) return cleanup(rc);
     if ((rc = in->alloc(&in->d_gen, 1))) return cleanup(rc);
@@ -541,7 +542,7 @@ int pe_create(const pe_config *cfg, const int8_t *aa_idx, int32_t aa_len, const 
     CKC(cudaMemcpyAsync(in->sc.trank, trank.data(), trank.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
     CKC(cudaMemcpyAsync(in->d_order, ident.data(), ident.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
     CKC(cudaMemsetAsync(in->d_counter, 0, (size_t)N2 * sizeof(int32_t), st));
-    CKC(cudaMemsetAsync(in->d_scanned, 0, 2 * sizeof(unsigned long long), st));
+    CKC(cudaMemsetAsync(in->d_scanned, 0, 3 * sizeof(unsigned long long), st));
     CKC(cudaMemsetAsync(in->d_status, 0, sizeof(int32_t), st));
     CKC(cudaMemsetAsync(in->d_ext, 0, (size_t)s.M * s.M * sizeof(float), st));
     CKC(cudaMemsetAsync(in->d_gen, 0, sizeof(uint32_t), st));
@@ -926,6 +927,32 @@ int pe_scan_cells(pe_instance *in, uint64_t *cells)
     return PE_OK;
 }
 
+int pe_scan_fallbacks(pe_instance *in, uint64_t *count)
+{
+    if (!in || !count) return fail(PE_ERR_ARG, "null argument");
+    unsigned long long v = 0;
+    CK(cudaMemcpyAsync(&v, in->d_scanned + 2, sizeof v, cudaMemcpyDeviceToHost, in->stream));
+    CK(cudaStreamSynchronize(in->stream));
+    *count = (uint64_t)v;
+    return PE_OK;
+}
+
+int pe_set_scan_method(pe_instance *in, int32_t method)
+{
+    if (!in) return fail(PE_ERR_ARG, "null instance");
+    if (method != 0 && method != 1) return fail(PE_ERR_ARG, "scan method must be 0 (seeded) or 1 (band scan), got %d", method);
+    CK(cudaStreamSynchronize(in->stream));
+    if (method != in->s.sl_method) {
+        in->s.sl_method = method;
+        for (int i = 0; i < 2; i++)
+            if (in->graph[i]) {
+                cudaGraphExecDestroy(in->graph[i]);
+                in->graph[i] = nullptr;
+            }
+    }
+    return PE_OK;
+}
+
 int pe_instance_bytes(const pe_config *cfg, int32_t aa_len, uint64_t *bytes)
 {
     if (!cfg || !bytes || aa_len < 3 || cfg->pop_size < 1 || cfg->n_cds < 2) return fail(PE_ERR_ARG, "bad arguments");
@@ -947,7 +974,7 @@ int pe_instance_bytes(const pe_config *cfg, int32_t aa_len, uint64_t *bytes)
          2 * r(R * 4) + r((N2 + M) * 4) + r(32) + r(72);
     const uint64_t nres = cfg->sl_kind == PE_SL_LRCS ? m * (m + 1) / 2 : m;
     t += r(N2 * nres * 8) + r(N2 * 4) + r(4) + r(M * M * 4) + r(4);
-    t += 2 * r(N2 * nres * 8) + r(16);  // per-CDS (per-pair) string results of both buffers, scan counts
+    t += 2 * r(N2 * nres * 8) + r(24);  // per-CDS (per-pair) string results of both buffers, scan counts
     t += 2 * r(N2 * (5 * m + m * (m - 1) / 2) * 4);  // per-CDS sums of the light objectives, both buffers
     *bytes = t;
     return PE_OK;
@@ -995,7 +1022,7 @@ int pe_init_population(pe_instance *in)
     CK(launch_init(s, in->d_tab, in->d_aa, in->buf[0], in->d_surv, in->stream));
     bool scanned = false;
     if (in->cfg.sl_threads == 0 && s.sl_threads == 0) {
-        const SlTuneKey key{in->device, s.L, s.m, s.N};
+        const SlTuneKey key{in->device, s.L, s.m, s.N, s.sl_kind, s.sl_method};
         s.sl_threads = sl_tuned(key);
         if (s.sl_threads == 0) {
             // pick the hairpin-scan CTA size: after one warm scan of the initial population,
@@ -1150,7 +1177,7 @@ int pe_eval_objectives(pe_instance *in, const uint8_t *codon_idx, int32_t n, flo
     CK(cudaMemcpy2DAsync(b.ids, (size_t)s.Lp, codon_idx, (size_t)s.L, (size_t)s.L, (size_t)n * s.m,
                          cudaMemcpyHostToDevice, in->stream));
     CK(launch_light_eval(s, in->d_tab, in->d_aa, b, 0, n, in->stream));
-    CK(launch_sl(s, b, 0, n, part, counter, in->d_status, in->stream));
+    CK(launch_sl(s, b, 0, n, part, counter, in->d_status, in->stream, in->d_scanned));
     if (obj) CK(cudaMemcpyAsync(obj, b.obj, (size_t)n * s.M * sizeof(float), cudaMemcpyDeviceToHost, in->stream));
     if (objidx) CK(cudaMemcpyAsync(objidx, b.objidx, (size_t)n * 2 * s.M, cudaMemcpyDeviceToHost, in->stream));
     if (pql) CK(cudaMemcpyAsync(pql, b.pql, (size_t)n * 3 * sizeof(int32_t), cudaMemcpyDeviceToHost, in->stream));

@@ -1568,6 +1568,168 @@ __device__ void sl_band_scan(const uint4 *__restrict__ E4, const int *__restrict
     __syncwarp();
 }
 
+// ---------------------------------------------------------------------------
+// Seeded scan: the first pass for CDSs short enough for a table of their words.
+//
+// A counted run of >= 8 pairing cells on shift delta that starts at row a has
+// S's nucleotides a .. a+7 equal to T's a+delta .. a+delta+7 (T is the reverse
+// complement for the hairpin, the other CDS for LRCS, so a cell pairs exactly
+// when the two planes' nucleotides are equal).  So each run start is a pair of
+// equal 8-nucleotide words, S's at a and T's at i = a + delta.  T's n-7 words go
+// into a chained hash table (16-bit bucket heads; one node per position i: the
+// word in the high 16 bits, the next position of the chain in the low 16), and
+// each S word walks its chain.  An equal word whose shift is scanned and whose
+// rows a .. a+7 are counted joins its warp's queue; the warp measures queued
+// words 32 at a time, one per lane: a word is a run start when row a-1 is not
+// counted or does not pair, and the run is followed 32 rows at a time to its end
+// and clipped to the diagonal's counted range, as the band scan measures its
+// marked runs.  Every counted run of >= 8 is found exactly once, so (longest,
+// smallest key) is the band scan's.  The lanes of a warp walk their chains in
+// step and meet in the queue, so neither the uneven chain lengths nor the rare
+// equal words split the warp for long.
+//
+// For random-like CDSs the chains hold under one node and the work is linear in
+// n instead of the n^2/2 cells.  A repetitive CDS makes long chains (many equal
+// words): each thread bounds the nodes and run words it visits, and when any
+// thread passes its bound the CTA drops the partial result and the band scan runs.
+constexpr int kSeedMaxN = 12288;  // longest CDS (nucleotides) with a seeded scan
+constexpr int kSeedMaxBits = 13;  // hash buckets: the power of two >= 2n, at most 2^13
+constexpr uint32_t kSeedEnd = 0xffffu;
+
+__host__ __device__ __forceinline__ int sl_seed_bits(int n)
+{
+    int b = 6;
+    while ((1 << b) < 2 * n && b < kSeedMaxBits) b++;
+    return b;
+}
+__host__ __device__ __forceinline__ bool sl_seeded(const Shape &s) { return s.sl_method == 0 && s.n >= 8 && s.n <= kSeedMaxN; }
+// heads (16 bits each), then the nodes (4-byte aligned)
+__host__ __device__ __forceinline__ size_t sl_seed_head_bytes(int n) { return ((size_t)1 << sl_seed_bits(n)) * 2; }
+__host__ __device__ __forceinline__ size_t sl_seed_bytes(int n) { return sl_seed_head_bytes(n) + (size_t)n * 4; }
+
+// the 8 nucleotides from bit sh of (w0, w1) of both planes as a 16-bit word, twice:
+// plane-0 bits in bytes 0 and 2, plane-1 bits in bytes 1 and 3
+__device__ __forceinline__ uint32_t seed_word(uint32_t lo0, uint32_t lo1, uint32_t hi0, uint32_t hi1, int sh)
+{
+    return __byte_perm(fshr(lo0, lo1, sh), fshr(hi0, hi1, sh), 0x4040);
+}
+__device__ __forceinline__ uint32_t seed_hash(uint32_t w, int hb) { return (w * 0x9E3779B1u) >> (32 - hb); }
+
+// Measures the queued equal word e = a | i << 16 (rows a .. a+7 pair on delta = i - a
+// and are counted): when it starts a run, the run's counted length against
+// (best, bestd).  Adds the run words it read to work.
+template <int FL>
+__device__ __forceinline__ void seed_measure(uint32_t e, const SlGeo &geo, const uint2 *__restrict__ S,
+                                             const uint32_t *__restrict__ Tlo, const uint32_t *__restrict__ Thi,
+                                             int &work, int &best, int &bestd)
+{
+    const int n = geo.n, G = kSlGuardRows;
+    const int a = (int)(e & 0xffffu), j = (int)(e >> 16), delta = j - a;
+    int r_lo, r_hi;
+    sl_diag_rows<FL>(n, delta, r_lo, r_hi);
+    if (a > r_lo) {  // row a-1 counted: a starts a run only if it does not pair
+        const int p = a - 1, i = j - 1;
+        const uint32_t tl = Tlo[(i >> 5) + G] >> (i & 31), th = Thi[(i >> 5) + G] >> (i & 31);
+        const uint2 sp = S[p >> 5];
+        if (((((sp.x >> (p & 31)) ^ tl) | ((sp.y >> (p & 31)) ^ th)) & 1u) == 0u) return;
+    }
+    int last = a + 7;  // last row known to pair
+    while (last < r_hi) {
+        work++;
+        const int p = last + 1, i = p + delta;
+        const int ws = p >> 5, wt = (i >> 5) + G;
+        const uint32_t sl = fshr(S[ws].x, S[ws + 1].x, p & 31), sh2 = fshr(S[ws].y, S[ws + 1].y, p & 31);
+        const uint32_t tl = fshr(Tlo[wt], Tlo[wt + 1], i & 31), th = fshr(Thi[wt], Thi[wt + 1], i & 31);
+        const uint32_t mm = ~((sl ^ tl) | (sh2 ^ th));
+        if (mm != 0xffffffffu) {
+            last += __ffs(~mm) - 1;
+            break;
+        }
+        last += 32;
+    }
+    const int L = min(last, r_hi) - a + 1, d = sl_key<FL>(n, delta);
+    if (L > best || (L == best && d < bestd)) {
+        best = L;
+        bestd = d;
+    }
+}
+
+// Returns false (CTA-uniform) when some thread passed its bound; (best, bestd) then
+// hold a partial result that the caller discards.  q: this warp's queue, 64 words.
+template <int FL>
+__device__ bool sl_seed_scan(const SlGeo &geo, const uint2 *__restrict__ S, const uint32_t *__restrict__ Tlo,
+                             const uint32_t *__restrict__ Thi, unsigned short *heads, uint32_t *nodes, uint32_t *q,
+                             int tid, int nth, int &best, int &bestd)
+{
+    const int n = geo.n, G = kSlGuardRows, lane = tid & 31;
+    const int hb = sl_seed_bits(n), npos = n - 7;  // word starts 0 .. n-8
+    for (int h = tid; h < (1 << hb); h += nth) heads[h] = (unsigned short)kSeedEnd;
+    __syncthreads();
+    bool over = false;
+    for (int i = tid; i < npos; i += nth) {
+        const int w = (i >> 5) + G, sh = i & 31;
+        const uint32_t c = seed_word(Tlo[w], Tlo[w + 1], Thi[w], Thi[w + 1], sh);
+        // push i onto its bucket's chain (lock-free: a failed swap means another
+        // position went in first; bounded all the same, and a CTA whose swap gives up
+        // leaves the CDS to the band scan)
+        unsigned short *hp = heads + seed_hash(c, hb);
+        unsigned short old = *hp, seen;
+        int tries = 0;
+        while ((seen = atomicCAS(hp, old, (unsigned short)i)) != old && ++tries < (1 << 16)) old = seen;
+        over = over || seen != old;
+        nodes[i] = (c & 0xffff0000u) | old;
+    }
+    if (__syncthreads_or(over)) return false;
+    // nodes and run words a thread may visit: about where the band scan, whose work per
+    // thread grows as n^2, becomes the cheaper pass (n/64 per word looked up, at least 8)
+    const int budget = max(8, n >> 6) * ((npos + nth - 1) / nth) + 64;
+    const unsigned lt = (1u << lane) - 1u;
+    int work = 0, qn = 0;  // qn: entries in this warp's queue (warp-uniform)
+    for (int a0 = tid - lane; a0 < npos; a0 += nth) {
+        const int a = a0 + lane;
+        uint32_t c = 0, j = kSeedEnd;
+        if (a < npos) {
+            const int w = a >> 5, sh = a & 31;
+            const uint2 s0 = S[w], s1 = S[w + 1];
+            c = seed_word(s0.x, s1.x, s0.y, s1.y, sh);
+            j = heads[seed_hash(c, hb)];
+        }
+        // the lanes walk their chains in step; equal words join the queue
+        while (__any_sync(0xffffffffu, j != kSeedEnd)) {
+            bool hit = false;
+            const uint32_t jc = j;
+            if (j != kSeedEnd) {
+                const uint32_t node = nodes[j];
+                j = ++work > budget ? kSeedEnd : (node & 0xffffu);  // past the bound: stop walking
+                if ((node ^ c) < 0x10000u) {  // the same word: rows a .. a+7 pair on delta
+                    const int delta = (int)jc - a;
+                    int r_lo, r_hi;
+                    sl_diag_rows<FL>(n, delta, r_lo, r_hi);
+                    hit = delta >= geo.dlo && delta <= geo.dhi && a + 7 <= r_hi;
+                }
+            }
+            const unsigned hm = __ballot_sync(0xffffffffu, hit);
+            if (hm) {
+                if (hit) q[qn + __popc(hm & lt)] = (uint32_t)a | (jc << 16);
+                qn += __popc(hm);
+                __syncwarp();
+                if (qn >= 32) {
+                    seed_measure<FL>(q[lane], geo, S, Tlo, Thi, work, best, bestd);
+                    __syncwarp();
+                    if (lane < qn - 32) q[lane] = q[32 + lane];
+                    qn -= 32;
+                    __syncwarp();
+                }
+            }
+        }
+        over = over || work > budget;
+        if (__any_sync(0xffffffffu, over)) break;
+    }
+    if (lane < qn) seed_measure<FL>(q[lane], geo, S, Tlo, Thi, work, best, bestd);
+    over = over || work > budget;
+    return !__syncthreads_or(over);
+}
+
 // T's equality plane for nucleotide v (4 = the zero plane) at T word w, zero
 // outside [0, n)
 __device__ __forceinline__ uint32_t eq_word(const uint32_t *Tlo, const uint32_t *Thi, int W, int n, int v, int w)
@@ -1605,6 +1767,34 @@ __device__ __forceinline__ int plane_nt(const uint2 *P, int x)
 
 template <int FL> __device__ void lrcs_combine(const Shape &s, PopBuf &buf, size_t gsol, const int2 *res,
                                                unsigned char *tab, int tid, int lane, int warp, int *shared_res);
+
+// Warp-wide: the result with the longest run among res[0 .. count-1], read in
+// parallel (one L2 round trip for up to 32 results); ties go to the largest index
+// (last_on_tie) or to the smallest.  Every lane returns it.
+__device__ __forceinline__ void warp_pick_result(const int2 *res, int count, bool last_on_tie, int lane, int &L, int &idx,
+                                                 int &y)
+{
+    L = -1;
+    idx = -1;
+    y = 0;
+    for (int r = lane; r < count; r += 32) {  // r rises within a lane
+        const int2 v = __ldcg(&res[r]);
+        if (v.x > L || (last_on_tie && v.x == L)) {
+            L = v.x;
+            idx = r;
+            y = v.y;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const int L2 = __shfl_xor_sync(0xffffffffu, L, o), i2 = __shfl_xor_sync(0xffffffffu, idx, o),
+                  y2 = __shfl_xor_sync(0xffffffffu, y, o);
+        if (L2 > L || (L2 == L && (last_on_tie ? i2 > idx : i2 < idx))) {
+            L = L2;
+            idx = i2;
+            y = y2;
+        }
+    }
+}
 
 // One scan item: result `item` = sol * nres + c of solution base + sol (CDS c, or CDS
 // pair c for LRCS), then, in the last of the solution's items to finish, the combine.
@@ -1708,66 +1898,82 @@ __device__ void sl_item(const Shape &s, PopBuf buf, int base, int2 *part, int32_
             Thi[e] = hi;
         }
         __syncthreads();
-        // band-scan tables, in the space the shifted copies of T take later:
-        //   E4[v][x]      E_v words x-kEqGuard .. x+3-kEqGuard, v = 0..3 nucleotides, 4 the zero plane
-        //   poffT[sp][i]  rows r = 32(sp-1)+2i, r+1: E4 entries v(r)*PS + sp-1 in the low and high
-        //                 16 bits (v(r) = 4 outside [0, n); 5*PS < 65536 since E4's 80*PS bytes fit in
-        //                 shared memory); pitch 17 words
-        //   gstart[g]     first item of band group g (items: the group's 32-row segments)
-        const int PS = sl_plane_stride(W), NSP = W + 2;
         const SlGeo geo = sl_geo<FL>(n, pa == pb);
-        const int ng = geo.ng, D0 = geo.D0;
-        uint4 *E4 = reinterpret_cast<uint4 *>(tab);
-        int *poffT = reinterpret_cast<int *>(E4 + 5 * PS);
-        int *gstart = poffT + kSegPitch * NSP;
-        // each equality word once, stored into the four entries that hold it (entry x holds
-        // words x - kEqGuard .. x + 3 - kEqGuard, word j of the entry being word x - kEqGuard + j)
-        uint32_t *E4w = reinterpret_cast<uint32_t *>(E4);
-        for (int e = tid; e < 5 * (PS + 3); e += nth) {
-            const int v = e / (PS + 3), w = e - v * (PS + 3) - kEqGuard;
-            const uint32_t word = eq_word(Tlo, Thi, W, n, v, w);
-    #pragma unroll
-            for (int j = 0; j < 4; j++) {
-                const int x = w + kEqGuard - j;
-                if (x >= 0 && x < PS) E4w[(v * PS + x) * 4 + j] = word;
-            }
-        }
-        for (int e = tid; e < kSegPitch * NSP; e += nth) {
-            const int sp = e / kSegPitch, i = e - sp * kSegPitch;
-            int word = (4 * PS + sp - 1) * 0x10001;  // both rows outside [0, n): the zero plane
-            if (i < 16 && sp >= 1 && sp - 1 < W) {   // rows r = 32(sp-1) + 2i and r + 1
-                const uint2 sw = S[sp - 1];
-                const int b = 2 * i, r = 32 * (sp - 1) + b;
-                const int v0 = r < n ? (int)(((sw.x >> b) & 1u) | (((sw.y >> b) & 1u) << 1)) : 4;
-                const int v1 = r + 1 < n ? (int)(((sw.x >> (b + 1)) & 1u) | (((sw.y >> (b + 1)) & 1u) << 1)) : 4;
-                word = (v0 * PS + sp - 1) | ((v1 * PS + sp - 1) << 16);  // E4 entries of rows r, r + 1
-            }
-            poffT[e] = word;
-        }
-        if (warp == 0) {
-            int carry = 0;
-            for (int g0 = 0; g0 < ng; g0 += 32) {
-                const int g = g0 + lane;
-                int x = 0;
-                if (g < ng) {
-                    int s_lo, s_hi;
-                    sl_group_rows<FL>(n, D0 + 32 * kBandGroup * g, s_lo, s_hi);
-                    x = max(0, s_hi - s_lo + 1);
-                }
-                for (int o = 1; o < 32; o <<= 1) {
-                    const int y = __shfl_up_sync(0xffffffffu, x, o);
-                    if (lane >= o) x += y;
-                }
-                if (g < ng) gstart[g + 1] = carry + x;
-                carry += __shfl_sync(0xffffffffu, x, 31);
-            }
-            if (lane == 0) gstart[0] = 0;
-        }
-        if (tid == 0) sm.next_chunk = 0;
-        __syncthreads();
-
         int best = 0, bestd = 0x7fffffff;
-        sl_band_scan<FL>(E4, poffT, gstart, geo, S, Tlo, Thi, sm.queue[warp], &sm.next_chunk, lane, best, bestd);
+        // the seeded scan where the CDS fits its table, else (or when it gives up on a
+        // repetitive CDS) the band scan
+        bool band = true;
+        if (sl_seeded(s)) {
+            unsigned short *heads = reinterpret_cast<unsigned short *>(tab);
+            uint32_t *nodes = reinterpret_cast<uint32_t *>(tab + sl_seed_head_bytes(n));
+            band = !sl_seed_scan<FL>(geo, S, Tlo, Thi, heads, nodes, reinterpret_cast<uint32_t *>(sm.queue[warp]), tid,
+                                     nth, best, bestd);
+            if (band) {
+                best = 0;
+                bestd = 0x7fffffff;
+                if (tid == 0 && scanned) atomicAdd(&scanned[2], 1ull);
+            }
+        }
+        if (band) {
+            // band-scan tables (their space is free again: the seeded scan's last reads
+            // came before its closing barrier):
+            //   E4[v][x]      E_v words x-kEqGuard .. x+3-kEqGuard, v = 0..3 nucleotides, 4 the zero plane
+            //   poffT[sp][i]  rows r = 32(sp-1)+2i, r+1: E4 entries v(r)*PS + sp-1 in the low and high
+            //                 16 bits (v(r) = 4 outside [0, n); 5*PS < 65536 since E4's 80*PS bytes fit in
+            //                 shared memory); pitch 17 words
+            //   gstart[g]     first item of band group g (items: the group's 32-row segments)
+            const int PS = sl_plane_stride(W), NSP = W + 2;
+            const int ng = geo.ng, D0 = geo.D0;
+            uint4 *E4 = reinterpret_cast<uint4 *>(tab);
+            int *poffT = reinterpret_cast<int *>(E4 + 5 * PS);
+            int *gstart = poffT + kSegPitch * NSP;
+            // each equality word once, stored into the four entries that hold it (entry x holds
+            // words x - kEqGuard .. x + 3 - kEqGuard, word j of the entry being word x - kEqGuard + j)
+            uint32_t *E4w = reinterpret_cast<uint32_t *>(E4);
+            for (int e = tid; e < 5 * (PS + 3); e += nth) {
+                const int v = e / (PS + 3), w = e - v * (PS + 3) - kEqGuard;
+                const uint32_t word = eq_word(Tlo, Thi, W, n, v, w);
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const int x = w + kEqGuard - j;
+                    if (x >= 0 && x < PS) E4w[(v * PS + x) * 4 + j] = word;
+                }
+            }
+            for (int e = tid; e < kSegPitch * NSP; e += nth) {
+                const int sp = e / kSegPitch, i = e - sp * kSegPitch;
+                int word = (4 * PS + sp - 1) * 0x10001;  // both rows outside [0, n): the zero plane
+                if (i < 16 && sp >= 1 && sp - 1 < W) {   // rows r = 32(sp-1) + 2i and r + 1
+                    const uint2 sw = S[sp - 1];
+                    const int b = 2 * i, r = 32 * (sp - 1) + b;
+                    const int v0 = r < n ? (int)(((sw.x >> b) & 1u) | (((sw.y >> b) & 1u) << 1)) : 4;
+                    const int v1 = r + 1 < n ? (int)(((sw.x >> (b + 1)) & 1u) | (((sw.y >> (b + 1)) & 1u) << 1)) : 4;
+                    word = (v0 * PS + sp - 1) | ((v1 * PS + sp - 1) << 16);  // E4 entries of rows r, r + 1
+                }
+                poffT[e] = word;
+            }
+            if (warp == 0) {
+                int carry = 0;
+                for (int g0 = 0; g0 < ng; g0 += 32) {
+                    const int g = g0 + lane;
+                    int x = 0;
+                    if (g < ng) {
+                        int s_lo, s_hi;
+                        sl_group_rows<FL>(n, D0 + 32 * kBandGroup * g, s_lo, s_hi);
+                        x = max(0, s_hi - s_lo + 1);
+                    }
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const int y = __shfl_up_sync(0xffffffffu, x, o);
+                        if (lane >= o) x += y;
+                    }
+                    if (g < ng) gstart[g + 1] = carry + x;
+                    carry += __shfl_sync(0xffffffffu, x, 31);
+                }
+                if (lane == 0) gstart[0] = 0;
+            }
+            if (tid == 0) sm.next_chunk = 0;
+            __syncthreads();
+            sl_band_scan<FL>(E4, poffT, gstart, geo, S, Tlo, Thi, sm.queue[warp], &sm.next_chunk, lane, best, bestd);
+        }
         // CTA reduction of (best, smallest anti-diagonal)
         for (int o = 16; o > 0; o >>= 1) {
             int ob = __shfl_xor_sync(0xffffffffu, best, o), od = __shfl_xor_sync(0xffffffffu, bestd, o);
@@ -1835,20 +2041,15 @@ __device__ void sl_item(const Shape &s, PopBuf buf, int base, int2 *part, int32_
         return;
     }
     // ---- last CTA of this solution: combine CDSs (largest CDS index on ties)
-    if (tid == 0) {
-        int Lb = -1, cb = 0, db = 0;
-        for (int cc = 0; cc < s.m; cc++) {
-            int2 v = __ldcg(&res[cc]);
-            if (v.x >= Lb) {
-                Lb = v.x;
-                cb = cc;
-                db = v.y;
-            }
+    if (warp == 0) {
+        int Lb, cb, db;
+        warp_pick_result(res, s.m, true, lane, Lb, cb, db);
+        if (lane == 0) {
+            sm.res[0] = Lb;
+            sm.res[1] = cb;
+            sm.res[2] = db;
+            counter[sol] = 0;
         }
-        sm.res[0] = Lb;
-        sm.res[1] = cb;
-        sm.res[2] = db;
-        counter[sol] = 0;
     }
     __syncthreads();
     const int Lb = sm.res[0], cb = sm.res[1], d = sm.res[2];
@@ -2038,19 +2239,14 @@ __global__ void __launch_bounds__(NT) k_sl_queue(const SlJob *__restrict__ jobs,
 template <int FL> __device__ void lrcs_combine(const Shape &s, PopBuf &buf, size_t gsol, const int2 *res,
                                                unsigned char *tab, int tid, int lane, int warp, int *shared_res)
 {
-    if (tid == 0) {
-        int Lb = 0, rb = 0, kb = s.n;
-        for (int r = 0; r < s.nres; r++) {
-            const int2 v = __ldcg(&res[r]);
-            if (v.x > Lb) {
-                Lb = v.x;
-                rb = r;
-                kb = v.y;
-            }
+    if (warp == 0) {  // the first pair on ties; no pair with a run: length 0 (nothing else is read)
+        int Lb, rb, kb;
+        warp_pick_result(res, s.nres, false, lane, Lb, rb, kb);
+        if (lane == 0) {
+            shared_res[0] = Lb;
+            shared_res[1] = rb;
+            shared_res[2] = kb;
         }
-        shared_res[0] = Lb;
-        shared_res[1] = rb;
-        shared_res[2] = kb;
     }
     __syncthreads();
     const int Lb = shared_res[0], n = s.n, delta = shared_res[2] - n;
@@ -2145,7 +2341,7 @@ static size_t sl_smem_bytes_nt(const Shape &s, size_t head)
     const int ng = s.sl_kind == PE_SL_LRCS ? sl_geo<1>(s.n, false).ng : sl_num_groups(s.n);
     const size_t band = (size_t)5 * sl_plane_stride(W) * sizeof(uint4) + (size_t)kSegPitch * (W + 2) * sizeof(int) +
                         (size_t)(ng + 1) * sizeof(int);
-    b += band;
+    b += sl_seeded(s) ? std::max(band, sl_seed_bytes(s.n)) : band;  // the two passes share the space
     return b;
 }
 

@@ -42,6 +42,7 @@ struct Shape {
     int nres;        // string-objective results per solution: m CDSs (hairpin) or m(m+1)/2 CDS pairs (LRCS)
     int wait_limit;  // polls of a bounded device wait: 0 = the default, < 0 = give up at once (tests)
     int naux;        // int32 words of per-CDS sums per solution: AUX_HD(m) + m(m-1)/2
+    int sl_method;   // first pass of the string scan: 0 seeded (word table) where the CDS fits, 1 band scan
 };
 
 // Per-solution sums of the light objectives (PopBuf.aux), int32 words: per CDS c the

@@ -10,14 +10,21 @@ pytestmark = pytest.mark.gpu
 
 
 def check(pe, orc, aa, tabc, ids):
+    """Both first passes (seeded word table, band scan) against the oracle; returns the
+    engine's result and the seeded run's hand-overs to the band scan."""
     tab = tabc.arrays()
     m = ids.shape[1]
-    with pe.Engine(aa, tabc, m, 8, 0.05, objectives=1, ref_p=2) as eng:
-        g = eng.evaluate(ids)
     o = orc.Problem(aa, tab, m, 8, 0.05, objset=1, p=2).evaluate(ids)
-    for what, u, v in zip(("obj", "objidx", "pql"), g, o):
-        assert same(u, v), f"{what}: gpu {u[:4]} oracle {v[:4]}"
-    return g
+    handed = []
+    for method in (0, 1):
+        with pe.Engine(aa, tabc, m, 8, 0.05, objectives=1, ref_p=2) as eng:
+            eng.set_scan_method(method)
+            g = eng.evaluate(ids)
+            handed.append(eng.scan_fallbacks())
+        for what, u, v in zip(("obj", "objidx", "pql"), g, o):
+            assert same(u, v), f"scan method {method}, {what}: gpu {u[:4]} oracle {v[:4]}"
+    assert handed[1] == 0
+    return g, handed[0]
 
 
 @pytest.mark.parametrize("L,m,n", [(51, 3, 16), (151, 2, 12), (400, 3, 6), (1001, 8, 3), (2001, 2, 2), (3334, 2, 1)])
@@ -25,9 +32,10 @@ def test_random_cds(pe, orc, gpu, L, m, n):
     tabc = pe.dirichlet_table(L)
     aa = pe.synthetic_protein(L - 1, 1000 + L)
     ids = rand_ids(np.random.default_rng(L), aa, tabc.arrays(), m, n)
-    g = check(pe, orc, aa, tabc, ids)
+    g, handed = check(pe, orc, aa, tabc, ids)
     if L >= 400:
-        assert (g[2][:, 2] >= 8).all()      # the band scan decides these
+        assert (g[2][:, 2] >= 8).all()      # the first pass decides these
+    assert handed == 0                      # random-like CDSs: the seeded pass never gives up
 
 
 def test_long_perfect_hairpin(pe, orc, gpu):
@@ -44,8 +52,9 @@ def test_long_perfect_hairpin(pe, orc, gpu):
     ids[0, 0, :300], ids[0, 0, 300:600] = aaa, uuu
     ids[1, 2, 100:300], ids[1, 2, 300:500] = aaa, uuu
     ids[2, 1, 290:300], ids[2, 1, 300:310] = aaa, uuu
-    g = check(pe, orc, aa, tabc, ids)
+    g, handed = check(pe, orc, aa, tabc, ids)
     assert g[2][0, 2] > 800
+    assert handed > 0                       # the AAA..A UUU..U CDSs: long chains, band scan
 
 
 def test_low_complexity_many_runs(pe, orc, gpu):

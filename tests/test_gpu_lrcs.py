@@ -33,13 +33,16 @@ def same(a, b):
 def check_eval(pe, orc, aa, tabc, ids, objset=1):
     m = ids.shape[1]
     tab = tabc.arrays()
-    with pe.Engine(aa, tabc, m, 8, 0.05, objectives=objset, ref_p=2, sl_kind=pe.SL_LRCS) as eng:
-        g = eng.evaluate(ids)
     o = orc.Problem(aa, tab, m, 8, 0.05, objset=objset, p=2, slkind=1).evaluate(ids)
-    for what, a, b in zip(("obj", "objidx", "pql"), g, o):
-        ok = np.all((a == b) if a.dtype.kind != "f" else (a.view(np.uint32) == b.view(np.uint32)), axis=1)
-        bad = np.flatnonzero(~ok)
-        assert len(bad) == 0, f"{what} differs for solutions {bad[:5]}: gpu {a[bad[0]]} oracle {b[bad[0]]}"
+    for method in (0, 1):  # seeded word table, band scan
+        with pe.Engine(aa, tabc, m, 8, 0.05, objectives=objset, ref_p=2, sl_kind=pe.SL_LRCS) as eng:
+            eng.set_scan_method(method)
+            g = eng.evaluate(ids)
+        for what, a, b in zip(("obj", "objidx", "pql"), g, o):
+            ok = np.all((a == b) if a.dtype.kind != "f" else (a.view(np.uint32) == b.view(np.uint32)), axis=1)
+            bad = np.flatnonzero(~ok)
+            assert len(bad) == 0, (f"scan method {method}, {what} differs for solutions {bad[:5]}: "
+                                   f"gpu {a[bad[0]]} oracle {b[bad[0]]}")
 
 
 @pytest.mark.parametrize("L,m,n", [(201, 2, 64), (120, 4, 48), (1001, 8, 6), (33, 10, 32), (12, 3, 48), (5, 2, 32)])
