@@ -1571,69 +1571,82 @@ __device__ void sl_band_scan(const uint4 *__restrict__ E4, const int *__restrict
 // ---------------------------------------------------------------------------
 // Seeded scan: the first pass for CDSs short enough for a table of their words.
 //
-// A counted run of >= 8 pairing cells on shift delta that starts at row a has
-// S's nucleotides a .. a+7 equal to T's a+delta .. a+delta+7 (T is the reverse
-// complement for the hairpin, the other CDS for LRCS, so a cell pairs exactly
-// when the two planes' nucleotides are equal).  So each run start is a pair of
-// equal 8-nucleotide words, S's at a and T's at i = a + delta.  T's n-7 words go
-// into a chained hash table (16-bit bucket heads; one node per position i: the
-// word in the high 16 bits, the next position of the chain in the low 16), and
-// each S word walks its chain.  An equal word whose shift is scanned and whose
-// rows a .. a+7 are counted joins its warp's queue; the warp measures queued
-// words 32 at a time, one per lane: a word is a run start when row a-1 is not
-// counted or does not pair, and the run is followed 32 rows at a time to its end
-// and clipped to the diagonal's counted range, as the band scan measures its
-// marked runs.  Every counted run of >= 8 is found exactly once, so (longest,
-// smallest key) is the band scan's.  The lanes of a warp walk their chains in
-// step and meet in the queue, so neither the uneven chain lengths nor the rare
-// equal words split the warp for long.
+// A cell (r, delta) pairs exactly when S's nucleotide r equals T's r + delta (T is
+// the reverse complement for the hairpin, the other CDS for LRCS).  A counted run
+// of >= 8 pairing rows st .. st+L-1 on shift delta holds, at its even row e = st or
+// st+1, seven rows e .. e+6 that pair: S's 7-nucleotide word at e equals T's at
+// e + delta.  So T's n-6 words (every position) go into a chained hash table
+// (32-bit bucket heads; one node per position i: the word in the high 16 bits, the
+// next position of the chain in the low 16), and S's words at even positions walk
+// their chains.  An equal word (e, i) whose shift is scanned and whose rows up to
+// e+6 are counted joins its warp's queue; the warp measures queued words 32 at a
+// time, one per lane.  The run's start is e when row e-1 is not counted or does
+// not pair, e-1 when row e-1 pairs and row e-2 does not (or is not counted); when
+// both pair, the run is the one found from the even row e-2 and this word is
+// dropped.  The run is followed 32 rows at a time to its end and clipped to the
+// diagonal's counted range, as the band scan measures its marked runs.  Every
+// counted run of >= 8 is measured exactly once, so (longest, smallest key) is the
+// band scan's when the longest reaches 8 (shorter ones may be measured too; a
+// result below 8 sends the CDS to the exact word scan).  The lanes of a warp walk
+// their chains in step and meet in the queue, so neither the uneven chain
+// lengths nor the rare equal words split the warp for long.
 //
-// For random-like CDSs the chains hold under one node and the work is linear in
+// For random-like CDSs the chains hold about one node and the work is linear in
 // n instead of the n^2/2 cells.  A repetitive CDS makes long chains (many equal
 // words): each thread bounds the nodes and run words it visits, and when any
 // thread passes its bound the CTA drops the partial result and the band scan runs.
 constexpr int kSeedMaxN = 12288;  // longest CDS (nucleotides) with a seeded scan
-constexpr int kSeedMaxBits = 13;  // hash buckets: the power of two >= 2n, at most 2^13
+constexpr int kSeedMaxBits = 12;  // hash buckets: the power of two >= n, at most 2^12
 constexpr uint32_t kSeedEnd = 0xffffu;
 
 __host__ __device__ __forceinline__ int sl_seed_bits(int n)
 {
     int b = 6;
-    while ((1 << b) < 2 * n && b < kSeedMaxBits) b++;
+    while ((1 << b) < n && b < kSeedMaxBits) b++;
     return b;
 }
 __host__ __device__ __forceinline__ bool sl_seeded(const Shape &s) { return s.sl_method == 0 && s.n >= 8 && s.n <= kSeedMaxN; }
-// heads (16 bits each), then the nodes (4-byte aligned)
-__host__ __device__ __forceinline__ size_t sl_seed_head_bytes(int n) { return ((size_t)1 << sl_seed_bits(n)) * 2; }
+// heads (32 bits each), then the nodes
+__host__ __device__ __forceinline__ size_t sl_seed_head_bytes(int n) { return ((size_t)1 << sl_seed_bits(n)) * 4; }
 __host__ __device__ __forceinline__ size_t sl_seed_bytes(int n) { return sl_seed_head_bytes(n) + (size_t)n * 4; }
 
-// the 8 nucleotides from bit sh of (w0, w1) of both planes as a 16-bit word, twice:
+// the 7 nucleotides from bit sh of (w0, w1) of both planes as a 16-bit word, twice:
 // plane-0 bits in bytes 0 and 2, plane-1 bits in bytes 1 and 3
 __device__ __forceinline__ uint32_t seed_word(uint32_t lo0, uint32_t lo1, uint32_t hi0, uint32_t hi1, int sh)
 {
-    return __byte_perm(fshr(lo0, lo1, sh), fshr(hi0, hi1, sh), 0x4040);
+    return __byte_perm(fshr(lo0, lo1, sh), fshr(hi0, hi1, sh), 0x4040) & 0x7f7f7f7fu;
 }
 __device__ __forceinline__ uint32_t seed_hash(uint32_t w, int hb) { return (w * 0x9E3779B1u) >> (32 - hb); }
 
-// Measures the queued equal word e = a | i << 16 (rows a .. a+7 pair on delta = i - a
-// and are counted): when it starts a run, the run's counted length against
-// (best, bestd).  Adds the run words it read to work.
+// row p pairs on shift delta (p and p + delta inside [0, n))
+__device__ __forceinline__ bool seed_pairs(const uint2 *__restrict__ S, const uint32_t *__restrict__ Tlo,
+                                           const uint32_t *__restrict__ Thi, int p, int i)
+{
+    const int G = kSlGuardRows;
+    const uint32_t tl = Tlo[(i >> 5) + G] >> (i & 31), th = Thi[(i >> 5) + G] >> (i & 31);
+    const uint2 sp = S[p >> 5];
+    return ((((sp.x >> (p & 31)) ^ tl) | ((sp.y >> (p & 31)) ^ th)) & 1u) == 0u;
+}
+
+// Measures the queued equal word q = e | i << 16 (rows e .. e+6 pair on delta = i - e,
+// e+6 is counted): the run it belongs to, when this word is the one that owns it,
+// against (best, bestd).  Adds the run words it read to work.
 template <int FL>
-__device__ __forceinline__ void seed_measure(uint32_t e, const SlGeo &geo, const uint2 *__restrict__ S,
+__device__ __forceinline__ void seed_measure(uint32_t q, const SlGeo &geo, const uint2 *__restrict__ S,
                                              const uint32_t *__restrict__ Tlo, const uint32_t *__restrict__ Thi,
                                              int &work, int &best, int &bestd)
 {
     const int n = geo.n, G = kSlGuardRows;
-    const int a = (int)(e & 0xffffu), j = (int)(e >> 16), delta = j - a;
+    const int e = (int)(q & 0xffffu), j = (int)(q >> 16), delta = j - e;
     int r_lo, r_hi;
     sl_diag_rows<FL>(n, delta, r_lo, r_hi);
-    if (a > r_lo) {  // row a-1 counted: a starts a run only if it does not pair
-        const int p = a - 1, i = j - 1;
-        const uint32_t tl = Tlo[(i >> 5) + G] >> (i & 31), th = Thi[(i >> 5) + G] >> (i & 31);
-        const uint2 sp = S[p >> 5];
-        if (((((sp.x >> (p & 31)) ^ tl) | ((sp.y >> (p & 31)) ^ th)) & 1u) == 0u) return;
+    int st = e;
+    if (e - 1 >= r_lo && seed_pairs(S, Tlo, Thi, e - 1, j - 1)) {
+        if (e - 2 >= r_lo && seed_pairs(S, Tlo, Thi, e - 2, j - 2)) return;  // the even row e-2 owns the run
+        st = e - 1;
     }
-    int last = a + 7;  // last row known to pair
+    if (st + 7 > r_hi) return;  // fewer than 8 counted rows from st
+    int last = e + 6;           // last row known to pair
     while (last < r_hi) {
         work++;
         const int p = last + 1, i = p + delta;
@@ -1647,7 +1660,7 @@ __device__ __forceinline__ void seed_measure(uint32_t e, const SlGeo &geo, const
         }
         last += 32;
     }
-    const int L = min(last, r_hi) - a + 1, d = sl_key<FL>(n, delta);
+    const int L = min(last, r_hi) - st + 1, d = sl_key<FL>(n, delta);
     if (L > best || (L == best && d < bestd)) {
         best = L;
         bestd = d;
@@ -1658,35 +1671,29 @@ __device__ __forceinline__ void seed_measure(uint32_t e, const SlGeo &geo, const
 // hold a partial result that the caller discards.  q: this warp's queue, 64 words.
 template <int FL>
 __device__ bool sl_seed_scan(const SlGeo &geo, const uint2 *__restrict__ S, const uint32_t *__restrict__ Tlo,
-                             const uint32_t *__restrict__ Thi, unsigned short *heads, uint32_t *nodes, uint32_t *q,
-                             int tid, int nth, int &best, int &bestd)
+                             const uint32_t *__restrict__ Thi, uint32_t *heads, uint32_t *nodes, uint32_t *q, int tid,
+                             int nth, int &best, int &bestd)
 {
     const int n = geo.n, G = kSlGuardRows, lane = tid & 31;
-    const int hb = sl_seed_bits(n), npos = n - 7;  // word starts 0 .. n-8
-    for (int h = tid; h < (1 << hb); h += nth) heads[h] = (unsigned short)kSeedEnd;
+    const int hb = sl_seed_bits(n), npos = n - 6;  // word starts 0 .. n-7
+    for (int h = tid; h < (1 << hb); h += nth) heads[h] = kSeedEnd;
     __syncthreads();
-    bool over = false;
     for (int i = tid; i < npos; i += nth) {
         const int w = (i >> 5) + G, sh = i & 31;
         const uint32_t c = seed_word(Tlo[w], Tlo[w + 1], Thi[w], Thi[w + 1], sh);
-        // push i onto its bucket's chain (lock-free: a failed swap means another
-        // position went in first; bounded all the same, and a CTA whose swap gives up
-        // leaves the CDS to the band scan)
-        unsigned short *hp = heads + seed_hash(c, hb);
-        unsigned short old = *hp, seen;
-        int tries = 0;
-        while ((seen = atomicCAS(hp, old, (unsigned short)i)) != old && ++tries < (1 << 16)) old = seen;
-        over = over || seen != old;
+        const uint32_t old = atomicExch(&heads[seed_hash(c, hb)], (uint32_t)i);
         nodes[i] = (c & 0xffff0000u) | old;
     }
-    if (__syncthreads_or(over)) return false;
+    __syncthreads();
     // nodes and run words a thread may visit: about where the band scan, whose work per
-    // thread grows as n^2, becomes the cheaper pass (n/64 per word looked up, at least 8)
-    const int budget = max(8, n >> 6) * ((npos + nth - 1) / nth) + 64;
+    // thread grows as n^2, becomes the cheaper pass (n/32 per word looked up, at least 16)
+    const int nlook = (npos + 1) >> 1;  // even starts
+    const int budget = max(16, n >> 5) * ((nlook + nth - 1) / nth) + 64;
     const unsigned lt = (1u << lane) - 1u;
     int work = 0, qn = 0;  // qn: entries in this warp's queue (warp-uniform)
-    for (int a0 = tid - lane; a0 < npos; a0 += nth) {
-        const int a = a0 + lane;
+    bool over = false;
+    for (int k0 = tid - lane; k0 < nlook; k0 += nth) {
+        const int a = 2 * (k0 + lane);
         uint32_t c = 0, j = kSeedEnd;
         if (a < npos) {
             const int w = a >> 5, sh = a & 31;
@@ -1701,11 +1708,11 @@ __device__ bool sl_seed_scan(const SlGeo &geo, const uint2 *__restrict__ S, cons
             if (j != kSeedEnd) {
                 const uint32_t node = nodes[j];
                 j = ++work > budget ? kSeedEnd : (node & 0xffffu);  // past the bound: stop walking
-                if ((node ^ c) < 0x10000u) {  // the same word: rows a .. a+7 pair on delta
+                if ((node ^ c) < 0x10000u) {  // the same word: rows a .. a+6 pair on delta
                     const int delta = (int)jc - a;
                     int r_lo, r_hi;
                     sl_diag_rows<FL>(n, delta, r_lo, r_hi);
-                    hit = delta >= geo.dlo && delta <= geo.dhi && a + 7 <= r_hi;
+                    hit = delta >= geo.dlo && delta <= geo.dhi && a + 6 <= r_hi;
                 }
             }
             const unsigned hm = __ballot_sync(0xffffffffu, hit);
@@ -1904,7 +1911,7 @@ __device__ void sl_item(const Shape &s, PopBuf buf, int base, int2 *part, int32_
         // repetitive CDS) the band scan
         bool band = true;
         if (sl_seeded(s)) {
-            unsigned short *heads = reinterpret_cast<unsigned short *>(tab);
+            uint32_t *heads = reinterpret_cast<uint32_t *>(tab);
             uint32_t *nodes = reinterpret_cast<uint32_t *>(tab + sl_seed_head_bytes(n));
             band = !sl_seed_scan<FL>(geo, S, Tlo, Thi, heads, nodes, reinterpret_cast<uint32_t *>(sm.queue[warp]), tid,
                                      nth, best, bestd);
