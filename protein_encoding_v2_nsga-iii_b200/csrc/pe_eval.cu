@@ -1678,11 +1678,17 @@ __device__ bool sl_seed_scan(const SlGeo &geo, const uint2 *__restrict__ S, cons
     const int hb = sl_seed_bits(n), npos = n - 6;  // word starts 0 .. n-7
     for (int h = tid; h < (1 << hb); h += nth) heads[h] = kSeedEnd;
     __syncthreads();
-    for (int i = tid; i < npos; i += nth) {
-        const int w = (i >> 5) + G, sh = i & 31;
+    // two positions per thread and step, so their exchanges are in flight together
+    for (int i = tid; i < npos; i += 2 * nth) {
+        const int i2 = i + nth;
+        const bool two = i2 < npos;
+        const int w = (i >> 5) + G, sh = i & 31, w2 = (i2 >> 5) + G, sh2 = i2 & 31;
         const uint32_t c = seed_word(Tlo[w], Tlo[w + 1], Thi[w], Thi[w + 1], sh);
+        const uint32_t c2 = two ? seed_word(Tlo[w2], Tlo[w2 + 1], Thi[w2], Thi[w2 + 1], sh2) : 0u;
         const uint32_t old = atomicExch(&heads[seed_hash(c, hb)], (uint32_t)i);
+        const uint32_t old2 = two ? atomicExch(&heads[seed_hash(c2, hb)], (uint32_t)i2) : 0u;
         nodes[i] = (c & 0xffff0000u) | old;
+        if (two) nodes[i2] = (c2 & 0xffff0000u) | old2;
     }
     __syncthreads();
     // nodes and run words a thread may visit: about where the band scan, whose work per
@@ -1692,42 +1698,53 @@ __device__ bool sl_seed_scan(const SlGeo &geo, const uint2 *__restrict__ S, cons
     const unsigned lt = (1u << lane) - 1u;
     int work = 0, qn = 0;  // qn: entries in this warp's queue (warp-uniform)
     bool over = false;
-    for (int k0 = tid - lane; k0 < nlook; k0 += nth) {
-        const int a = 2 * (k0 + lane);
-        uint32_t c = 0, j = kSeedEnd;
+    // an equal word (rows a .. a+6 pair on shift jc - a) joins the warp's queue when its
+    // shift is scanned and row a+6 is counted; 32 queued words are measured at once
+    auto push = [&](uint32_t node, uint32_t c, uint32_t jc, int a) {
+        bool hit = false;
+        if (jc != kSeedEnd && (node ^ c) < 0x10000u) {
+            const int delta = (int)jc - a;
+            int r_lo, r_hi;
+            sl_diag_rows<FL>(n, delta, r_lo, r_hi);
+            hit = delta >= geo.dlo && delta <= geo.dhi && a + 6 <= r_hi;
+        }
+        const unsigned hm = __ballot_sync(0xffffffffu, hit);
+        if (hm) {
+            if (hit) q[qn + __popc(hm & lt)] = (uint32_t)a | (jc << 16);
+            qn += __popc(hm);
+            __syncwarp();
+            if (qn >= 32) {
+                seed_measure<FL>(q[lane], geo, S, Tlo, Thi, work, best, bestd);
+                __syncwarp();
+                if (lane < qn - 32) q[lane] = q[32 + lane];
+                qn -= 32;
+                __syncwarp();
+            }
+        }
+    };
+    // two words per lane and step (even rows a and a + 2*nth), their chains walked together
+    for (int k0 = tid - lane; k0 < nlook; k0 += 2 * nth) {
+        const int a = 2 * (k0 + lane), a2 = a + 2 * nth;
+        uint32_t c = 0, j = kSeedEnd, c2 = 0, j2 = kSeedEnd;
         if (a < npos) {
             const int w = a >> 5, sh = a & 31;
             const uint2 s0 = S[w], s1 = S[w + 1];
             c = seed_word(s0.x, s1.x, s0.y, s1.y, sh);
             j = heads[seed_hash(c, hb)];
         }
-        // the lanes walk their chains in step; equal words join the queue
-        while (__any_sync(0xffffffffu, j != kSeedEnd)) {
-            bool hit = false;
-            const uint32_t jc = j;
-            if (j != kSeedEnd) {
-                const uint32_t node = nodes[j];
-                j = ++work > budget ? kSeedEnd : (node & 0xffffu);  // past the bound: stop walking
-                if ((node ^ c) < 0x10000u) {  // the same word: rows a .. a+6 pair on delta
-                    const int delta = (int)jc - a;
-                    int r_lo, r_hi;
-                    sl_diag_rows<FL>(n, delta, r_lo, r_hi);
-                    hit = delta >= geo.dlo && delta <= geo.dhi && a + 6 <= r_hi;
-                }
-            }
-            const unsigned hm = __ballot_sync(0xffffffffu, hit);
-            if (hm) {
-                if (hit) q[qn + __popc(hm & lt)] = (uint32_t)a | (jc << 16);
-                qn += __popc(hm);
-                __syncwarp();
-                if (qn >= 32) {
-                    seed_measure<FL>(q[lane], geo, S, Tlo, Thi, work, best, bestd);
-                    __syncwarp();
-                    if (lane < qn - 32) q[lane] = q[32 + lane];
-                    qn -= 32;
-                    __syncwarp();
-                }
-            }
+        if (a2 < npos) {
+            const int w = a2 >> 5, sh = a2 & 31;
+            const uint2 s0 = S[w], s1 = S[w + 1];
+            c2 = seed_word(s0.x, s1.x, s0.y, s1.y, sh);
+            j2 = heads[seed_hash(c2, hb)];
+        }
+        while (__any_sync(0xffffffffu, j != kSeedEnd || j2 != kSeedEnd)) {
+            const uint32_t jc = j, jc2 = j2;
+            const uint32_t node = jc != kSeedEnd ? nodes[jc] : 0u, node2 = jc2 != kSeedEnd ? nodes[jc2] : 0u;
+            if (jc != kSeedEnd) j = ++work > budget ? kSeedEnd : (node & 0xffffu);  // past the bound: stop
+            if (jc2 != kSeedEnd) j2 = ++work > budget ? kSeedEnd : (node2 & 0xffffu);
+            push(node, c, jc, a);
+            push(node2, c2, jc2, a2);
         }
         over = over || work > budget;
         if (__any_sync(0xffffffffu, over)) break;
