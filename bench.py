@@ -70,23 +70,25 @@ def set_workload(shape: str | None, six: bool, lrcs: bool = False):
 METRIC = "generations/s"
 L2_FLUSH_BYTES = 256 << 20
 # The string-objective kernel (k_sl) per flavour, from one ncu capture of one launch each
-# (the committed k_sl profile summaries give the commands and these same numbers): ALU-pipe
-# warp instructions, shared-memory data-pipe wavefronts, thread instructions and DRAM bytes
-# of the launch, the counted cells it covered, and the percentages ncu reported.  The
-# roofline scales the counts by the cells a timed generation scanned.  `source` is the
-# sha256 prefix of the kernel's source section (pe_eval.cu from the k_sl banner on) at the
-# capture; a host test fails when the source changes without a new capture.
+# (the committed k_sl profile summaries give the commands and these same numbers): warp
+# instructions issued, ALU-pipe warp instructions, shared-memory data-pipe wavefronts,
+# thread instructions and DRAM bytes of the launch, the scans (CDSs, LRCS CDS pairs) it ran
+# and their counted cells, and the percentages ncu reported.  The seeded first pass does
+# work linear in the CDS length per scan, so the roofline scales the counts by the scans a
+# timed generation ran.  `source` is the sha256 prefix of the kernel's source section
+# (pe_eval.cu from the k_sl banner on) at the capture; a host test fails when the source
+# changes without a new capture.
 SL_NCU = {
     "hairpin": {"workload": "L=1000 m=8 N=1024, generation 1 (2311 CDSs scanned)",
-                "cells": 10389102811, "smem_wavefronts": 27777210, "alu_warp_inst": 46313626,
-                "thread_inst": 2487732762, "dram_bytes": 2481920, "smem_pct": 73.05, "alu_pct": 68.92,
-                "source": "d65b815633479dcb"},
+                "scans": 2311, "cells": 10389102811, "warp_inst": 38644132, "alu_warp_inst": 16336904,
+                "smem_wavefronts": 4544143, "thread_inst": 1110401631, "dram_bytes": 2492672,
+                "issue_pct": 58.47, "alu_pct": 48.82, "smem_pct": 23.53, "source": "6a58280fc2787798"},
     "lrcs": {"workload": "L=3000 m=4 N=4096, generation 1 (18320 CDS pairs scanned)",
-             "cells": 1250515745682, "smem_wavefronts": 2679486081, "alu_warp_inst": 5439675210,
-             "thread_inst": 252279307777, "dram_bytes": 34455552, "smem_pct": 72.65, "alu_pct": 74.60,
-             "source": "d65b815633479dcb"},
+             "scans": 18320, "cells": 1250515745682, "warp_inst": 1619890383, "alu_warp_inst": 737375756,
+             "smem_wavefronts": 180629560, "thread_inst": 44756907945, "dram_bytes": 34465792,
+             "issue_pct": 45.97, "alu_pct": 41.75, "smem_pct": 20.23, "source": "6a58280fc2787798"},
 }
-SM_COUNT, SMEM_WAVEFRONTS_PER_SM_CLK, ALU_WARP_INST_PER_SM_CLK = 148, 1, 2
+SM_COUNT, ISSUE_WARP_INST_PER_SM_CLK, SMEM_WAVEFRONTS_PER_SM_CLK, ALU_WARP_INST_PER_SM_CLK = 148, 4, 1, 2
 # kernels one generation launches (one CUDA graph replay): k_variation, k_sl, k_dominance,
 # k_fronts, k_select, k_assoc, k_niche
 KERNELS_PER_GENERATION = 7
@@ -107,41 +109,46 @@ def hairpin_cells_per_cds(n: int) -> int:
     return k * (k + 1) // 2 if k > 0 else 0
 
 
-def roofline(cells: float, sl_seconds: float, clocks: dict, kind: str = "hairpin") -> dict:
-    """Roofline of the string-objective scan (integer bit work on shared-memory tables) on
-    its two busiest units: the ALU pipe (achieved = ALU warp instructions per launch, ncu,
-    scaled to the cells scanned, / the launch time measured here; peak = 2 per SM per clock
-    x 148 SMs x the SM clock sampled during the timed region) and the shared-memory data
-    pipe (wavefronts per launch against 1 per SM per clock).  The headline figures are those
-    of the unit with the larger fraction; the other is reported beside them."""
+def roofline(scans: float, cells: float, sl_seconds: float, clocks: dict, kind: str = "hairpin") -> dict:
+    """Roofline of the string-objective scan (integer work on shared-memory tables: a
+    hash-table join of 7-nucleotide words, then the runs it finds measured on bit planes)
+    on its three candidate bounds: instruction issue (4 warp instructions per SM per clock),
+    the ALU pipe (2 per SM per clock) and the shared-memory data pipe (1 wavefront per SM per
+    clock), each x 148 SMs x the SM clock sampled during the timed region.  Achieved = the
+    launch's count (ncu, scaled to the scans run) / the launch time measured here.  The
+    headline figures are those of the unit with the largest fraction; the others are
+    reported beside them."""
     c = SL_NCU[kind]
-    scale = cells / c["cells"]
-    mhz = clocks.get("sm_mhz") or 1965.0
-    smem = c["smem_wavefronts"] * scale / sl_seconds / 1e9
-    smem_peak = SM_COUNT * SMEM_WAVEFRONTS_PER_SM_CLK * mhz * 1e6 / 1e9
-    alu = c["alu_warp_inst"] * scale / sl_seconds / 1e9
-    alu_peak = SM_COUNT * ALU_WARP_INST_PER_SM_CLK * mhz * 1e6 / 1e9
-    units = {
-        "alu": {"achieved": alu, "peak": alu_peak, "frac": alu / alu_peak, "unit": "G ALU warp-inst/s",
-                "peak_source": "ALU pipe 2 warp-inst/SM/clk (ncu peak_sustained) x 148 SMs at the sampled SM clock"},
-        "smem": {"achieved": smem, "peak": smem_peak, "frac": smem / smem_peak, "unit": "G wavefronts/s",
-                 "peak_source": "shared-memory data pipe 1 wavefront/SM/clk (ncu peak_sustained) x 148 SMs at the "
-                                "sampled SM clock"},
-    }
+    scale = scans / c["scans"]
+    hz = (clocks.get("sm_mhz") or 1965.0) * 1e6
+    src = "(ncu peak_sustained) x 148 SMs at the sampled SM clock"
+    units = {}
+    for name, count, per_clk, unit, what in (
+            ("issue", "warp_inst", ISSUE_WARP_INST_PER_SM_CLK, "G warp-inst/s", "instruction issue 4 warp-inst/SM/clk"),
+            ("alu", "alu_warp_inst", ALU_WARP_INST_PER_SM_CLK, "G ALU warp-inst/s", "ALU pipe 2 warp-inst/SM/clk"),
+            ("smem", "smem_wavefronts", SMEM_WAVEFRONTS_PER_SM_CLK, "G wavefronts/s",
+             "shared-memory data pipe 1 wavefront/SM/clk")):
+        achieved = c[count] * scale / sl_seconds / 1e9
+        peak = SM_COUNT * per_clk * hz / 1e9
+        units[name] = {"achieved": achieved, "peak": peak, "frac": achieved / peak, "unit": unit,
+                       "peak_source": f"{what} {src}"}
     bound = max(units, key=lambda k: units[k]["frac"])
-    other = "smem" if bound == "alu" else "alu"
     head = units[bound]
     name = "k_sl (hairpin-stem scan)" if kind == "hairpin" else "k_sl (longest repeated/common substring scan)"
-    return {"bound": bound, "kernel": name, "unit": head["unit"], "achieved": head["achieved"],
-            "peak": head["peak"], "frac": head["frac"], "traffic": c["dram_bytes"] * scale,
-            "peak_source": head["peak_source"] + "; MEASURED_PEAKS.json has no integer or shared-memory peak",
-            other: {k: v for k, v in units[other].items() if k != "peak_source"},
-            "algorithmic_bytes_per_launch": c["dram_bytes"] * scale,
-            "cells_per_launch": cells, "cells_per_s": cells / sl_seconds,
-            "counted_cells": "cells of the scans run (unchanged CDSs keep their parents' results)",
-            "lane_ops_per_cell": c["thread_inst"] / c["cells"],
-            "ncu_pct_of_peak": {"smem_wavefronts": c["smem_pct"], "alu_pipe": c["alu_pct"]},
-            "instruction_count": f"ncu, {c['workload']}; scaled by cells"}
+    out = {"bound": bound, "kernel": name, "unit": head["unit"], "achieved": head["achieved"],
+           "peak": head["peak"], "frac": head["frac"], "traffic": c["dram_bytes"] * scale,
+           "peak_source": head["peak_source"] + "; MEASURED_PEAKS.json has no integer or issue peak"}
+    for k, v in units.items():
+        if k != bound:
+            out[k] = {kk: vv for kk, vv in v.items() if kk != "peak_source"}
+    out.update({"algorithmic_bytes_per_launch": c["dram_bytes"] * scale,
+                "scans_per_launch": scans, "cells_per_launch": cells, "cells_per_s": cells / sl_seconds,
+                "counted_cells": "cells of the scans run (unchanged CDSs keep their parents' results)",
+                "warp_inst_per_scan": c["warp_inst"] / c["scans"],
+                "lane_ops_per_cell": c["thread_inst"] / c["cells"],
+                "ncu_pct_of_peak": {"issue": c["issue_pct"], "alu_pipe": c["alu_pct"], "smem_wavefronts": c["smem_pct"]},
+                "instruction_count": f"ncu, {c['workload']}; scaled by scans"})
+    return out
 
 
 class ClockSampler:
@@ -366,6 +373,7 @@ def run_ours(args, world, rank, local):
     # a child's CDS (LRCS: CDS pair) that its mutation left unchanged keeps its parent's
     # result: the string-objective work is the cells of the scans actually run
     cells = (eng.scan_cells() - cells0) / args.steps
+    scans = (eng.scan_count() - scans0) / args.steps
     sl_s = stage_ms[1] / 1000.0
 
     # end-to-end through the public API with host buffers: every rank runs whole design jobs
@@ -422,7 +430,7 @@ def run_ours(args, world, rank, local):
             "designs_per_s": value / G_JOB,
             "stage_ms": {"variation_eval": stage_ms[0], "hairpin_scan": stage_ms[1], "selection": stage_ms[2]},
             "stage_ms_windows": windows,
-            "roofline": roofline(cells, sl_s, clocks, "lrcs" if SL_KIND else "hairpin"),
+            "roofline": roofline(scans, cells, sl_s, clocks, "lrcs" if SL_KIND else "hairpin"),
             "clocks": clocks,
             "e2e": {"value": world * G_E2E / e2e_s, "unit": "generations/s", "h2d_bytes_per_step": world * h2d / G_E2E,
                     "d2h_bytes_per_step": world * d2h,

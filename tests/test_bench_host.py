@@ -23,25 +23,25 @@ def load_bench():
 
 
 @pytest.mark.parametrize("kind", ["hairpin", "lrcs"])
-def test_roofline_reports_the_busier_unit_and_scales_by_scanned_cells(kind):
+def test_roofline_reports_the_busiest_unit_and_scales_by_scans(kind):
     b = load_bench()
     c = b.SL_NCU[kind]
     clocks = {"sm_mhz": 1965.0}
     t = 1.0e-4
-    full = b.roofline(c["cells"], t, clocks, kind)
-    half = b.roofline(c["cells"] / 2, t / 2, clocks, kind)
-    # achieved rates are counts per launch, scaled by the counted cells, over the launch time
-    smem = c["smem_wavefronts"] / t / 1e9
-    alu = c["alu_warp_inst"] / t / 1e9
-    smem_peak = b.SM_COUNT * b.SMEM_WAVEFRONTS_PER_SM_CLK * 1965.0e6 / 1e9
-    alu_peak = b.SM_COUNT * b.ALU_WARP_INST_PER_SM_CLK * 1965.0e6 / 1e9
-    fr = {"smem": smem / smem_peak, "alu": alu / alu_peak}
+    full = b.roofline(c["scans"], c["cells"], t, clocks, kind)
+    half = b.roofline(c["scans"] / 2, c["cells"] / 2, t / 2, clocks, kind)
+    # achieved rates are counts per launch, scaled by the scans run, over the launch time
+    hz = 1965.0e6
+    fr = {"issue": c["warp_inst"] / t / (b.SM_COUNT * b.ISSUE_WARP_INST_PER_SM_CLK * hz),
+          "alu": c["alu_warp_inst"] / t / (b.SM_COUNT * b.ALU_WARP_INST_PER_SM_CLK * hz),
+          "smem": c["smem_wavefronts"] / t / (b.SM_COUNT * b.SMEM_WAVEFRONTS_PER_SM_CLK * hz)}
     bound = max(fr, key=fr.get)
     assert full["bound"] == bound
     assert math.isclose(full["frac"], fr[bound], rel_tol=1e-9)
-    other = "alu" if bound == "smem" else "smem"
-    assert math.isclose(full[other]["frac"], fr[other], rel_tol=1e-9)
-    # half the cells in half the time: the same rates
+    for other in fr:
+        if other != bound:
+            assert math.isclose(full[other]["frac"], fr[other], rel_tol=1e-9)
+    # half the scans in half the time: the same rates
     assert math.isclose(half["frac"], full["frac"], rel_tol=1e-6)
     assert math.isclose(full["cells_per_s"], c["cells"] / t, rel_tol=1e-12)
     assert math.isclose(full["traffic"], c["dram_bytes"], rel_tol=1e-12)
