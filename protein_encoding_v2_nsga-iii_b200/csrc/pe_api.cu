@@ -1025,13 +1025,18 @@ int pe_init_population(pe_instance *in)
         const SlTuneKey key{in->device, s.L, s.m, s.N, s.sl_kind, s.sl_method};
         s.sl_threads = sl_tuned(key);
         if (s.sl_threads == 0) {
-            // pick the hairpin-scan CTA size: after one warm scan of the initial population,
-            // time one scan with each size (they all give the same result) and keep the
-            // fastest; the choice is remembered for this shape on this device
-            cudaEvent_t ev[4] = {};
+            // pick the string-scan CTA size: after one warm scan of the initial population,
+            // time two scans with each size, in the orders 64, 128, 256 and 256, 128, 64
+            // (they all give the same result), and keep the size with the fastest one;
+            // the choice is remembered for this shape on this device.  The timed scans
+            // cover a third of the population, about the share of CDSs a generation's
+            // mutations change: the best size for few items per SM differs from the
+            // best for a full scan (a fuller grid favours smaller CTAs)
+            constexpr int kRuns = 6;
+            cudaEvent_t ev[kRuns + 1] = {};
             cudaError_t e = cudaSuccess;
-            for (int k = 0; k < 4 && e == cudaSuccess; k++) e = cudaEventCreate(&ev[k]);
-            const int sizes[3] = {64, 128, 256};
+            for (int k = 0; k <= kRuns && e == cudaSuccess; k++) e = cudaEventCreate(&ev[k]);
+            const int sizes[kRuns] = {64, 128, 256, 256, 128, 64};
             s.sl_threads = 128;
             // the warm scan stores the per-CDS results; the timed ones scan every CDS
             // (no carried results) and rewrite the same objectives
@@ -1040,16 +1045,18 @@ int pe_init_population(pe_instance *in)
             if (e == cudaSuccess)
                 e = launch_sl(s, in->buf[0], 0, s.N, in->d_part, in->d_counter, in->d_status, in->stream,
                               in->d_scanned);
-            for (int k = 0; k < 3 && e == cudaSuccess; k++) {
+            for (int k = 0; k < kRuns && e == cudaSuccess; k++) {
                 s.sl_threads = sizes[k];
                 e = cudaEventRecord(ev[k], in->stream);
-                if (e == cudaSuccess) e = launch_sl(s, full, 0, s.N, in->d_part, in->d_counter, in->d_status, in->stream);
+                if (e == cudaSuccess)
+                    e = launch_sl(s, full, 0, std::max(1, s.N / 3), in->d_part, in->d_counter, in->d_status,
+                                  in->stream);
             }
-            if (e == cudaSuccess) e = cudaEventRecord(ev[3], in->stream);
-            if (e == cudaSuccess) e = cudaEventSynchronize(ev[3]);
+            if (e == cudaSuccess) e = cudaEventRecord(ev[kRuns], in->stream);
+            if (e == cudaSuccess) e = cudaEventSynchronize(ev[kRuns]);
             float best_ms = 0.0f;
             int best = 128;
-            for (int k = 0; k < 3 && e == cudaSuccess; k++) {
+            for (int k = 0; k < kRuns && e == cudaSuccess; k++) {
                 float ms = 0.0f;
                 e = cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
                 if (e == cudaSuccess && (k == 0 || ms < best_ms)) {
@@ -1057,7 +1064,7 @@ int pe_init_population(pe_instance *in)
                     best = sizes[k];
                 }
             }
-            for (int k = 0; k < 4; k++)
+            for (int k = 0; k <= kRuns; k++)
                 if (ev[k]) cudaEventDestroy(ev[k]);
             s.sl_threads = best;
             if (e != cudaSuccess) return fail(PE_ERR_CUDA, "hairpin-scan tuning: %s", cudaGetErrorString(e));
