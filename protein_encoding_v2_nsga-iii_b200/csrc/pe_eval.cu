@@ -1572,51 +1572,75 @@ __device__ void sl_band_scan(const uint4 *__restrict__ E4, const int *__restrict
 // Seeded scan: the first pass for CDSs short enough for a table of their words.
 //
 // A cell (r, delta) pairs exactly when S's nucleotide r equals T's r + delta (T is
-// the reverse complement for the hairpin, the other CDS for LRCS).  A counted run
-// of >= 8 pairing rows st .. st+L-1 on shift delta holds, at its even row e = st or
-// st+1, seven rows e .. e+6 that pair: S's 7-nucleotide word at e equals T's at
-// e + delta.  So T's n-6 words (every position) go into a chained hash table
-// (32-bit bucket heads; one node per position i: the word in the high 16 bits, the
-// next position of the chain in the low 16), and S's words at even positions walk
-// their chains.  An equal word (e, i) whose shift is scanned and whose rows up to
-// e+6 are counted joins its warp's queue; the warp measures queued words 32 at a
-// time, one per lane.  The run's start is e when row e-1 is not counted or does
-// not pair, e-1 when row e-1 pairs and row e-2 does not (or is not counted); when
-// both pair, the run is the one found from the even row e-2 and this word is
-// dropped.  The run is followed 32 rows at a time to its end and clipped to the
-// diagonal's counted range, as the band scan measures its marked runs.  Every
-// counted run of >= 8 is measured exactly once, so (longest, smallest key) is the
-// band scan's when the longest reaches 8 (shorter ones may be measured too; a
-// result below 8 sends the CDS to the exact word scan).  The lanes of a warp walk
-// their chains in step and meet in the queue, so neither the uneven chain
-// lengths nor the rare equal words split the warp for long.
+// the reverse complement for the hairpin, the other CDS for LRCS).  With words of K
+// nucleotides looked up at rows that are multiples of t = 9 - K, a counted run of
+// >= 8 pairing rows st .. st+L-1 on shift delta holds, at its row e in
+// [st, st + t - 1] with e a multiple of t, K pairing rows e .. e+K-1: S's K-word at
+// e equals T's at e + delta.  T's n-K+1 words (every position) go into a chained
+// table and S's words at rows that are multiples of t walk their chains.  An equal
+// word whose shift is scanned and whose row e+K-1 is counted joins its warp's
+// queue; the warp measures queued words 32 at a time, one per lane.  The run's
+// start is found by walking back at most t-1 rows (the first row that does not
+// pair or is not counted ends the walk); when rows e-1 .. e-t all pair, the run is
+// the one found from row e-t and this word is dropped.  The run is followed 32 rows
+// at a time to its end and clipped to the diagonal's counted range, as the band
+// scan measures its marked runs.  Every counted run of >= 8 is measured exactly
+// once, so (longest, smallest key) is the band scan's when the longest reaches 8
+// (shorter ones may be measured too; a result below 8 sends the CDS to the exact
+// word scan).  Each lane walks two chains at once, and the lanes of a warp walk in
+// step and meet in the queue, so neither the uneven chain lengths nor the dependent
+// loads of a chain split the warp for long.
 //
-// For random-like CDSs the chains hold about one node and the work is linear in
+// The hairpin uses K = 6, t = 3: a 6-word has 4096 values and indexes the table's
+// heads directly (no hash, no word compare, every node an equal word; 16-bit nodes
+// holding the next position).  LRCS compares CDSs that encode the same protein and
+// share many short words, so it uses K = 7, t = 2 with fewer equal words: hashed
+// 32-bit heads (the power of two >= n, at most 4096) and 32-bit nodes holding the
+// word (high half) and the next position (low half).
+//
+// For random-like CDSs the chains hold about n/4096 nodes and the work is linear in
 // n instead of the n^2/2 cells.  A repetitive CDS makes long chains (many equal
 // words): each thread bounds the nodes and run words it visits, and when any
 // thread passes its bound the CTA drops the partial result and the band scan runs.
 constexpr int kSeedMaxN = 12288;  // longest CDS (nucleotides) with a seeded scan
-constexpr int kSeedMaxBits = 12;  // hash buckets: the power of two >= n, at most 2^12
 constexpr uint32_t kSeedEnd = 0xffffu;
+template <int FL> struct Seed {
+    static constexpr int K = FL == 0 ? 6 : 7;  // word length
+    static constexpr int step = 9 - K;         // rows between looked-up words
+    static constexpr bool direct = FL == 0;    // the word indexes the heads
+};
 
-__host__ __device__ __forceinline__ int sl_seed_bits(int n)
+__host__ __device__ __forceinline__ int sl_seed_bits(int n, bool direct)
 {
+    if (direct) return 12;
     int b = 6;
-    while ((1 << b) < n && b < kSeedMaxBits) b++;
+    while ((1 << b) < n && b < 12) b++;
     return b;
 }
 __host__ __device__ __forceinline__ bool sl_seeded(const Shape &s) { return s.sl_method == 0 && s.n >= 8 && s.n <= kSeedMaxN; }
-// heads (32 bits each), then the nodes
-__host__ __device__ __forceinline__ size_t sl_seed_head_bytes(int n) { return ((size_t)1 << sl_seed_bits(n)) * 4; }
-__host__ __device__ __forceinline__ size_t sl_seed_bytes(int n) { return sl_seed_head_bytes(n) + (size_t)n * 4; }
+// 32-bit heads, then the nodes (16-bit next positions, or 32-bit word and next)
+__host__ __device__ __forceinline__ size_t sl_seed_head_bytes(int n, bool direct)
+{
+    return ((size_t)1 << sl_seed_bits(n, direct)) * 4;
+}
+__host__ __device__ __forceinline__ size_t sl_seed_bytes(int n, bool direct)
+{
+    return sl_seed_head_bytes(n, direct) + (((size_t)n * (direct ? 2 : 4) + 15) & ~size_t(15));
+}
 
-// the 7 nucleotides from bit sh of (w0, w1) of both planes as a 16-bit word, twice:
-// plane-0 bits in bytes 0 and 2, plane-1 bits in bytes 1 and 3
+// The K-nucleotide word from bit sh of (w0, w1) of both planes: for the direct table
+// its 12-bit index (plane-0 bits low); else the 7-bit plane bytes twice (plane 0 in
+// bytes 0 and 2, plane 1 in bytes 1 and 3), which the hash and the node compare use.
+template <int FL>
 __device__ __forceinline__ uint32_t seed_word(uint32_t lo0, uint32_t lo1, uint32_t hi0, uint32_t hi1, int sh)
 {
+    if (Seed<FL>::direct) return (fshr(lo0, lo1, sh) & 63u) | ((fshr(hi0, hi1, sh) & 63u) << 6);
     return __byte_perm(fshr(lo0, lo1, sh), fshr(hi0, hi1, sh), 0x4040) & 0x7f7f7f7fu;
 }
-__device__ __forceinline__ uint32_t seed_hash(uint32_t w, int hb) { return (w * 0x9E3779B1u) >> (32 - hb); }
+template <int FL> __device__ __forceinline__ uint32_t seed_bucket(uint32_t w, int hb)
+{
+    return Seed<FL>::direct ? w : (w * 0x9E3779B1u) >> (32 - hb);
+}
 
 // row p pairs on shift delta (p and p + delta inside [0, n))
 __device__ __forceinline__ bool seed_pairs(const uint2 *__restrict__ S, const uint32_t *__restrict__ Tlo,
@@ -1628,25 +1652,24 @@ __device__ __forceinline__ bool seed_pairs(const uint2 *__restrict__ S, const ui
     return ((((sp.x >> (p & 31)) ^ tl) | ((sp.y >> (p & 31)) ^ th)) & 1u) == 0u;
 }
 
-// Measures the queued equal word q = e | i << 16 (rows e .. e+6 pair on delta = i - e,
-// e+6 is counted): the run it belongs to, when this word is the one that owns it,
+// Measures the queued equal word q = e | i << 16 (rows e .. e+K-1 pair on delta = i - e,
+// e+K-1 is counted): the run it belongs to, when this word is the one that owns it,
 // against (best, bestd).  Adds the run words it read to work.
 template <int FL>
 __device__ __forceinline__ void seed_measure(uint32_t q, const SlGeo &geo, const uint2 *__restrict__ S,
                                              const uint32_t *__restrict__ Tlo, const uint32_t *__restrict__ Thi,
                                              int &work, int &best, int &bestd)
 {
+    constexpr int t = Seed<FL>::step;
     const int n = geo.n, G = kSlGuardRows;
     const int e = (int)(q & 0xffffu), j = (int)(q >> 16), delta = j - e;
     int r_lo, r_hi;
     sl_diag_rows<FL>(n, delta, r_lo, r_hi);
     int st = e;
-    if (e - 1 >= r_lo && seed_pairs(S, Tlo, Thi, e - 1, j - 1)) {
-        if (e - 2 >= r_lo && seed_pairs(S, Tlo, Thi, e - 2, j - 2)) return;  // the even row e-2 owns the run
-        st = e - 1;
-    }
+    while (st > e - t && st - 1 >= r_lo && seed_pairs(S, Tlo, Thi, st - 1, st - 1 + delta)) st--;
+    if (st == e - t) return;    // rows e-t .. e pair: the word at e-t owns the run
     if (st + 7 > r_hi) return;  // fewer than 8 counted rows from st
-    int last = e + 6;           // last row known to pair
+    int last = e + Seed<FL>::K - 1;  // last row known to pair
     while (last < r_hi) {
         work++;
         const int p = last + 1, i = p + delta;
@@ -1668,45 +1691,57 @@ __device__ __forceinline__ void seed_measure(uint32_t q, const SlGeo &geo, const
 }
 
 // Returns false (CTA-uniform) when some thread passed its bound; (best, bestd) then
-// hold a partial result that the caller discards.  q: this warp's queue, 64 words.
+// hold a partial result that the caller discards.  table: the heads, then the nodes;
+// q: this warp's queue, 64 words.
 template <int FL>
 __device__ bool sl_seed_scan(const SlGeo &geo, const uint2 *__restrict__ S, const uint32_t *__restrict__ Tlo,
-                             const uint32_t *__restrict__ Thi, uint32_t *heads, uint32_t *nodes, uint32_t *q, int tid,
-                             int nth, int &best, int &bestd)
+                             const uint32_t *__restrict__ Thi, unsigned char *table, uint32_t *q, int tid, int nth,
+                             int &best, int &bestd)
 {
+    constexpr int K = Seed<FL>::K, t = Seed<FL>::step;
+    constexpr bool direct = Seed<FL>::direct;
     const int n = geo.n, G = kSlGuardRows, lane = tid & 31;
-    const int hb = sl_seed_bits(n), npos = n - 6;  // word starts 0 .. n-7
-    for (int h = tid; h < (1 << hb); h += nth) heads[h] = kSeedEnd;
+    const int hb = sl_seed_bits(n, direct), npos = n - K + 1;  // word starts 0 .. n-K
+    uint32_t *heads = reinterpret_cast<uint32_t *>(table);
+    unsigned short *next16 = reinterpret_cast<unsigned short *>(table + sl_seed_head_bytes(n, direct));
+    uint32_t *node32 = reinterpret_cast<uint32_t *>(table + sl_seed_head_bytes(n, direct));
+    uint4 *h4 = reinterpret_cast<uint4 *>(heads);
+    for (int h = tid; h < (1 << hb) / 4; h += nth) h4[h] = make_uint4(kSeedEnd, kSeedEnd, kSeedEnd, kSeedEnd);
     __syncthreads();
     // two positions per thread and step, so their exchanges are in flight together
     for (int i = tid; i < npos; i += 2 * nth) {
         const int i2 = i + nth;
         const bool two = i2 < npos;
         const int w = (i >> 5) + G, sh = i & 31, w2 = (i2 >> 5) + G, sh2 = i2 & 31;
-        const uint32_t c = seed_word(Tlo[w], Tlo[w + 1], Thi[w], Thi[w + 1], sh);
-        const uint32_t c2 = two ? seed_word(Tlo[w2], Tlo[w2 + 1], Thi[w2], Thi[w2 + 1], sh2) : 0u;
-        const uint32_t old = atomicExch(&heads[seed_hash(c, hb)], (uint32_t)i);
-        const uint32_t old2 = two ? atomicExch(&heads[seed_hash(c2, hb)], (uint32_t)i2) : 0u;
-        nodes[i] = (c & 0xffff0000u) | old;
-        if (two) nodes[i2] = (c2 & 0xffff0000u) | old2;
+        const uint32_t c = seed_word<FL>(Tlo[w], Tlo[w + 1], Thi[w], Thi[w + 1], sh);
+        const uint32_t c2 = two ? seed_word<FL>(Tlo[w2], Tlo[w2 + 1], Thi[w2], Thi[w2 + 1], sh2) : 0u;
+        const uint32_t old = atomicExch(&heads[seed_bucket<FL>(c, hb)], (uint32_t)i);
+        const uint32_t old2 = two ? atomicExch(&heads[seed_bucket<FL>(c2, hb)], (uint32_t)i2) : 0u;
+        if (direct) {
+            next16[i] = (unsigned short)old;
+            if (two) next16[i2] = (unsigned short)old2;
+        } else {
+            node32[i] = (c & 0xffff0000u) | old;
+            if (two) node32[i2] = (c2 & 0xffff0000u) | old2;
+        }
     }
     __syncthreads();
     // nodes and run words a thread may visit: about where the band scan, whose work per
     // thread grows as n^2, becomes the cheaper pass (n/32 per word looked up, at least 16)
-    const int nlook = (npos + 1) >> 1;  // even starts
+    const int nlook = (npos + t - 1) / t;  // starts that are multiples of t
     const int budget = max(16, n >> 5) * ((nlook + nth - 1) / nth) + 64;
     const unsigned lt = (1u << lane) - 1u;
     int work = 0, qn = 0;  // qn: entries in this warp's queue (warp-uniform)
     bool over = false;
-    // an equal word (rows a .. a+6 pair on shift jc - a) joins the warp's queue when its
-    // shift is scanned and row a+6 is counted; 32 queued words are measured at once
-    auto push = [&](uint32_t node, uint32_t c, uint32_t jc, int a) {
+    // an equal word (rows a .. a+K-1 pair on shift jc - a) joins the warp's queue when
+    // its shift is scanned and row a+K-1 is counted; 32 queued words are measured at once
+    auto push = [&](bool equal, uint32_t jc, int a) {
         bool hit = false;
-        if (jc != kSeedEnd && (node ^ c) < 0x10000u) {
+        if (equal) {
             const int delta = (int)jc - a;
             int r_lo, r_hi;
             sl_diag_rows<FL>(n, delta, r_lo, r_hi);
-            hit = delta >= geo.dlo && delta <= geo.dhi && a + 6 <= r_hi;
+            hit = delta >= geo.dlo && delta <= geo.dhi && a + K - 1 <= r_hi;
         }
         const unsigned hm = __ballot_sync(0xffffffffu, hit);
         if (hm) {
@@ -1722,29 +1757,45 @@ __device__ bool sl_seed_scan(const SlGeo &geo, const uint2 *__restrict__ S, cons
             }
         }
     };
-    // two words per lane and step (even rows a and a + 2*nth), their chains walked together
+    // one chain step: the node at jc (kSeedEnd: none); returns the next position and
+    // whether jc holds the word c
+    auto step = [&](uint32_t jc, uint32_t c, bool &equal) -> uint32_t {
+        equal = false;
+        if (jc == kSeedEnd) return kSeedEnd;
+        uint32_t nx;
+        if (direct) {
+            nx = next16[jc];
+            equal = true;
+        } else {
+            const uint32_t node = node32[jc];
+            nx = node & 0xffffu;
+            equal = (node ^ c) < 0x10000u;
+        }
+        return ++work > budget ? kSeedEnd : nx;  // past the bound: stop walking
+    };
+    // two words per lane and step (rows a and a + t*nth), their chains walked together
     for (int k0 = tid - lane; k0 < nlook; k0 += 2 * nth) {
-        const int a = 2 * (k0 + lane), a2 = a + 2 * nth;
+        const int a = t * (k0 + lane), a2 = a + t * nth;
         uint32_t c = 0, j = kSeedEnd, c2 = 0, j2 = kSeedEnd;
         if (a < npos) {
             const int w = a >> 5, sh = a & 31;
             const uint2 s0 = S[w], s1 = S[w + 1];
-            c = seed_word(s0.x, s1.x, s0.y, s1.y, sh);
-            j = heads[seed_hash(c, hb)];
+            c = seed_word<FL>(s0.x, s1.x, s0.y, s1.y, sh);
+            j = heads[seed_bucket<FL>(c, hb)];
         }
         if (a2 < npos) {
             const int w = a2 >> 5, sh = a2 & 31;
             const uint2 s0 = S[w], s1 = S[w + 1];
-            c2 = seed_word(s0.x, s1.x, s0.y, s1.y, sh);
-            j2 = heads[seed_hash(c2, hb)];
+            c2 = seed_word<FL>(s0.x, s1.x, s0.y, s1.y, sh);
+            j2 = heads[seed_bucket<FL>(c2, hb)];
         }
         while (__any_sync(0xffffffffu, j != kSeedEnd || j2 != kSeedEnd)) {
             const uint32_t jc = j, jc2 = j2;
-            const uint32_t node = jc != kSeedEnd ? nodes[jc] : 0u, node2 = jc2 != kSeedEnd ? nodes[jc2] : 0u;
-            if (jc != kSeedEnd) j = ++work > budget ? kSeedEnd : (node & 0xffffu);  // past the bound: stop
-            if (jc2 != kSeedEnd) j2 = ++work > budget ? kSeedEnd : (node2 & 0xffffu);
-            push(node, c, jc, a);
-            push(node2, c2, jc2, a2);
+            bool eq, eq2;
+            j = step(jc, c, eq);
+            j2 = step(jc2, c2, eq2);
+            push(eq, jc, a);
+            push(eq2, jc2, a2);
         }
         over = over || work > budget;
         if (__any_sync(0xffffffffu, over)) break;
@@ -1928,10 +1979,8 @@ __device__ void sl_item(const Shape &s, PopBuf buf, int base, int2 *part, int32_
         // repetitive CDS) the band scan
         bool band = true;
         if (sl_seeded(s)) {
-            uint32_t *heads = reinterpret_cast<uint32_t *>(tab);
-            uint32_t *nodes = reinterpret_cast<uint32_t *>(tab + sl_seed_head_bytes(n));
-            band = !sl_seed_scan<FL>(geo, S, Tlo, Thi, heads, nodes, reinterpret_cast<uint32_t *>(sm.queue[warp]), tid,
-                                     nth, best, bestd);
+            band = !sl_seed_scan<FL>(geo, S, Tlo, Thi, tab, reinterpret_cast<uint32_t *>(sm.queue[warp]), tid, nth, best,
+                                     bestd);
             if (band) {
                 best = 0;
                 bestd = 0x7fffffff;
@@ -2365,7 +2414,8 @@ static size_t sl_smem_bytes_nt(const Shape &s, size_t head)
     const int ng = s.sl_kind == PE_SL_LRCS ? sl_geo<1>(s.n, false).ng : sl_num_groups(s.n);
     const size_t band = (size_t)5 * sl_plane_stride(W) * sizeof(uint4) + (size_t)kSegPitch * (W + 2) * sizeof(int) +
                         (size_t)(ng + 1) * sizeof(int);
-    b += sl_seeded(s) ? std::max(band, sl_seed_bytes(s.n)) : band;  // the two passes share the space
+    // the two passes share the space
+    b += sl_seeded(s) ? std::max(band, sl_seed_bytes(s.n, s.sl_kind != PE_SL_LRCS)) : band;
     return b;
 }
 
