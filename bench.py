@@ -80,13 +80,13 @@ L2_FLUSH_BYTES = 256 << 20
 # changes without a new capture.
 SL_NCU = {
     "hairpin": {"workload": "L=1000 m=8 N=1024, generation 1 (2311 CDSs scanned)",
-                "scans": 2311, "cells": 10389102811, "warp_inst": 38644132, "alu_warp_inst": 16336904,
-                "smem_wavefronts": 4544143, "thread_inst": 1110401631, "dram_bytes": 2492672,
-                "issue_pct": 58.47, "alu_pct": 48.82, "smem_pct": 23.53, "source": "6a58280fc2787798"},
+                "scans": 2311, "cells": 10389102811, "warp_inst": 34128981, "alu_warp_inst": 12873520,
+                "smem_wavefronts": 4730663, "thread_inst": 950952081, "dram_bytes": 2492928,
+                "issue_pct": 61.54, "alu_pct": 45.37, "smem_pct": 27.74, "source": "4fbbb133abb0113c"},
     "lrcs": {"workload": "L=3000 m=4 N=4096, generation 1 (18320 CDS pairs scanned)",
-             "scans": 18320, "cells": 1250515745682, "warp_inst": 1619890383, "alu_warp_inst": 737375756,
-             "smem_wavefronts": 180629560, "thread_inst": 44756907945, "dram_bytes": 34465792,
-             "issue_pct": 45.97, "alu_pct": 41.75, "smem_pct": 20.23, "source": "6a58280fc2787798"},
+             "scans": 18320, "cells": 1250515745682, "warp_inst": 1541348024, "alu_warp_inst": 658973581,
+             "smem_wavefronts": 180118816, "thread_inst": 42529904948, "dram_bytes": 34464512,
+             "issue_pct": 46.06, "alu_pct": 39.32, "smem_pct": 21.25, "source": "4fbbb133abb0113c"},
 }
 SM_COUNT, ISSUE_WARP_INST_PER_SM_CLK, SMEM_WAVEFRONTS_PER_SM_CLK, ALU_WARP_INST_PER_SM_CLK = 148, 4, 1, 2
 # kernels one generation launches (one CUDA graph replay): k_variation, k_sl, k_dominance,
@@ -111,7 +111,7 @@ def hairpin_cells_per_cds(n: int) -> int:
 
 def roofline(scans: float, cells: float, sl_seconds: float, clocks: dict, kind: str = "hairpin") -> dict:
     """Roofline of the string-objective scan (integer work on shared-memory tables: a
-    hash-table join of 7-nucleotide words, then the runs it finds measured on bit planes)
+    table join of 6- or 7-nucleotide words, then the runs it finds measured on bit planes)
     on its three candidate bounds: instruction issue (4 warp instructions per SM per clock),
     the ALU pipe (2 per SM per clock) and the shared-memory data pipe (1 wavefront per SM per
     clock), each x 148 SMs x the SM clock sampled during the timed region.  Achieved = the

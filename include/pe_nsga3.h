@@ -307,7 +307,7 @@ int pe_scan_count(pe_instance *inst, uint64_t *count);
  * instance's stream. */
 int pe_scan_cells(pe_instance *inst, uint64_t *cells);
 /* Scans whose seeded first pass gave up (no reference counterpart).  The string
- * scan first looks up T's 7-nucleotide words in a table (linear in n for
+ * scan first looks up T's 6- or 7-nucleotide words in a table (linear in n for
  * random-like CDSs); on a repetitive CDS, whose table chains grow long, it hands
  * the CDS to the band scan, which visits every counted cell.  Both give the same
  * result.  Waits for the instance's stream. */
