@@ -1660,16 +1660,40 @@ __device__ __forceinline__ void seed_measure(uint32_t q, const SlGeo &geo, const
                                              const uint32_t *__restrict__ Tlo, const uint32_t *__restrict__ Thi,
                                              int &work, int &best, int &bestd)
 {
-    constexpr int t = Seed<FL>::step;
+    constexpr int t = Seed<FL>::step, K = Seed<FL>::K;
     const int n = geo.n, G = kSlGuardRows;
     const int e = (int)(q & 0xffffu), j = (int)(q >> 16), delta = j - e;
     int r_lo, r_hi;
     sl_diag_rows<FL>(n, delta, r_lo, r_hi);
-    int st = e;
-    while (st > e - t && st - 1 >= r_lo && seed_pairs(S, Tlo, Thi, st - 1, st - 1 + delta)) st--;
-    if (st == e - t) return;    // rows e-t .. e pair: the word at e-t owns the run
+    int st = e, last = e + K - 1;  // first row of the run; last row known to pair
+    if (e >= t && j >= t) {
+        // one window of 32 rows from e-t: bit k pairs row e-t+k (rows below r_lo cleared);
+        // the ones below bit t walk the run back, the first zero from bit t+K ends it
+        const int p0 = e - t, i0 = j - t, ws = p0 >> 5, wt = (i0 >> 5) + G;
+        const uint32_t sl = fshr(S[ws].x, S[ws + 1].x, p0 & 31), sh2 = fshr(S[ws].y, S[ws + 1].y, p0 & 31);
+        const uint32_t tl = fshr(Tlo[wt], Tlo[wt + 1], i0 & 31), th = fshr(Thi[wt], Thi[wt + 1], i0 & 31);
+        uint32_t m = ~((sl ^ tl) | (sh2 ^ th));
+        if (r_lo > p0) m &= 0xffffffffu << (r_lo - p0);  // r_lo - p0 <= t
+        const int back = __clz(~(m << (32 - t)));        // pairing rows e-1, e-2, ... (at most t)
+        if (back >= t) return;                           // rows e-t .. e pair: the word at e-t owns the run
+        st = e - back;
+        const uint32_t ahead = ~(m >> (t + K));          // zeros of rows e+K .. e-t+31 (ones above them)
+        const int runs = __ffs(ahead) - 1;               // pairing rows from e+K on
+        last = e + K - 1 + runs;
+        if (runs < 32 - t - K) {                         // the run ends inside the window
+            if (st + 7 > r_hi) return;
+            const int L = min(last, r_hi) - st + 1, d = sl_key<FL>(n, delta);
+            if (L > best || (L == best && d < bestd)) {
+                best = L;
+                bestd = d;
+            }
+            return;
+        }
+    } else {
+        while (st > e - t && st - 1 >= r_lo && seed_pairs(S, Tlo, Thi, st - 1, st - 1 + delta)) st--;
+        if (st == e - t) return;  // rows e-t .. e pair: the word at e-t owns the run
+    }
     if (st + 7 > r_hi) return;  // fewer than 8 counted rows from st
-    int last = e + Seed<FL>::K - 1;  // last row known to pair
     while (last < r_hi) {
         work++;
         const int p = last + 1, i = p + delta;
