@@ -2125,7 +2125,9 @@ __device__ void sl_item(const Shape &s, PopBuf buf, int base, int2 *part, int32_
                 atomicAdd(&scanned[1], cells);
             }
         }
-        __threadfence();
+        // a scan's result must be visible before the count says it is there (a carried
+        // result wrote nothing); the solution's last CTA fences again before it reads
+        if (!reuse) __threadfence();
         int old = atomicAdd(&counter[sol], 1);
         sm.last = (old == nres - 1);
     }
