@@ -163,7 +163,7 @@ struct pe_instance {
     int2 *d_part = nullptr;
     int32_t *d_counter = nullptr;
     int32_t *d_status = nullptr;
-    unsigned long long *d_scanned = nullptr;  // [0] string-objective scans run, [1] their counted cells,
+    unsigned long long *d_scanned = nullptr;  // [0] string-objective scans run, [1] LRCS self-pair scans,
                                               // [2] seeded scans handed to the band scan
     float *d_ext = nullptr;
     uint32_t *d_gen = nullptr;
@@ -920,10 +920,14 @@ int pe_scan_count(pe_instance *in, uint64_t *count)
 int pe_scan_cells(pe_instance *in, uint64_t *cells)
 {
     if (!in || !cells) return fail(PE_ERR_ARG, "null argument");
-    unsigned long long v = 0;
-    CK(cudaMemcpyAsync(&v, in->d_scanned + 1, sizeof v, cudaMemcpyDeviceToHost, in->stream));
+    unsigned long long v[2] = {0, 0};  // scans, LRCS scans of a CDS against itself
+    CK(cudaMemcpyAsync(v, in->d_scanned, sizeof v, cudaMemcpyDeviceToHost, in->stream));
     CK(cudaStreamSynchronize(in->stream));
-    *cells = (uint64_t)v;
+    const uint64_t n = (uint64_t)in->s.n;
+    if (in->s.sl_kind == PE_SL_LRCS)
+        *cells = (uint64_t)v[1] * (n * (n - 1) / 2) + (uint64_t)(v[0] - v[1]) * (n * n);
+    else
+        *cells = (uint64_t)v[0] * (n > 5 ? (n - 5) * (n - 4) / 2 : 0);
     return PE_OK;
 }
 

@@ -2114,22 +2114,19 @@ __device__ void sl_item(const Shape &s, PopBuf buf, int base, int2 *part, int32_
         }
     }
     if (tid == 0) {
-        if (!reuse) {
-            res[c] = make_int2(sm.res[0], sm.res[1]);
-            if (scanned) {
-                // scans, and the counted cells they covered
-                unsigned long long cells;
-                if (FL == 1) cells = pa == pb ? (unsigned long long)n * (n - 1) / 2 : (unsigned long long)n * n;
-                else cells = n > 5 ? (unsigned long long)(n - 5) * (n - 4) / 2 : 0ull;
-                atomicAdd(&scanned[0], 1ull);
-                atomicAdd(&scanned[1], cells);
-            }
-        }
+        if (!reuse) res[c] = make_int2(sm.res[0], sm.res[1]);
         // a scan's result must be visible before the count says it is there (a carried
         // result wrote nothing); the solution's last CTA fences again before it reads
         if (!reuse) __threadfence();
         int old = atomicAdd(&counter[sol], 1);
         sm.last = (old == nres - 1);
+        if (!reuse && scanned) {
+            // scans, and the LRCS scans of a CDS against itself (the host derives the
+            // counted cells from them); after the counter, so the fence does not wait
+            // for these adds that every scanning CTA makes to the same words
+            atomicAdd(&scanned[0], 1ull);
+            if (FL == 1 && pa == pb) atomicAdd(&scanned[1], 1ull);
+        }
     }
     __syncthreads();
     if (!sm.last) return;
