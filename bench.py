@@ -80,13 +80,13 @@ L2_FLUSH_BYTES = 256 << 20
 # changes without a new capture.
 SL_NCU = {
     "hairpin": {"workload": "L=1000 m=8 N=1024, generation 1 (2311 CDSs scanned)",
-                "scans": 2311, "cells": 10389102811, "warp_inst": 34128981, "alu_warp_inst": 12873520,
-                "smem_wavefronts": 4730663, "thread_inst": 950952081, "dram_bytes": 2492928,
-                "issue_pct": 61.54, "alu_pct": 45.37, "smem_pct": 27.74, "source": "4fbbb133abb0113c"},
+                "scans": 2311, "cells": 10389102811, "warp_inst": 31711459, "alu_warp_inst": 11571228,
+                "smem_wavefronts": 4345472, "thread_inst": 912949553, "dram_bytes": 2492672,
+                "issue_pct": 62.70, "alu_pct": 44.67, "smem_pct": 27.95, "source": "61df6e3d380e6958"},
     "lrcs": {"workload": "L=3000 m=4 N=4096, generation 1 (18320 CDS pairs scanned)",
-             "scans": 18320, "cells": 1250515745682, "warp_inst": 1541348024, "alu_warp_inst": 658973581,
-             "smem_wavefronts": 180118816, "thread_inst": 42529904948, "dram_bytes": 34464512,
-             "issue_pct": 46.06, "alu_pct": 39.32, "smem_pct": 21.25, "source": "4fbbb133abb0113c"},
+             "scans": 18320, "cells": 1250515745682, "warp_inst": 1459835043, "alu_warp_inst": 612847231,
+             "smem_wavefronts": 156405835, "thread_inst": 41135915424, "dram_bytes": 34466048,
+             "issue_pct": 45.30, "alu_pct": 37.92, "smem_pct": 19.13, "source": "61df6e3d380e6958"},
 }
 SM_COUNT, ISSUE_WARP_INST_PER_SM_CLK, SMEM_WAVEFRONTS_PER_SM_CLK, ALU_WARP_INST_PER_SM_CLK = 148, 4, 1, 2
 # kernels one generation launches (one CUDA graph replay): k_variation, k_sl, k_dominance,
