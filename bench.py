@@ -80,13 +80,13 @@ L2_FLUSH_BYTES = 256 << 20
 # changes without a new capture.
 SL_NCU = {
     "hairpin": {"workload": "L=1000 m=8 N=1024, generation 1 (2311 CDSs scanned)",
-                "scans": 2311, "cells": 10389102811, "warp_inst": 31711459, "alu_warp_inst": 11571228,
-                "smem_wavefronts": 4345472, "thread_inst": 912949553, "dram_bytes": 2492672,
-                "issue_pct": 62.70, "alu_pct": 44.67, "smem_pct": 27.95, "source": "61df6e3d380e6958"},
+                "scans": 2311, "cells": 10389102811, "warp_inst": 31266336, "alu_warp_inst": 11443642,
+                "smem_wavefronts": 4298609, "thread_inst": 902922790, "dram_bytes": 2336000,
+                "issue_pct": 65.40, "alu_pct": 46.42, "smem_pct": 28.82, "source": "47194a0c7b06c89a"},
     "lrcs": {"workload": "L=3000 m=4 N=4096, generation 1 (18320 CDS pairs scanned)",
-             "scans": 18320, "cells": 1250515745682, "warp_inst": 1459835043, "alu_warp_inst": 612847231,
-             "smem_wavefronts": 156405835, "thread_inst": 41135915424, "dram_bytes": 34466048,
-             "issue_pct": 45.30, "alu_pct": 37.92, "smem_pct": 19.13, "source": "61df6e3d380e6958"},
+             "scans": 18320, "cells": 1250515745682, "warp_inst": 1456922853, "alu_warp_inst": 611990996,
+             "smem_wavefronts": 156125635, "thread_inst": 41066332937, "dram_bytes": 31110656,
+             "issue_pct": 45.90, "alu_pct": 38.43, "smem_pct": 19.38, "source": "47194a0c7b06c89a"},
 }
 SM_COUNT, ISSUE_WARP_INST_PER_SM_CLK, SMEM_WAVEFRONTS_PER_SM_CLK, ALU_WARP_INST_PER_SM_CLK = 148, 4, 1, 2
 # kernels one generation launches (one CUDA graph replay): k_variation, k_sl, k_dominance,

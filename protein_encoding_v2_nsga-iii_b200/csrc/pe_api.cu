@@ -271,11 +271,13 @@ cudaError_t enqueue_generation(pe_instance *in, int src)
     int dst = 1 - src;
     cudaError_t e = mark(in, 0);
     if (e != cudaSuccess) return e;
+    // the variation kernel presets each child's scan counter to the string results it
+    // kept, so the scan's CTAs for those results leave at once
     e = launch_mutate(s, in->d_tab, in->d_aa, in->buf[src], in->buf[dst], in->d_surv, nullptr, s.N, 0, s.N, in->d_gen,
-                      nullptr, in->d_order, in->stream);
+                      nullptr, in->d_order, in->stream, nullptr, nullptr, in->d_counter);
     if (e != cudaSuccess) return e;
     if ((e = mark(in, 1)) != cudaSuccess) return e;
-    e = launch_sl(s, in->buf[dst], s.N, s.N, in->d_part, in->d_counter, in->d_status, in->stream, in->d_scanned);
+    e = launch_sl(s, in->buf[dst], s.N, s.N, in->d_part, in->d_counter, in->d_status, in->stream, in->d_scanned, true);
     if (e != cudaSuccess) return e;
     if ((e = mark(in, 2)) != cudaSuccess) return e;
     e = launch_select(s, in->buf[dst].obj, in->d_ext, in->d_ref, in->sc, in->d_surv, in->d_gen, 1, in->stream);

@@ -989,50 +989,40 @@ __global__ void __launch_bounds__(kVarThreads, 4) k_variation(Shape s, const Dev
                 dst.cds[(size_t)out_slot * s.nres + c] = changed ? make_int2(-1, 0) : src.cds[(size_t)par * s.nres + c];
             }
         }
-        if (q_count) {
-            // queued scan (batches): the results this child's mutation invalidated go to the
-            // queue, in result order; the solution's counter starts at the results kept, so
-            // the combine runs after the last queued one.  A child with none keeps its
-            // parent's string objective, as the combine of the parent's results gives.
+        if (q_counter) {
+            // The results this child's mutation invalidated are the only ones the scan
+            // will count: the solution's counter starts at the results kept, so the
+            // combine runs after the last scanned one and a carried result takes no count.
+            // A child with none keeps its parent's string objective, as the combine of the
+            // parent's results gives.  With a queue (batches) the invalidated results are
+            // also appended to it, in result order.
             const int par = parent_of[i], nres = s.nres, lane = tid & 31;
             if (tid < 32) {
+                auto invalid = [&](int r) {
+                    if (r >= nres) return false;
+                    if (s.sl_kind == PE_SL_LRCS) {
+                        int a, b;
+                        lrcs_pair_of(s.m, r, a, b);
+                        return (((ch >> a) | (ch >> b)) & 1ull) != 0ull;
+                    }
+                    return ((ch >> r) & 1ull) != 0ull;
+                };
                 int nq = 0;
-                for (int rb = 0; rb < nres; rb += 32) {
-                    const int r = rb + lane;
-                    bool on = false;
-                    if (r < nres) {
-                        if (s.sl_kind == PE_SL_LRCS) {
-                            int a, b;
-                            lrcs_pair_of(s.m, r, a, b);
-                            on = ((ch >> a) | (ch >> b)) & 1ull;
-                        } else {
-                            on = (ch >> r) & 1ull;
-                        }
+                for (int rb = 0; rb < nres; rb += 32) nq += __popc(__ballot_sync(0xffffffffu, invalid(rb + lane)));
+                if (q_count) {
+                    int qb = 0;
+                    if (lane == 0 && nq > 0) qb = atomicAdd(q_count, nq);
+                    qb = __shfl_sync(0xffffffffu, qb, 0);
+                    int run = 0;
+                    for (int rb = 0; rb < nres; rb += 32) {
+                        const bool on = invalid(rb + lane);
+                        const unsigned bal = __ballot_sync(0xffffffffu, on);
+                        if (on) q_items[qb + run + __popc(bal & ((1u << lane) - 1u))] = i * nres + rb + lane;
+                        run += __popc(bal);
                     }
-                    nq += __popc(__ballot_sync(0xffffffffu, on));
-                }
-                int qb = 0;
-                if (lane == 0 && nq > 0) qb = atomicAdd(q_count, nq);
-                qb = __shfl_sync(0xffffffffu, qb, 0);
-                int run = 0;
-                for (int rb = 0; rb < nres; rb += 32) {
-                    const int r = rb + lane;
-                    bool on = false;
-                    if (r < nres) {
-                        if (s.sl_kind == PE_SL_LRCS) {
-                            int a, b;
-                            lrcs_pair_of(s.m, r, a, b);
-                            on = ((ch >> a) | (ch >> b)) & 1ull;
-                        } else {
-                            on = (ch >> r) & 1ull;
-                        }
-                    }
-                    const unsigned bal = __ballot_sync(0xffffffffu, on);
-                    if (on) q_items[qb + run + __popc(bal & ((1u << lane) - 1u))] = i * nres + r;
-                    run += __popc(bal);
                 }
                 if (lane == 0) {
-                    // (with nothing queued the counter stays 0, ready for a plain scan later)
+                    // (with nothing invalidated the counter stays 0, ready for a full scan later)
                     if (nq > 0) q_counter[i] = nres - nq;
                     if (nq == 0) {
                         const int sl = s.slot[K_SL];
@@ -1127,7 +1117,8 @@ cudaError_t launch_mutate(const Shape &s, const DevTables *tab, const int8_t *aa
 {
     if (count <= 0) return cudaSuccess;
     // a queued scan needs the parents' results to carry the unchanged ones
-    if (q_count && (src.cds == nullptr || dst.cds == nullptr)) return cudaErrorInvalidValue;
+    if ((q_count || q_counter) && (src.cds == nullptr || dst.cds == nullptr)) return cudaErrorInvalidValue;
+    if (q_count && !q_counter) return cudaErrorInvalidValue;
     // a child reuses its parent's per-CDS sums only when both buffers carry them
     if ((src.aux == nullptr) != (dst.aux == nullptr)) return cudaErrorInvalidValue;
     size_t smem = var_smem_bytes(s);
@@ -1898,9 +1889,11 @@ __device__ __forceinline__ void warp_pick_result(const int2 *res, int count, boo
 // One scan item: result `item` = sol * nres + c of solution base + sol (CDS c, or CDS
 // pair c for LRCS), then, in the last of the solution's items to finish, the combine.
 // Called by the whole CTA with the CTA's dynamic shared memory.
+// preset: the variation kernel set each child's counter to the results it kept, so a
+// CTA whose result is carried over has nothing to count and leaves at once.
 template <int NT, int FL>
 __device__ void sl_item(const Shape &s, PopBuf buf, int base, int2 *part, int32_t *counter, int32_t *status,
-                        unsigned long long *scanned, int item, unsigned char *smem_raw)
+                        unsigned long long *scanned, int item, unsigned char *smem_raw, bool preset = false)
 {
     SlSmem<NT> &sm = *reinterpret_cast<SlSmem<NT> *>(smem_raw);
     const int G = kSlGuardRows;
@@ -1924,6 +1917,7 @@ __device__ void sl_item(const Shape &s, PopBuf buf, int base, int2 *part, int32_
     // the CDS (both CDSs) as it was, else found by the scan below
     int2 *res = buf.cds ? buf.cds + gsol * nres : part + (size_t)sol * nres;
     const bool reuse = buf.cds != nullptr && res[c].x >= 0;
+    if (reuse && preset) return;
     if (!reuse) {
         // stage S (the CDS planes) with one bulk async copy (TMA engine)
         {
@@ -2268,10 +2262,10 @@ __device__ void sl_item(const Shape &s, PopBuf buf, int base, int2 *part, int32_
 // one CTA per result of solutions base .. base + count - 1
 template <int NT, int FL>
 __global__ void __launch_bounds__(NT) k_sl(Shape s, PopBuf buf, int base, int2 *part, int32_t *counter,
-                                                 int32_t *status, unsigned long long *scanned)
+                                                 int32_t *status, unsigned long long *scanned, int preset)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    sl_item<NT, FL>(s, buf, base, part, counter, status, scanned, (int)blockIdx.x, smem_raw);
+    sl_item<NT, FL>(s, buf, base, part, counter, status, scanned, (int)blockIdx.x, smem_raw, preset != 0);
 }
 
 // The scan items of a whole batch: the variation kernels of the batch's instances
@@ -2491,29 +2485,29 @@ cudaError_t launch_sl_queue(const SlJob *jobs, int njobs, int32_t *ticket, int n
 
 template <int NT>
 static cudaError_t launch_sl_nt(const Shape &s, PopBuf buf, int base, int count, int2 *part, int32_t *counter,
-                                int32_t *status, cudaStream_t st, unsigned long long *scanned)
+                                int32_t *status, cudaStream_t st, unsigned long long *scanned, bool preset)
 {
     const size_t smem = sl_smem_bytes_nt(s, sizeof(SlSmem<NT>));
     if (s.sl_kind == PE_SL_LRCS) {
         cudaError_t e = raise_smem_limit((const void *)k_sl<NT, 1>, smem);
         if (e != cudaSuccess) return e;
-        k_sl<NT, 1><<<count * s.nres, NT, smem, st>>>(s, buf, base, part, counter, status, scanned);
+        k_sl<NT, 1><<<count * s.nres, NT, smem, st>>>(s, buf, base, part, counter, status, scanned, (int)preset);
         return cudaGetLastError();
     }
     cudaError_t e = raise_smem_limit((const void *)k_sl<NT, 0>, smem);
     if (e != cudaSuccess) return e;
-    k_sl<NT, 0><<<count * s.m, NT, smem, st>>>(s, buf, base, part, counter, status, scanned);
+    k_sl<NT, 0><<<count * s.m, NT, smem, st>>>(s, buf, base, part, counter, status, scanned, (int)preset);
     return cudaGetLastError();
 }
 
 cudaError_t launch_sl(const Shape &s, PopBuf buf, int base, int count, int2 *part, int32_t *counter, int32_t *status,
-                      cudaStream_t st, unsigned long long *scanned)
+                      cudaStream_t st, unsigned long long *scanned, bool preset)
 {
     if (count <= 0) return cudaSuccess;
     switch (s.sl_threads) {
-    case 64: return launch_sl_nt<64>(s, buf, base, count, part, counter, status, st, scanned);
-    case 256: return launch_sl_nt<256>(s, buf, base, count, part, counter, status, st, scanned);
-    default: return launch_sl_nt<128>(s, buf, base, count, part, counter, status, st, scanned);
+    case 64: return launch_sl_nt<64>(s, buf, base, count, part, counter, status, st, scanned, preset);
+    case 256: return launch_sl_nt<256>(s, buf, base, count, part, counter, status, st, scanned, preset);
+    default: return launch_sl_nt<128>(s, buf, base, count, part, counter, status, st, scanned, preset);
     }
 }
 

@@ -136,8 +136,10 @@ cudaError_t launch_mutate(const Shape &s, const DevTables *tab, const int8_t *aa
                           const int32_t *parent_of, const int32_t *rng_idx, int count, int copy_base, int child_base,
                           const uint32_t *d_gen, int32_t *ops, int32_t *order, cudaStream_t st,
                           int32_t *q_items = nullptr, int32_t *q_count = nullptr, int32_t *q_counter = nullptr);
+// preset: the variation kernel preset each child's counter to the results it kept
+// (launch_mutate's q_counter); CTAs whose result is carried over then leave at once
 cudaError_t launch_sl(const Shape &s, PopBuf buf, int base, int count, int2 *part, int32_t *counter,
-                      int32_t *status, cudaStream_t st, unsigned long long *scanned = nullptr);
+                      int32_t *status, cudaStream_t st, unsigned long long *scanned = nullptr, bool preset = false);
 size_t sl_smem_bytes(const Shape &s);
 // the batch's queued stem scan (k_sl_queue): shared memory of a job at CTA size nt,
 // resident CTAs per SM, and the launch of one wave over jobs[0 .. njobs)
