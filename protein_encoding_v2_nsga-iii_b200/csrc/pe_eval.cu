@@ -997,7 +997,11 @@ __global__ void __launch_bounds__(kVarThreads, 4) k_variation(Shape s, const Dev
             // parent's results gives.  With a queue (batches) the invalidated results are
             // also appended to it, in result order.
             const int par = parent_of[i], nres = s.nres, lane = tid & 31;
-            if (tid < 32) {
+            // results invalidated: the changed CDSs (hairpin), or the CDS pairs with a
+            // changed member (LRCS: all pairs but those of the u unchanged CDSs)
+            const int nch = __popcll(ch), u = s.m - nch;
+            const int nq = s.sl_kind == PE_SL_LRCS ? nres - u * (u + 1) / 2 : nch;
+            if (q_count && tid < 32) {
                 auto invalid = [&](int r) {
                     if (r >= nres) return false;
                     if (s.sl_kind == PE_SL_LRCS) {
@@ -1007,30 +1011,26 @@ __global__ void __launch_bounds__(kVarThreads, 4) k_variation(Shape s, const Dev
                     }
                     return ((ch >> r) & 1ull) != 0ull;
                 };
-                int nq = 0;
-                for (int rb = 0; rb < nres; rb += 32) nq += __popc(__ballot_sync(0xffffffffu, invalid(rb + lane)));
-                if (q_count) {
-                    int qb = 0;
-                    if (lane == 0 && nq > 0) qb = atomicAdd(q_count, nq);
-                    qb = __shfl_sync(0xffffffffu, qb, 0);
-                    int run = 0;
-                    for (int rb = 0; rb < nres; rb += 32) {
-                        const bool on = invalid(rb + lane);
-                        const unsigned bal = __ballot_sync(0xffffffffu, on);
-                        if (on) q_items[qb + run + __popc(bal & ((1u << lane) - 1u))] = i * nres + rb + lane;
-                        run += __popc(bal);
-                    }
+                int qb = 0;
+                if (lane == 0 && nq > 0) qb = atomicAdd(q_count, nq);
+                qb = __shfl_sync(0xffffffffu, qb, 0);
+                int run = 0;
+                for (int rb = 0; rb < nres; rb += 32) {
+                    const bool on = invalid(rb + lane);
+                    const unsigned bal = __ballot_sync(0xffffffffu, on);
+                    if (on) q_items[qb + run + __popc(bal & ((1u << lane) - 1u))] = i * nres + rb + lane;
+                    run += __popc(bal);
                 }
-                if (lane == 0) {
-                    // (with nothing invalidated the counter stays 0, ready for a full scan later)
-                    if (nq > 0) q_counter[i] = nres - nq;
-                    if (nq == 0) {
-                        const int sl = s.slot[K_SL];
-                        dst.obj[(size_t)out_slot * s.M + sl] = src.obj[(size_t)par * s.M + sl];
-                        dst.objidx[(size_t)out_slot * 2 * s.M + 2 * sl] = src.objidx[(size_t)par * 2 * s.M + 2 * sl];
-                        dst.objidx[(size_t)out_slot * 2 * s.M + 2 * sl + 1] = src.objidx[(size_t)par * 2 * s.M + 2 * sl + 1];
-                        for (int k = 0; k < 3; k++) dst.pql[(size_t)out_slot * 3 + k] = src.pql[(size_t)par * 3 + k];
-                    }
+            }
+            if (tid == 0) {
+                // (with nothing invalidated the counter stays 0, ready for a full scan later)
+                if (nq > 0) q_counter[i] = nres - nq;
+                if (nq == 0) {
+                    const int sl = s.slot[K_SL];
+                    dst.obj[(size_t)out_slot * s.M + sl] = src.obj[(size_t)par * s.M + sl];
+                    dst.objidx[(size_t)out_slot * 2 * s.M + 2 * sl] = src.objidx[(size_t)par * 2 * s.M + 2 * sl];
+                    dst.objidx[(size_t)out_slot * 2 * s.M + 2 * sl + 1] = src.objidx[(size_t)par * 2 * s.M + 2 * sl + 1];
+                    for (int k = 0; k < 3; k++) dst.pql[(size_t)out_slot * 3 + k] = src.pql[(size_t)par * 3 + k];
                 }
             }
         }
